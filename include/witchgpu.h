@@ -1,0 +1,114 @@
+/* witchgpu.h -- C ABI of the B200 Seed Check engine (libwitchgpu.so).
+ *
+ * Plain C types only: opaque engine handle, caller-owned buffers, int status returns
+ * (WG_OK = 0), no exit() inside the library.  One engine owns one CUDA context binding,
+ * one stream and its work buffers; an engine is not thread-safe (use one per thread),
+ * matching the one-ctx-per-thread rule of the reference's lysh API
+ * (engine/tools/lysh/src/eval.h:40-47).
+ *
+ * Each entry point names the reference interface it replaces.  A ctypes / cgo binding of
+ * these is shown in INTEGRATION.md.
+ */
+#ifndef WITCHGPU_H
+#define WITCHGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define WG_OK           0
+#define WG_ERR_ARG      1   /* invalid argument (empty rect, null buffer, unknown name) */
+#define WG_ERR_CUDA     2   /* a CUDA call failed; wg_engine_error() has the message */
+#define WG_ERR_NOMEM    3   /* device or host allocation failed */
+#define WG_ERR_CAPACITY 4   /* a work list stayed full even at the smallest batch */
+#define WG_ERR_NODEV    5   /* no CUDA device / the requested device is absent */
+
+typedef struct wg_engine wg_engine;
+
+/* Version / preset bits; field-for-field the layout of lysh_phase1_opts
+ * (engine/tools/lysh/src/phase1.h:45-57).  All-zero = 26.2 rules, NORMAL preset. */
+typedef struct {
+    int mc_1_18_2;      /* temperature gate: lower bound only */
+    int single_biome;   /* SINGLE_BIOME preset: climate / continentalness gates skipped */
+    int pre_26_2;       /* 1 = rules before 26.2 (no ridge <= -0.91 rejection) */
+    int large_biomes;   /* LARGE_BIOMES preset: *_large climate noises */
+    int biome_tree;     /* 0 = chosen from the bits above, else 1 + biome tree index */
+} wg_opts;
+
+/* One phase-1 survivor: a (seed, swamp-hut region) that passed every phase-1 gate.
+ * The hut's block position is (chunk_x * 16, chunk_z * 16). */
+typedef struct {
+    uint64_t seed_index;   /* index of the seed in the request (list position / generator step) */
+    int64_t seed;          /* world seed */
+    int32_t rx, rz;        /* region */
+    int32_t chunk_x, chunk_z;
+} wg_candidate;
+
+/* Funnel and timing of one Seed Check request. */
+typedef struct {
+    int64_t scanned;              /* (seed, region) checks */
+    int64_t accepted;             /* phase-1 survivors */
+    int64_t climate_survivors;    /* passed erosion / temperature / ridge */
+    int64_t deep_candidates;      /* also passed Entrance(50) and Entrance(60) */
+    int64_t reject_hist[11];      /* per LYSH_P1_REJECT_* code; [10] = accepted */
+    int64_t tier_hist[7];         /* erosion tier that rejected (lysh's tier histogram) */
+    int64_t batches;              /* device batches run */
+    int64_t retries;              /* batches re-run smaller after a full work list */
+    double gpu_ms;                /* device time, CUDA events on the engine stream */
+    double wall_ms;               /* host wall time of the call */
+} wg_scan_stats;
+
+/* Create an engine on CUDA device `device`: context binding, stream, noise tables and work
+ * buffers.  Replaces phase1_scan's allocateBuffers() and its one-context-per-process
+ * set-up (engine/gpu/low54/phase1_scan.cu:825-866, :1492-1513). */
+int wg_engine_open(int device, wg_engine **out);
+
+/* Release everything wg_engine_open made (phase1_scan.cu:868-879).  NULL is a no-op. */
+void wg_engine_close(wg_engine *e);
+
+/* Message of the engine's last failure ("" if none). */
+const char *wg_engine_error(const wg_engine *e);
+
+/* lysh's --version / --preset names -> option bits
+ * (engine/tools/lysh/src/main.c:104-132).  0 on success, WG_ERR_ARG if unknown. */
+int wg_parse_version(const char *name, wg_opts *opts);
+int wg_parse_preset(const char *name, wg_opts *opts);
+
+/* Seed Check phase 1 over every seed x every region of [rx0,rx1) x [rz0,rz1).
+ * Seeds are seeds[0..n_seeds) (host memory) or, when seeds is NULL, the generator
+ * splitmix64(gen_base + i) of phase1_scan's --seed-gen.  Writes up to `cap` survivors to
+ * `out` (host memory), sorted by (seed_index, rz, rx); *n_out = the number found, which may
+ * exceed cap (then only the first cap are written).  `stats` may be NULL.
+ * Replaces phase1_scan's runScan() batch loop (phase1_scan.cu:881-1342) and the phase-1
+ * pass of lysh_scan_rect (engine/tools/lysh/src/search.c:198-265); the survivor set is
+ * exactly lysh_phase1_check_ex's (phase1.c:130-200), without the GPU density prefilter. */
+int wg_seed_check(wg_engine *e, const int64_t *seeds, uint64_t gen_base, uint64_t n_seeds,
+                  const wg_opts *opts, int max_height, int salt,
+                  int rx0, int rx1, int rz0, int rz1,
+                  wg_candidate *out, uint64_t cap, uint64_t *n_out, wg_scan_stats *stats);
+
+/* Same request with device-resident buffers: d_seeds (device, or NULL for the generator)
+ * and d_out (device, unsorted), work enqueued on `stream` (a cudaStream_t, NULL = the
+ * engine's own stream).  The call returns when the work is complete. */
+int wg_seed_check_device(wg_engine *e, const int64_t *d_seeds, uint64_t gen_base, uint64_t n_seeds,
+                         const wg_opts *opts, int max_height, int salt,
+                         int rx0, int rx1, int rz0, int rz1,
+                         wg_candidate *d_out, uint64_t cap, uint64_t *n_out, wg_scan_stats *stats,
+                         void *stream);
+
+/* Per-region phase-1 verdicts for parity checks: codes / tiers (host, n_seeds * R entries,
+ * seed-major, rz outer, rx inner) receive the LYSH_P1_REJECT_* code and the erosion tier
+ * (-1 if none) of every (seed, region), as lysh_phase1_check_ex reports them
+ * (phase1.c:130-200, search.c:148-160). */
+int wg_phase1_codes(wg_engine *e, const int64_t *seeds, uint64_t gen_base, uint64_t n_seeds,
+                    const wg_opts *opts, int max_height, int salt,
+                    int rx0, int rx1, int rz0, int rz1, int8_t *codes, int8_t *tiers);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WITCHGPU_H */

@@ -1,0 +1,221 @@
+"""B200 Seed Check engine: Python binding of libwitchgpu.so (include/witchgpu.h).
+
+The engine runs the reference's Seed Check phase 1 (lysh_phase1_check_ex,
+engine/tools/lysh/src/phase1.c:130-200) on the GPU: world seeds -> swamp-hut region
+placement -> erosion / temperature / ridge gates -> cave ladder -> continentalness ->
+floodedness.  This module is a thin ctypes layer; all work happens in the CUDA library,
+and every call fails loudly when the library or a GPU is missing (there is no CPU path).
+
+The package directory name is not a Python identifier; load it with
+importlib.util.spec_from_file_location (registering it in sys.modules first), as
+bench.py and tests/conftest.py do.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libwitchgpu.so")
+WORKER_PATH = os.path.join(HERE, "phase1_scan")
+HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "witchgpu.h")
+
+WG_OK, WG_ERR_ARG, WG_ERR_CUDA, WG_ERR_NOMEM, WG_ERR_CAPACITY, WG_ERR_NODEV = 0, 1, 2, 3, 4, 5
+
+# Reject codes (LYSH_P1_REJECT_*, engine/tools/lysh/src/phase1.h:61-74).
+REJECT_NAMES = ("erosion < 0.55", "temperature", "ridge", "Entrance@50", "Entrance@60", "cave@maxHeight",
+                "cave ladder (y<=0)", "cave ladder (y>0)", "continentalness < -0.11", "floodedness > 0.41",
+                "ACCEPT")
+ACCEPT = 10
+DEFAULT_VERSION = "1.19.x~26.1"   # the hunt driver's version (hunt.py DEFAULTS)
+SALT = 14357620
+
+
+class Opts(C.Structure):
+    """wg_opts: field-for-field lysh_phase1_opts."""
+    _fields_ = [("mc_1_18_2", C.c_int), ("single_biome", C.c_int), ("pre_26_2", C.c_int),
+                ("large_biomes", C.c_int), ("biome_tree", C.c_int)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("scanned", C.c_int64), ("accepted", C.c_int64), ("climate_survivors", C.c_int64),
+                ("deep_candidates", C.c_int64), ("reject_hist", C.c_int64 * 11), ("tier_hist", C.c_int64 * 7),
+                ("batches", C.c_int64), ("retries", C.c_int64), ("gpu_ms", C.c_double), ("wall_ms", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {"scanned": self.scanned, "accepted": self.accepted, "climate_survivors": self.climate_survivors,
+                "deep_candidates": self.deep_candidates, "reject_hist": list(self.reject_hist),
+                "tier_hist": list(self.tier_hist), "batches": self.batches, "retries": self.retries,
+                "gpu_ms": self.gpu_ms, "wall_ms": self.wall_ms}
+
+
+CANDIDATE_DTYPE = np.dtype([("seed_index", "<u8"), ("seed", "<i8"), ("rx", "<i4"), ("rz", "<i4"),
+                            ("chunk_x", "<i4"), ("chunk_z", "<i4")])
+
+# Every symbol include/witchgpu.h declares.
+EXPORTS = ("wg_engine_open", "wg_engine_close", "wg_engine_error", "wg_parse_version", "wg_parse_preset",
+           "wg_seed_check", "wg_seed_check_device", "wg_phase1_codes")
+
+_lib = None
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+def library() -> C.CDLL:
+    """The loaded CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise EngineError(f"{LIB_PATH} is missing: build the CUDA extension first (make -C {HERE})")
+    lib = C.CDLL(LIB_PATH)
+    vp, i64, u64, i32 = C.c_void_p, C.c_int64, C.c_uint64, C.c_int
+    lib.wg_engine_open.argtypes = [i32, C.POINTER(vp)]
+    lib.wg_engine_close.argtypes = [vp]
+    lib.wg_engine_close.restype = None
+    lib.wg_engine_error.argtypes = [vp]
+    lib.wg_engine_error.restype = C.c_char_p
+    lib.wg_parse_version.argtypes = [C.c_char_p, C.POINTER(Opts)]
+    lib.wg_parse_preset.argtypes = [C.c_char_p, C.POINTER(Opts)]
+    common = [vp, vp, u64, u64, C.POINTER(Opts), i32, i32, i32, i32, i32, i32]
+    lib.wg_seed_check.argtypes = common + [vp, u64, C.POINTER(u64), C.POINTER(Stats)]
+    lib.wg_seed_check_device.argtypes = common + [vp, u64, C.POINTER(u64), C.POINTER(Stats), vp]
+    lib.wg_phase1_codes.argtypes = common + [vp, vp]
+    _lib = lib
+    return lib
+
+
+def make_opts(version: str = DEFAULT_VERSION, preset: str = "NORMAL") -> Opts:
+    """lysh's --version / --preset names -> option bits (engine/tools/lysh/src/main.c:104-132)."""
+    lib = library()
+    o = Opts()
+    if lib.wg_parse_version(version.encode(), C.byref(o)):
+        raise ValueError(f"unknown version {version!r}")
+    if lib.wg_parse_preset(preset.encode(), C.byref(o)):
+        raise ValueError(f"unknown preset {preset!r}")
+    return o
+
+
+def region_rect_for_area(area_blocks: int) -> tuple[int, int, int, int]:
+    """hunt.py ScanRun.rect(): a square about `area` blocks out, in hut regions."""
+    r = int(area_blocks // 512) + 1
+    return (-r, r, -r, r)
+
+
+class ScanResult:
+    """candidates: CANDIDATE_DTYPE array sorted by (seed_index, rz, rx); stats: the funnel."""
+
+    def __init__(self, candidates: np.ndarray, stats: dict):
+        self.candidates = candidates
+        self.stats = stats
+
+
+class Engine:
+    """One engine = one device, one stream, one set of work buffers (not thread-safe)."""
+
+    def __init__(self, device: int = 0):
+        lib = library()
+        h = C.c_void_p()
+        rc = lib.wg_engine_open(device, C.byref(h))
+        if rc != WG_OK:
+            raise EngineError(f"wg_engine_open(device={device}) failed with status {rc}"
+                              + (" (no CUDA device)" if rc == WG_ERR_NODEV else ""))
+        self._h = h
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            library().wg_engine_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _err(self, rc: int, what: str) -> EngineError:
+        msg = library().wg_engine_error(self._h).decode(errors="replace")
+        return EngineError(f"{what} failed with status {rc}: {msg}")
+
+    @staticmethod
+    def _seeds(seeds, gen):
+        if seeds is not None:
+            arr = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64).view(np.int64))
+            return arr, arr.ctypes.data, 0, len(arr)
+        if gen is None:
+            raise ValueError("give seeds or gen=(base, count)")
+        base, count = gen
+        return None, None, int(base) & 0xFFFFFFFFFFFFFFFF, int(count)
+
+    def seed_check(self, seeds=None, gen=None, rect=(-4, 5, -4, 5), max_height: int = -50,
+                   version: str = DEFAULT_VERSION, preset: str = "NORMAL", salt: int = 0,
+                   opts: Opts | None = None) -> ScanResult:
+        """Phase-1 survivors of every seed x every region of rect = (rx0, rx1, rz0, rz1)."""
+        keep, ptr, base, n = self._seeds(seeds, gen)
+        o = opts if opts is not None else make_opts(version, preset)
+        cap = 1 << 12
+        while True:
+            out = np.zeros(cap, CANDIDATE_DTYPE)
+            found = C.c_uint64()
+            st = Stats()
+            rc = library().wg_seed_check(self._h, ptr, base, n, C.byref(o), max_height, salt, *rect,
+                                         out.ctypes.data, cap, C.byref(found), C.byref(st))
+            if rc != WG_OK:
+                raise self._err(rc, "wg_seed_check")
+            if found.value <= cap:
+                return ScanResult(out[:found.value].copy(), st.as_dict())
+            cap = int(found.value)
+
+    def seed_check_device(self, d_seeds_ptr, gen_base: int, n_seeds: int, rect, max_height: int,
+                          opts: Opts, d_out_ptr: int, cap: int, stream_ptr: int | None = None,
+                          salt: int = 0) -> tuple[int, dict]:
+        """Device-buffer variant (raw CUDA pointers, e.g. torch tensor.data_ptr())."""
+        found = C.c_uint64()
+        st = Stats()
+        rc = library().wg_seed_check_device(self._h, d_seeds_ptr, gen_base & 0xFFFFFFFFFFFFFFFF, n_seeds,
+                                            C.byref(opts), max_height, salt, *rect, d_out_ptr, cap,
+                                            C.byref(found), C.byref(st), stream_ptr)
+        if rc != WG_OK:
+            raise self._err(rc, "wg_seed_check_device")
+        return int(found.value), st.as_dict()
+
+    def phase1_codes(self, seeds=None, gen=None, rect=(-4, 5, -4, 5), max_height: int = -50,
+                     version: str = DEFAULT_VERSION, preset: str = "NORMAL", salt: int = 0,
+                     opts: Opts | None = None) -> tuple[np.ndarray, np.ndarray]:
+        """(codes, tiers), each [n_seeds, n_regions] int8: lysh's per-region phase-1 verdicts."""
+        keep, ptr, base, n = self._seeds(seeds, gen)
+        o = opts if opts is not None else make_opts(version, preset)
+        nreg = (rect[1] - rect[0]) * (rect[3] - rect[2])
+        codes = np.empty((n, nreg), np.int8)
+        tiers = np.empty((n, nreg), np.int8)
+        rc = library().wg_phase1_codes(self._h, ptr, base, n, C.byref(o), max_height, salt, *rect,
+                                       codes.ctypes.data, tiers.ctypes.data)
+        if rc != WG_OK:
+            raise self._err(rc, "wg_phase1_codes")
+        return codes, tiers
+
+
+def splitmix64(x: int) -> int:
+    """The --seed-gen stream: splitmix64(base + i) with the golden-gamma pre-add."""
+    m = 0xFFFFFFFFFFFFFFFF
+    x = (x + 0x9E3779B97F4A7C15) & m
+    z = x
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+    return z ^ (z >> 31)
+
+
+def to_signed(v: int) -> int:
+    v &= 0xFFFFFFFFFFFFFFFF
+    return v - (1 << 64) if v >= (1 << 63) else v

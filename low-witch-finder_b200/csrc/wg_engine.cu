@@ -1,0 +1,479 @@
+// Host engine behind include/witchgpu.h: batch planning, device work buffers, the
+// three-kernel phase-1 pipeline per batch, overflow retry and the funnel statistics.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/witchgpu.h"
+#include "wg_catalog.h"
+#include "wg_phase1.cuh"
+
+using namespace wg;
+
+namespace {
+
+// Per-batch work budget: (seed, region) checks per batch and units per batch.
+constexpr uint64_t kWorkPerBatch = 1ull << 27;
+constexpr uint32_t kMaxUnits = 1u << 20;
+constexpr uint32_t kCapRec = kMaxUnits + (1u << 16);
+constexpr uint32_t kCapSurv = 1u << 23;
+constexpr uint32_t kCapDeep = 1u << 20;
+constexpr uint32_t kCapOut = 1u << 20;
+
+// Regions per unit window: a whole seed when its rect is small, else 2048-region windows.
+uint32_t window_for(uint64_t n_regions) { return n_regions <= 4096 ? (uint32_t)n_regions : 2048u; }
+
+// Climate evaluation steps (see ClimateStep): the tiered erosion sequence
+// (engine/tools/lysh/src/noise.c:387-459) followed by plain y=0 DoublePerlin samples of
+// temperature and ridge (noise.c:320-342).
+void build_steps(const NoiseSpec *specs, int erosion, int temperature, ClimateStep *st) {
+    static const double thr[7] = {0.05, 0.22, 0.42, 0.45, 0.49, 0.51, 0.55};
+    std::memset(st, 0, sizeof(ClimateStep) * kClimateSteps);
+    const NoiseSpec &e = specs[erosion];
+    int k = 0;
+    for (int p = 0; p < e.npresent; p++)
+        for (int sub = 0; sub < 2; sub++, k++) {
+            ClimateStep &s = st[k];
+            s.slot = sub * e.npresent + p;
+            s.sc = sub ? 1.0181268882175227 : 1.0;
+            s.lac = e.lac[p];
+            s.c1 = e.amp[p] * e.per[p];
+            s.c2 = 1.0;
+            s.amp = e.amplitude;
+            if (k >= 1) {
+                s.act = (k == 7) ? ACT_TIER_LAST : ACT_TIER;
+                s.tier = k - 1;
+                s.thr = thr[k - 1];
+            }
+        }
+    int base = 2 * e.npresent;
+    const int plain[2] = {temperature, N_RIDGE};
+    for (int q = 0; q < 2; q++) {
+        const NoiseSpec &n = specs[plain[q]];
+        for (int sub = 0; sub < 2; sub++)
+            for (int p = 0; p < n.npresent; p++, k++) {
+                ClimateStep &s = st[k];
+                s.slot = base + sub * n.npresent + p;
+                s.sc = sub ? 1.0181268882175227 : 1.0;
+                s.lac = n.lac[p];
+                s.c1 = n.amp[p];
+                s.c2 = n.per[p];
+                s.amp = n.amplitude;
+                if (p == n.npresent - 1) s.act = sub ? (q == 0 ? ACT_TEMPERATURE : ACT_RIDGE) : ACT_END_SUB_A;
+            }
+        base += 2 * n.npresent;
+    }
+}
+
+}  // namespace
+
+struct wg_engine {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+
+    uint32_t *rec_unit = nullptr, *rec_off = nullptr, *rec_cnt = nullptr, *surv = nullptr, *deep = nullptr;
+    Candidate *out = nullptr;
+    uint32_t *counters = nullptr;
+    unsigned long long *hist = nullptr;
+    uint32_t *h_counters = nullptr;         // pinned
+    unsigned long long *h_hist = nullptr;   // pinned
+    int64_t *d_seed_list = nullptr;
+    uint64_t d_seed_cap = 0;
+
+    int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
+        char buf[512];
+        if (e != cudaSuccess) std::snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+        else std::snprintf(buf, sizeof buf, "%s", what);
+        err = buf;
+        return code;
+    }
+};
+
+#define WG_CUDA(call, what)                                        \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return eng->fail(WG_ERR_CUDA, what, e_); \
+    } while (0)
+
+namespace {
+
+struct Request {
+    const int64_t *d_seeds;   // device seeds or nullptr (generator)
+    uint64_t gen_base;
+    uint64_t n_seeds;
+    wg_opts opts;
+    int max_height, salt;
+    int rx0, rx1, rz0, rz1;
+    int8_t *d_codes, *d_tiers;   // optional per-region verdicts (device)
+};
+
+struct Sink {            // where phase-1 survivors go after each batch
+    std::vector<Candidate> *host = nullptr;
+    Candidate *dev = nullptr;
+    uint64_t dev_cap = 0;
+    uint64_t found = 0;
+};
+
+int run_batch(wg_engine *eng, const Request &rq, const BatchArgs &proto, uint64_t unit0, uint32_t n_units,
+              Sink &sink, wg_scan_stats &st) {
+    BatchArgs a = proto;
+    a.unit0 = unit0;
+    a.n_units = n_units;
+    WG_CUDA(cudaMemsetAsync(eng->counters, 0, sizeof(uint32_t) * CNT_WORDS, eng->stream), "memset counters");
+    WG_CUDA(cudaMemsetAsync(eng->hist, 0, sizeof(unsigned long long) * (P1_KINDS + kTiers), eng->stream),
+            "memset hist");
+    launch_climate(a, eng->stream);
+    launch_entrance(a, eng->sm_count, eng->stream);
+    launch_ladder(a, eng->sm_count * 8, eng->stream);
+    WG_CUDA(cudaGetLastError(), "kernel launch");
+    WG_CUDA(cudaMemcpyAsync(eng->h_counters, eng->counters, sizeof(uint32_t) * CNT_WORDS, cudaMemcpyDeviceToHost,
+                            eng->stream),
+            "copy counters");
+    WG_CUDA(cudaMemcpyAsync(eng->h_hist, eng->hist, sizeof(unsigned long long) * (P1_KINDS + kTiers),
+                            cudaMemcpyDeviceToHost, eng->stream),
+            "copy hist");
+    WG_CUDA(cudaStreamSynchronize(eng->stream), "batch");
+    st.batches++;
+    if (eng->h_counters[CNT_OVERFLOW]) {
+        if (n_units <= 32) return eng->fail(WG_ERR_CAPACITY, "phase-1 work list full even for 32 units");
+        st.retries++;
+        uint32_t half = n_units / 2;
+        int rc = run_batch(eng, rq, proto, unit0, half, sink, st);
+        if (rc) return rc;
+        return run_batch(eng, rq, proto, unit0 + half, n_units - half, sink, st);
+    }
+    for (int i = 0; i < P1_KINDS; i++) st.reject_hist[i] += (int64_t)eng->h_hist[i];
+    for (int i = 0; i < kTiers; i++) st.tier_hist[i] += (int64_t)eng->h_hist[P1_KINDS + i];
+    st.climate_survivors += eng->h_counters[CNT_SURVIVORS];
+    st.deep_candidates += eng->h_counters[CNT_DEEP];
+    uint32_t nf = eng->h_counters[CNT_FINAL];
+    if (nf) {
+        if (sink.host) {
+            size_t at = sink.host->size();
+            sink.host->resize(at + nf);
+            WG_CUDA(cudaMemcpy(sink.host->data() + at, eng->out, sizeof(Candidate) * nf, cudaMemcpyDeviceToHost),
+                    "copy survivors");
+        } else if (sink.dev && sink.found < sink.dev_cap) {
+            uint64_t n = std::min<uint64_t>(nf, sink.dev_cap - sink.found);
+            WG_CUDA(cudaMemcpyAsync(sink.dev + sink.found, eng->out, sizeof(Candidate) * n, cudaMemcpyDeviceToDevice,
+                                    eng->stream),
+                    "copy survivors");
+        }
+    }
+    sink.found += nf;
+    return WG_OK;
+}
+
+int run_request(wg_engine *eng, const Request &rq, Sink &sink, wg_scan_stats &st) {
+    if (rq.rx1 <= rq.rx0 || rq.rz1 <= rq.rz0 || rq.n_seeds == 0) return eng->fail(WG_ERR_ARG, "empty request");
+    const uint64_t rw = (uint64_t)((int64_t)rq.rx1 - rq.rx0), rh = (uint64_t)((int64_t)rq.rz1 - rq.rz0);
+    const uint64_t n_regions = rw * rh;
+    const uint32_t win = window_for(n_regions);
+    const uint64_t n_win = (n_regions + win - 1) / win;
+    const uint64_t units = rq.n_seeds * n_win;
+
+    BatchArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.seeds = rq.d_seeds;
+    a.gen_base = rq.gen_base;
+    a.win = win;
+    a.n_win = n_win;
+    a.n_regions = n_regions;
+    a.rx0 = rq.rx0;
+    a.rz0 = rq.rz0;
+    a.rw = (int)rw;
+    a.rh = (int)rh;
+    a.salt = rq.salt ? rq.salt : 14357620;
+    a.max_height = rq.max_height;
+    a.mc_1_18_2 = rq.opts.mc_1_18_2;
+    a.pre_26_2 = rq.opts.pre_26_2;
+    a.single_biome = rq.opts.single_biome;
+    a.large_biomes = rq.opts.large_biomes;
+    a.rec_unit = eng->rec_unit;
+    a.rec_off = eng->rec_off;
+    a.rec_cnt = eng->rec_cnt;
+    a.surv_region = eng->surv;
+    a.deep = eng->deep;
+    a.out = eng->out;
+    a.cap_rec = kCapRec;
+    a.cap_surv = kCapSurv;
+    a.cap_deep = kCapDeep;
+    a.cap_out = kCapOut;
+    a.counters = eng->counters;
+    a.hist = eng->hist;
+    a.codes = rq.d_codes;
+    a.tiers = rq.d_tiers;
+
+    uint64_t per_batch = std::min<uint64_t>(kMaxUnits, std::max<uint64_t>(32, kWorkPerBatch / win));
+    if (rq.opts.single_biome)  // every region survives the climate stage
+        per_batch = std::min<uint64_t>(per_batch, std::max<uint64_t>(32, kCapSurv / 2 / win));
+    st.scanned = (int64_t)(rq.n_seeds * n_regions);
+    for (uint64_t u0 = 0; u0 < units; u0 += per_batch) {
+        uint32_t n = (uint32_t)std::min<uint64_t>(per_batch, units - u0);
+        int rc = run_batch(eng, rq, a, u0, n, sink, st);
+        if (rc) return rc;
+    }
+    st.accepted = (int64_t)sink.found;
+    return WG_OK;
+}
+
+int stage_seeds(wg_engine *eng, const int64_t *seeds, uint64_t n, const int64_t **d_seeds) {
+    *d_seeds = nullptr;
+    if (!seeds) return WG_OK;
+    if (n > eng->d_seed_cap) {
+        if (eng->d_seed_list) cudaFree(eng->d_seed_list);
+        eng->d_seed_list = nullptr;
+        eng->d_seed_cap = 0;
+        WG_CUDA(cudaMalloc(&eng->d_seed_list, sizeof(int64_t) * n), "alloc seed list");
+        eng->d_seed_cap = n;
+    }
+    WG_CUDA(cudaMemcpyAsync(eng->d_seed_list, seeds, sizeof(int64_t) * n, cudaMemcpyHostToDevice, eng->stream),
+            "upload seeds");
+    *d_seeds = eng->d_seed_list;
+    return WG_OK;
+}
+
+Request make_request(const wg_opts *opts, uint64_t gen_base, uint64_t n_seeds, int max_height, int salt, int rx0,
+                     int rx1, int rz0, int rz1) {
+    Request rq;
+    std::memset(&rq, 0, sizeof rq);
+    if (opts) rq.opts = *opts;
+    rq.gen_base = gen_base;
+    rq.n_seeds = n_seeds;
+    rq.max_height = max_height;
+    rq.salt = salt;
+    rq.rx0 = rx0;
+    rq.rx1 = rx1;
+    rq.rz0 = rz0;
+    rq.rz1 = rz1;
+    return rq;
+}
+
+// Version names with a biome tree (the reference's biome_trees.h version table): tree
+// index, 1.18 rules, pre-26.2 rules.
+struct VersionName {
+    const char *name;
+    int tree, is_118, pre_262;
+};
+const VersionName kVersions[] = {
+    {"1.18", 0, 1, 1},   {"1.18.1", 0, 1, 1},  {"1.18.2", 0, 1, 1},  {"1.19", 1, 0, 1},    {"1.19.2", 1, 0, 1},
+    {"1.19.3", 2, 0, 1}, {"1.19.4", 2, 0, 1},  {"1.20", 3, 0, 1},    {"1.20.1", 3, 0, 1},  {"1.20.2", 3, 0, 1},
+    {"1.20.4", 3, 0, 1}, {"1.20.5", 3, 0, 1},  {"1.20.6", 3, 0, 1},  {"1.21", 3, 0, 1},    {"1.21.1", 3, 0, 1},
+    {"1.21.2", 3, 0, 1}, {"1.21.3", 3, 0, 1},  {"1.21.4", 4, 0, 1},  {"1.21.5", 5, 0, 1},  {"1.21.8", 5, 0, 1},
+    {"1.21.11", 5, 0, 1}, {"26.1", 5, 0, 1},   {"26.2", 6, 0, 0},    {"26.3", 7, 0, 0},
+};
+
+}  // namespace
+
+extern "C" {
+
+int wg_parse_version(const char *s, wg_opts *o) {
+    if (!s || !o) return WG_ERR_ARG;
+    for (const VersionName &v : kVersions)
+        if (!std::strcmp(v.name, s)) {
+            o->mc_1_18_2 = v.is_118;
+            o->pre_26_2 = v.pre_262;
+            o->biome_tree = v.tree + 1;
+            return WG_OK;
+        }
+    static const char *v118[] = {"1.18.x", nullptr};
+    static const char *vpre[] = {"1.19.x", "1.20.x", "1.21.x~26.1", "1.21.5~26.1", "1.19.x~26.1", nullptr};
+    for (int i = 0; v118[i]; i++)
+        if (!std::strcmp(s, v118[i])) { o->mc_1_18_2 = 1; o->pre_26_2 = 1; return WG_OK; }
+    for (int i = 0; vpre[i]; i++)
+        if (!std::strcmp(s, vpre[i])) { o->mc_1_18_2 = 0; o->pre_26_2 = 1; return WG_OK; }
+    if (!std::strcmp(s, "26.2~26.3")) { o->mc_1_18_2 = 0; o->pre_26_2 = 0; return WG_OK; }
+    return WG_ERR_ARG;
+}
+
+int wg_parse_preset(const char *s, wg_opts *o) {
+    if (!s || !o) return WG_ERR_ARG;
+    if (!std::strcmp(s, "NORMAL")) return WG_OK;
+    if (!std::strcmp(s, "LARGE_BIOMES")) { o->large_biomes = 1; return WG_OK; }
+    if (!std::strcmp(s, "SINGLE_BIOME")) { o->single_biome = 1; return WG_OK; }
+    return WG_ERR_ARG;
+}
+
+int wg_engine_open(int device, wg_engine **out) {
+    if (!out) return WG_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || device < 0 || device >= ndev) return WG_ERR_NODEV;
+    wg_engine *eng = new (std::nothrow) wg_engine();
+    if (!eng) return WG_ERR_NOMEM;
+    eng->device = device;
+    int rc = [&]() -> int {
+        WG_CUDA(cudaSetDevice(device), "cudaSetDevice");
+        WG_CUDA(cudaDeviceGetAttribute(&eng->sm_count, cudaDevAttrMultiProcessorCount, device), "device attr");
+        WG_CUDA(cudaStreamCreateWithFlags(&eng->stream, cudaStreamNonBlocking), "stream");
+        WG_CUDA(cudaEventCreate(&eng->ev0), "event");
+        WG_CUDA(cudaEventCreate(&eng->ev1), "event");
+        NoiseSpec specs[N_NOISE_COUNT];
+        build_noise_specs(specs);
+        ClimateStep normal[kClimateSteps], large[kClimateSteps];
+        build_steps(specs, N_EROSION, N_TEMPERATURE, normal);
+        build_steps(specs, N_EROSION_LARGE, N_TEMPERATURE_LARGE, large);
+        upload_tables(specs, normal, large);
+        WG_CUDA(cudaGetLastError(), "upload tables");
+        WG_CUDA(cudaMalloc(&eng->rec_unit, sizeof(uint32_t) * kCapRec), "alloc");
+        WG_CUDA(cudaMalloc(&eng->rec_off, sizeof(uint32_t) * kCapRec), "alloc");
+        WG_CUDA(cudaMalloc(&eng->rec_cnt, sizeof(uint32_t) * kCapRec), "alloc");
+        WG_CUDA(cudaMalloc(&eng->surv, sizeof(uint32_t) * kCapSurv), "alloc");
+        WG_CUDA(cudaMalloc(&eng->deep, sizeof(uint32_t) * 2 * kCapDeep), "alloc");
+        WG_CUDA(cudaMalloc(&eng->out, sizeof(Candidate) * kCapOut), "alloc");
+        WG_CUDA(cudaMalloc(&eng->counters, sizeof(uint32_t) * CNT_WORDS), "alloc");
+        WG_CUDA(cudaMalloc(&eng->hist, sizeof(unsigned long long) * (P1_KINDS + kTiers)), "alloc");
+        WG_CUDA(cudaMallocHost(&eng->h_counters, sizeof(uint32_t) * CNT_WORDS), "alloc");
+        WG_CUDA(cudaMallocHost(&eng->h_hist, sizeof(unsigned long long) * (P1_KINDS + kTiers)), "alloc");
+        return WG_OK;
+    }();
+    if (rc) {
+        wg_engine_close(eng);
+        return rc;
+    }
+    *out = eng;
+    return WG_OK;
+}
+
+void wg_engine_close(wg_engine *eng) {
+    if (!eng) return;
+    cudaSetDevice(eng->device);
+    if (eng->stream) cudaStreamSynchronize(eng->stream);
+    cudaFree(eng->rec_unit);
+    cudaFree(eng->rec_off);
+    cudaFree(eng->rec_cnt);
+    cudaFree(eng->surv);
+    cudaFree(eng->deep);
+    cudaFree(eng->out);
+    cudaFree(eng->counters);
+    cudaFree(eng->hist);
+    cudaFree(eng->d_seed_list);
+    cudaFreeHost(eng->h_counters);
+    cudaFreeHost(eng->h_hist);
+    if (eng->ev0) cudaEventDestroy(eng->ev0);
+    if (eng->ev1) cudaEventDestroy(eng->ev1);
+    if (eng->stream) cudaStreamDestroy(eng->stream);
+    delete eng;
+}
+
+const char *wg_engine_error(const wg_engine *eng) { return eng ? eng->err.c_str() : "no engine"; }
+
+int wg_seed_check(wg_engine *eng, const int64_t *seeds, uint64_t gen_base, uint64_t n_seeds, const wg_opts *opts,
+                  int max_height, int salt, int rx0, int rx1, int rz0, int rz1, wg_candidate *out, uint64_t cap,
+                  uint64_t *n_out, wg_scan_stats *stats) {
+    if (!eng || (cap && !out)) return WG_ERR_ARG;
+    auto t0 = std::chrono::steady_clock::now();
+    WG_CUDA(cudaSetDevice(eng->device), "cudaSetDevice");
+    Request rq = make_request(opts, gen_base, n_seeds, max_height, salt, rx0, rx1, rz0, rz1);
+    int rc = stage_seeds(eng, seeds, n_seeds, &rq.d_seeds);
+    if (rc) return rc;
+    wg_scan_stats st;
+    std::memset(&st, 0, sizeof st);
+    std::vector<Candidate> found;
+    Sink sink;
+    sink.host = &found;
+    WG_CUDA(cudaEventRecord(eng->ev0, eng->stream), "event");
+    rc = run_request(eng, rq, sink, st);
+    if (rc) return rc;
+    WG_CUDA(cudaEventRecord(eng->ev1, eng->stream), "event");
+    WG_CUDA(cudaEventSynchronize(eng->ev1), "event");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, eng->ev0, eng->ev1);
+    std::sort(found.begin(), found.end(), [](const Candidate &x, const Candidate &y) {
+        if (x.seed_index != y.seed_index) return x.seed_index < y.seed_index;
+        if (x.rz != y.rz) return x.rz < y.rz;
+        return x.rx < y.rx;
+    });
+    uint64_t n = std::min<uint64_t>(cap, found.size());
+    for (uint64_t i = 0; i < n; i++) {
+        const Candidate &c = found[i];
+        out[i].seed_index = c.seed_index;
+        out[i].seed = c.seed;
+        out[i].rx = c.rx;
+        out[i].rz = c.rz;
+        out[i].chunk_x = c.chunk_x;
+        out[i].chunk_z = c.chunk_z;
+    }
+    if (n_out) *n_out = found.size();
+    st.gpu_ms = ms;
+    st.wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (stats) *stats = st;
+    return WG_OK;
+}
+
+int wg_seed_check_device(wg_engine *eng, const int64_t *d_seeds, uint64_t gen_base, uint64_t n_seeds,
+                         const wg_opts *opts, int max_height, int salt, int rx0, int rx1, int rz0, int rz1,
+                         wg_candidate *d_out, uint64_t cap, uint64_t *n_out, wg_scan_stats *stats, void *stream) {
+    if (!eng || (cap && !d_out)) return WG_ERR_ARG;
+    static_assert(sizeof(wg_candidate) == sizeof(Candidate), "candidate layout");
+    auto t0 = std::chrono::steady_clock::now();
+    WG_CUDA(cudaSetDevice(eng->device), "cudaSetDevice");
+    cudaStream_t user = (cudaStream_t)stream;
+    if (user) {  // order the engine stream after the caller's prior work
+        WG_CUDA(cudaEventRecord(eng->ev0, user), "event");
+        WG_CUDA(cudaStreamWaitEvent(eng->stream, eng->ev0, 0), "wait");
+    }
+    Request rq = make_request(opts, gen_base, n_seeds, max_height, salt, rx0, rx1, rz0, rz1);
+    rq.d_seeds = d_seeds;
+    wg_scan_stats st;
+    std::memset(&st, 0, sizeof st);
+    Sink sink;
+    sink.dev = reinterpret_cast<Candidate *>(d_out);
+    sink.dev_cap = cap;
+    WG_CUDA(cudaEventRecord(eng->ev0, eng->stream), "event");
+    int rc = run_request(eng, rq, sink, st);
+    if (rc) return rc;
+    WG_CUDA(cudaEventRecord(eng->ev1, eng->stream), "event");
+    WG_CUDA(cudaEventSynchronize(eng->ev1), "event");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, eng->ev0, eng->ev1);
+    if (n_out) *n_out = sink.found;
+    st.gpu_ms = ms;
+    st.wall_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (stats) *stats = st;
+    return WG_OK;
+}
+
+int wg_phase1_codes(wg_engine *eng, const int64_t *seeds, uint64_t gen_base, uint64_t n_seeds, const wg_opts *opts,
+                    int max_height, int salt, int rx0, int rx1, int rz0, int rz1, int8_t *codes, int8_t *tiers) {
+    if (!eng || !codes || !tiers || rx1 <= rx0 || rz1 <= rz0) return WG_ERR_ARG;
+    WG_CUDA(cudaSetDevice(eng->device), "cudaSetDevice");
+    const uint64_t total = n_seeds * (uint64_t)((int64_t)rx1 - rx0) * (uint64_t)((int64_t)rz1 - rz0);
+    Request rq = make_request(opts, gen_base, n_seeds, max_height, salt, rx0, rx1, rz0, rz1);
+    int rc = stage_seeds(eng, seeds, n_seeds, &rq.d_seeds);
+    if (rc) return rc;
+    int8_t *dc = nullptr, *dt = nullptr;
+    WG_CUDA(cudaMalloc(&dc, total), "alloc codes");
+    if (cudaMalloc(&dt, total) != cudaSuccess) {
+        cudaFree(dc);
+        return eng->fail(WG_ERR_NOMEM, "alloc tiers");
+    }
+    cudaMemsetAsync(dc, -1, total, eng->stream);
+    cudaMemsetAsync(dt, -1, total, eng->stream);
+    rq.d_codes = dc;
+    rq.d_tiers = dt;
+    wg_scan_stats st;
+    std::memset(&st, 0, sizeof st);
+    std::vector<Candidate> found;
+    Sink sink;
+    sink.host = &found;
+    rc = run_request(eng, rq, sink, st);
+    if (!rc) {
+        cudaError_t e1 = cudaMemcpy(codes, dc, total, cudaMemcpyDeviceToHost);
+        cudaError_t e2 = cudaMemcpy(tiers, dt, total, cudaMemcpyDeviceToHost);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) rc = eng->fail(WG_ERR_CUDA, "copy codes", e1 ? e1 : e2);
+    }
+    cudaFree(dc);
+    cudaFree(dt);
+    return rc;
+}
+
+}  // extern "C"

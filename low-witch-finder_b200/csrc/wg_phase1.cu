@@ -1,0 +1,526 @@
+// Seed Check phase-1 kernels; see wg_phase1.cuh for the pipeline.
+#include <cuda_runtime.h>
+
+#include "wg_device.cuh"
+#include "wg_phase1.cuh"
+
+namespace wg {
+
+__constant__ NoiseSpec c_noise[N_NOISE_COUNT];
+__constant__ ClimateStep c_steps[2][kClimateSteps];     // [large_biomes][step]
+__constant__ int8_t c_slot_a[2][kSlotsA][3];             // climate slots: noise, sub, octave
+__constant__ int8_t c_slot_c[2][kSlotsC][3];             // cave slots (the entrance kernel uses the first 18)
+
+// Slot bases of each noise inside the cave slot set (sub 0 octaves, then sub 1 octaves).
+constexpr int kBaseEntrance = 0, kBaseRarity = 6, kBaseThickness = 8, kBaseSp1 = 10, kBaseSp2 = 12;
+constexpr int kBaseRmod = 14, kBaseRough = 16, kBaseLayer = 18, kBaseCheese = 20, kBaseCont = 34;
+constexpr int kBaseFlood = 52;
+
+static void fill_slots(int8_t (*dst)[3], const NoiseSpec *specs, const int *noises, int nn, int expect) {
+    int s = 0;
+    for (int q = 0; q < nn; q++) {
+        int np = specs[noises[q]].npresent;
+        for (int sub = 0; sub < 2; sub++)
+            for (int p = 0; p < np; p++) {
+                dst[s][0] = (int8_t)noises[q];
+                dst[s][1] = (int8_t)sub;
+                dst[s][2] = (int8_t)p;
+                s++;
+            }
+    }
+    (void)expect;
+}
+
+void upload_tables(const NoiseSpec *specs, const ClimateStep *steps_normal, const ClimateStep *steps_large) {
+    cudaMemcpyToSymbol(c_noise, specs, sizeof(NoiseSpec) * N_NOISE_COUNT);
+    ClimateStep st[2][kClimateSteps];
+    for (int i = 0; i < kClimateSteps; i++) {
+        st[0][i] = steps_normal[i];
+        st[1][i] = steps_large[i];
+    }
+    cudaMemcpyToSymbol(c_steps, st, sizeof(st));
+    int8_t sa[2][kSlotsA][3], sc[2][kSlotsC][3];
+    for (int lg = 0; lg < 2; lg++) {
+        int na[3] = {lg ? N_EROSION_LARGE : N_EROSION, lg ? N_TEMPERATURE_LARGE : N_TEMPERATURE, N_RIDGE};
+        fill_slots(sa[lg], specs, na, 3, kSlotsA);
+        int nc[11] = {N_CAVE_ENTRANCE, N_SPAGHETTI_RARITY, N_SPAGHETTI_THICKNESS, N_SPAGHETTI_1, N_SPAGHETTI_2,
+                      N_ROUGHNESS_MODULATOR, N_ROUGHNESS, N_CAVE_LAYER, N_CAVE_CHEESE,
+                      lg ? N_CONTINENTALNESS_LARGE : N_CONTINENTALNESS, N_FLOODEDNESS};
+        fill_slots(sc[lg], specs, nc, 11, kSlotsC);
+    }
+    cudaMemcpyToSymbol(c_slot_a, sa, sizeof(sa));
+    cudaMemcpyToSymbol(c_slot_c, sc, sizeof(sc));
+}
+
+// ------------------------------------------------------------------------------------
+// helpers
+// ------------------------------------------------------------------------------------
+// Global seed index and region of a batch-local unit / window offset.
+__device__ __forceinline__ uint64_t unit_seed_index(const BatchArgs &a, uint32_t u) { return (a.unit0 + u) / a.n_win; }
+__device__ __forceinline__ uint64_t unit_window(const BatchArgs &a, uint32_t u) { return (a.unit0 + u) % a.n_win; }
+__device__ __forceinline__ uint64_t seed_value(const BatchArgs &a, uint64_t g) {
+    return a.seeds ? (uint64_t)a.seeds[g] : splitmix64(a.gen_base + g);
+}
+// Number of regions in a unit's window.
+__device__ __forceinline__ uint32_t window_len(const BatchArgs &a, uint64_t w) {
+    uint64_t start = w * a.win;
+    uint64_t left = a.n_regions - start;
+    return (uint32_t)(left < a.win ? left : a.win);
+}
+// Region (rx, rz) of global region index r (rz outer, rx inner: search.c:148-149).
+__device__ __forceinline__ void region_xz(const BatchArgs &a, uint64_t r, int &rx, int &rz) {
+    rz = a.rz0 + (int)(r / (uint64_t)a.rw);
+    rx = a.rx0 + (int)(r % (uint64_t)a.rw);
+}
+
+__device__ __forceinline__ void note_code(const BatchArgs &a, uint64_t g, uint64_t r, int code, int tier) {
+    if (a.codes) {
+        size_t at = (size_t)g * (size_t)a.n_regions + (size_t)r;
+        a.codes[at] = (int8_t)code;
+        a.tiers[at] = (int8_t)tier;
+    }
+}
+
+// Table sources: where a sampler's permutation table and origin live.
+struct SrcIl {  // bank-interleaved shared block per slot, origins [slot][32]
+    const uint8_t *perm;
+    const double *ox, *oy, *oz;
+    int lane;
+    __device__ __forceinline__ double p3(int slot, double x, double y, double z) const {
+        IlTable T{perm + slot * 8192 + lane * 4};
+        int o = slot * 32 + lane;
+        return perlin_3d(T, ox[o], oy[o], oz[o], x, y, z);
+    }
+};
+struct SrcFlat {  // contiguous 256-byte tables, origins [slot][3]
+    const uint8_t *perm;
+    const double *org;
+    __device__ __forceinline__ double p3(int slot, double x, double y, double z) const {
+        FlatTable T{perm + slot * 256};
+        return perlin_3d(T, org[3 * slot], org[3 * slot + 1], org[3 * slot + 2], x, y, z);
+    }
+};
+
+// DoublePerlinNoiseSampler.sample (noise.c:263-289).
+template <class S>
+__device__ double dbl3d(const S &src, int noise, int base, double x, double y, double z) {
+    const NoiseSpec &ns = c_noise[noise];
+    const int np = ns.npresent;
+    double a = 0.0;
+    for (int p = 0; p < np; p++) {
+        double l = ns.lac[p];
+        double v = src.p3(base + p, keep_precision(x * l), keep_precision(y * l), keep_precision(z * l));
+        a += (ns.amp[p] * v) * ns.per[p];
+    }
+    double xs = x * kDblScale, ys = y * kDblScale, zs = z * kDblScale;
+    double b = 0.0;
+    for (int p = 0; p < np; p++) {
+        double l = ns.lac[p];
+        double v = src.p3(base + np + p, keep_precision(xs * l), keep_precision(ys * l), keep_precision(zs * l));
+        b += (ns.amp[p] * v) * ns.per[p];
+    }
+    return (a + b) * ns.amplitude;
+}
+
+// SearchCoords cave heuristics (caves.c:41-130).
+__device__ __forceinline__ double tunnel_scale(double v) {
+    if (v < -0.5) return 0.75;
+    if (v < 0.0) return 1.0;
+    if (v < 0.5) return 1.5;
+    return 2.0;
+}
+
+template <class S>
+__device__ double spaghetti(const S &src, int x, int y, int z) {
+    double e = tunnel_scale(dbl3d(src, N_SPAGHETTI_RARITY, kBaseRarity, (double)(int)((uint32_t)x * 2u), (double)y,
+                                  (double)(int)((uint32_t)z * 2u)));
+    double tv = dbl3d(src, N_SPAGHETTI_THICKNESS, kBaseThickness, (double)x, (double)y, (double)z);
+    double h = lerp((tv - -1.0) / (1.0 - -1.0), 0.065, 0.088);
+    double l = dbl3d(src, N_SPAGHETTI_1, kBaseSp1, (double)x / e, (double)y / e, (double)z / e);
+    double m = fabs(e * l) - h;
+    double n = dbl3d(src, N_SPAGHETTI_2, kBaseSp2, (double)x / e, (double)y / e, (double)z / e);
+    double o = fabs(e * n) - h;
+    double p = clampd(jmax(m, o), -1.0, 1.0);
+    double mod = dbl3d(src, N_ROUGHNESS_MODULATOR, kBaseRmod, (double)x, (double)y, (double)z);
+    double rgh = dbl3d(src, N_ROUGHNESS, kBaseRough, (double)x, (double)y, (double)z);
+    double q = (-0.05 + (-0.05 * mod)) * (-0.4 + fabs(rgh));
+    return p + q;
+}
+
+template <class S>
+__device__ double entrance(const S &src, int x, int y, int z) {
+    double ent = dbl3d(src, N_CAVE_ENTRANCE, kBaseEntrance, (double)x * 0.75, (double)y * 0.5, (double)z * 0.75);
+    double t = (10.0 + (double)y) / 40.0;
+    double cl = t < 0.0 ? 0.3 : (t > 1.0 ? 0.0 : lerp(t, 0.3, 0.0));
+    double cc = ent + 0.37 + cl;
+    return jmin(cc, spaghetti(src, x, y, z));
+}
+
+template <class S>
+__device__ double cheese(const S &src, int x, int y, int z) {
+    double layer = dbl3d(src, N_CAVE_LAYER, kBaseLayer, (double)x, (double)(int)((uint32_t)y * 8u), (double)z);
+    double av = 4.0 * layer * layer;
+    double raw = dbl3d(src, N_CAVE_CHEESE, kBaseCheese, (double)x, (double)y * 0.6666666666666666, (double)z);
+    return av + clampd(0.27 + raw, -1.0, 1.0);
+}
+
+// ------------------------------------------------------------------------------------
+// climate kernel
+// ------------------------------------------------------------------------------------
+struct ClimateSmem {
+    uint8_t perm[kSlotsA * 8192];
+    double ox[kSlotsA * 32], oz[kSlotsA * 32], hy[kSlotsA * 32], fy[kSlotsA * 32];
+    int jy[kSlotsA * 32];
+    uint32_t surv[32 * kRecordCap];
+    uint32_t cnt[32];
+    unsigned int hist[P1_KINDS + kTiers];
+    ClimateStep steps[kClimateSteps];
+};
+
+size_t climate_smem_bytes() { return sizeof(ClimateSmem); }
+
+// A record holding one survivor, for a unit whose shared list is full.
+__device__ void emit_single(const BatchArgs &a, uint32_t u, uint32_t off_in_win) {
+    uint32_t ri = atomicAdd(&a.counters[CNT_RECORDS], 1u);
+    uint32_t off = atomicAdd(&a.counters[CNT_SURVIVORS], 1u);
+    if (ri < a.cap_rec && off < a.cap_surv) {
+        a.rec_unit[ri] = u;
+        a.rec_off[ri] = off;
+        a.rec_cnt[ri] = 1;
+        a.surv_region[off] = off_in_win;
+    } else {
+        if (ri < a.cap_rec) a.rec_cnt[ri] = 0;  // a reserved record is never left stale
+        atomicOr(&a.counters[CNT_OVERFLOW], 1u);
+    }
+}
+
+__device__ __forceinline__ void keep_survivor(ClimateSmem &S, const BatchArgs &a, int lane, uint32_t u, uint32_t j) {
+    uint32_t q = atomicAdd(&S.cnt[lane], 1u);
+    if (q < kRecordCap) S.surv[lane * kRecordCap + q] = j;
+    else emit_single(a, u, j);
+}
+
+__global__ void __launch_bounds__(kThreadsA, 1) climate_kernel(BatchArgs a) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    ClimateSmem &S = *reinterpret_cast<ClimateSmem *>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int large = a.large_biomes ? 1 : 0;
+    if (threadIdx.x < 32) S.cnt[threadIdx.x] = 0;
+    if (threadIdx.x < P1_KINDS + kTiers) S.hist[threadIdx.x] = 0;
+    if (threadIdx.x < kClimateSteps) S.steps[threadIdx.x] = c_steps[large][threadIdx.x];
+
+    const uint32_t u = blockIdx.x * 32u + (uint32_t)lane;
+    const bool valid = u < a.n_units;
+    const uint64_t g = valid ? unit_seed_index(a, u) : 0;
+    const uint64_t w = valid ? unit_window(a, u) : 0;
+    const uint64_t seed = valid ? seed_value(a, g) : 0;
+    const uint32_t len = valid ? window_len(a, w) : 0;
+    const uint64_t r_base = w * a.win;
+
+    // ---- build: warp w builds climate slot w for the CTA's 32 units ----
+    if (valid && !a.single_biome) {
+        const int noise = c_slot_a[large][warp][0], sub = c_slot_a[large][warp][1], p = c_slot_a[large][warp][2];
+        Xr r = octave_rng(c_noise[noise], seed_fork_of(seed), sub, p);
+        double ox, oy, oz;
+        perlin_build_il(S.perm + warp * 8192 + lane * 4, r, ox, oy, oz);
+        const int o = warp * 32 + lane;
+        int jy = (int)floor(oy);
+        double hy = oy - jy;
+        S.ox[o] = ox;
+        S.oz[o] = oz;
+        S.hy[o] = hy;
+        S.fy[o] = fade(hy);
+        S.jy[o] = jy;
+    }
+    __syncthreads();
+
+    // ---- evaluate: lane = unit, warp w walks window offsets w, w+18, ...; one Perlin
+    // sample per loop trip, so lanes at different gate depths stay converged ----
+    if (valid) {
+        uint32_t next_j = (uint32_t)warp, cur = 0;
+        bool have = false;
+        int k = 0;
+        double xc = 0.0, zc = 0.0, sum = 0.0, sum_a = 0.0;
+        const uint8_t *lane_perm = S.perm + lane * 4;
+        for (;;) {
+            if (!have) {
+                if (next_j >= len) break;
+                cur = next_j;
+                next_j += kSlotsA;
+                int rx, rz, cx, cz;
+                region_xz(a, r_base + cur, rx, rz);
+                hut_chunk(seed, rx, rz, a.salt, cx, cz);
+                if (a.single_biome) {  // phase1.c:96: the climate gates are skipped
+                    keep_survivor(S, a, lane, u, cur);
+                    continue;
+                }
+                xc = (cx * 16 + 8) / 4.0;
+                zc = (cz * 16 + 8) / 4.0;
+                k = 0;
+                sum = 0.0;
+                have = true;
+            }
+            const ClimateStep &st = S.steps[k];
+            const int o = st.slot * 32 + lane;
+            IlTable T{lane_perm + st.slot * 8192};
+            double v = perlin_y0(T, S.ox[o], S.oz[o], S.jy[o], S.hy[o], S.fy[o],
+                                 keep_precision((xc * st.sc) * st.lac), keep_precision((zc * st.sc) * st.lac));
+            sum += (st.c1 * v) * st.c2;
+            int code = -1, tier = -1;
+            switch (st.act) {
+                case ACT_TIER:
+                case ACT_TIER_LAST:
+                    if (sum * st.amp < st.thr) {
+                        code = P1_EROSION;
+                        tier = st.tier;
+                    } else if (st.act == ACT_TIER_LAST) {
+                        sum = 0.0;
+                    }
+                    break;
+                case ACT_END_SUB_A:
+                    sum_a = sum;
+                    sum = 0.0;
+                    break;
+                case ACT_TEMPERATURE: {
+                    double t = (sum_a + sum) * st.amp;
+                    bool bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
+                    if (bad) code = P1_TEMPERATURE;
+                    sum = 0.0;
+                    break;
+                }
+                case ACT_RIDGE: {
+                    double rg = (sum_a + sum) * st.amp;
+                    if ((rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91))
+                        code = P1_RIDGE;
+                    else
+                        code = P1_ACCEPT;  // climate survivor, not yet a verdict
+                    break;
+                }
+                default:
+                    break;
+            }
+            if (code >= 0) {
+                have = false;
+                if (code == P1_ACCEPT) {
+                    keep_survivor(S, a, lane, u, cur);
+                } else {
+                    atomicAdd(&S.hist[code], 1u);
+                    if (tier >= 0) atomicAdd(&S.hist[P1_KINDS + tier], 1u);
+                    note_code(a, g, r_base + cur, code, tier);
+                }
+            } else {
+                k++;
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- one record per unit with survivors ----
+    if (warp == 0 && valid) {
+        uint32_t n = min(S.cnt[lane], (uint32_t)kRecordCap);
+        if (n) {
+            uint32_t ri = atomicAdd(&a.counters[CNT_RECORDS], 1u);
+            uint32_t off = atomicAdd(&a.counters[CNT_SURVIVORS], n);
+            if (ri < a.cap_rec && off + n <= a.cap_surv) {
+                a.rec_unit[ri] = u;
+                a.rec_off[ri] = off;
+                a.rec_cnt[ri] = n;
+                for (uint32_t q = 0; q < n; q++) a.surv_region[off + q] = S.surv[lane * kRecordCap + q];
+            } else {
+                if (ri < a.cap_rec) a.rec_cnt[ri] = 0;
+                atomicOr(&a.counters[CNT_OVERFLOW], 1u);
+            }
+        }
+    }
+    if (threadIdx.x < P1_KINDS + kTiers && S.hist[threadIdx.x])
+        atomicAdd(&a.hist[threadIdx.x], (unsigned long long)S.hist[threadIdx.x]);
+}
+
+void launch_climate(const BatchArgs &a, cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(climate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ClimateSmem));
+        attr = true;
+    }
+    int grid = (int)((a.n_units + 31) / 32);
+    climate_kernel<<<grid, kThreadsA, sizeof(ClimateSmem), s>>>(a);
+}
+
+// ------------------------------------------------------------------------------------
+// entrance kernel: Entrance(50) / Entrance(60) for every climate survivor
+// ------------------------------------------------------------------------------------
+struct EntranceSmem {
+    uint8_t perm[kSlotsB * 8192];
+    double ox[kSlotsB * 32], oy[kSlotsB * 32], oz[kSlotsB * 32];
+    unsigned int hist[P1_KINDS];
+};
+
+size_t entrance_smem_bytes() { return sizeof(EntranceSmem); }
+
+__global__ void __launch_bounds__(kThreadsB, 1) entrance_kernel(BatchArgs a) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    EntranceSmem &S = *reinterpret_cast<EntranceSmem *>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x < P1_KINDS) S.hist[threadIdx.x] = 0;
+    // A full list means the host discards this batch and re-runs it smaller.
+    if (a.counters[CNT_OVERFLOW]) return;
+    const uint32_t n_rec = min(a.counters[CNT_RECORDS], a.cap_rec);
+    const uint32_t n_tiles = (n_rec + 31) / 32;
+    const SrcIl src{S.perm, S.ox, S.oy, S.oz, lane};
+    for (uint32_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const uint32_t ri = tile * 32 + (uint32_t)lane;
+        const bool valid = ri < n_rec;
+        uint32_t u = 0, off = 0, cnt = 0;
+        uint64_t g = 0, r_base = 0, seed = 0;
+        if (valid) {
+            u = a.rec_unit[ri];
+            off = a.rec_off[ri];
+            cnt = a.rec_cnt[ri];
+            if (u >= a.n_units || off >= a.cap_surv || cnt > a.cap_surv - off) cnt = 0;
+            g = unit_seed_index(a, u);
+            r_base = unit_window(a, u) * a.win;
+            seed = seed_value(a, g);
+            const int noise = c_slot_c[0][warp][0], sub = c_slot_c[0][warp][1], p = c_slot_c[0][warp][2];
+            Xr r = octave_rng(c_noise[noise], seed_fork_of(seed), sub, p);
+            double ox, oy, oz;
+            perlin_build_il(S.perm + warp * 8192 + lane * 4, r, ox, oy, oz);
+            const int o = warp * 32 + lane;
+            S.ox[o] = ox;
+            S.oy[o] = oy;
+            S.oz[o] = oz;
+        }
+        __syncthreads();
+        if (valid) {
+            for (uint32_t j = (uint32_t)warp; j < cnt; j += kSlotsB) {
+                const uint32_t jr = a.surv_region[off + j];
+                int rx, rz, cx, cz;
+                region_xz(a, r_base + jr, rx, rz);
+                hut_chunk(seed, rx, rz, a.salt, cx, cz);
+                const int hx = cx * 16 + 3, hz = cz * 16 + 3;
+                int code = -1;
+                if (entrance(src, hx, 50, hz) >= 0) code = P1_ENTRANCE_50;
+                else if (entrance(src, hx, 60, hz) >= 0) code = P1_ENTRANCE_60;
+                if (code >= 0) {
+                    atomicAdd(&S.hist[code], 1u);
+                    note_code(a, g, r_base + jr, code, -1);
+                } else {
+                    uint32_t di = atomicAdd(&a.counters[CNT_DEEP], 1u);
+                    if (di < a.cap_deep) {
+                        a.deep[2 * di] = u;
+                        a.deep[2 * di + 1] = jr;
+                    } else {
+                        atomicOr(&a.counters[CNT_OVERFLOW], 2u);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < P1_KINDS && S.hist[threadIdx.x])
+        atomicAdd(&a.hist[threadIdx.x], (unsigned long long)S.hist[threadIdx.x]);
+}
+
+void launch_entrance(const BatchArgs &a, int grid, cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(entrance_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(EntranceSmem));
+        attr = true;
+    }
+    entrance_kernel<<<grid, kThreadsB, sizeof(EntranceSmem), s>>>(a);
+}
+
+// ------------------------------------------------------------------------------------
+// ladder kernel: the rest of lysh_phase1_check_ex for candidates past Entrance(60)
+// ------------------------------------------------------------------------------------
+struct LadderSmem {
+    uint8_t perm[kSlotsC * 256];
+    double org[kSlotsC * 3];
+};
+
+__global__ void __launch_bounds__(kThreadsC) ladder_kernel(BatchArgs a) {
+    __shared__ __align__(16) LadderSmem S;
+    const int large = a.large_biomes ? 1 : 0;
+    if (a.counters[CNT_OVERFLOW]) return;
+    const uint32_t n_deep = min(a.counters[CNT_DEEP], a.cap_deep);
+    const SrcFlat src{S.perm, S.org};
+    for (uint32_t q = blockIdx.x; q < n_deep; q += gridDim.x) {
+        const uint32_t u = a.deep[2 * q], jr = a.deep[2 * q + 1];
+        const uint64_t g = unit_seed_index(a, u);
+        const uint64_t r = unit_window(a, u) * a.win + jr;
+        const uint64_t seed = seed_value(a, g);
+        const int t = threadIdx.x;
+        if (t < kSlotsC) {
+            const int noise = c_slot_c[large][t][0], sub = c_slot_c[large][t][1], p = c_slot_c[large][t][2];
+            Xr rng = octave_rng(c_noise[noise], seed_fork_of(seed), sub, p);
+            double ox, oy, oz;
+            perlin_build_flat(S.perm + t * 256, rng, ox, oy, oz);
+            S.org[3 * t] = ox;
+            S.org[3 * t + 1] = oy;
+            S.org[3 * t + 2] = oz;
+        }
+        __syncthreads();
+        if (t == 0) {
+            int rx, rz, cx, cz;
+            region_xz(a, r, rx, rz);
+            hut_chunk(seed, rx, rz, a.salt, cx, cz);
+            const int hut_x = cx * 16, hut_z = cz * 16;
+            const int hx = hut_x + 3, hz = hut_z + 3, mh = a.max_height;
+            int code = P1_ACCEPT;
+            if (spaghetti(src, hx, mh, hz) >= 0 && cheese(src, hx, mh, hz) >= 0) code = P1_CAVE_AT_MAXH;
+            if (code == P1_ACCEPT) {
+                int floor_y = (-40 < mh) ? -40 : mh;
+                if (floor_y < -50) floor_y = -50;
+                for (int y = 0; y >= floor_y; y -= 10)
+                    if (mh < y && spaghetti(src, hx, y, hz) >= 0 && cheese(src, hx, y, hz) >= 0) {
+                        code = P1_LADDER_NEG;
+                        break;
+                    }
+            }
+            if (code == P1_ACCEPT) {
+                for (int y = 10; y <= 40; y += 10)
+                    if (entrance(src, hx, y, hz) >= 0 && cheese(src, hx, y, hz) >= 0) {
+                        code = P1_LADDER_POS;
+                        break;
+                    }
+            }
+            if (code == P1_ACCEPT && !a.single_biome) {
+                // The y = 0 climate sample equals the 3-D sample at y = 0 bit for bit.
+                double c = dbl3d(src, large ? N_CONTINENTALNESS_LARGE : N_CONTINENTALNESS, kBaseCont,
+                                 (hut_x + 8) / 4.0, 0.0, (hut_z + 8) / 4.0);
+                if (c < -0.11) code = P1_CONTINENTALNESS;
+            }
+            if (code == P1_ACCEPT) {
+                for (int y = mh; y <= 60; y += 10) {
+                    double f = dbl3d(src, N_FLOODEDNESS, kBaseFlood, (double)(hut_x + 3), (double)y * 0.67,
+                                     (double)(hut_z + 3));
+                    if (f > 0.41) {
+                        code = P1_FLOODEDNESS;
+                        break;
+                    }
+                }
+            }
+            atomicAdd(&a.hist[code], 1ull);
+            note_code(a, g, r, code, -1);
+            if (code == P1_ACCEPT) {
+                uint32_t oi = atomicAdd(&a.counters[CNT_FINAL], 1u);
+                if (oi < a.cap_out) {
+                    Candidate c;
+                    c.seed_index = g;
+                    c.seed = (int64_t)seed;
+                    c.rx = rx;
+                    c.rz = rz;
+                    c.chunk_x = cx;
+                    c.chunk_z = cz;
+                    a.out[oi] = c;
+                } else {
+                    atomicOr(&a.counters[CNT_OVERFLOW], 4u);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+void launch_ladder(const BatchArgs &a, int grid, cudaStream_t s) { ladder_kernel<<<grid, kThreadsC, 0, s>>>(a); }
+
+}  // namespace wg

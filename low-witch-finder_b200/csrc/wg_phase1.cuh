@@ -1,0 +1,115 @@
+// Seed Check phase 1 on the GPU: the shared definitions between the kernels
+// (wg_phase1.cu) and the host engine (wg_engine.cu).
+//
+// Phase 1 restates lysh_phase1_check_ex (engine/tools/lysh/src/phase1.c:130-200) per
+// (seed, region) and is split into three kernels by how often each stage is reached:
+//
+//   climate  every seed     builds the 18 climate Perlins of 32 seeds per CTA in shared
+//                           memory, runs the tiered erosion / temperature / ridge gates for
+//                           every region, and emits per-seed records of the survivors
+//                           (~1.7% of regions at 9x9).
+//   entrance seeds with     builds the 18 Perlins of cave_entrance + the spaghetti set for
+//            survivors      32 records per CTA, evaluates Entrance(50) and Entrance(60)
+//                           (97% of climate survivors stop here).
+//   ladder   the rest       one CTA per remaining candidate builds all 54 cave / continent /
+//                           floodedness Perlins and finishes the ladder in lysh's order.
+#pragma once
+
+#include <cstdint>
+
+#include "wg_catalog.h"
+
+namespace wg {
+
+// Reject codes, identical to LYSH_P1_REJECT_* (engine/tools/lysh/src/phase1.h:61-74).
+enum : int {
+    P1_EROSION = 0,
+    P1_TEMPERATURE = 1,
+    P1_RIDGE = 2,
+    P1_ENTRANCE_50 = 3,
+    P1_ENTRANCE_60 = 4,
+    P1_CAVE_AT_MAXH = 5,
+    P1_LADDER_NEG = 6,
+    P1_LADDER_POS = 7,
+    P1_CONTINENTALNESS = 8,
+    P1_FLOODEDNESS = 9,
+    P1_ACCEPT = 10,
+    P1_KINDS = 11
+};
+constexpr int kTiers = 7;
+
+constexpr int kLanes = 32;          // seeds (or records) per CTA in the climate / entrance kernels
+constexpr int kSlotsA = 18;         // erosion 8 + temperature 4 + ridge 6
+constexpr int kSlotsB = 18;         // cave_entrance 6 + six one-octave spaghetti noises x 2
+constexpr int kSlotsC = 54;         // kSlotsB + cave_layer 2 + cave_cheese 14 + continentalness 18 + floodedness 2
+constexpr int kThreadsA = kSlotsA * 32;
+constexpr int kThreadsB = kSlotsB * 32;
+constexpr int kThreadsC = 64;
+constexpr int kRecordCap = 64;      // survivors held per unit record in the climate kernel
+
+// Counter block written by the kernels (one per engine, reset per batch).
+enum : int {
+    CNT_RECORDS = 0,   // per-seed survivor records emitted by the climate kernel
+    CNT_SURVIVORS,     // climate survivors (entries of surv_region)
+    CNT_DEEP,          // candidates that passed Entrance(50) and Entrance(60)
+    CNT_FINAL,         // phase-1 survivors
+    CNT_OVERFLOW,      // bit 0 records/survivors, bit 1 deep list, bit 2 final list
+    CNT_WORDS = 8
+};
+
+// Final phase-1 survivor; the layout of wg_candidate in include/witchgpu.h.
+struct Candidate {
+    uint64_t seed_index;
+    int64_t seed;
+    int32_t rx, rz;
+    int32_t chunk_x, chunk_z;
+};
+
+// Work is cut into "units": unit u of a request is (seed u / n_win, region window
+// u % n_win); a window is `win` consecutive regions of the rect (rz outer, rx inner).  One
+// lane of the climate kernel owns one unit, so a request with few seeds and a huge rect
+// (a whole-world scan of one seed) fills the GPU as well as many seeds x 9x9 regions.
+// Everything a phase-1 batch needs (device pointers only).
+struct BatchArgs {
+    const int64_t *seeds;         // all request seeds (global seed index), or nullptr: splitmix64(gen_base + i)
+    uint64_t gen_base;
+    uint64_t unit0;               // global index of the batch's first unit
+    uint32_t n_units;             // units in this batch
+    uint32_t win;                 // regions per window
+    uint64_t n_win;               // windows per seed
+    uint64_t n_regions;           // regions per seed (rw * rh)
+    int rx0, rz0, rw, rh;         // region rect origin and size
+    int salt;
+    int max_height;
+    int mc_1_18_2, pre_26_2, single_biome, large_biomes;
+
+    uint32_t *rec_unit;           // [cap_rec] batch-local unit of each record
+    uint32_t *rec_off;            // [cap_rec] first entry in surv_region
+    uint32_t *rec_cnt;            // [cap_rec]
+    uint32_t *surv_region;        // [cap_surv] region offset inside the unit's window
+    uint32_t *deep;               // [cap_deep * 2] (batch-local unit, region offset)
+    Candidate *out;               // [cap_out] phase-1 survivors of this batch
+    uint32_t cap_rec, cap_surv, cap_deep, cap_out;
+    uint32_t *counters;           // [CNT_WORDS], zeroed per batch
+    unsigned long long *hist;     // [P1_KINDS + kTiers] funnel + erosion tier histogram, zeroed per batch
+    int8_t *codes;                // optional [n_seeds * n_regions] reject code per (seed, region)
+    int8_t *tiers;                // optional, same shape: erosion tier (-1 if none)
+};
+
+// One evaluation step of the climate state machine (a single y=0 Perlin sample).
+struct ClimateStep {
+    double sc, lac, c1, c2, thr, amp;
+    int slot, act, tier, pad;
+};
+enum : int { ACT_NONE = 0, ACT_TIER, ACT_TIER_LAST, ACT_END_SUB_A, ACT_TEMPERATURE, ACT_RIDGE };
+constexpr int kClimateSteps = kSlotsA;
+
+// Launchers (wg_phase1.cu).
+void upload_tables(const NoiseSpec *specs, const ClimateStep *steps_normal, const ClimateStep *steps_large);
+void launch_climate(const BatchArgs &a, cudaStream_t s);
+void launch_entrance(const BatchArgs &a, int grid, cudaStream_t s);
+void launch_ladder(const BatchArgs &a, int grid, cudaStream_t s);
+size_t climate_smem_bytes();
+size_t entrance_smem_bytes();
+
+}  // namespace wg

@@ -1,0 +1,194 @@
+"""Test infrastructure only: ctypes bindings of the two CPU checkers.
+
+* ``Port``  -- oracle/_build/libwitch_oracle.so, the C restatement (oracle/witch_oracle.c).
+* ``Ref``   -- oracle/_ref/liblysh_ref.so, the reference's own lysh compiled from its sources
+  (oracle/Makefile) plus the flat wrappers of oracle/ref_harness.c.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "_build", "libwitch_oracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "liblysh_ref.so")
+REF_BIN = os.path.join(HERE, "_ref", "lysh")
+REF_SRC = "/root/reference/engine/tools/lysh/src"
+
+
+def build(ref: bool | None = None) -> None:
+    """Compile the restatement, and the reference checker when its sources are present."""
+    subprocess.run(["make", "-s", "-C", HERE, "port"], check=True)
+    if ref is None:
+        ref = os.path.isdir(REF_SRC)
+    if ref:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8"], check=True)
+
+
+class WoOpts(C.Structure):
+    _fields_ = [("mc_1_18_2", C.c_int), ("single_biome", C.c_int), ("pre_26_2", C.c_int),
+                ("large_biomes", C.c_int)]
+
+
+CANDIDATE_DTYPE = np.dtype([("seed_index", "<u8"), ("seed", "<i8"), ("rx", "<i4"), ("rz", "<i4"),
+                            ("chunk_x", "<i4"), ("chunk_z", "<i4")])
+
+# version name -> (mc_1_18_2, pre_26_2) for the phase-1 rules (engine/tools/lysh/src/main.c:104-125)
+PHASE1_RULES = {"1.19.x~26.1": (0, 1), "1.21": (0, 1), "1.21.5": (0, 1), "26.2": (0, 0), "26.2~26.3": (0, 0),
+                "1.18.2": (1, 1), "1.18.x": (1, 1), "1.20.1": (0, 1), "26.1": (0, 1)}
+
+
+def rules(version: str, preset: str = "NORMAL") -> dict:
+    mc, pre = PHASE1_RULES[version]
+    return {"mc_1_18_2": mc, "pre_26_2": pre, "large_biomes": int(preset == "LARGE_BIOMES"),
+            "single_biome": int(preset == "SINGLE_BIOME")}
+
+
+class Port:
+    """The C restatement of the phase-1 path."""
+
+    def __init__(self, path: str = PORT_LIB):
+        if not os.path.exists(path):
+            build(ref=False)
+        lib = C.CDLL(path)
+        lib.wo_splitmix64.restype = C.c_uint64
+        lib.wo_splitmix64.argtypes = [C.c_uint64]
+        lib.wo_orientation.argtypes = [C.c_uint64, C.c_int, C.c_int]
+        lib.wo_hut_in_region.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        lib.wo_noise_dump.argtypes = [C.c_uint64, C.c_char_p] + [C.c_void_p] * 4
+        lib.wo_phase1_rect.restype = C.c_longlong
+        lib.wo_phase1_rect.argtypes = [C.c_uint64, C.POINTER(WoOpts)] + [C.c_int] * 6 + [C.c_void_p] * 4
+        lib.wo_probe.argtypes = [C.c_uint64, C.POINTER(WoOpts), C.c_int, C.c_int, C.c_int, C.c_void_p]
+        lib.wo_scan_seeds.restype = C.c_longlong
+        lib.wo_scan_seeds.argtypes = [C.c_void_p, C.c_uint64, C.c_longlong, C.POINTER(WoOpts)] + [C.c_int] * 7 + \
+            [C.c_void_p, C.c_longlong, C.c_void_p]
+        self.lib = lib
+
+    @staticmethod
+    def _o(r: dict) -> WoOpts:
+        return WoOpts(r["mc_1_18_2"], r["single_biome"], r["pre_26_2"], r["large_biomes"])
+
+    def splitmix64(self, x: int) -> int:
+        return int(self.lib.wo_splitmix64(x & 0xFFFFFFFFFFFFFFFF))
+
+    def hut_chunk(self, seed: int, rx: int, rz: int, salt: int = 14357620) -> tuple[int, int]:
+        cx, cz = C.c_int(), C.c_int()
+        self.lib.wo_hut_in_region(seed & 0xFFFFFFFFFFFFFFFF, rx, rz, salt, C.byref(cx), C.byref(cz))
+        return cx.value, cz.value
+
+    def orientation(self, seed: int, hut_x: int, hut_z: int) -> int:
+        return int(self.lib.wo_orientation(seed & 0xFFFFFFFFFFFFFFFF, hut_x, hut_z))
+
+    def phase1_rect(self, seed: int, r: dict, max_height: int, rect, salt: int = 0):
+        n = (rect[1] - rect[0]) * (rect[3] - rect[2])
+        codes, tiers = np.zeros(n, np.int8), np.zeros(n, np.int8)
+        cx, cz = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        o = self._o(r)
+        self.lib.wo_phase1_rect(seed & 0xFFFFFFFFFFFFFFFF, C.byref(o), max_height, salt, *rect,
+                                codes.ctypes.data, tiers.ctypes.data, cx.ctypes.data, cz.ctypes.data)
+        return codes, tiers, cx, cz
+
+    def probe(self, seed: int, r: dict, hut_x: int, hut_z: int, max_height: int) -> np.ndarray:
+        out = np.zeros(38)
+        o = self._o(r)
+        self.lib.wo_probe(seed & 0xFFFFFFFFFFFFFFFF, C.byref(o), hut_x, hut_z, max_height, out.ctypes.data)
+        return out
+
+    def noise_dump(self, seed: int, name: str):
+        h, pr, org, pm = np.zeros(6), np.zeros(32, np.int32), np.zeros(96), np.zeros(32 * 256, np.uint8)
+        self.lib.wo_noise_dump(seed & 0xFFFFFFFFFFFFFFFF, name.encode(), h.ctypes.data, pr.ctypes.data,
+                               org.ctypes.data, pm.ctypes.data)
+        return h, pr, org, pm
+
+    def scan_seeds(self, r: dict, max_height: int, rect, seeds=None, gen=None, threads: int = 0, salt: int = 0,
+                   cap: int = 1 << 16):
+        """Phase-1 survivors of many seeds, sorted by (seed_index, rz, rx), plus the funnel."""
+        if seeds is not None:
+            arr = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64))
+            ptr, base, n = arr.ctypes.data, 0, len(arr)
+        else:
+            arr = None
+            ptr, base, n = None, gen[0] & 0xFFFFFFFFFFFFFFFF, gen[1]
+        out = np.zeros(cap, CANDIDATE_DTYPE)
+        hist = np.zeros(11, np.int64)
+        o = self._o(r)
+        found = self.lib.wo_scan_seeds(ptr, base, n, C.byref(o), max_height, salt, *rect, threads,
+                                       out.ctypes.data, cap, hist.ctypes.data)
+        if found > cap:
+            return self.scan_seeds(r, max_height, rect, seeds, gen, threads, salt, cap=int(found))
+        out = out[:found]
+        out.sort(order=["seed_index", "rz", "rx"])
+        return out, hist
+
+
+class Ref:
+    """The reference's lysh, compiled from its sources into oracle/_ref/."""
+
+    def __init__(self, path: str = REF_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is missing (make -C oracle ref needs the reference sources)")
+        lib = C.CDLL(path)
+        lib.refh_parse_version.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.refh_hut_in_region.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        lib.refh_hut_orientation.argtypes = [C.c_uint64, C.c_int, C.c_int]
+        lib.refh_phase1_rect.restype = C.c_longlong
+        lib.refh_phase1_rect.argtypes = [C.c_uint64] + [C.c_int] * 11 + [C.c_void_p] * 4
+        lib.refh_probe.argtypes = [C.c_uint64] + [C.c_int] * 8 + [C.c_void_p]
+        lib.refh_noise_dump.argtypes = [C.c_uint64, C.c_char_p] + [C.c_void_p] * 4
+        lib.refh_ctx_new.restype = C.c_void_p
+        lib.refh_ctx_new.argtypes = [C.c_uint64] + [C.c_int] * 6
+        lib.refh_ctx_free.argtypes = [C.c_void_p]
+        lib.refh_ctx_eval.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        lib.refh_ctx_height.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        lib.refh_ctx_density.restype = C.c_double
+        lib.refh_ctx_density.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        lib.refh_ctx_block.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+        lib.refh_grade_scan.argtypes = [C.c_uint64] + [C.c_int] * 14 + [C.c_void_p, C.c_int, C.c_void_p]
+        lib.refh_phase1_seeds.restype = C.c_double
+        lib.refh_phase1_seeds.argtypes = [C.c_void_p, C.c_longlong] + [C.c_int] * 12 + [C.c_void_p]
+        lib.refh_cpu_count.restype = C.c_int
+        self.lib = lib
+
+    def version(self, name: str) -> tuple[int, int, int]:
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        if self.lib.refh_parse_version(name.encode(), C.byref(a), C.byref(b), C.byref(c)):
+            raise ValueError(name)
+        return a.value, b.value, c.value
+
+    def phase1_rect(self, seed: int, r: dict, max_height: int, rect, salt: int = 0, tree: int = 0):
+        n = (rect[1] - rect[0]) * (rect[3] - rect[2])
+        codes, tiers = np.zeros(n, np.int8), np.zeros(n, np.int8)
+        cx, cz = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        self.lib.refh_phase1_rect(seed & 0xFFFFFFFFFFFFFFFF, r["mc_1_18_2"], r["pre_26_2"], r["large_biomes"],
+                                  r["single_biome"], tree, max_height, salt, *rect, codes.ctypes.data,
+                                  tiers.ctypes.data, cx.ctypes.data, cz.ctypes.data)
+        return codes, tiers, cx, cz
+
+    def probe(self, seed: int, r: dict, hut_x: int, hut_z: int, max_height: int) -> np.ndarray:
+        out = np.zeros(38)
+        self.lib.refh_probe(seed & 0xFFFFFFFFFFFFFFFF, r["mc_1_18_2"], r["pre_26_2"], r["large_biomes"],
+                            r["single_biome"], 0, hut_x, hut_z, max_height, out.ctypes.data)
+        return out
+
+    def noise_dump(self, seed: int, name: str):
+        h, pr, org, pm = np.zeros(6), np.zeros(32, np.int32), np.zeros(96), np.zeros(32 * 256, np.uint8)
+        self.lib.refh_noise_dump(seed & 0xFFFFFFFFFFFFFFFF, name.encode(), h.ctypes.data, pr.ctypes.data,
+                                 org.ctypes.data, pm.ctypes.data)
+        return h, pr, org, pm
+
+    def phase1_seeds(self, seeds, r: dict, max_height: int, rect, threads: int = 0, salt: int = 0):
+        """Times lysh's own phase-1 scan over many seeds; returns (seconds, accepted per seed)."""
+        arr = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64))
+        acc = np.zeros(len(arr), np.int64)
+        secs = self.lib.refh_phase1_seeds(arr.ctypes.data, len(arr), r["mc_1_18_2"], r["pre_26_2"],
+                                          r["large_biomes"], r["single_biome"], 0, max_height, salt, *rect,
+                                          threads, acc.ctypes.data)
+        return secs, acc
+
+    def cpu_count(self) -> int:
+        return int(self.lib.refh_cpu_count())
