@@ -1,0 +1,326 @@
+"""Seed Check benchmark (config 2: 2^24 splitmix64(2 + i) world seeds x 9x9 swamp-hut regions,
+phase-1 gate at floor -50, version rules 1.19.x~26.1).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = the whole phase-1 Seed Check of one rank's 2^24 seeds (1.36e9 (seed, region)
+checks).  Multi-GPU runs shard seeds (weak scaling: every rank checks its own 2^24 seeds of
+the stream); the only exchange is a max-reduce of the timings.  Prints one JSON line.
+
+`value` is measured with the seeds already resident in HBM (wg_seed_check_device on torch's
+stream, CUDA events around each step); `e2e` goes through the public host API
+(wg_seed_check) with the seeds in pinned host memory, so the host->device copy of the seeds and
+the device->host read of the survivors are inside the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+N_SEEDS = 1 << 24
+RECT = (-4, 5, -4, 5)
+MAX_HEIGHT = -50
+VERSION = "1.19.x~26.1"
+GEN_BASE = 2
+METRIC = "seeds/s"
+
+
+def load_package():
+    name = "low_witch_finder_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "low-witch-finder_b200", "__init__.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+# ------------------------------------------------------------------------------------------
+# algorithmic work model of the climate kernel (lane-operations, counted from the source)
+# ------------------------------------------------------------------------------------------
+OPS_PERLIN_BUILD = 7160      # 259 Xoroshiro128++ steps, 256 Lemire draws + byte swaps, RNG derivation
+OPS_Y0_SAMPLE = 244          # 14 table lookups, 62 FP64 ops (x2 issue slots), bit-op gradients
+OPS_REGION = 40              # java.util.Random placement (2 x nextInt(24)) + coordinates
+BYTES_PER_SEED_IN = 8        # the int64 seed read from HBM
+BYTES_PER_RECORD = 12        # (unit, offset, count) per seed with climate survivors
+BYTES_PER_SURVIVOR = 4       # region offset per climate survivor
+
+
+def climate_work(st: dict, n_seeds: int, n_regions: int) -> tuple[float, float]:
+    """(lane-ops, algorithmic bytes) of the climate kernel over a request, from its funnel."""
+    th = st["tier_hist"]
+    rh = st["reject_hist"]
+    y0 = sum((t + 2) * th[t] for t in range(7)) + 12 * rh[1] + 18 * (rh[2] + st["climate_survivors"])
+    ops = 18 * n_seeds * OPS_PERLIN_BUILD + y0 * OPS_Y0_SAMPLE + n_seeds * n_regions * OPS_REGION
+    nbytes = n_seeds * BYTES_PER_SEED_IN + st["climate_survivors"] * BYTES_PER_SURVIVOR
+    return float(ops), float(nbytes)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows: list[list[str]] = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(n_sample: int) -> dict:
+    """The reference's own lysh (oracle/_ref, compiled from its sources) on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import bind
+    wg = load_package()
+    seeds = np.array([wg.splitmix64(GEN_BASE + i) for i in range(n_sample)], dtype=np.uint64)
+    r = bind.rules(VERSION)
+    cores = os.cpu_count() or 1
+    if os.path.exists(bind.REF_LIB):
+        ref = bind.Ref()
+        secs, _ = ref.phase1_seeds(seeds, r, MAX_HEIGHT, RECT, threads=cores)
+        kind = "reference"
+    else:
+        port = bind.Port()
+        t0 = time.perf_counter()
+        port.scan_seeds(r, MAX_HEIGHT, RECT, seeds=seeds, threads=cores)
+        secs = time.perf_counter() - t0
+        kind = "port"
+    return {"value": n_sample / secs, "unit": METRIC, "cores": cores, "kind": kind,
+            "sample": f"first {n_sample} seeds of config 2 (splitmix64(2 + i)), 9x9 regions, lysh phase-1 scan "
+                      f"(lysh_scan_rect per seed, one seed per thread)", "seconds": secs}
+
+
+def run_reference(args) -> None:
+    """--impl reference: the reference's CPU scanner on the host cores, same metric."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n_sample = 1 << 18
+    for _ in range(args.warmup):
+        cpu_baseline(n_sample // 8)
+    vals = [cpu_baseline(n_sample) for _ in range(args.steps)]
+    v = statistics.median(x["value"] for x in vals)
+    cb = dict(vals[0])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n_sample / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "config 2 sample: splitmix64(2 + i) seeds x 9x9 regions, floor -50, "
+                                   f"{VERSION}; {n_sample} seeds per step", "seeds_per_step": n_sample},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    wg = load_package()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    eng = wg.Engine(local)
+    opts = wg.make_opts(VERSION)
+    first = rank * N_SEEDS                       # weak scaling: each rank owns 2^24 seeds of the stream
+    seeds_host = torch.empty(N_SEEDS, dtype=torch.int64, pin_memory=True)
+    seeds_np = seeds_host.numpy()
+    idx = np.arange(first, first + N_SEEDS, dtype=np.uint64) + np.uint64(GEN_BASE)
+    with np.errstate(over="ignore"):   # splitmix64 over the whole array, mod 2^64
+        z = idx + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    seeds_np[:] = z.view(np.int64)
+    seeds_dev = seeds_host.to(f"cuda:{local}")
+    out_cap = 1 << 16
+    out_dev = torch.zeros((out_cap, 4), dtype=torch.int64, device=f"cuda:{local}")
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=f"cuda:{local}")   # 256 MiB > 126 MB L2
+    stream = torch.cuda.current_stream()
+
+    def step_device():
+        return eng.seed_check_device(seeds_dev.data_ptr(), 0, N_SEEDS, RECT, MAX_HEIGHT, opts, out_dev.data_ptr(),
+                                     out_cap, stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    # ---- device-resident timed region ----
+    times, kernel_ms, kernel_launches, found, stats = [], [0.0, 0.0, 0.0], [0, 0, 0], 0, None
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            found, stats = step_device()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+            for k in range(3):
+                kernel_ms[k] += stats["kernel_ms"][k]
+                kernel_launches[k] += stats["kernel_launches"][k]
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    total_ms = sum(times)
+
+    # ---- end to end through the public host API ----
+    e2e_ms = []
+    for i in range(1 + args.steps):
+        t0 = time.perf_counter()
+        res = eng.seed_check(seeds=seeds_np, rect=RECT, max_height=MAX_HEIGHT, opts=opts)
+        dt = (time.perf_counter() - t0) * 1e3
+        if i:
+            e2e_ms.append(dt)
+    e2e_total = sum(e2e_ms)
+    survivors_e2e = len(res.candidates)
+    d2h = survivors_e2e * 32 + res.stats["batches"] * (32 + 18 * 8)
+
+    if world > 1:
+        t = torch.tensor([total_ms, e2e_total], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_total = float(t[0]), float(t[1])
+        n_found = torch.tensor([found], dtype=torch.int64, device=f"cuda:{local}")
+        dist.all_reduce(n_found)
+        found_all = int(n_found.item())
+    else:
+        found_all = found
+
+    if rank == 0:
+        n_total = N_SEEDS * world
+        value = n_total * args.steps / (total_ms / 1e3)
+        e2e_value = n_total * args.steps / (e2e_total / 1e3)
+        n_regions = (RECT[1] - RECT[0]) * (RECT[3] - RECT[2])
+        peaks = measured_peaks()
+        sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+        max_mhz = float(peaks.get("sm_max_mhz", 1965.0))
+        peak_ops = sm_count * 128 * max_mhz * 1e6
+        ops, nbytes = climate_work(stats, N_SEEDS, n_regions)
+        launch_ms = kernel_ms[0] / max(1, kernel_launches[0])
+        ops_per_launch = ops / max(1, stats["kernel_launches"][0])
+        bytes_per_launch = nbytes / max(1, stats["kernel_launches"][0])
+        achieved = ops_per_launch / (launch_ms / 1e3)
+        hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+        cs = clocks.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "config 2: Seed Check phase 1, 2^24 splitmix64(2 + i) world seeds per GPU x 9x9 "
+                                   "swamp-hut regions (1.36e9 (seed, region) checks), floor -50, rules "
+                                   f"{VERSION}, bit-exact FP64", "seeds_per_gpu": N_SEEDS,
+                       "regions_per_seed": n_regions, "max_height": MAX_HEIGHT, "parallelism": f"seed-shard x{world}",
+                       "l2": "256 MiB buffer written between timed steps (outside the events); seed input 134 MB",
+                       "inputs": "seed list resident in HBM (value); pinned host seeds via wg_seed_check (e2e)"},
+            "survivors_per_step": found_all,
+            "funnel": stats["reject_hist"],
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": N_SEEDS * 8,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_total / args.steps},
+            "gpu_launches": sum(kernel_launches),
+            "kernel_ms_per_step": [k / args.steps for k in kernel_ms],
+            "roofline": {
+                "bound": "issue", "kernel": "climate_kernel", "unit": "Tlane-op/s",
+                "achieved": achieved / 1e12, "peak": peak_ops / 1e12, "frac": achieved / peak_ops,
+                "peak_source": f"nominal INT32/FP32 issue rate: {sm_count} SMs x 128 lanes x {max_mhz:.0f} MHz "
+                               "(sm_max_mhz of MEASURED_PEAKS.json); the kernel is not HBM- or tensor-bound",
+                "ops_per_launch": ops_per_launch, "launch_ms": launch_ms,
+                "traffic": None,
+                "hbm": {"achieved_gbs": bytes_per_launch / (launch_ms / 1e3) / 1e9, "peak_gbs": hbm_peak,
+                        "frac": bytes_per_launch / (launch_ms / 1e3) / 1e9 / hbm_peak,
+                        "peak_source": "hbm_gbs of MEASURED_PEAKS.json"},
+            },
+            "clocks": cs,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(1 << 19)
+        print(json.dumps(line), flush=True)
+
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -57,7 +57,9 @@ typedef struct {
     int64_t tier_hist[7];         /* erosion tier that rejected (lysh's tier histogram) */
     int64_t batches;              /* device batches run */
     int64_t retries;              /* batches re-run smaller after a full work list */
-    double gpu_ms;                /* device time, CUDA events on the engine stream */
+    int64_t kernel_launches[3];   /* climate, entrance, ladder kernel launches */
+    double kernel_ms[3];          /* their summed device time (CUDA events around each launch) */
+    double gpu_ms;                /* device time of the whole call, CUDA events on its stream */
     double wall_ms;               /* host wall time of the call */
 } wg_scan_stats;
 
@@ -91,8 +93,9 @@ int wg_seed_check(wg_engine *e, const int64_t *seeds, uint64_t gen_base, uint64_
                   wg_candidate *out, uint64_t cap, uint64_t *n_out, wg_scan_stats *stats);
 
 /* Same request with device-resident buffers: d_seeds (device, or NULL for the generator)
- * and d_out (device, unsorted), work enqueued on `stream` (a cudaStream_t, NULL = the
- * engine's own stream).  The call returns when the work is complete. */
+ * and d_out (device, unsorted).  All work is enqueued on `stream` (a cudaStream_t; NULL =
+ * the engine's own stream), so events the caller records on that stream bracket it.  The
+ * call returns when the work is complete. */
 int wg_seed_check_device(wg_engine *e, const int64_t *d_seeds, uint64_t gen_base, uint64_t n_seeds,
                          const wg_opts *opts, int max_height, int salt,
                          int rx0, int rx1, int rz0, int rz1,

@@ -42,12 +42,14 @@ class Opts(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("scanned", C.c_int64), ("accepted", C.c_int64), ("climate_survivors", C.c_int64),
                 ("deep_candidates", C.c_int64), ("reject_hist", C.c_int64 * 11), ("tier_hist", C.c_int64 * 7),
-                ("batches", C.c_int64), ("retries", C.c_int64), ("gpu_ms", C.c_double), ("wall_ms", C.c_double)]
+                ("batches", C.c_int64), ("retries", C.c_int64), ("kernel_launches", C.c_int64 * 3),
+                ("kernel_ms", C.c_double * 3), ("gpu_ms", C.c_double), ("wall_ms", C.c_double)]
 
     def as_dict(self) -> dict:
         return {"scanned": self.scanned, "accepted": self.accepted, "climate_survivors": self.climate_survivors,
                 "deep_candidates": self.deep_candidates, "reject_hist": list(self.reject_hist),
                 "tier_hist": list(self.tier_hist), "batches": self.batches, "retries": self.retries,
+                "kernel_launches": list(self.kernel_launches), "kernel_ms": list(self.kernel_ms),
                 "gpu_ms": self.gpu_ms, "wall_ms": self.wall_ms}
 
 
@@ -151,7 +153,7 @@ class Engine:
     @staticmethod
     def _seeds(seeds, gen):
         if seeds is not None:
-            arr = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64).view(np.int64))
+            arr = as_seed_array(seeds)
             return arr, arr.ctypes.data, 0, len(arr)
         if gen is None:
             raise ValueError("give seeds or gen=(base, count)")
@@ -206,6 +208,13 @@ class Engine:
         return codes, tiers
 
 
+def as_seed_array(seeds) -> np.ndarray:
+    """Seeds as contiguous int64 (Java longs); accepts signed or unsigned 64-bit spellings."""
+    if isinstance(seeds, np.ndarray) and seeds.dtype in (np.int64, np.uint64):
+        return np.ascontiguousarray(seeds).view(np.int64)
+    return np.array([int(s) & 0xFFFFFFFFFFFFFFFF for s in seeds], dtype=np.uint64).view(np.int64)
+
+
 def splitmix64(x: int) -> int:
     """The --seed-gen stream: splitmix64(base + i) with the golden-gamma pre-add."""
     m = 0xFFFFFFFFFFFFFFFF
@@ -219,3 +228,12 @@ def splitmix64(x: int) -> int:
 def to_signed(v: int) -> int:
     v &= 0xFFFFFFFFFFFFFFFF
     return v - (1 << 64) if v >= (1 << 63) else v
+
+
+def shard(n_total: int, rank: int, world: int) -> tuple[int, int]:
+    """Seed-index range [lo, hi) of rank `rank` out of `world`: contiguous, disjoint, covering
+    [0, n_total), sizes differing by at most one.  Seeds are independent units, so a
+    multi-GPU run shards seeds with no exchange beyond concatenating survivor lists."""
+    if world <= 0 or not 0 <= rank < world:
+        raise ValueError("bad rank / world")
+    return (n_total * rank) // world, (n_total * (rank + 1)) // world

@@ -85,6 +85,7 @@ struct wg_engine {
     unsigned long long *hist = nullptr;
     uint32_t *h_counters = nullptr;         // pinned
     unsigned long long *h_hist = nullptr;   // pinned
+    cudaEvent_t kev[4] = {nullptr, nullptr, nullptr, nullptr};   // around the three kernels of a batch
     int64_t *d_seed_list = nullptr;
     uint64_t d_seed_cap = 0;
 
@@ -130,9 +131,13 @@ int run_batch(wg_engine *eng, const Request &rq, const BatchArgs &proto, uint64_
     WG_CUDA(cudaMemsetAsync(eng->counters, 0, sizeof(uint32_t) * CNT_WORDS, eng->stream), "memset counters");
     WG_CUDA(cudaMemsetAsync(eng->hist, 0, sizeof(unsigned long long) * (P1_KINDS + kTiers), eng->stream),
             "memset hist");
+    WG_CUDA(cudaEventRecord(eng->kev[0], eng->stream), "event");
     launch_climate(a, eng->stream);
+    WG_CUDA(cudaEventRecord(eng->kev[1], eng->stream), "event");
     launch_entrance(a, eng->sm_count, eng->stream);
+    WG_CUDA(cudaEventRecord(eng->kev[2], eng->stream), "event");
     launch_ladder(a, eng->sm_count * 8, eng->stream);
+    WG_CUDA(cudaEventRecord(eng->kev[3], eng->stream), "event");
     WG_CUDA(cudaGetLastError(), "kernel launch");
     WG_CUDA(cudaMemcpyAsync(eng->h_counters, eng->counters, sizeof(uint32_t) * CNT_WORDS, cudaMemcpyDeviceToHost,
                             eng->stream),
@@ -142,6 +147,12 @@ int run_batch(wg_engine *eng, const Request &rq, const BatchArgs &proto, uint64_
             "copy hist");
     WG_CUDA(cudaStreamSynchronize(eng->stream), "batch");
     st.batches++;
+    for (int k = 0; k < 3; k++) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, eng->kev[k], eng->kev[k + 1]);
+        st.kernel_ms[k] += ms;
+        st.kernel_launches[k]++;
+    }
     if (eng->h_counters[CNT_OVERFLOW]) {
         if (n_units <= 32) return eng->fail(WG_ERR_CAPACITY, "phase-1 work list full even for 32 units");
         st.retries++;
@@ -316,6 +327,7 @@ int wg_engine_open(int device, wg_engine **out) {
         WG_CUDA(cudaStreamCreateWithFlags(&eng->stream, cudaStreamNonBlocking), "stream");
         WG_CUDA(cudaEventCreate(&eng->ev0), "event");
         WG_CUDA(cudaEventCreate(&eng->ev1), "event");
+        for (int k = 0; k < 4; k++) WG_CUDA(cudaEventCreate(&eng->kev[k]), "event");
         NoiseSpec specs[N_NOISE_COUNT];
         build_noise_specs(specs);
         ClimateStep normal[kClimateSteps], large[kClimateSteps];
@@ -360,6 +372,8 @@ void wg_engine_close(wg_engine *eng) {
     cudaFreeHost(eng->h_hist);
     if (eng->ev0) cudaEventDestroy(eng->ev0);
     if (eng->ev1) cudaEventDestroy(eng->ev1);
+    for (int k = 0; k < 4; k++)
+        if (eng->kev[k]) cudaEventDestroy(eng->kev[k]);
     if (eng->stream) cudaStreamDestroy(eng->stream);
     delete eng;
 }
@@ -416,11 +430,13 @@ int wg_seed_check_device(wg_engine *eng, const int64_t *d_seeds, uint64_t gen_ba
     static_assert(sizeof(wg_candidate) == sizeof(Candidate), "candidate layout");
     auto t0 = std::chrono::steady_clock::now();
     WG_CUDA(cudaSetDevice(eng->device), "cudaSetDevice");
-    cudaStream_t user = (cudaStream_t)stream;
-    if (user) {  // order the engine stream after the caller's prior work
-        WG_CUDA(cudaEventRecord(eng->ev0, user), "event");
-        WG_CUDA(cudaStreamWaitEvent(eng->stream, eng->ev0, 0), "wait");
-    }
+    // Run on the caller's stream for this call, so the caller's events bracket the work.
+    struct StreamSwap {
+        wg_engine *e;
+        cudaStream_t saved;
+        ~StreamSwap() { e->stream = saved; }
+    } swap{eng, eng->stream};
+    if (stream) eng->stream = (cudaStream_t)stream;
     Request rq = make_request(opts, gen_base, n_seeds, max_height, salt, rx0, rx1, rz0, rz1);
     rq.d_seeds = d_seeds;
     wg_scan_stats st;

@@ -43,6 +43,12 @@ PHASE1_RULES = {"1.19.x~26.1": (0, 1), "1.21": (0, 1), "1.21.5": (0, 1), "26.2":
                 "1.18.2": (1, 1), "1.18.x": (1, 1), "1.20.1": (0, 1), "26.1": (0, 1)}
 
 
+def as_u64(seeds) -> np.ndarray:
+    if isinstance(seeds, np.ndarray) and seeds.dtype in (np.int64, np.uint64):
+        return np.ascontiguousarray(seeds).view(np.uint64)
+    return np.array([int(s) & 0xFFFFFFFFFFFFFFFF for s in seeds], dtype=np.uint64)
+
+
 def rules(version: str, preset: str = "NORMAL") -> dict:
     mc, pre = PHASE1_RULES[version]
     return {"mc_1_18_2": mc, "pre_26_2": pre, "large_biomes": int(preset == "LARGE_BIOMES"),
@@ -109,7 +115,7 @@ class Port:
                    cap: int = 1 << 16):
         """Phase-1 survivors of many seeds, sorted by (seed_index, rz, rx), plus the funnel."""
         if seeds is not None:
-            arr = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64))
+            arr = as_u64(seeds)
             ptr, base, n = arr.ctypes.data, 0, len(arr)
         else:
             arr = None
@@ -183,7 +189,7 @@ class Ref:
 
     def phase1_seeds(self, seeds, r: dict, max_height: int, rect, threads: int = 0, salt: int = 0):
         """Times lysh's own phase-1 scan over many seeds; returns (seconds, accepted per seed)."""
-        arr = np.ascontiguousarray(np.asarray(seeds, dtype=np.uint64))
+        arr = as_u64(seeds)
         acc = np.zeros(len(arr), np.int64)
         secs = self.lib.refh_phase1_seeds(arr.ctypes.data, len(arr), r["mc_1_18_2"], r["pre_26_2"],
                                           r["large_biomes"], r["single_biome"], 0, max_height, salt, *rect,

@@ -1,0 +1,40 @@
+"""CPU: the phase1_scan worker's command-line contract (engine/gpu/low54/phase1_scan.cu:561-601):
+usage, argument errors and a loud failure when no GPU is present."""
+from __future__ import annotations
+
+import subprocess
+
+import pytest
+
+
+def run(wg, *args, stdin=None, timeout=60):
+    return subprocess.run([wg.WORKER_PATH, *args], input=stdin, capture_output=True, text=True, timeout=timeout)
+
+
+def test_usage(wg):
+    r = run(wg, "--help")
+    assert r.returncode == 0 and "--worker" in r.stdout and "--seed-gen" in r.stdout
+    assert run(wg).returncode == 2
+
+
+@pytest.mark.parametrize("args", [["--seed"], ["--seed", "1", "--bogus"], ["--seed-gen", "1", "0"],
+                                  ["--seed", "1", "--seed-gen", "1", "5"], ["--seed", "1", "--min-region-x", "5",
+                                                                            "--max-region-x", "5"],
+                                  ["--seed", "1", "--version", "9.9"], ["--seed", "1", "--quad-bases", "f"],
+                                  ["--seed-list", "/nonexistent/file"]])
+def test_bad_arguments(wg, args):
+    r = run(wg, *args)
+    assert r.returncode == 2
+    assert r.stderr.strip()
+
+
+def test_no_gpu_worker_fails_loudly(wg):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    r = run(wg, "--worker", stdin="--seed 1 --out x.csv\n")
+    assert r.returncode == 1 and "cannot open the GPU engine" in r.stderr
+    assert "WORKER_READY" not in r.stdout
