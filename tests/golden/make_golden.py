@@ -149,10 +149,20 @@ def main() -> None:
     surv = np.array(surv, dtype=bind.CANDIDATE_DTYPE)
     np.savez_compressed(os.path.join(OUT, "c2_sample.npz"), survivors=surv, hist=hist)
 
-    # 7. config 2, first 2^22 seeds: every phase-1 survivor (lysh's own threaded scan finds the
-    # seeds, lysh_phase1_rect gives their regions and chunks)
-    n = 1 << 22
-    seeds2 = np.array([splitmix64(2 + i) for i in range(n)], dtype=np.uint64)
+    # 7. config 2, first 2^22 seeds and all 2^24 seeds: every phase-1 survivor (lysh's own threaded
+    # scan finds the seeds, lysh_phase1_rect gives their regions and chunks)
+    for n, name in ((1 << 22, "c2_4m_survivors.npz"), (1 << 24, "c2_full_survivors.npz")):
+        c2_survivors(ref, r, n, name)
+    print("golden fixtures written to", OUT)
+
+
+def c2_survivors(ref, r, n, name):
+    idx = np.arange(n, dtype=np.uint64) + np.uint64(2)
+    with np.errstate(over="ignore"):
+        z = idx + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        seeds2 = z ^ (z >> np.uint64(31))
     _, acc = ref.phase1_seeds(seeds2, r, -50, RECT9)
     surv = []
     for i in np.nonzero(acc)[0]:
@@ -161,9 +171,7 @@ def main() -> None:
         for k in np.nonzero(c == 10)[0]:
             surv.append((int(i), s - (1 << 64) if s >= (1 << 63) else s,
                          int(k % 9) - 4, int(k // 9) - 4, int(cx[k]), int(cz[k])))
-    np.savez_compressed(os.path.join(OUT, "c2_4m_survivors.npz"),
-                        survivors=np.array(surv, dtype=bind.CANDIDATE_DTYPE), n_seeds=n)
-    print("golden fixtures written to", OUT)
+    np.savez_compressed(os.path.join(OUT, name), survivors=np.array(surv, dtype=bind.CANDIDATE_DTYPE), n_seeds=n)
 
 
 if __name__ == "__main__":

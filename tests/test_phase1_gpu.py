@@ -73,16 +73,17 @@ def test_c2_first_4m_seeds_survivors(engine, golden):
     assert sum(res.stats["reject_hist"]) == res.stats["scanned"] == int(g["n_seeds"]) * 81
 
 
-def test_full_config2_properties(engine, port, bind_mod):
-    """All 2^24 seeds of config 2: every survivor is re-verified by the oracle region by region,
-    the funnel adds up, and the list-fed run equals the generator-fed run."""
+def test_full_config2(engine, port, bind_mod, golden):
+    """All 2^24 seeds of config 2: the survivor list equals the reference's exactly, the funnel adds
+    up, and every survivor is re-verified by the oracle region by region."""
+    g = golden("c2_full_survivors.npz")
     n = 1 << 24
     res = engine.seed_check(gen=(2, n), rect=RECT9, max_height=-50)
     st = res.stats
+    assert np.array_equal(res.candidates, g["survivors"])
     assert sum(st["reject_hist"]) == st["scanned"] == n * 81
-    assert st["reject_hist"][10] == st["accepted"] == len(res.candidates)
+    assert st["reject_hist"][10] == st["accepted"] == len(res.candidates) == len(g["survivors"])
     assert sum(st["tier_hist"]) == st["reject_hist"][0]
-    assert 200 < len(res.candidates) < 500          # ~1 in 4e6 regions survive at -50
     r = bind_mod.rules("1.19.x~26.1")
     for c in res.candidates:
         assert int(c["seed"]) == wg_signed(port.splitmix64(2 + int(c["seed_index"])))
