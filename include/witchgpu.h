@@ -110,6 +110,29 @@ int wg_phase1_codes(wg_engine *e, const int64_t *seeds, uint64_t gen_base, uint6
                     const wg_opts *opts, int max_height, int salt,
                     int rx0, int rx1, int rz0, int rz1, int8_t *codes, int8_t *tiers);
 
+/* Seed Check phase 1 that allocates nothing, for callers that cannot call cudaMalloc: a
+ * process whose device memory belongs to another allocator (a framework's caching allocator,
+ * a serving loop with a fixed budget), or a latency-critical stream on which cudaMalloc /
+ * cudaFree could synchronize the device or fail under fragmentation.  No counterpart in the
+ * reference.
+ *
+ * The caller passes device buffers: d_seeds (or NULL for splitmix64(gen_base + i)) and d_out
+ * (room for `cap` candidates, unsorted); *n_out (host) receives the number found, which may
+ * exceed cap (only cap are written).  Work runs on `stream` (NULL = the default stream) and
+ * the call returns when it is done.  The current CUDA device is used.
+ *
+ * Limits: n_seeds <= 65,536 and at most 4,096 regions per seed per call, else WG_ERR_CAPACITY;
+ * WG_ERR_CAPACITY also when a call's climate survivors exceed 1,048,576 (or its unit records
+ * 131,072, or its deep candidates 65,536).  The work lists live in one 6 MiB file-scope
+ * __device__ array that every GPU loading the library holds until the process exits.  The
+ * first call on a device uploads the noise tables and looks up that array's address, so make
+ * it before any stream capture.  All calls share the array: calls that overlap on the GPU
+ * (other streams or host threads) race on it. */
+int wg_seed_check_noalloc(const int64_t *d_seeds, uint64_t gen_base, uint32_t n_seeds,
+                          const wg_opts *opts, int max_height, int salt,
+                          int rx0, int rx1, int rz0, int rz1,
+                          wg_candidate *d_out, uint32_t cap, uint32_t *n_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

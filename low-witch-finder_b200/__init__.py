@@ -58,7 +58,7 @@ CANDIDATE_DTYPE = np.dtype([("seed_index", "<u8"), ("seed", "<i8"), ("rx", "<i4"
 
 # Every symbol include/witchgpu.h declares.
 EXPORTS = ("wg_engine_open", "wg_engine_close", "wg_engine_error", "wg_parse_version", "wg_parse_preset",
-           "wg_seed_check", "wg_seed_check_device", "wg_phase1_codes")
+           "wg_seed_check", "wg_seed_check_device", "wg_phase1_codes", "wg_seed_check_noalloc")
 
 _lib = None
 
@@ -87,6 +87,8 @@ def library() -> C.CDLL:
     lib.wg_seed_check.argtypes = common + [vp, u64, C.POINTER(u64), C.POINTER(Stats)]
     lib.wg_seed_check_device.argtypes = common + [vp, u64, C.POINTER(u64), C.POINTER(Stats), vp]
     lib.wg_phase1_codes.argtypes = common + [vp, vp]
+    lib.wg_seed_check_noalloc.argtypes = [vp, u64, C.c_uint32, C.POINTER(Opts), i32, i32, i32, i32, i32, i32,
+                                          vp, C.c_uint32, C.POINTER(C.c_uint32), vp]
     _lib = lib
     return lib
 
@@ -237,3 +239,15 @@ def shard(n_total: int, rank: int, world: int) -> tuple[int, int]:
     if world <= 0 or not 0 <= rank < world:
         raise ValueError("bad rank / world")
     return (n_total * rank) // world, (n_total * (rank + 1)) // world
+
+
+def seed_check_noalloc(d_seeds_ptr, gen_base: int, n_seeds: int, rect, max_height: int, opts: Opts,
+                       d_out_ptr: int, cap: int, stream_ptr: int | None = None, salt: int = 0) -> int:
+    """wg_seed_check_noalloc on the current CUDA device: no engine, no device allocation (the work
+    lists live in the library's fixed scratch array).  Returns the number of survivors."""
+    n = C.c_uint32()
+    rc = library().wg_seed_check_noalloc(d_seeds_ptr, gen_base & 0xFFFFFFFFFFFFFFFF, n_seeds, C.byref(opts),
+                                         max_height, salt, *rect, d_out_ptr, cap, C.byref(n), stream_ptr)
+    if rc != WG_OK:
+        raise EngineError(f"wg_seed_check_noalloc failed with status {rc}")
+    return int(n.value)

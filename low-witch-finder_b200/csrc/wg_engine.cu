@@ -28,10 +28,12 @@ constexpr uint32_t kCapOut = 1u << 20;
 // Regions per unit window: a whole seed when its rect is small, else 2048-region windows.
 uint32_t window_for(uint64_t n_regions) { return n_regions <= 4096 ? (uint32_t)n_regions : 2048u; }
 
+}  // namespace
+
 // Climate evaluation steps (see ClimateStep): the tiered erosion sequence
 // (engine/tools/lysh/src/noise.c:387-459) followed by plain y=0 DoublePerlin samples of
 // temperature and ridge (noise.c:320-342).
-void build_steps(const NoiseSpec *specs, int erosion, int temperature, ClimateStep *st) {
+void wg::build_climate_steps(const NoiseSpec *specs, int erosion, int temperature, ClimateStep *st) {
     static const double thr[7] = {0.05, 0.22, 0.42, 0.45, 0.49, 0.51, 0.55};
     std::memset(st, 0, sizeof(ClimateStep) * kClimateSteps);
     const NoiseSpec &e = specs[erosion];
@@ -69,8 +71,6 @@ void build_steps(const NoiseSpec *specs, int erosion, int temperature, ClimateSt
         base += 2 * n.npresent;
     }
 }
-
-}  // namespace
 
 struct wg_engine {
     int device = 0;
@@ -331,8 +331,8 @@ int wg_engine_open(int device, wg_engine **out) {
         NoiseSpec specs[N_NOISE_COUNT];
         build_noise_specs(specs);
         ClimateStep normal[kClimateSteps], large[kClimateSteps];
-        build_steps(specs, N_EROSION, N_TEMPERATURE, normal);
-        build_steps(specs, N_EROSION_LARGE, N_TEMPERATURE_LARGE, large);
+        build_climate_steps(specs, N_EROSION, N_TEMPERATURE, normal);
+        build_climate_steps(specs, N_EROSION_LARGE, N_TEMPERATURE_LARGE, large);
         upload_tables(specs, normal, large);
         WG_CUDA(cudaGetLastError(), "upload tables");
         WG_CUDA(cudaMalloc(&eng->rec_unit, sizeof(uint32_t) * kCapRec), "alloc");

@@ -104,6 +104,9 @@ struct ClimateStep {
 enum : int { ACT_NONE = 0, ACT_TIER, ACT_TIER_LAST, ACT_END_SUB_A, ACT_TEMPERATURE, ACT_RIDGE };
 constexpr int kClimateSteps = kSlotsA;
 
+// Host: the 18-step climate sequence for one preset (wg_engine.cu).
+void build_climate_steps(const NoiseSpec *specs, int erosion, int temperature, ClimateStep *steps);
+
 // Launchers (wg_phase1.cu).
 void upload_tables(const NoiseSpec *specs, const ClimateStep *steps_normal, const ClimateStep *steps_large);
 void launch_climate(const BatchArgs &a, cudaStream_t s);
