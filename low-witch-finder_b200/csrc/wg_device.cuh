@@ -6,11 +6,12 @@
 // -fmad=false, so results are bit-identical to the reference CPU scanner built with
 // -ffp-contract=off.
 //
-// Table layouts.  A Perlin permutation table is 256 bytes.  The hot kernels build 32
-// tables per warp, one per lane, in a 8 KiB "bank-interleaved" block: byte k of lane L
-// lives at ((k & ~3) * 32) + 4 L + (k & 3).  Every byte a lane touches is in bank L, so
-// both the shuffle (random swap partner per lane) and later lookups by the same lane are
-// free of bank conflicts.  Rare-path kernels use plain contiguous 256-byte tables.
+// Table layouts.  A Perlin permutation table is 256 bytes.  The hot kernels keep the tables of
+// one sampler slot for all the CTA's units in one byte-interleaved block of 256 rows: byte k of
+// unit u sits at k * U + u (U = units per CTA).  Any lookup is then one multiply-add away from
+// its index, and the 4-byte words of a row are shared by 4 units, so the random lookups of a
+// warp spread over all banks (about 2-way conflicts).  Rare-path kernels use plain contiguous
+// 256-byte tables (stride 1).
 #pragma once
 
 #include <cstdint>
@@ -69,6 +70,43 @@ __device__ __forceinline__ int xr_bounded(Xr &s, uint32_t bound) {
 __device__ __forceinline__ double xr_double(Xr &s) {
     return (double)(xr_next(s) >> 11) * 1.1102230246251565E-16;
 }
+
+// The same generator with the state as four 32-bit words, for the 256 nextInt(bound) draws of
+// a Perlin shuffle: next32() returns only the low 32 bits of the output, which is all
+// nextInt(bound) reads, and spells the 64-bit adds / rotates / shifts as 32-bit carry adds and
+// funnel shifts.
+struct Xr32 {
+    uint32_t l0, l1, h0, h1;   // lo = (l1:l0), hi = (h1:h0)
+    __device__ __forceinline__ explicit Xr32(const Xr &x)
+        : l0((uint32_t)x.lo), l1((uint32_t)(x.lo >> 32)), h0((uint32_t)x.hi), h1((uint32_t)(x.hi >> 32)) {}
+    __device__ __forceinline__ uint32_t next32() {
+        uint32_t s0, s1;   // s = lo + hi
+        asm("add.cc.u32 %0, %2, %3;\n\taddc.u32 %1, %4, %5;" : "=r"(s0), "=r"(s1) : "r"(l0), "r"(h0), "r"(l1), "r"(h1));
+        const uint32_t out = __funnelshift_l(s1, s0, 17) + l0;            // low word of rotl(s, 17) + lo
+        const uint32_t x0 = h0 ^ l0, x1 = h1 ^ l1;                          // hi ^= lo
+        const uint32_t r0 = __funnelshift_r(l0, l1, 15), r1 = __funnelshift_r(l1, l0, 15);   // rotl(lo, 49)
+        const uint32_t t0 = x0 << 21, t1 = __funnelshift_l(x0, x1, 21);   // hi << 21
+        l0 = r0 ^ x0 ^ t0;
+        l1 = r1 ^ x1 ^ t1;
+        h0 = __funnelshift_l(x1, x0, 28);                                   // rotl(hi, 28)
+        h1 = __funnelshift_l(x0, x1, 28);
+        return out;
+    }
+    // Java 17 nextInt(bound): Lemire's multiply-and-reject on the low 32 bits.
+    __device__ __forceinline__ uint32_t bounded(uint32_t bound) {
+        uint32_t x = next32();
+        uint32_t lo = x * bound, j = __umulhi(x, bound);
+        if (lo < bound) {
+            const uint32_t m = (0u - bound) % bound;
+            while (lo < m) {
+                x = next32();
+                lo = x * bound;
+                j = __umulhi(x, bound);
+            }
+        }
+        return j;
+    }
+};
 
 // RNG of octave `p` (index into NoiseSpec octave arrays) of sub `sub` of noise `ns`,
 // given the seed fork (the per-seed createRandomDeriver state).
@@ -148,53 +186,49 @@ __host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
 // ------------------------------------------------------------------------------------
 // Perlin permutation tables
 // ------------------------------------------------------------------------------------
-__device__ __forceinline__ int il_off(int k) { return ((k & 0xFC) << 5) | (k & 3); }
+// Fills `words` 32-bit words of a set of byte-interleaved blocks with the identity permutation:
+// a block holds 256 rows of `stride` bytes (one column per table), row k all equal to k.  Called
+// by every thread of the CTA (thread tid of nthreads), followed by a barrier.
+template <int STRIDE>
+__device__ __forceinline__ void perm_blocks_init(uint8_t *base, int words, int tid, int nthreads) {
+    static_assert(STRIDE % 4 == 0, "rows must be whole words");
+    uint32_t *w = reinterpret_cast<uint32_t *>(base);
+    for (int q = tid; q < words; q += nthreads)
+        w[q] = (uint32_t)((q % (64 * STRIDE)) / (STRIDE / 4)) * 0x01010101u;
+}
 
-// Builds one Perlin sampler (3 nextDouble origins + 256-step shuffle, noise.c:61-78)
-// into this lane's column of a bank-interleaved block; tb = block + 4 * lane.
-__device__ __forceinline__ void perlin_build_il(uint8_t *tb, Xr r, double &ox, double &oy, double &oz) {
+// The 256-step Fisher-Yates shuffle of one Perlin sampler (noise.c:61-72) on an initialised
+// column: byte k of this table is at t[k * STRIDE].  Draws the three origins first.
+template <int STRIDE>
+__device__ __forceinline__ void perlin_shuffle(uint8_t *t, Xr r, double &ox, double &oy, double &oz) {
     ox = xr_double(r) * 256.0;
     oy = xr_double(r) * 256.0;
     oz = xr_double(r) * 256.0;
-    uint32_t *w = reinterpret_cast<uint32_t *>(tb);
+    Xr32 q(r);
 #pragma unroll 8
-    for (int q = 0; q < 64; q++) w[q * 32] = 0x03020100u + 0x04040404u * (uint32_t)q;
-#pragma unroll 4
     for (int i = 0; i < 256; i++) {
-        int k = i + xr_bounded(r, (uint32_t)(256 - i));
-        uint8_t *pi = tb + il_off(i);
-        uint8_t *pk = tb + il_off(k);
-        uint8_t a = *pi, b = *pk;
-        *pi = b;
-        *pk = a;
+        const int k = i + (int)q.bounded((uint32_t)(256 - i));
+        uint8_t a = t[i * STRIDE], b = t[k * STRIDE];
+        t[i * STRIDE] = b;
+        t[k * STRIDE] = a;
     }
 }
+
+// Table reader: byte k of a column with the given row stride.
+template <int STRIDE>
+struct ColTable {
+    const uint8_t *t;
+    __device__ __forceinline__ int operator()(int k) const { return t[k * STRIDE]; }
+};
 
 // Same construction into a contiguous 256-byte table (rare-path kernels).
 __device__ __forceinline__ void perlin_build_flat(uint8_t *t, Xr r, double &ox, double &oy, double &oz) {
-    ox = xr_double(r) * 256.0;
-    oy = xr_double(r) * 256.0;
-    oz = xr_double(r) * 256.0;
     uint32_t *w = reinterpret_cast<uint32_t *>(t);
 #pragma unroll 8
     for (int q = 0; q < 64; q++) w[q] = 0x03020100u + 0x04040404u * (uint32_t)q;
-#pragma unroll 4
-    for (int i = 0; i < 256; i++) {
-        int k = i + xr_bounded(r, (uint32_t)(256 - i));
-        uint8_t a = t[i], b = t[k];
-        t[i] = b;
-        t[k] = a;
-    }
+    perlin_shuffle<1>(t, r, ox, oy, oz);
 }
 
-struct IlTable {
-    const uint8_t *tb;  // block + 4 * lane
-    __device__ __forceinline__ int operator()(int k) const { return tb[il_off(k)]; }
-};
-struct FlatTable {
-    const uint8_t *t;
-    __device__ __forceinline__ int operator()(int k) const { return t[k & 255]; }
-};
 
 // ------------------------------------------------------------------------------------
 // Perlin sampling (noise.c:224-342)
@@ -202,29 +236,30 @@ struct FlatTable {
 __device__ __forceinline__ double fade(double d) { return d * d * d * (d * (d * 6.0 - 15.0) + 10.0); }
 __device__ __forceinline__ double lerp(double t, double a, double b) { return a + t * (b - a); }
 
-// g * v for a gradient component g in {-1, 0, 1}: exactly the IEEE product (v, -v, or a
-// zero carrying v's sign), written as bit operations.
-__device__ __forceinline__ double gmul(double v, uint32_t h, uint32_t zero_mask, uint32_t neg_mask) {
-    long long b = __double_as_longlong(v);
-    long long keep = ((zero_mask >> h) & 1u) ? (long long)0x8000000000000000ULL : -1LL;
-    long long flip = ((neg_mask >> h) & 1u) ? (long long)0x8000000000000000ULL : 0LL;
-    return __longlong_as_double((b & keep) ^ flip);
+// The game's 16-entry gradient table (noise.c:15-20) as 2-bit codes per component and hash:
+// 0 = 0, 1 = +1, 3 = -1 (bits 2h..2h+1 of each constant).
+__host__ __device__ constexpr uint32_t grad_codes(int c) {
+    // rows: {gx, gy, gz} of hashes 0..15
+    const int g[16][3] = {{1, 1, 0}, {-1, 1, 0}, {1, -1, 0}, {-1, -1, 0}, {1, 0, 1}, {-1, 0, 1},
+                          {1, 0, -1}, {-1, 0, -1}, {0, 1, 1}, {0, -1, 1}, {0, 1, -1}, {0, -1, -1},
+                          {1, 1, 0}, {0, -1, 1}, {-1, 1, 0}, {0, -1, -1}};
+    uint32_t v = 0;
+    for (int h = 0; h < 16; h++) v |= (uint32_t)(g[h][c] == 0 ? 0 : (g[h][c] > 0 ? 1 : 3)) << (2 * h);
+    return v;
+}
+constexpr uint32_t kGradX = grad_codes(0), kGradY = grad_codes(1), kGradZ = grad_codes(2);
+
+// The double -1.0 / 0.0 / +1.0 of a 2-bit gradient code, built from its bits.
+__device__ __forceinline__ double grad_component(uint32_t codes, uint32_t shift) {
+    const uint32_t c = (codes >> shift) & 3u;
+    const uint32_t hi = ((c & 1u) * 0x3FF00000u) | ((c & 2u) << 30);
+    return __hiloint2double((int)hi, 0);
 }
 
-// The game's 16-entry gradient table, as zero / negative bit masks per component.
-constexpr uint32_t kGxZero = (1u << 8) | (1u << 9) | (1u << 10) | (1u << 11) | (1u << 13) | (1u << 15);
-constexpr uint32_t kGxNeg = (1u << 1) | (1u << 3) | (1u << 5) | (1u << 7) | (1u << 14);
-constexpr uint32_t kGyZero = (1u << 4) | (1u << 5) | (1u << 6) | (1u << 7);
-constexpr uint32_t kGyNeg = (1u << 2) | (1u << 3) | (1u << 9) | (1u << 11) | (1u << 13) | (1u << 15);
-constexpr uint32_t kGzZero = (1u << 0) | (1u << 1) | (1u << 2) | (1u << 3) | (1u << 12) | (1u << 14);
-constexpr uint32_t kGzNeg = (1u << 6) | (1u << 7) | (1u << 10) | (1u << 11) | (1u << 15);
-
+// (double)g[0] * x + (double)g[1] * y + (double)g[2] * z, as the reference writes it.
 __device__ __forceinline__ double grad(int hash, double x, double y, double z) {
-    uint32_t h = (uint32_t)hash & 15u;
-    double gx = gmul(x, h, kGxZero, kGxNeg);
-    double gy = gmul(y, h, kGyZero, kGyNeg);
-    double gz = gmul(z, h, kGzZero, kGzNeg);
-    return gx + gy + gz;
+    const uint32_t sh = ((uint32_t)hash & 15u) * 2u;
+    return grad_component(kGradX, sh) * x + grad_component(kGradY, sh) * y + grad_component(kGradZ, sh) * z;
 }
 
 template <class T>
@@ -259,7 +294,8 @@ __device__ __forceinline__ double perlin_y0(const T &P, double ox, double oz, in
     double d = x + ox, f = z + oz;
     double fd = floor(d), ff = floor(f);
     int i = (int)fd, k = (int)ff;
-    double g = d - i, l = f - k;
+    // d - (double)(int)floor(d) == d - floor(d): |d| < 2^31 here, so the int round trip is exact
+    double g = d - fd, l = f - ff;
     return perlin_core(P, i, jy, k, g, hy, hy - 1.0, l, fade(g), fy, fade(l));
 }
 
@@ -268,8 +304,9 @@ template <class T>
 __device__ __forceinline__ double perlin_3d(const T &P, double ox, double oy, double oz, double x, double y,
                                             double z) {
     double d = x + ox, e = y + oy, f = z + oz;
-    int i = (int)floor(d), j = (int)floor(e), k = (int)floor(f);
-    double g = d - i, h = e - j, l = f - k;
+    double fd = floor(d), fe = floor(e), ff = floor(f);
+    int i = (int)fd, j = (int)fe, k = (int)ff;
+    double g = d - fd, h = e - fe, l = f - ff;
     double hm = h - 0.0;
     return perlin_core(P, i, j, k, g, hm, hm - 1, l, fade(g), fade(h), fade(l));
 }

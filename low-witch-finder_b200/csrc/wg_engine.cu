@@ -134,7 +134,7 @@ int run_batch(wg_engine *eng, const Request &rq, const BatchArgs &proto, uint64_
     WG_CUDA(cudaEventRecord(eng->kev[0], eng->stream), "event");
     launch_climate(a, eng->stream);
     WG_CUDA(cudaEventRecord(eng->kev[1], eng->stream), "event");
-    launch_entrance(a, eng->sm_count, eng->stream);
+    launch_entrance(a, eng->sm_count * 2, eng->stream);
     WG_CUDA(cudaEventRecord(eng->kev[2], eng->stream), "event");
     launch_ladder(a, eng->sm_count * 8, eng->stream);
     WG_CUDA(cudaEventRecord(eng->kev[3], eng->stream), "event");

@@ -82,13 +82,13 @@ __device__ __forceinline__ void note_code(const BatchArgs &a, uint64_t g, uint64
 }
 
 // Table sources: where a sampler's permutation table and origin live.
-struct SrcIl {  // bank-interleaved shared block per slot, origins [slot][32]
+struct SrcCols {  // byte-interleaved blocks of kUnits columns, origins [slot][unit]
     const uint8_t *perm;
     const double *ox, *oy, *oz;
-    int lane;
+    int unit;
     __device__ __forceinline__ double p3(int slot, double x, double y, double z) const {
-        IlTable T{perm + slot * 8192 + lane * 4};
-        int o = slot * 32 + lane;
+        ColTable<kUnits> T{perm + slot * (256 * kUnits) + unit};
+        int o = slot * kUnits + unit;
         return perlin_3d(T, ox[o], oy[o], oz[o], x, y, z);
     }
 };
@@ -96,7 +96,7 @@ struct SrcFlat {  // contiguous 256-byte tables, origins [slot][3]
     const uint8_t *perm;
     const double *org;
     __device__ __forceinline__ double p3(int slot, double x, double y, double z) const {
-        FlatTable T{perm + slot * 256};
+        ColTable<1> T{perm + slot * 256};
         return perlin_3d(T, org[3 * slot], org[3 * slot + 1], org[3 * slot + 2], x, y, z);
     }
 };
@@ -167,14 +167,24 @@ __device__ double cheese(const S &src, int x, int y, int z) {
 // ------------------------------------------------------------------------------------
 // climate kernel
 // ------------------------------------------------------------------------------------
+// Step parameters are stored field by field (structure of arrays): threads sit at different
+// steps, and consecutive 8-byte entries fall in different banks.
+struct ClimateSteps {
+    double sc[kClimateSteps], lac[kClimateSteps], c1[kClimateSteps], c2[kClimateSteps];
+    double thr[kClimateSteps], amp[kClimateSteps];
+    int slot[kClimateSteps], act[kClimateSteps], tier[kClimateSteps];
+};
+
 struct ClimateSmem {
-    uint8_t perm[kSlotsA * 8192];
-    double ox[kSlotsA * 32], oz[kSlotsA * 32], hy[kSlotsA * 32], fy[kSlotsA * 32];
-    int jy[kSlotsA * 32];
-    uint32_t surv[32 * kRecordCap];
-    uint32_t cnt[32];
+    uint8_t perm[kSlotsA * 256 * kUnits];     // slot s, row k, unit u at (s * 256 + k) * kUnits + u
+    double ox[kSlotsA * kUnits], oz[kSlotsA * kUnits], hy[kSlotsA * kUnits], fy[kSlotsA * kUnits];
+    int jy[kSlotsA * kUnits];
+    int2 pos[kChunk * kUnits];                 // hut chunk (cx, cz) of window offset c0 + j, unit u
+    uint32_t surv[kUnits * kRecordCap];
+    uint32_t cnt[kUnits];
+    uint32_t next[kUnits];                     // next window offset to hand out, per unit
     unsigned int hist[P1_KINDS + kTiers];
-    ClimateStep steps[kClimateSteps];
+    ClimateSteps steps;
 };
 
 size_t climate_smem_bytes() { return sizeof(ClimateSmem); }
@@ -194,22 +204,41 @@ __device__ void emit_single(const BatchArgs &a, uint32_t u, uint32_t off_in_win)
     }
 }
 
-__device__ __forceinline__ void keep_survivor(ClimateSmem &S, const BatchArgs &a, int lane, uint32_t u, uint32_t j) {
-    uint32_t q = atomicAdd(&S.cnt[lane], 1u);
-    if (q < kRecordCap) S.surv[lane * kRecordCap + q] = j;
+__device__ __forceinline__ void keep_survivor(ClimateSmem &S, const BatchArgs &a, int uu, uint32_t u, uint32_t j) {
+    uint32_t q = atomicAdd(&S.cnt[uu], 1u);
+    if (q < kRecordCap) S.surv[uu * kRecordCap + q] = j;
     else emit_single(a, u, j);
 }
 
-__global__ void __launch_bounds__(kThreadsA, 1) climate_kernel(BatchArgs a) {
+// Thread t owns table (slot t / kUnits, unit t % kUnits) during the build and works for unit
+// t % kUnits during the evaluation: each unit's regions are handed out one at a time to its 18
+// threads (spread over all warps), and each loop trip is one Perlin sample, so threads at
+// different gate depths stay converged.
+__global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     ClimateSmem &S = *reinterpret_cast<ClimateSmem *>(smem_raw);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tid = threadIdx.x;
+    const int my_slot = tid / kUnits, uu = tid % kUnits;
     const int large = a.large_biomes ? 1 : 0;
-    if (threadIdx.x < 32) S.cnt[threadIdx.x] = 0;
-    if (threadIdx.x < P1_KINDS + kTiers) S.hist[threadIdx.x] = 0;
-    if (threadIdx.x < kClimateSteps) S.steps[threadIdx.x] = c_steps[large][threadIdx.x];
+    if (tid < kUnits) {
+        S.cnt[tid] = 0;
+        S.next[tid] = 0;
+    }
+    if (tid < P1_KINDS + kTiers) S.hist[tid] = 0;
+    if (tid < kClimateSteps) {
+        const ClimateStep &c = c_steps[large][tid];
+        S.steps.sc[tid] = c.sc;
+        S.steps.lac[tid] = c.lac;
+        S.steps.c1[tid] = c.c1;
+        S.steps.c2[tid] = c.c2;
+        S.steps.thr[tid] = c.thr;
+        S.steps.amp[tid] = c.amp;
+        S.steps.slot[tid] = c.slot;
+        S.steps.act[tid] = c.act;
+        S.steps.tier[tid] = c.tier;
+    }
 
-    const uint32_t u = blockIdx.x * 32u + (uint32_t)lane;
+    const uint32_t u = blockIdx.x * kUnits + (uint32_t)uu;
     const bool valid = u < a.n_units;
     const uint64_t g = valid ? unit_seed_index(a, u) : 0;
     const uint64_t w = valid ? unit_window(a, u) : 0;
@@ -217,107 +246,134 @@ __global__ void __launch_bounds__(kThreadsA, 1) climate_kernel(BatchArgs a) {
     const uint32_t len = valid ? window_len(a, w) : 0;
     const uint64_t r_base = w * a.win;
 
-    // ---- build: warp w builds climate slot w for the CTA's 32 units ----
-    if (valid && !a.single_biome) {
-        const int noise = c_slot_a[large][warp][0], sub = c_slot_a[large][warp][1], p = c_slot_a[large][warp][2];
-        Xr r = octave_rng(c_noise[noise], seed_fork_of(seed), sub, p);
-        double ox, oy, oz;
-        perlin_build_il(S.perm + warp * 8192 + lane * 4, r, ox, oy, oz);
-        const int o = warp * 32 + lane;
-        int jy = (int)floor(oy);
-        double hy = oy - jy;
-        S.ox[o] = ox;
-        S.oz[o] = oz;
-        S.hy[o] = hy;
-        S.fy[o] = fade(hy);
-        S.jy[o] = jy;
-    }
-    __syncthreads();
-
-    // ---- evaluate: lane = unit, warp w walks window offsets w, w+18, ...; one Perlin
-    // sample per loop trip, so lanes at different gate depths stay converged ----
-    if (valid) {
-        uint32_t next_j = (uint32_t)warp, cur = 0;
-        bool have = false;
-        int k = 0;
-        double xc = 0.0, zc = 0.0, sum = 0.0, sum_a = 0.0;
-        const uint8_t *lane_perm = S.perm + lane * 4;
-        for (;;) {
-            if (!have) {
-                if (next_j >= len) break;
-                cur = next_j;
-                next_j += kSlotsA;
-                int rx, rz, cx, cz;
-                region_xz(a, r_base + cur, rx, rz);
-                hut_chunk(seed, rx, rz, a.salt, cx, cz);
-                if (a.single_biome) {  // phase1.c:96: the climate gates are skipped
-                    keep_survivor(S, a, lane, u, cur);
-                    continue;
-                }
-                xc = (cx * 16 + 8) / 4.0;
-                zc = (cz * 16 + 8) / 4.0;
-                k = 0;
-                sum = 0.0;
-                have = true;
-            }
-            const ClimateStep &st = S.steps[k];
-            const int o = st.slot * 32 + lane;
-            IlTable T{lane_perm + st.slot * 8192};
-            double v = perlin_y0(T, S.ox[o], S.oz[o], S.jy[o], S.hy[o], S.fy[o],
-                                 keep_precision((xc * st.sc) * st.lac), keep_precision((zc * st.sc) * st.lac));
-            sum += (st.c1 * v) * st.c2;
-            int code = -1, tier = -1;
-            switch (st.act) {
-                case ACT_TIER:
-                case ACT_TIER_LAST:
-                    if (sum * st.amp < st.thr) {
-                        code = P1_EROSION;
-                        tier = st.tier;
-                    } else if (st.act == ACT_TIER_LAST) {
-                        sum = 0.0;
-                    }
-                    break;
-                case ACT_END_SUB_A:
-                    sum_a = sum;
-                    sum = 0.0;
-                    break;
-                case ACT_TEMPERATURE: {
-                    double t = (sum_a + sum) * st.amp;
-                    bool bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
-                    if (bad) code = P1_TEMPERATURE;
-                    sum = 0.0;
-                    break;
-                }
-                case ACT_RIDGE: {
-                    double rg = (sum_a + sum) * st.amp;
-                    if ((rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91))
-                        code = P1_RIDGE;
-                    else
-                        code = P1_ACCEPT;  // climate survivor, not yet a verdict
-                    break;
-                }
-                default:
-                    break;
-            }
-            if (code >= 0) {
-                have = false;
-                if (code == P1_ACCEPT) {
-                    keep_survivor(S, a, lane, u, cur);
-                } else {
-                    atomicAdd(&S.hist[code], 1u);
-                    if (tier >= 0) atomicAdd(&S.hist[P1_KINDS + tier], 1u);
-                    note_code(a, g, r_base + cur, code, tier);
-                }
-            } else {
-                k++;
-            }
+    // ---- build: every thread shuffles one table ----
+    if (!a.single_biome) {
+        perm_blocks_init<kUnits>(S.perm, kSlotsA * 64 * kUnits, tid, kThreadsA);
+        __syncthreads();
+        if (valid) {
+            const int noise = c_slot_a[large][my_slot][0], sub = c_slot_a[large][my_slot][1],
+                      p = c_slot_a[large][my_slot][2];
+            Xr r = octave_rng(c_noise[noise], seed_fork_of(seed), sub, p);
+            double ox, oy, oz;
+            perlin_shuffle<kUnits>(S.perm + my_slot * (256 * kUnits) + uu, r, ox, oy, oz);
+            const int o = my_slot * kUnits + uu;
+            int jy = (int)floor(oy);
+            double hy = oy - jy;
+            S.ox[o] = ox;
+            S.oz[o] = oz;
+            S.hy[o] = hy;
+            S.fy[o] = fade(hy);
+            S.jy[o] = jy;
         }
     }
+    __shared__ uint32_t max_len;
+    if (tid == 0) max_len = 0;
     __syncthreads();
+    if (valid && tid < kUnits) atomicMax(&max_len, len);
+    __syncthreads();
+    const uint32_t cta_len = max_len;
+    const ClimateSteps &st = S.steps;
+
+    for (uint32_t c0 = 0; c0 < cta_len; c0 += kChunk) {
+        // ---- stage the hut chunks of this chunk of regions, all units at once ----
+        for (int q = tid; q < kChunk * kUnits; q += kThreadsA) {
+            const int qu = q % kUnits, qj = q / kUnits;
+            const uint32_t qunit = blockIdx.x * kUnits + (uint32_t)qu;
+            if (qunit >= a.n_units) continue;
+            const uint64_t qg = unit_seed_index(a, qunit), qw = unit_window(a, qunit);
+            const uint32_t j = c0 + (uint32_t)qj;
+            if (j >= window_len(a, qw)) continue;
+            const uint64_t qr = qw * a.win + j;
+            int rx, rz, cx, cz;
+            region_xz(a, qr, rx, rz);
+            hut_chunk(seed_value(a, qg), rx, rz, a.salt, cx, cz);
+            S.pos[q] = make_int2(cx, cz);
+        }
+        if (tid < kUnits) S.next[tid] = c0;
+        __syncthreads();
+        const uint32_t c1 = min(len, c0 + (uint32_t)kChunk);
+        if (valid && c0 < len) {
+            uint32_t cur = 0;
+            bool have = false;
+            int k = 0;
+            double xc = 0.0, zc = 0.0, sum = 0.0, sum_a = 0.0;
+            const uint8_t *unit_perm = S.perm + uu;
+            for (;;) {
+                if (!have) {
+                    cur = atomicAdd(&S.next[uu], 1u);
+                    if (cur >= c1) break;
+                    const int2 cz2 = S.pos[(cur - c0) * kUnits + uu];
+                    if (a.single_biome) {  // phase1.c:96: the climate gates are skipped
+                        keep_survivor(S, a, uu, u, cur);
+                        continue;
+                    }
+                    xc = (cz2.x * 16 + 8) / 4.0;
+                    zc = (cz2.y * 16 + 8) / 4.0;
+                    k = 0;
+                    sum = 0.0;
+                    have = true;
+                }
+                const int slot = st.slot[k];
+                const int o = slot * kUnits + uu;
+                const double sc = st.sc[k], lac = st.lac[k];
+                ColTable<kUnits> T{unit_perm + slot * (256 * kUnits)};
+                double v = perlin_y0(T, S.ox[o], S.oz[o], S.jy[o], S.hy[o], S.fy[o],
+                                     keep_precision((xc * sc) * lac), keep_precision((zc * sc) * lac));
+                sum += (st.c1[k] * v) * st.c2[k];
+                int code = -1, tier = -1;
+                const int act = st.act[k];
+                switch (act) {
+                    case ACT_TIER:
+                    case ACT_TIER_LAST:
+                        if (sum * st.amp[k] < st.thr[k]) {
+                            code = P1_EROSION;
+                            tier = st.tier[k];
+                        } else if (act == ACT_TIER_LAST) {
+                            sum = 0.0;
+                        }
+                        break;
+                    case ACT_END_SUB_A:
+                        sum_a = sum;
+                        sum = 0.0;
+                        break;
+                    case ACT_TEMPERATURE: {
+                        double t = (sum_a + sum) * st.amp[k];
+                        bool bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
+                        if (bad) code = P1_TEMPERATURE;
+                        sum = 0.0;
+                        break;
+                    }
+                    case ACT_RIDGE: {
+                        double rg = (sum_a + sum) * st.amp[k];
+                        if ((rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91))
+                            code = P1_RIDGE;
+                        else
+                            code = P1_ACCEPT;  // climate survivor, not yet a verdict
+                        break;
+                    }
+                    default:
+                        break;
+                }
+                if (code >= 0) {
+                    have = false;
+                    if (code == P1_ACCEPT) {
+                        keep_survivor(S, a, uu, u, cur);
+                    } else {
+                        atomicAdd(&S.hist[code], 1u);
+                        if (tier >= 0) atomicAdd(&S.hist[P1_KINDS + tier], 1u);
+                        note_code(a, g, r_base + cur, code, tier);
+                    }
+                } else {
+                    k++;
+                }
+            }
+        }
+        __syncthreads();
+    }
 
     // ---- one record per unit with survivors ----
-    if (warp == 0 && valid) {
-        uint32_t n = min(S.cnt[lane], (uint32_t)kRecordCap);
+    if (tid < kUnits && valid) {
+        uint32_t n = min(S.cnt[tid], (uint32_t)kRecordCap);
         if (n) {
             uint32_t ri = atomicAdd(&a.counters[CNT_RECORDS], 1u);
             uint32_t off = atomicAdd(&a.counters[CNT_SURVIVORS], n);
@@ -325,53 +381,130 @@ __global__ void __launch_bounds__(kThreadsA, 1) climate_kernel(BatchArgs a) {
                 a.rec_unit[ri] = u;
                 a.rec_off[ri] = off;
                 a.rec_cnt[ri] = n;
-                for (uint32_t q = 0; q < n; q++) a.surv_region[off + q] = S.surv[lane * kRecordCap + q];
+                for (uint32_t q = 0; q < n; q++) a.surv_region[off + q] = S.surv[tid * kRecordCap + q];
             } else {
                 if (ri < a.cap_rec) a.rec_cnt[ri] = 0;
                 atomicOr(&a.counters[CNT_OVERFLOW], 1u);
             }
         }
     }
-    if (threadIdx.x < P1_KINDS + kTiers && S.hist[threadIdx.x])
-        atomicAdd(&a.hist[threadIdx.x], (unsigned long long)S.hist[threadIdx.x]);
+    if (tid < P1_KINDS + kTiers && S.hist[tid]) atomicAdd(&a.hist[tid], (unsigned long long)S.hist[tid]);
+}
+
+// cudaFuncSetAttribute applies to the device current at the call, so it is made once per device.
+template <class K>
+static void allow_dynamic_smem(K kernel, size_t bytes, unsigned long long &done_mask) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && (done_mask >> dev) & 1ull) return;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (dev >= 0 && dev < 64) done_mask |= 1ull << dev;
 }
 
 void launch_climate(const BatchArgs &a, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(climate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ClimateSmem));
-        attr = true;
-    }
-    int grid = (int)((a.n_units + 31) / 32);
+    static unsigned long long done = 0;
+    allow_dynamic_smem(climate_kernel, sizeof(ClimateSmem), done);
+    int grid = (int)((a.n_units + kUnits - 1) / kUnits);
     climate_kernel<<<grid, kThreadsA, sizeof(ClimateSmem), s>>>(a);
 }
 
 // ------------------------------------------------------------------------------------
 // entrance kernel: Entrance(50) / Entrance(60) for every climate survivor
+//
+// Thread t builds table (slot t / kUnits, record t % kUnits).  Afterwards it samples only that
+// table, for up to kEntChunk survivors of its record at y = 50 and y = 60, into shared memory;
+// the tunnel scale e (from the rarity slots) is formed between the two sampling rounds, because
+// spaghetti_3d_1/2 are sampled at (x/e, y/e, z/e).  One pass then sums the samples in the
+// reference's order (DoublePerlin: sub 0 octaves, then sub 1, times the amplitude;
+// caves.c:83-113).  Entrance(60) is computed for every survivor but only decides those with
+// Entrance(50) < 0, as in lysh.
 // ------------------------------------------------------------------------------------
+constexpr int kEntChunk = 4;
+
 struct EntranceSmem {
-    uint8_t perm[kSlotsB * 8192];
-    double ox[kSlotsB * 32], oy[kSlotsB * 32], oz[kSlotsB * 32];
+    uint8_t perm[kSlotsB * 256 * kUnits];
+    double ox[kSlotsB * kUnits], oy[kSlotsB * kUnits], oz[kSlotsB * kUnits];
+    double val[kSlotsB][2][kEntChunk][kUnits];   // [slot][y=50,60][survivor in chunk][record]
+    double tun[2][kEntChunk][kUnits];            // tunnel scale e per survivor and height
     unsigned int hist[P1_KINDS];
+    unsigned int max_cnt;
 };
 
 size_t entrance_smem_bytes() { return sizeof(EntranceSmem); }
 
-__global__ void __launch_bounds__(kThreadsB, 1) entrance_kernel(BatchArgs a) {
+// Base (unscaled) sampling point of cave noise `noise` at block (x, y, z); e = tunnel scale.
+__device__ __forceinline__ void cave_point(int noise, int x, int y, int z, double e, double &px, double &py,
+                                           double &pz) {
+    switch (noise) {
+        case N_CAVE_ENTRANCE:
+            px = (double)x * 0.75; py = (double)y * 0.5; pz = (double)z * 0.75;
+            break;
+        case N_SPAGHETTI_RARITY:
+            px = (double)(int)((uint32_t)x * 2u); py = (double)y; pz = (double)(int)((uint32_t)z * 2u);
+            break;
+        case N_SPAGHETTI_1:
+        case N_SPAGHETTI_2:
+            px = (double)x / e; py = (double)y / e; pz = (double)z / e;
+            break;
+        default:
+            px = (double)x; py = (double)y; pz = (double)z;
+            break;
+    }
+}
+
+// One octave of one sub-sampler of a DoublePerlin at a base point (noise.c:263-289 inner step).
+__device__ __forceinline__ double slot_sample(const SrcCols &src, int slot, const NoiseSpec &ns, int sub, int p,
+                                              double px, double py, double pz) {
+    if (sub) {
+        px = px * kDblScale;
+        py = py * kDblScale;
+        pz = pz * kDblScale;
+    }
+    const double l = ns.lac[p];
+    return src.p3(slot, keep_precision(px * l), keep_precision(py * l), keep_precision(pz * l));
+}
+
+// DoublePerlin value from its per-octave samples stored at val[base .. base + 2 np).
+__device__ __forceinline__ double combine(const EntranceSmem &S, int noise, int base, int h, int jj, int rr) {
+    const NoiseSpec &ns = c_noise[noise];
+    const int np = ns.npresent;
+    double a = 0.0, b = 0.0;
+    for (int p = 0; p < np; p++) a += (ns.amp[p] * S.val[base + p][h][jj][rr]) * ns.per[p];
+    for (int p = 0; p < np; p++) b += (ns.amp[p] * S.val[base + np + p][h][jj][rr]) * ns.per[p];
+    return (a + b) * ns.amplitude;
+}
+
+__device__ __forceinline__ void survivor_block(const BatchArgs &a, uint64_t seed, uint64_t r_base, uint32_t jr,
+                                               int &hx, int &hz) {
+    int rx, rz, cx, cz;
+    region_xz(a, r_base + jr, rx, rz);
+    hut_chunk(seed, rx, rz, a.salt, cx, cz);
+    hx = cx * 16 + 3;
+    hz = cz * 16 + 3;
+}
+
+__global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     EntranceSmem &S = *reinterpret_cast<EntranceSmem *>(smem_raw);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x < P1_KINDS) S.hist[threadIdx.x] = 0;
+    const int tid = threadIdx.x;
+    const int my_slot = tid / kUnits, rr = tid % kUnits;
+    if (tid < P1_KINDS) S.hist[tid] = 0;
     // A full list means the host discards this batch and re-runs it smaller.
     if (a.counters[CNT_OVERFLOW]) return;
     const uint32_t n_rec = min(a.counters[CNT_RECORDS], a.cap_rec);
-    const uint32_t n_tiles = (n_rec + 31) / 32;
-    const SrcIl src{S.perm, S.ox, S.oy, S.oz, lane};
+    const uint32_t n_tiles = (n_rec + kUnits - 1) / kUnits;
+    const SrcCols src{S.perm, S.ox, S.oy, S.oz, rr};
+    const int my_noise = c_slot_c[0][my_slot][0], my_sub = c_slot_c[0][my_slot][1], my_p = c_slot_c[0][my_slot][2];
+    const bool my_needs_e = (my_noise == N_SPAGHETTI_1 || my_noise == N_SPAGHETTI_2);
+    const NoiseSpec &ns = c_noise[my_noise];
     for (uint32_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-        const uint32_t ri = tile * 32 + (uint32_t)lane;
+        const uint32_t ri = tile * kUnits + (uint32_t)rr;
         const bool valid = ri < n_rec;
         uint32_t u = 0, off = 0, cnt = 0;
         uint64_t g = 0, r_base = 0, seed = 0;
+        if (tid == 0) S.max_cnt = 0;
+        perm_blocks_init<kUnits>(S.perm, kSlotsB * 64 * kUnits, tid, kThreadsB);
+        __syncthreads();
         if (valid) {
             u = a.rec_unit[ri];
             off = a.rec_off[ri];
@@ -380,52 +513,121 @@ __global__ void __launch_bounds__(kThreadsB, 1) entrance_kernel(BatchArgs a) {
             g = unit_seed_index(a, u);
             r_base = unit_window(a, u) * a.win;
             seed = seed_value(a, g);
-            const int noise = c_slot_c[0][warp][0], sub = c_slot_c[0][warp][1], p = c_slot_c[0][warp][2];
-            Xr r = octave_rng(c_noise[noise], seed_fork_of(seed), sub, p);
+            Xr r = octave_rng(ns, seed_fork_of(seed), my_sub, my_p);
             double ox, oy, oz;
-            perlin_build_il(S.perm + warp * 8192 + lane * 4, r, ox, oy, oz);
-            const int o = warp * 32 + lane;
+            perlin_shuffle<kUnits>(S.perm + my_slot * (256 * kUnits) + rr, r, ox, oy, oz);
+            const int o = my_slot * kUnits + rr;
             S.ox[o] = ox;
             S.oy[o] = oy;
             S.oz[o] = oz;
+            if (my_slot == 0 && cnt) atomicMax(&S.max_cnt, cnt);
         }
         __syncthreads();
-        if (valid) {
-            for (uint32_t j = (uint32_t)warp; j < cnt; j += kSlotsB) {
-                const uint32_t jr = a.surv_region[off + j];
-                int rx, rz, cx, cz;
-                region_xz(a, r_base + jr, rx, rz);
-                hut_chunk(seed, rx, rz, a.salt, cx, cz);
-                const int hx = cx * 16 + 3, hz = cz * 16 + 3;
-                int code = -1;
-                if (entrance(src, hx, 50, hz) >= 0) code = P1_ENTRANCE_50;
-                else if (entrance(src, hx, 60, hz) >= 0) code = P1_ENTRANCE_60;
-                if (code >= 0) {
-                    atomicAdd(&S.hist[code], 1u);
-                    note_code(a, g, r_base + jr, code, -1);
-                } else {
-                    uint32_t di = atomicAdd(&a.counters[CNT_DEEP], 1u);
-                    if (di < a.cap_deep) {
-                        a.deep[2 * di] = u;
-                        a.deep[2 * di + 1] = jr;
-                    } else {
-                        atomicOr(&a.counters[CNT_OVERFLOW], 2u);
+        const uint32_t max_cnt = S.max_cnt;
+        for (uint32_t c0 = 0; c0 < max_cnt; c0 += kEntChunk) {
+            // round 1: every slot that does not depend on the tunnel scale
+            if (!my_needs_e) {
+                for (int jj = 0; jj < kEntChunk; jj++) {
+                    const uint32_t j = c0 + jj;
+                    if (j >= cnt) break;
+                    int hx, hz;
+                    survivor_block(a, seed, r_base, a.surv_region[off + j], hx, hz);
+                    for (int h = 0; h < 2; h++) {
+                        double px, py, pz;
+                        cave_point(my_noise, hx, h ? 60 : 50, hz, 1.0, px, py, pz);
+                        S.val[my_slot][h][jj][rr] = slot_sample(src, my_slot, ns, my_sub, my_p, px, py, pz);
                     }
                 }
             }
+            __syncthreads();
+            // tunnel scale from the rarity samples
+            if (tid < kEntChunk * kUnits) {
+                const int jj = tid / kUnits, r2 = tid % kUnits;
+                const uint32_t cnt2 = (tile * kUnits + r2 < n_rec) ? a.rec_cnt[tile * kUnits + r2] : 0;
+                if (c0 + jj < cnt2)
+                    for (int h = 0; h < 2; h++)
+                        S.tun[h][jj][r2] = tunnel_scale(combine(S, N_SPAGHETTI_RARITY, kBaseRarity, h, jj, r2));
+            }
+            __syncthreads();
+            // round 2: spaghetti_3d_1 / _2 at (x/e, y/e, z/e)
+            if (my_needs_e) {
+                for (int jj = 0; jj < kEntChunk; jj++) {
+                    const uint32_t j = c0 + jj;
+                    if (j >= cnt) break;
+                    int hx, hz;
+                    survivor_block(a, seed, r_base, a.surv_region[off + j], hx, hz);
+                    for (int h = 0; h < 2; h++) {
+                        double px, py, pz;
+                        cave_point(my_noise, hx, h ? 60 : 50, hz, S.tun[h][jj][rr], px, py, pz);
+                        S.val[my_slot][h][jj][rr] = slot_sample(src, my_slot, ns, my_sub, my_p, px, py, pz);
+                    }
+                }
+            }
+            __syncthreads();
+            // combine in the reference's order and decide: thread (jj, r2)
+            if (tid < kEntChunk * kUnits) {
+                const int jj = tid / kUnits, r2 = tid % kUnits;
+                const uint32_t ri2 = tile * kUnits + (uint32_t)r2;
+                uint32_t u2 = 0, off2 = 0, cnt2 = 0;
+                if (ri2 < n_rec) {
+                    u2 = a.rec_unit[ri2];
+                    off2 = a.rec_off[ri2];
+                    cnt2 = a.rec_cnt[ri2];
+                    if (u2 >= a.n_units || off2 >= a.cap_surv || cnt2 > a.cap_surv - off2) cnt2 = 0;
+                }
+                const uint32_t j = c0 + jj;
+                if (j < cnt2) {
+                    double ent_v[2];
+                    for (int h = 0; h < 2; h++) {
+                        const int y = h ? 60 : 50;
+                        const double e = S.tun[h][jj][r2];
+                        double ent = combine(S, N_CAVE_ENTRANCE, kBaseEntrance, h, jj, r2);
+                        double t = (10.0 + (double)y) / 40.0;
+                        double cl = t < 0.0 ? 0.3 : (t > 1.0 ? 0.0 : lerp(t, 0.3, 0.0));
+                        double cc = ent + 0.37 + cl;
+                        double tv = combine(S, N_SPAGHETTI_THICKNESS, kBaseThickness, h, jj, r2);
+                        double hh = lerp((tv - -1.0) / (1.0 - -1.0), 0.065, 0.088);
+                        double l = combine(S, N_SPAGHETTI_1, kBaseSp1, h, jj, r2);
+                        double m = fabs(e * l) - hh;
+                        double n = combine(S, N_SPAGHETTI_2, kBaseSp2, h, jj, r2);
+                        double o = fabs(e * n) - hh;
+                        double pp = clampd(jmax(m, o), -1.0, 1.0);
+                        double mod = combine(S, N_ROUGHNESS_MODULATOR, kBaseRmod, h, jj, r2);
+                        double rgh = combine(S, N_ROUGHNESS, kBaseRough, h, jj, r2);
+                        double q = (-0.05 + (-0.05 * mod)) * (-0.4 + fabs(rgh));
+                        ent_v[h] = jmin(cc, pp + q);
+                    }
+                    const uint32_t jr = a.surv_region[off2 + j];
+                    const uint64_t g2 = unit_seed_index(a, u2);
+                    const uint64_t rb2 = unit_window(a, u2) * a.win;
+                    int code = -1;
+                    if (ent_v[0] >= 0) code = P1_ENTRANCE_50;
+                    else if (ent_v[1] >= 0) code = P1_ENTRANCE_60;
+                    if (code >= 0) {
+                        atomicAdd(&S.hist[code], 1u);
+                        note_code(a, g2, rb2 + jr, code, -1);
+                    } else {
+                        uint32_t di = atomicAdd(&a.counters[CNT_DEEP], 1u);
+                        if (di < a.cap_deep) {
+                            a.deep[2 * di] = u2;
+                            a.deep[2 * di + 1] = jr;
+                        } else {
+                            atomicOr(&a.counters[CNT_OVERFLOW], 2u);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
         }
         __syncthreads();
     }
-    if (threadIdx.x < P1_KINDS && S.hist[threadIdx.x])
-        atomicAdd(&a.hist[threadIdx.x], (unsigned long long)S.hist[threadIdx.x]);
+    __syncthreads();
+    if (tid < P1_KINDS && S.hist[tid]) atomicAdd(&a.hist[tid], (unsigned long long)S.hist[tid]);
 }
 
 void launch_entrance(const BatchArgs &a, int grid, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(entrance_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(EntranceSmem));
-        attr = true;
-    }
+    static unsigned long long done = 0;
+    allow_dynamic_smem(entrance_kernel, sizeof(EntranceSmem), done);
     entrance_kernel<<<grid, kThreadsB, sizeof(EntranceSmem), s>>>(a);
 }
 

@@ -4,13 +4,15 @@
 // Phase 1 restates lysh_phase1_check_ex (engine/tools/lysh/src/phase1.c:130-200) per
 // (seed, region) and is split into three kernels by how often each stage is reached:
 //
-//   climate  every seed     builds the 18 climate Perlins of 32 seeds per CTA in shared
+//   climate  every seed     builds the 18 climate Perlins of 16 units per CTA in shared
 //                           memory, runs the tiered erosion / temperature / ridge gates for
-//                           every region, and emits per-seed records of the survivors
+//                           every region, and emits per-unit records of the survivors
 //                           (~1.7% of regions at 9x9).
 //   entrance seeds with     builds the 18 Perlins of cave_entrance + the spaghetti set for
-//            survivors      32 records per CTA, evaluates Entrance(50) and Entrance(60)
+//            survivors      16 records per CTA, evaluates Entrance(50) and Entrance(60)
 //                           (97% of climate survivors stop here).
+// Both hot kernels use ~100 KiB of shared memory, so two CTAs share an SM and one CTA's table
+// build overlaps the other's evaluation.
 //   ladder   the rest       one CTA per remaining candidate builds all 54 cave / continent /
 //                           floodedness Perlins and finishes the ladder in lysh's order.
 #pragma once
@@ -38,14 +40,15 @@ enum : int {
 };
 constexpr int kTiers = 7;
 
-constexpr int kLanes = 32;          // seeds (or records) per CTA in the climate / entrance kernels
+constexpr int kUnits = 16;          // units (climate) or records (entrance) per CTA
 constexpr int kSlotsA = 18;         // erosion 8 + temperature 4 + ridge 6
 constexpr int kSlotsB = 18;         // cave_entrance 6 + six one-octave spaghetti noises x 2
 constexpr int kSlotsC = 54;         // kSlotsB + cave_layer 2 + cave_cheese 14 + continentalness 18 + floodedness 2
-constexpr int kThreadsA = kSlotsA * 32;
-constexpr int kThreadsB = kSlotsB * 32;
+constexpr int kThreadsA = kSlotsA * kUnits;   // one thread per (slot, unit) table
+constexpr int kThreadsB = kSlotsB * kUnits;
 constexpr int kThreadsC = 64;
 constexpr int kRecordCap = 64;      // survivors held per unit record in the climate kernel
+constexpr int kChunk = 128;         // regions per unit whose hut positions are staged at a time
 
 // Counter block written by the kernels (one per engine, reset per batch).
 enum : int {
