@@ -214,11 +214,24 @@ __device__ __forceinline__ void perlin_shuffle(uint8_t *t, Xr r, double &ox, dou
     }
 }
 
-// Table reader: byte k of a column with the given row stride.
+// The high 32-bit words of the doubles -1.0 / 0.0 / +1.0 of the game's 16-entry gradient table
+// (noise.c:15-20), [component * 16 + hash], kept in shared memory by every sampling kernel: a
+// warp's reads of one component touch at most 16 words in 16 distinct banks.
+constexpr int kGradWords = 48;
+__device__ __forceinline__ void fill_grad_table(uint32_t *gt, int tid);
+
+// Table reader: byte k of a column with the given row stride, plus the gradient products.
 template <int STRIDE>
 struct ColTable {
     const uint8_t *t;
+    const uint32_t *gt;
     __device__ __forceinline__ int operator()(int k) const { return t[k * STRIDE]; }
+    // (double)g[0] * x + (double)g[1] * y + (double)g[2] * z, as the reference writes it
+    __device__ __forceinline__ double grad(int hash, double x, double y, double z) const {
+        const int h = hash & 15;
+        return __hiloint2double((int)gt[h], 0) * x + __hiloint2double((int)gt[16 + h], 0) * y +
+               __hiloint2double((int)gt[32 + h], 0) * z;
+    }
 };
 
 // Same construction into a contiguous 256-byte table (rare-path kernels).
@@ -247,19 +260,16 @@ __host__ __device__ constexpr uint32_t grad_codes(int c) {
     for (int h = 0; h < 16; h++) v |= (uint32_t)(g[h][c] == 0 ? 0 : (g[h][c] > 0 ? 1 : 3)) << (2 * h);
     return v;
 }
-constexpr uint32_t kGradX = grad_codes(0), kGradY = grad_codes(1), kGradZ = grad_codes(2);
 
-// The double -1.0 / 0.0 / +1.0 of a 2-bit gradient code, built from its bits.
-__device__ __forceinline__ double grad_component(uint32_t codes, uint32_t shift) {
-    const uint32_t c = (codes >> shift) & 3u;
-    const uint32_t hi = ((c & 1u) * 0x3FF00000u) | ((c & 2u) << 30);
-    return __hiloint2double((int)hi, 0);
-}
+constexpr uint32_t kGradCodeX = grad_codes(0), kGradCodeY = grad_codes(1), kGradCodeZ = grad_codes(2);
 
-// (double)g[0] * x + (double)g[1] * y + (double)g[2] * z, as the reference writes it.
-__device__ __forceinline__ double grad(int hash, double x, double y, double z) {
-    const uint32_t sh = ((uint32_t)hash & 15u) * 2u;
-    return grad_component(kGradX, sh) * x + grad_component(kGradY, sh) * y + grad_component(kGradZ, sh) * z;
+__device__ __forceinline__ void fill_grad_table(uint32_t *gt, int tid) {
+    if (tid < kGradWords) {
+        const int c = tid / 16;
+        const uint32_t codes = c == 0 ? kGradCodeX : (c == 1 ? kGradCodeY : kGradCodeZ);
+        const uint32_t code = (codes >> (2 * (tid % 16))) & 3u;
+        gt[tid] = code == 0 ? 0u : (code == 1 ? 0x3FF00000u : 0xBFF00000u);
+    }
 }
 
 template <class T>
@@ -268,14 +278,14 @@ __device__ __forceinline__ double perlin_core(const T &P, int i, int j, int k, d
     int a = P(i & 255), b = P((i + 1) & 255);
     int c = P((a + j) & 255), d = P((a + j + 1) & 255);
     int e = P((b + j) & 255), f = P((b + j + 1) & 255);
-    double v000 = grad(P((c + k) & 255), x, y, z);
-    double v100 = grad(P((e + k) & 255), x - 1, y, z);
-    double v010 = grad(P((d + k) & 255), x, y1, z);
-    double v110 = grad(P((f + k) & 255), x - 1, y1, z);
-    double v001 = grad(P((c + k + 1) & 255), x, y, z - 1);
-    double v101 = grad(P((e + k + 1) & 255), x - 1, y, z - 1);
-    double v011 = grad(P((d + k + 1) & 255), x, y1, z - 1);
-    double v111 = grad(P((f + k + 1) & 255), x - 1, y1, z - 1);
+    double v000 = P.grad(P((c + k) & 255), x, y, z);
+    double v100 = P.grad(P((e + k) & 255), x - 1, y, z);
+    double v010 = P.grad(P((d + k) & 255), x, y1, z);
+    double v110 = P.grad(P((f + k) & 255), x - 1, y1, z);
+    double v001 = P.grad(P((c + k + 1) & 255), x, y, z - 1);
+    double v101 = P.grad(P((e + k + 1) & 255), x - 1, y, z - 1);
+    double v011 = P.grad(P((d + k + 1) & 255), x, y1, z - 1);
+    double v111 = P.grad(P((f + k + 1) & 255), x - 1, y1, z - 1);
     double x00 = lerp(fx, v000, v100), x10 = lerp(fx, v010, v110);
     double x01 = lerp(fx, v001, v101), x11 = lerp(fx, v011, v111);
     return lerp(fz, lerp(fy, x00, x10), lerp(fy, x01, x11));

@@ -85,9 +85,10 @@ __device__ __forceinline__ void note_code(const BatchArgs &a, uint64_t g, uint64
 struct SrcCols {  // byte-interleaved blocks of kUnits columns, origins [slot][unit]
     const uint8_t *perm;
     const double *ox, *oy, *oz;
+    const uint32_t *gt;
     int unit;
     __device__ __forceinline__ double p3(int slot, double x, double y, double z) const {
-        ColTable<kUnits> T{perm + slot * (256 * kUnits) + unit};
+        ColTable<kUnits> T{perm + slot * (256 * kUnits) + unit, gt};
         int o = slot * kUnits + unit;
         return perlin_3d(T, ox[o], oy[o], oz[o], x, y, z);
     }
@@ -95,8 +96,9 @@ struct SrcCols {  // byte-interleaved blocks of kUnits columns, origins [slot][u
 struct SrcFlat {  // contiguous 256-byte tables, origins [slot][3]
     const uint8_t *perm;
     const double *org;
+    const uint32_t *gt;
     __device__ __forceinline__ double p3(int slot, double x, double y, double z) const {
-        ColTable<1> T{perm + slot * 256};
+        ColTable<1> T{perm + slot * 256, gt};
         return perlin_3d(T, org[3 * slot], org[3 * slot + 1], org[3 * slot + 2], x, y, z);
     }
 };
@@ -184,6 +186,7 @@ struct ClimateSmem {
     uint32_t cnt[kUnits];
     uint32_t next[kUnits];                     // next window offset to hand out, per unit
     unsigned int hist[P1_KINDS + kTiers];
+    uint32_t grad[kGradWords];
     ClimateSteps steps;
 };
 
@@ -225,6 +228,7 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
         S.next[tid] = 0;
     }
     if (tid < P1_KINDS + kTiers) S.hist[tid] = 0;
+    fill_grad_table(S.grad, tid);
     if (tid < kClimateSteps) {
         const ClimateStep &c = c_steps[large][tid];
         S.steps.sc[tid] = c.sc;
@@ -316,7 +320,7 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                 const int slot = st.slot[k];
                 const int o = slot * kUnits + uu;
                 const double sc = st.sc[k], lac = st.lac[k];
-                ColTable<kUnits> T{unit_perm + slot * (256 * kUnits)};
+                ColTable<kUnits> T{unit_perm + slot * (256 * kUnits), S.grad};
                 double v = perlin_y0(T, S.ox[o], S.oz[o], S.jy[o], S.hy[o], S.fy[o],
                                      keep_precision((xc * sc) * lac), keep_precision((zc * sc) * lac));
                 sum += (st.c1[k] * v) * st.c2[k];
@@ -428,6 +432,7 @@ struct EntranceSmem {
     double tun[2][kEntChunk][kUnits];            // tunnel scale e per survivor and height
     unsigned int hist[P1_KINDS];
     unsigned int max_cnt;
+    uint32_t grad[kGradWords];
 };
 
 size_t entrance_smem_bytes() { return sizeof(EntranceSmem); }
@@ -489,11 +494,12 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
     const int tid = threadIdx.x;
     const int my_slot = tid / kUnits, rr = tid % kUnits;
     if (tid < P1_KINDS) S.hist[tid] = 0;
+    fill_grad_table(S.grad, tid);
     // A full list means the host discards this batch and re-runs it smaller.
     if (a.counters[CNT_OVERFLOW]) return;
     const uint32_t n_rec = min(a.counters[CNT_RECORDS], a.cap_rec);
     const uint32_t n_tiles = (n_rec + kUnits - 1) / kUnits;
-    const SrcCols src{S.perm, S.ox, S.oy, S.oz, rr};
+    const SrcCols src{S.perm, S.ox, S.oy, S.oz, S.grad, rr};
     const int my_noise = c_slot_c[0][my_slot][0], my_sub = c_slot_c[0][my_slot][1], my_p = c_slot_c[0][my_slot][2];
     const bool my_needs_e = (my_noise == N_SPAGHETTI_1 || my_noise == N_SPAGHETTI_2);
     const NoiseSpec &ns = c_noise[my_noise];
@@ -637,6 +643,7 @@ void launch_entrance(const BatchArgs &a, int grid, cudaStream_t s) {
 struct LadderSmem {
     uint8_t perm[kSlotsC * 256];
     double org[kSlotsC * 3];
+    uint32_t grad[kGradWords];
 };
 
 __global__ void __launch_bounds__(kThreadsC) ladder_kernel(BatchArgs a) {
@@ -644,7 +651,8 @@ __global__ void __launch_bounds__(kThreadsC) ladder_kernel(BatchArgs a) {
     const int large = a.large_biomes ? 1 : 0;
     if (a.counters[CNT_OVERFLOW]) return;
     const uint32_t n_deep = min(a.counters[CNT_DEEP], a.cap_deep);
-    const SrcFlat src{S.perm, S.org};
+    fill_grad_table(S.grad, threadIdx.x);
+    const SrcFlat src{S.perm, S.org, S.grad};
     for (uint32_t q = blockIdx.x; q < n_deep; q += gridDim.x) {
         const uint32_t u = a.deep[2 * q], jr = a.deep[2 * q + 1];
         const uint64_t g = unit_seed_index(a, u);
