@@ -182,9 +182,19 @@ struct ClimateSmem {
     double ox[kSlotsA * kUnits], oz[kSlotsA * kUnits], hy[kSlotsA * kUnits], fy[kSlotsA * kUnits];
     int jy[kSlotsA * kUnits];
     int2 pos[kChunk * kUnits];                 // hut chunk (cx, cz) of window offset c0 + j, unit u
+    union {
+        double tsum[kTierList];                // erosion partial sum of each tier-0 survivor
+        double val[kClimateList * 6];          // parallel temperature / ridge samples (after the tiers)
+    };
+    uint32_t tlist[kTierList];                 // tier-0 survivors of the chunk: unit << 16 | (j - c0)
+    uint32_t clist[kClimateList];              // erosion survivors of the chunk
+    uint32_t rlist[kClimateList];              // ... that also passed temperature
+    uint32_t n_tlist, t_next, n_clist, n_rlist;
     uint32_t surv[kUnits * kRecordCap];
     uint32_t cnt[kUnits];
     uint32_t next[kUnits];                     // next window offset to hand out, per unit
+    uint32_t end[kUnits];                      // end of the current chunk, per unit
+    uint64_t g[kUnits], rbase[kUnits];         // seed index and first region of each unit
     unsigned int hist[P1_KINDS + kTiers];
     uint32_t grad[kGradWords];
     ClimateSteps steps;
@@ -207,26 +217,107 @@ __device__ void emit_single(const BatchArgs &a, uint32_t u, uint32_t off_in_win)
     }
 }
 
-__device__ __forceinline__ void keep_survivor(ClimateSmem &S, const BatchArgs &a, int uu, uint32_t u, uint32_t j) {
-    uint32_t q = atomicAdd(&S.cnt[uu], 1u);
-    if (q < kRecordCap) S.surv[uu * kRecordCap + q] = j;
-    else emit_single(a, u, j);
+__device__ __forceinline__ void keep_survivor(ClimateSmem &S, const BatchArgs &a, int iu, uint32_t j) {
+    uint32_t q = atomicAdd(&S.cnt[iu], 1u);
+    if (q < kRecordCap) S.surv[iu * kRecordCap + q] = j;
+    else emit_single(a, blockIdx.x * kUnits + (uint32_t)iu, j);
 }
 
-// Thread t owns table (slot t / kUnits, unit t % kUnits) during the build and works for unit
-// t % kUnits during the evaluation: each unit's regions are handed out one at a time to its 18
-// threads (spread over all warps), and each loop trip is one Perlin sample, so threads at
-// different gate depths stay converged.
+__device__ __forceinline__ void climate_reject(ClimateSmem &S, const BatchArgs &a, int iu, uint32_t j, int code,
+                                               int tier) {
+    atomicAdd(&S.hist[code], 1u);
+    if (tier >= 0) atomicAdd(&S.hist[P1_KINDS + tier], 1u);
+    note_code(a, S.g[iu], S.rbase[iu] + j, code, tier);
+}
+
+// One y = 0 Perlin sample of climate step k for unit iu at climate point (xc, zc).
+__device__ __forceinline__ double climate_sample(const ClimateSmem &S, int iu, int k, double xc, double zc) {
+    const ClimateSteps &st = S.steps;
+    const int slot = st.slot[k];
+    const int o = slot * kUnits + iu;
+    const double sc = st.sc[k], lac = st.lac[k];
+    ColTable<kUnits> T{S.perm + slot * (256 * kUnits) + iu, S.grad};
+    return perlin_y0(T, S.ox[o], S.oz[o], S.jy[o], S.hy[o], S.fy[o], keep_precision((xc * sc) * lac),
+                     keep_precision((zc * sc) * lac));
+}
+
+__device__ __forceinline__ void climate_point(const ClimateSmem &S, int iu, uint32_t jl, double &xc, double &zc) {
+    const int2 c = S.pos[jl * kUnits + iu];
+    xc = (c.x * 16 + 8) / 4.0;
+    zc = (c.y * 16 + 8) / 4.0;
+}
+
+// The erosion tiers from step k0 for one region (e = unit << 16 | offset in the chunk), one Perlin
+// sample per loop trip.  A region that passes the last tier is handed to the climate list; if the
+// list is full, this thread also runs its temperature and ridge steps.
+__device__ void climate_rest(ClimateSmem &S, const BatchArgs &a, uint32_t e, uint32_t c0, int k0, double sum,
+                             double xc, double zc) {
+    const ClimateSteps &st = S.steps;
+    const int iu = (int)(e >> 16);
+    const uint32_t j = c0 + (e & 0xFFFFu);
+    double sum_a = 0.0;
+    for (int k = k0; k < kClimateSteps; k++) {
+        const double v = climate_sample(S, iu, k, xc, zc);
+        sum += (st.c1[k] * v) * st.c2[k];
+        switch (st.act[k]) {
+            case ACT_TIER:
+                if (sum * st.amp[k] < st.thr[k]) {
+                    climate_reject(S, a, iu, j, P1_EROSION, st.tier[k]);
+                    return;
+                }
+                break;
+            case ACT_TIER_LAST:
+                if (sum * st.amp[k] < st.thr[k]) {
+                    climate_reject(S, a, iu, j, P1_EROSION, st.tier[k]);
+                    return;
+                } else {
+                    const uint32_t q = atomicAdd(&S.n_clist, 1u);
+                    if (q < kClimateList) {
+                        S.clist[q] = e;
+                        return;
+                    }
+                    sum = 0.0;   // list full: finish it here
+                }
+                break;
+            case ACT_END_SUB_A:
+                sum_a = sum;
+                sum = 0.0;
+                break;
+            case ACT_TEMPERATURE: {
+                double t = (sum_a + sum) * st.amp[k];
+                bool bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
+                if (bad) {
+                    climate_reject(S, a, iu, j, P1_TEMPERATURE, -1);
+                    return;
+                }
+                sum = 0.0;
+                break;
+            }
+            case ACT_RIDGE: {
+                double rg = (sum_a + sum) * st.amp[k];
+                if ((rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91))
+                    climate_reject(S, a, iu, j, P1_RIDGE, -1);
+                else
+                    keep_survivor(S, a, iu, j);   // climate survivor, not yet a verdict
+                return;
+            }
+            default:
+                break;
+        }
+    }
+}
+
+// Thread t owns table (slot t / kUnits, unit t % kUnits) during the build.  The evaluation of a
+// chunk of regions runs in phases separated by barriers: (1) tier 0 (samples 0A, 0B) for every
+// region, a uniform loop that rejects ~57 %; (2) the remaining erosion tiers for the survivors,
+// taken from a shared list by any thread; (3) temperature and (4) ridge for the ~5 % that pass
+// erosion, one sample per thread, summed per region in the reference's order.
 __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     ClimateSmem &S = *reinterpret_cast<ClimateSmem *>(smem_raw);
     const int tid = threadIdx.x;
     const int my_slot = tid / kUnits, uu = tid % kUnits;
     const int large = a.large_biomes ? 1 : 0;
-    if (tid < kUnits) {
-        S.cnt[tid] = 0;
-        S.next[tid] = 0;
-    }
     if (tid < P1_KINDS + kTiers) S.hist[tid] = 0;
     fill_grad_table(S.grad, tid);
     if (tid < kClimateSteps) {
@@ -248,7 +339,11 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
     const uint64_t w = valid ? unit_window(a, u) : 0;
     const uint64_t seed = valid ? seed_value(a, g) : 0;
     const uint32_t len = valid ? window_len(a, w) : 0;
-    const uint64_t r_base = w * a.win;
+    if (tid < kUnits) {
+        S.cnt[tid] = 0;
+        S.g[tid] = g;
+        S.rbase[tid] = w * a.win;
+    }
 
     // ---- build: every thread shuffles one table ----
     if (!a.single_biome) {
@@ -293,84 +388,122 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
             hut_chunk(seed_value(a, qg), rx, rz, a.salt, cx, cz);
             S.pos[q] = make_int2(cx, cz);
         }
-        if (tid < kUnits) S.next[tid] = c0;
+        if (tid < kUnits) {
+            S.next[tid] = c0;
+            S.end[tid] = (valid && c0 < len) ? min(len, c0 + (uint32_t)kChunk) : c0;
+        }
+        if (tid == 0) {
+            S.n_tlist = 0;
+            S.t_next = 0;
+            S.n_clist = 0;
+            S.n_rlist = 0;
+        }
         __syncthreads();
-        const uint32_t c1 = min(len, c0 + (uint32_t)kChunk);
-        if (valid && c0 < len) {
-            uint32_t cur = 0;
-            bool have = false;
-            int k = 0;
-            double xc = 0.0, zc = 0.0, sum = 0.0, sum_a = 0.0;
-            const uint8_t *unit_perm = S.perm + uu;
-            for (;;) {
-                if (!have) {
-                    cur = atomicAdd(&S.next[uu], 1u);
-                    if (cur >= c1) break;
-                    const int2 cz2 = S.pos[(cur - c0) * kUnits + uu];
-                    if (a.single_biome) {  // phase1.c:96: the climate gates are skipped
-                        keep_survivor(S, a, uu, u, cur);
-                        continue;
-                    }
-                    xc = (cz2.x * 16 + 8) / 4.0;
-                    zc = (cz2.y * 16 + 8) / 4.0;
-                    k = 0;
-                    sum = 0.0;
-                    have = true;
+
+        // ---- tier 0 for every region: samples 0A and 0B with loop-invariant parameters ----
+        {
+            const int nq = kUnits * kChunk;
+            for (int q = tid; q < nq; q += kThreadsA) {
+                const int iu = q % kUnits;
+                const uint32_t jl = (uint32_t)(q / kUnits), j = c0 + jl;
+                if (j >= S.end[iu]) continue;
+                if (a.single_biome) {  // phase1.c:96: the climate gates are skipped
+                    keep_survivor(S, a, iu, j);
+                    continue;
                 }
-                const int slot = st.slot[k];
-                const int o = slot * kUnits + uu;
-                const double sc = st.sc[k], lac = st.lac[k];
-                ColTable<kUnits> T{unit_perm + slot * (256 * kUnits), S.grad};
-                double v = perlin_y0(T, S.ox[o], S.oz[o], S.jy[o], S.hy[o], S.fy[o],
-                                     keep_precision((xc * sc) * lac), keep_precision((zc * sc) * lac));
-                sum += (st.c1[k] * v) * st.c2[k];
-                int code = -1, tier = -1;
-                const int act = st.act[k];
-                switch (act) {
-                    case ACT_TIER:
-                    case ACT_TIER_LAST:
-                        if (sum * st.amp[k] < st.thr[k]) {
-                            code = P1_EROSION;
-                            tier = st.tier[k];
-                        } else if (act == ACT_TIER_LAST) {
-                            sum = 0.0;
-                        }
-                        break;
-                    case ACT_END_SUB_A:
-                        sum_a = sum;
-                        sum = 0.0;
-                        break;
-                    case ACT_TEMPERATURE: {
-                        double t = (sum_a + sum) * st.amp[k];
-                        bool bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
-                        if (bad) code = P1_TEMPERATURE;
-                        sum = 0.0;
-                        break;
-                    }
-                    case ACT_RIDGE: {
-                        double rg = (sum_a + sum) * st.amp[k];
-                        if ((rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91))
-                            code = P1_RIDGE;
-                        else
-                            code = P1_ACCEPT;  // climate survivor, not yet a verdict
-                        break;
-                    }
-                    default:
-                        break;
-                }
-                if (code >= 0) {
-                    have = false;
-                    if (code == P1_ACCEPT) {
-                        keep_survivor(S, a, uu, u, cur);
-                    } else {
-                        atomicAdd(&S.hist[code], 1u);
-                        if (tier >= 0) atomicAdd(&S.hist[P1_KINDS + tier], 1u);
-                        note_code(a, g, r_base + cur, code, tier);
-                    }
+                double xc, zc;
+                climate_point(S, iu, jl, xc, zc);
+                double sum = 0.0;
+                sum += (st.c1[0] * climate_sample(S, iu, 0, xc, zc)) * st.c2[0];
+                sum += (st.c1[1] * climate_sample(S, iu, 1, xc, zc)) * st.c2[1];
+                if (sum * st.amp[1] < st.thr[1]) {
+                    climate_reject(S, a, iu, j, P1_EROSION, st.tier[1]);
                 } else {
-                    k++;
+                    const uint32_t t = atomicAdd(&S.n_tlist, 1u);
+                    if (t < kTierList) {
+                        S.tlist[t] = ((uint32_t)iu << 16) | jl;
+                        S.tsum[t] = sum;
+                    } else {
+                        // list full: this thread walks the region through the rest itself
+                        uint32_t e = ((uint32_t)iu << 16) | jl;
+                        climate_rest(S, a, e, c0, 2, sum, xc, zc);
+                    }
                 }
             }
+        }
+        __syncthreads();
+
+        // ---- the remaining erosion tiers for the tier-0 survivors, any thread any region ----
+        {
+            const uint32_t n_t = min(S.n_tlist, (uint32_t)kTierList);
+            for (;;) {
+                const uint32_t t = atomicAdd(&S.t_next, 1u);
+                if (t >= n_t) break;
+                const uint32_t e = S.tlist[t];
+                double xc, zc;
+                climate_point(S, (int)(e >> 16), e & 0xFFFFu, xc, zc);
+                climate_rest(S, a, e, c0, 2, S.tsum[t], xc, zc);
+            }
+        }
+        __syncthreads();
+
+        // ---- temperature for the listed erosion survivors: one sample per thread ----
+        const uint32_t n_cl = min(S.n_clist, (uint32_t)kClimateList);
+        constexpr int kT0 = 8, kR0 = 12;   // first temperature / ridge step
+        for (uint32_t t = tid; t < n_cl * 4; t += kThreadsA) {
+            const uint32_t e = S.clist[t / 4];
+            const int iu = (int)(e >> 16);
+            double xc, zc;
+            climate_point(S, iu, e & 0xFFFFu, xc, zc);
+            S.val[t] = climate_sample(S, iu, kT0 + (int)(t % 4), xc, zc);
+        }
+        __syncthreads();
+        for (uint32_t i = tid; i < n_cl; i += kThreadsA) {
+            const uint32_t e = S.clist[i];
+            double sum = 0.0, sum_a = 0.0;
+            for (int p = 0; p < 4; p++) {   // the state machine's accumulation, steps kT0..kT0+3
+                const int k = kT0 + p;
+                sum += (st.c1[k] * S.val[i * 4 + p]) * st.c2[k];
+                if (st.act[k] == ACT_END_SUB_A) {
+                    sum_a = sum;
+                    sum = 0.0;
+                }
+            }
+            const double t = (sum_a + sum) * st.amp[kT0 + 3];
+            const bool bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
+            if (bad) climate_reject(S, a, (int)(e >> 16), c0 + (e & 0xFFFFu), P1_TEMPERATURE, -1);
+            else S.rlist[atomicAdd(&S.n_rlist, 1u)] = e;
+        }
+        __syncthreads();
+
+        // ---- ridge for those that passed temperature ----
+        const uint32_t n_rl = S.n_rlist;
+        for (uint32_t t = tid; t < n_rl * 6; t += kThreadsA) {
+            const uint32_t e = S.rlist[t / 6];
+            const int iu = (int)(e >> 16);
+            double xc, zc;
+            climate_point(S, iu, e & 0xFFFFu, xc, zc);
+            S.val[t] = climate_sample(S, iu, kR0 + (int)(t % 6), xc, zc);
+        }
+        __syncthreads();
+        for (uint32_t i = tid; i < n_rl; i += kThreadsA) {
+            const uint32_t e = S.rlist[i];
+            const int iu = (int)(e >> 16);
+            const uint32_t j = c0 + (e & 0xFFFFu);
+            double sum = 0.0, sum_a = 0.0;
+            for (int p = 0; p < 6; p++) {
+                const int k = kR0 + p;
+                sum += (st.c1[k] * S.val[i * 6 + p]) * st.c2[k];
+                if (st.act[k] == ACT_END_SUB_A) {
+                    sum_a = sum;
+                    sum = 0.0;
+                }
+            }
+            const double rg = (sum_a + sum) * st.amp[kR0 + 5];
+            if ((rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91))
+                climate_reject(S, a, iu, j, P1_RIDGE, -1);
+            else
+                keep_survivor(S, a, iu, j);
         }
         __syncthreads();
     }

@@ -48,7 +48,9 @@ constexpr int kThreadsA = kSlotsA * kUnits;   // one thread per (slot, unit) tab
 constexpr int kThreadsB = kSlotsB * kUnits;
 constexpr int kThreadsC = 64;
 constexpr int kRecordCap = 64;      // survivors held per unit record in the climate kernel
-constexpr int kChunk = 128;         // regions per unit whose hut positions are staged at a time
+constexpr int kChunk = 96;          // regions per unit whose hut positions are staged at a time
+constexpr int kClimateList = 128;   // erosion survivors per chunk finished in parallel (temperature, ridge)
+constexpr int kTierList = 768;      // tier-0 survivors per chunk carried into the remaining erosion tiers
 
 // Counter block written by the kernels (one per engine, reset per batch).
 enum : int {
