@@ -556,16 +556,23 @@ void launch_climate(const BatchArgs &a, cudaStream_t s) {
 // caves.c:83-113).  Entrance(60) is computed for every survivor but only decides those with
 // Entrance(50) < 0, as in lysh.
 // ------------------------------------------------------------------------------------
-constexpr int kEntChunk = 4;
+constexpr int kEntFlat = 64;                   // survivors evaluated per round of a tile
+constexpr int kEntList = kUnits * kRecordCap;  // survivors a tile can hold
 
 struct EntranceSmem {
     uint8_t perm[kSlotsB * 256 * kUnits];
     double ox[kSlotsB * kUnits], oy[kSlotsB * kUnits], oz[kSlotsB * kUnits];
-    double val[kSlotsB][2][kEntChunk][kUnits];   // [slot][y=50,60][survivor in chunk][record]
-    double tun[2][kEntChunk][kUnits];            // tunnel scale e per survivor and height
+    double val[kSlotsB][2][kEntFlat];     // [slot][y=50,60][survivor]
+    double tun[2][kEntFlat];              // tunnel scale e per survivor and height
+    int hx[kEntFlat], hz[kEntFlat];       // sampling block of each survivor
+    uint32_t emap[kEntList];              // tile survivor list: record << 16 | index in its record
+    uint64_t rseed[kUnits], rg[kUnits], rbase[kUnits];
+    uint32_t runit[kUnits], roff[kUnits];
     unsigned int hist[P1_KINDS];
-    unsigned int max_cnt;
+    unsigned int n_list;
     uint32_t grad[kGradWords];
+    double slot_lac[kSlotsB];             // per slot: the octave's lacunarity, noise id, sub
+    int slot_noise[kSlotsB], slot_sub[kSlotsB];
 };
 
 size_t entrance_smem_bytes() { return sizeof(EntranceSmem); }
@@ -590,37 +597,39 @@ __device__ __forceinline__ void cave_point(int noise, int x, int y, int z, doubl
     }
 }
 
-// One octave of one sub-sampler of a DoublePerlin at a base point (noise.c:263-289 inner step).
-__device__ __forceinline__ double slot_sample(const SrcCols &src, int slot, const NoiseSpec &ns, int sub, int p,
-                                              double px, double py, double pz) {
+// One octave of one sub-sampler of a DoublePerlin at a base point (noise.c:263-289 inner step);
+// l is that octave's lacunarity.
+template <class Src>
+__device__ __forceinline__ double slot_sample(const Src &src, int slot, int sub, double l, double px, double py,
+                                              double pz) {
     if (sub) {
         px = px * kDblScale;
         py = py * kDblScale;
         pz = pz * kDblScale;
     }
-    const double l = ns.lac[p];
     return src.p3(slot, keep_precision(px * l), keep_precision(py * l), keep_precision(pz * l));
 }
 
 // DoublePerlin value from its per-octave samples stored at val[base .. base + 2 np).
-__device__ __forceinline__ double combine(const EntranceSmem &S, int noise, int base, int h, int jj, int rr) {
+__device__ __forceinline__ double combine(const EntranceSmem &S, int noise, int base, int h, int e) {
     const NoiseSpec &ns = c_noise[noise];
     const int np = ns.npresent;
     double a = 0.0, b = 0.0;
-    for (int p = 0; p < np; p++) a += (ns.amp[p] * S.val[base + p][h][jj][rr]) * ns.per[p];
-    for (int p = 0; p < np; p++) b += (ns.amp[p] * S.val[base + np + p][h][jj][rr]) * ns.per[p];
+    for (int p = 0; p < np; p++) a += (ns.amp[p] * S.val[base + p][h][e]) * ns.per[p];
+    for (int p = 0; p < np; p++) b += (ns.amp[p] * S.val[base + np + p][h][e]) * ns.per[p];
     return (a + b) * ns.amplitude;
 }
 
-__device__ __forceinline__ void survivor_block(const BatchArgs &a, uint64_t seed, uint64_t r_base, uint32_t jr,
-                                               int &hx, int &hz) {
-    int rx, rz, cx, cz;
-    region_xz(a, r_base + jr, rx, rz);
-    hut_chunk(seed, rx, rz, a.salt, cx, cz);
-    hx = cx * 16 + 3;
-    hz = cz * 16 + 3;
-}
+// Slots that do not depend on the tunnel scale (everything but spaghetti_3d_1 / _2).
+__device__ __forceinline__ int free_slot(int i) { return i < kBaseSp1 ? i : i + 4; }
 
+// Thread t builds table (slot t / kUnits, record t % kUnits).  The tile's survivors are then
+// listed, and every Perlin sample they need — per survivor, slot and height (y = 50, 60) — is an
+// independent task spread over all threads: round 1 the 14 slots that do not depend on the
+// tunnel scale e, then e from the rarity samples, round 2 spaghetti_3d_1 / _2 at (x/e, y/e, z/e).
+// One pass sums the samples in the reference's order (DoublePerlin: sub 0 octaves, then sub 1,
+// times the amplitude; caves.c:83-113).  Entrance(60) is computed for every survivor but only
+// decides those with Entrance(50) < 0, as in lysh.
 __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     EntranceSmem &S = *reinterpret_cast<EntranceSmem *>(smem_raw);
@@ -628,137 +637,138 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
     const int my_slot = tid / kUnits, rr = tid % kUnits;
     if (tid < P1_KINDS) S.hist[tid] = 0;
     fill_grad_table(S.grad, tid);
+    if (tid < kSlotsB) {
+        const int noise = c_slot_c[0][tid][0];
+        S.slot_noise[tid] = noise;
+        S.slot_sub[tid] = c_slot_c[0][tid][1];
+        S.slot_lac[tid] = c_noise[noise].lac[c_slot_c[0][tid][2]];
+    }
     // A full list means the host discards this batch and re-runs it smaller.
     if (a.counters[CNT_OVERFLOW]) return;
     const uint32_t n_rec = min(a.counters[CNT_RECORDS], a.cap_rec);
     const uint32_t n_tiles = (n_rec + kUnits - 1) / kUnits;
-    const SrcCols src{S.perm, S.ox, S.oy, S.oz, S.grad, rr};
     const int my_noise = c_slot_c[0][my_slot][0], my_sub = c_slot_c[0][my_slot][1], my_p = c_slot_c[0][my_slot][2];
-    const bool my_needs_e = (my_noise == N_SPAGHETTI_1 || my_noise == N_SPAGHETTI_2);
-    const NoiseSpec &ns = c_noise[my_noise];
     for (uint32_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const uint32_t ri = tile * kUnits + (uint32_t)rr;
-        const bool valid = ri < n_rec;
-        uint32_t u = 0, off = 0, cnt = 0;
-        uint64_t g = 0, r_base = 0, seed = 0;
-        if (tid == 0) S.max_cnt = 0;
         perm_blocks_init<kUnits>(S.perm, kSlotsB * 64 * kUnits, tid, kThreadsB);
         __syncthreads();
-        if (valid) {
-            u = a.rec_unit[ri];
-            off = a.rec_off[ri];
+        uint32_t cnt = 0;
+        if (ri < n_rec) {
+            const uint32_t u = a.rec_unit[ri], off = a.rec_off[ri];
             cnt = a.rec_cnt[ri];
-            if (u >= a.n_units || off >= a.cap_surv || cnt > a.cap_surv - off) cnt = 0;
-            g = unit_seed_index(a, u);
-            r_base = unit_window(a, u) * a.win;
-            seed = seed_value(a, g);
-            Xr r = octave_rng(ns, seed_fork_of(seed), my_sub, my_p);
-            double ox, oy, oz;
-            perlin_shuffle<kUnits>(S.perm + my_slot * (256 * kUnits) + rr, r, ox, oy, oz);
-            const int o = my_slot * kUnits + rr;
-            S.ox[o] = ox;
-            S.oy[o] = oy;
-            S.oz[o] = oz;
-            if (my_slot == 0 && cnt) atomicMax(&S.max_cnt, cnt);
+            if (u >= a.n_units || off >= a.cap_surv || cnt > a.cap_surv - off || cnt > kRecordCap) cnt = 0;
+            const uint64_t g = unit_seed_index(a, u);
+            const uint64_t seed = seed_value(a, g);
+            if (my_slot == 0) {
+                S.rseed[rr] = seed;
+                S.rg[rr] = g;
+                S.rbase[rr] = unit_window(a, u) * a.win;
+                S.runit[rr] = u;
+                S.roff[rr] = off;
+            }
+            if (cnt) {
+                Xr r = octave_rng(c_noise[my_noise], seed_fork_of(seed), my_sub, my_p);
+                double ox, oy, oz;
+                perlin_shuffle<kUnits>(S.perm + my_slot * (256 * kUnits) + rr, r, ox, oy, oz);
+                const int o = my_slot * kUnits + rr;
+                S.ox[o] = ox;
+                S.oy[o] = oy;
+                S.oz[o] = oz;
+            }
+        }
+        if (tid == 0) S.n_list = 0;
+        __syncthreads();
+        // list this tile's survivors
+        if (my_slot == 0 && cnt) {
+            const uint32_t at = atomicAdd(&S.n_list, cnt);
+            for (uint32_t j = 0; j < cnt; j++) S.emap[at + j] = ((uint32_t)rr << 16) | j;
         }
         __syncthreads();
-        const uint32_t max_cnt = S.max_cnt;
-        for (uint32_t c0 = 0; c0 < max_cnt; c0 += kEntChunk) {
-            // round 1: every slot that does not depend on the tunnel scale
-            if (!my_needs_e) {
-                for (int jj = 0; jj < kEntChunk; jj++) {
-                    const uint32_t j = c0 + jj;
-                    if (j >= cnt) break;
-                    int hx, hz;
-                    survivor_block(a, seed, r_base, a.surv_region[off + j], hx, hz);
-                    for (int h = 0; h < 2; h++) {
-                        double px, py, pz;
-                        cave_point(my_noise, hx, h ? 60 : 50, hz, 1.0, px, py, pz);
-                        S.val[my_slot][h][jj][rr] = slot_sample(src, my_slot, ns, my_sub, my_p, px, py, pz);
-                    }
-                }
+        const uint32_t n_list = S.n_list;
+        for (uint32_t e0 = 0; e0 < n_list; e0 += kEntFlat) {
+            const uint32_t m = min((uint32_t)kEntFlat, n_list - e0);
+            for (uint32_t e = tid; e < m; e += kThreadsB) {
+                const uint32_t em = S.emap[e0 + e];
+                const int r2 = (int)(em >> 16);
+                const uint32_t jr = a.surv_region[S.roff[r2] + (em & 0xFFFFu)];
+                int rx, rz, cx, cz;
+                region_xz(a, S.rbase[r2] + jr, rx, rz);
+                hut_chunk(S.rseed[r2], rx, rz, a.salt, cx, cz);
+                S.hx[e] = cx * 16 + 3;
+                S.hz[e] = cz * 16 + 3;
             }
             __syncthreads();
-            // tunnel scale from the rarity samples
-            if (tid < kEntChunk * kUnits) {
-                const int jj = tid / kUnits, r2 = tid % kUnits;
-                const uint32_t cnt2 = (tile * kUnits + r2 < n_rec) ? a.rec_cnt[tile * kUnits + r2] : 0;
-                if (c0 + jj < cnt2)
-                    for (int h = 0; h < 2; h++)
-                        S.tun[h][jj][r2] = tunnel_scale(combine(S, N_SPAGHETTI_RARITY, kBaseRarity, h, jj, r2));
+            // round 1: 14 slots x 2 heights per survivor
+            for (uint32_t t = tid; t < m * 28; t += kThreadsB) {
+                const uint32_t e = t / 28, rem = t % 28;
+                const int slot = free_slot((int)(rem >> 1)), h = (int)(rem & 1);
+                const int r2 = (int)(S.emap[e0 + e] >> 16);
+                double px, py, pz;
+                cave_point(S.slot_noise[slot], S.hx[e], h ? 60 : 50, S.hz[e], 1.0, px, py, pz);
+                const SrcCols src{S.perm, S.ox, S.oy, S.oz, S.grad, r2};
+                S.val[slot][h][e] = slot_sample(src, slot, S.slot_sub[slot], S.slot_lac[slot], px, py, pz);
             }
             __syncthreads();
-            // round 2: spaghetti_3d_1 / _2 at (x/e, y/e, z/e)
-            if (my_needs_e) {
-                for (int jj = 0; jj < kEntChunk; jj++) {
-                    const uint32_t j = c0 + jj;
-                    if (j >= cnt) break;
-                    int hx, hz;
-                    survivor_block(a, seed, r_base, a.surv_region[off + j], hx, hz);
-                    for (int h = 0; h < 2; h++) {
-                        double px, py, pz;
-                        cave_point(my_noise, hx, h ? 60 : 50, hz, S.tun[h][jj][rr], px, py, pz);
-                        S.val[my_slot][h][jj][rr] = slot_sample(src, my_slot, ns, my_sub, my_p, px, py, pz);
-                    }
-                }
+            for (uint32_t t = tid; t < m * 2; t += kThreadsB) {
+                const uint32_t e = t >> 1;
+                const int h = (int)(t & 1);
+                S.tun[h][e] = tunnel_scale(combine(S, N_SPAGHETTI_RARITY, kBaseRarity, h, (int)e));
             }
             __syncthreads();
-            // combine in the reference's order and decide: thread (jj, r2)
-            if (tid < kEntChunk * kUnits) {
-                const int jj = tid / kUnits, r2 = tid % kUnits;
-                const uint32_t ri2 = tile * kUnits + (uint32_t)r2;
-                uint32_t u2 = 0, off2 = 0, cnt2 = 0;
-                if (ri2 < n_rec) {
-                    u2 = a.rec_unit[ri2];
-                    off2 = a.rec_off[ri2];
-                    cnt2 = a.rec_cnt[ri2];
-                    if (u2 >= a.n_units || off2 >= a.cap_surv || cnt2 > a.cap_surv - off2) cnt2 = 0;
+            // round 2: spaghetti_3d_1 / _2 (4 slots) x 2 heights per survivor
+            for (uint32_t t = tid; t < m * 8; t += kThreadsB) {
+                const uint32_t e = t / 8, rem = t % 8;
+                const int slot = kBaseSp1 + (int)(rem >> 1), h = (int)(rem & 1);
+                const int r2 = (int)(S.emap[e0 + e] >> 16);
+                double px, py, pz;
+                cave_point(S.slot_noise[slot], S.hx[e], h ? 60 : 50, S.hz[e], S.tun[h][e], px, py, pz);
+                const SrcCols src{S.perm, S.ox, S.oy, S.oz, S.grad, r2};
+                S.val[slot][h][e] = slot_sample(src, slot, S.slot_sub[slot], S.slot_lac[slot], px, py, pz);
+            }
+            __syncthreads();
+            // combine in the reference's order and decide
+            for (uint32_t e = tid; e < m; e += kThreadsB) {
+                double ent_v[2];
+                for (int h = 0; h < 2; h++) {
+                    const int y = h ? 60 : 50;
+                    const double te = S.tun[h][e];
+                    double ent = combine(S, N_CAVE_ENTRANCE, kBaseEntrance, h, (int)e);
+                    double t = (10.0 + (double)y) / 40.0;
+                    double cl = t < 0.0 ? 0.3 : (t > 1.0 ? 0.0 : lerp(t, 0.3, 0.0));
+                    double cc = ent + 0.37 + cl;
+                    double tv = combine(S, N_SPAGHETTI_THICKNESS, kBaseThickness, h, (int)e);
+                    double hh = lerp((tv - -1.0) / (1.0 - -1.0), 0.065, 0.088);
+                    double l = combine(S, N_SPAGHETTI_1, kBaseSp1, h, (int)e);
+                    double mm = fabs(te * l) - hh;
+                    double n = combine(S, N_SPAGHETTI_2, kBaseSp2, h, (int)e);
+                    double o = fabs(te * n) - hh;
+                    double pp = clampd(jmax(mm, o), -1.0, 1.0);
+                    double mod = combine(S, N_ROUGHNESS_MODULATOR, kBaseRmod, h, (int)e);
+                    double rgh = combine(S, N_ROUGHNESS, kBaseRough, h, (int)e);
+                    double q = (-0.05 + (-0.05 * mod)) * (-0.4 + fabs(rgh));
+                    ent_v[h] = jmin(cc, pp + q);
                 }
-                const uint32_t j = c0 + jj;
-                if (j < cnt2) {
-                    double ent_v[2];
-                    for (int h = 0; h < 2; h++) {
-                        const int y = h ? 60 : 50;
-                        const double e = S.tun[h][jj][r2];
-                        double ent = combine(S, N_CAVE_ENTRANCE, kBaseEntrance, h, jj, r2);
-                        double t = (10.0 + (double)y) / 40.0;
-                        double cl = t < 0.0 ? 0.3 : (t > 1.0 ? 0.0 : lerp(t, 0.3, 0.0));
-                        double cc = ent + 0.37 + cl;
-                        double tv = combine(S, N_SPAGHETTI_THICKNESS, kBaseThickness, h, jj, r2);
-                        double hh = lerp((tv - -1.0) / (1.0 - -1.0), 0.065, 0.088);
-                        double l = combine(S, N_SPAGHETTI_1, kBaseSp1, h, jj, r2);
-                        double m = fabs(e * l) - hh;
-                        double n = combine(S, N_SPAGHETTI_2, kBaseSp2, h, jj, r2);
-                        double o = fabs(e * n) - hh;
-                        double pp = clampd(jmax(m, o), -1.0, 1.0);
-                        double mod = combine(S, N_ROUGHNESS_MODULATOR, kBaseRmod, h, jj, r2);
-                        double rgh = combine(S, N_ROUGHNESS, kBaseRough, h, jj, r2);
-                        double q = (-0.05 + (-0.05 * mod)) * (-0.4 + fabs(rgh));
-                        ent_v[h] = jmin(cc, pp + q);
-                    }
-                    const uint32_t jr = a.surv_region[off2 + j];
-                    const uint64_t g2 = unit_seed_index(a, u2);
-                    const uint64_t rb2 = unit_window(a, u2) * a.win;
-                    int code = -1;
-                    if (ent_v[0] >= 0) code = P1_ENTRANCE_50;
-                    else if (ent_v[1] >= 0) code = P1_ENTRANCE_60;
-                    if (code >= 0) {
-                        atomicAdd(&S.hist[code], 1u);
-                        note_code(a, g2, rb2 + jr, code, -1);
+                const uint32_t em = S.emap[e0 + e];
+                const int r2 = (int)(em >> 16);
+                const uint32_t jr = a.surv_region[S.roff[r2] + (em & 0xFFFFu)];
+                int code = -1;
+                if (ent_v[0] >= 0) code = P1_ENTRANCE_50;
+                else if (ent_v[1] >= 0) code = P1_ENTRANCE_60;
+                if (code >= 0) {
+                    atomicAdd(&S.hist[code], 1u);
+                    note_code(a, S.rg[r2], S.rbase[r2] + jr, code, -1);
+                } else {
+                    uint32_t di = atomicAdd(&a.counters[CNT_DEEP], 1u);
+                    if (di < a.cap_deep) {
+                        a.deep[2 * di] = S.runit[r2];
+                        a.deep[2 * di + 1] = jr;
                     } else {
-                        uint32_t di = atomicAdd(&a.counters[CNT_DEEP], 1u);
-                        if (di < a.cap_deep) {
-                            a.deep[2 * di] = u2;
-                            a.deep[2 * di + 1] = jr;
-                        } else {
-                            atomicOr(&a.counters[CNT_OVERFLOW], 2u);
-                        }
+                        atomicOr(&a.counters[CNT_OVERFLOW], 2u);
                     }
                 }
             }
             __syncthreads();
         }
-        __syncthreads();
     }
     __syncthreads();
     if (tid < P1_KINDS && S.hist[tid]) atomicAdd(&a.hist[tid], (unsigned long long)S.hist[tid]);
