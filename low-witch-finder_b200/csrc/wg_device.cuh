@@ -10,8 +10,8 @@
 // one sampler slot for all the CTA's units in one byte-interleaved block of 256 rows: byte k of
 // unit u sits at k * U + u (U = units per CTA).  Any lookup is then one multiply-add away from
 // its index, and the 4-byte words of a row are shared by 4 units, so the random lookups of a
-// warp spread over all banks (about 2-way conflicts).  Rare-path kernels use plain contiguous
-// 256-byte tables (stride 1).
+// warp spread over all banks (about 2-way conflicts).  Blocks are padded so that neighbouring
+// slots start in different banks.
 #pragma once
 
 #include <cstdint>
@@ -186,15 +186,19 @@ __host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
 // ------------------------------------------------------------------------------------
 // Perlin permutation tables
 // ------------------------------------------------------------------------------------
-// Fills `words` 32-bit words of a set of byte-interleaved blocks with the identity permutation:
-// a block holds 256 rows of `stride` bytes (one column per table), row k all equal to k.  Called
-// by every thread of the CTA (thread tid of nthreads), followed by a barrier.
-template <int STRIDE>
-__device__ __forceinline__ void perm_blocks_init(uint8_t *base, int words, int tid, int nthreads) {
-    static_assert(STRIDE % 4 == 0, "rows must be whole words");
+// Fills `nblocks` byte-interleaved blocks with the identity permutation: a block holds 256 rows
+// of STRIDE bytes (one column per table), row k all equal to k, and blocks start PITCH bytes
+// apart (PITCH - 256 * STRIDE bytes of padding shift consecutive blocks to other banks).
+// Called by every thread of the CTA (thread tid of nthreads), followed by a barrier.
+template <int STRIDE, int PITCH>
+__device__ __forceinline__ void perm_blocks_init(uint8_t *base, int nblocks, int tid, int nthreads) {
+    static_assert(STRIDE % 4 == 0 && PITCH % 4 == 0 && PITCH >= 256 * STRIDE, "rows must be whole words");
+    constexpr int kRowWords = STRIDE / 4, kPitchWords = PITCH / 4;
     uint32_t *w = reinterpret_cast<uint32_t *>(base);
-    for (int q = tid; q < words; q += nthreads)
-        w[q] = (uint32_t)((q % (64 * STRIDE)) / (STRIDE / 4)) * 0x01010101u;
+    for (int q = tid; q < nblocks * kPitchWords; q += nthreads) {
+        const int in_block = q % kPitchWords;
+        w[q] = (uint32_t)(in_block / kRowWords) * 0x01010101u;   // padding words get junk; never read
+    }
 }
 
 // The 256-step Fisher-Yates shuffle of one Perlin sampler (noise.c:61-72) on an initialised
@@ -233,14 +237,6 @@ struct ColTable {
                __hiloint2double((int)gt[32 + h], 0) * z;
     }
 };
-
-// Same construction into a contiguous 256-byte table (rare-path kernels).
-__device__ __forceinline__ void perlin_build_flat(uint8_t *t, Xr r, double &ox, double &oy, double &oz) {
-    uint32_t *w = reinterpret_cast<uint32_t *>(t);
-#pragma unroll 8
-    for (int q = 0; q < 64; q++) w[q] = 0x03020100u + 0x04040404u * (uint32_t)q;
-    perlin_shuffle<1>(t, r, ox, oy, oz);
-}
 
 
 // ------------------------------------------------------------------------------------

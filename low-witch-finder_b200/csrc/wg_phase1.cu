@@ -81,6 +81,12 @@ __device__ __forceinline__ void note_code(const BatchArgs &a, uint64_t g, uint64
     }
 }
 
+// Bytes between consecutive slot blocks: 256 rows of kUnits columns plus 16 bytes, so the two
+// slots a warp builds at once (one per half-warp) sit 4 banks apart.
+constexpr int kPitch = 256 * kUnits + 16;
+// The ladder kernel keeps its 54 tables as columns of one block (pitch 56 bytes per row).
+constexpr int kLadderStride = 56;
+
 // Table sources: where a sampler's permutation table and origin live.
 struct SrcCols {  // byte-interleaved blocks of kUnits columns, origins [slot][unit]
     const uint8_t *perm;
@@ -88,17 +94,17 @@ struct SrcCols {  // byte-interleaved blocks of kUnits columns, origins [slot][u
     const uint32_t *gt;
     int unit;
     __device__ __forceinline__ double p3(int slot, double x, double y, double z) const {
-        ColTable<kUnits> T{perm + slot * (256 * kUnits) + unit, gt};
+        ColTable<kUnits> T{perm + slot * kPitch + unit, gt};
         int o = slot * kUnits + unit;
         return perlin_3d(T, ox[o], oy[o], oz[o], x, y, z);
     }
 };
-struct SrcFlat {  // contiguous 256-byte tables, origins [slot][3]
+struct SrcFlat {  // the ladder's block: table of slot s in column s, origins [slot][3]
     const uint8_t *perm;
     const double *org;
     const uint32_t *gt;
     __device__ __forceinline__ double p3(int slot, double x, double y, double z) const {
-        ColTable<1> T{perm + slot * 256, gt};
+        ColTable<kLadderStride> T{perm + slot, gt};
         return perlin_3d(T, org[3 * slot], org[3 * slot + 1], org[3 * slot + 2], x, y, z);
     }
 };
@@ -178,7 +184,7 @@ struct ClimateSteps {
 };
 
 struct ClimateSmem {
-    uint8_t perm[kSlotsA * 256 * kUnits];     // slot s, row k, unit u at (s * 256 + k) * kUnits + u
+    uint8_t perm[kSlotsA * kPitch];           // slot s, row k, unit u at s * kPitch + k * kUnits + u
     double ox[kSlotsA * kUnits], oz[kSlotsA * kUnits], hy[kSlotsA * kUnits], fy[kSlotsA * kUnits];
     int jy[kSlotsA * kUnits];
     int2 pos[kChunk * kUnits];                 // hut chunk (cx, cz) of window offset c0 + j, unit u
@@ -236,7 +242,7 @@ __device__ __forceinline__ double climate_sample(const ClimateSmem &S, int iu, i
     const int slot = st.slot[k];
     const int o = slot * kUnits + iu;
     const double sc = st.sc[k], lac = st.lac[k];
-    ColTable<kUnits> T{S.perm + slot * (256 * kUnits) + iu, S.grad};
+    ColTable<kUnits> T{S.perm + slot * kPitch + iu, S.grad};
     return perlin_y0(T, S.ox[o], S.oz[o], S.jy[o], S.hy[o], S.fy[o], keep_precision((xc * sc) * lac),
                      keep_precision((zc * sc) * lac));
 }
@@ -347,14 +353,14 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
 
     // ---- build: every thread shuffles one table ----
     if (!a.single_biome) {
-        perm_blocks_init<kUnits>(S.perm, kSlotsA * 64 * kUnits, tid, kThreadsA);
+        perm_blocks_init<kUnits, kPitch>(S.perm, kSlotsA, tid, kThreadsA);
         __syncthreads();
         if (valid) {
             const int noise = c_slot_a[large][my_slot][0], sub = c_slot_a[large][my_slot][1],
                       p = c_slot_a[large][my_slot][2];
             Xr r = octave_rng(c_noise[noise], seed_fork_of(seed), sub, p);
             double ox, oy, oz;
-            perlin_shuffle<kUnits>(S.perm + my_slot * (256 * kUnits) + uu, r, ox, oy, oz);
+            perlin_shuffle<kUnits>(S.perm + my_slot * kPitch + uu, r, ox, oy, oz);
             const int o = my_slot * kUnits + uu;
             int jy = (int)floor(oy);
             double hy = oy - jy;
@@ -560,7 +566,7 @@ constexpr int kEntFlat = 64;                   // survivors evaluated per round 
 constexpr int kEntList = kUnits * kRecordCap;  // survivors a tile can hold
 
 struct EntranceSmem {
-    uint8_t perm[kSlotsB * 256 * kUnits];
+    uint8_t perm[kSlotsB * kPitch];
     double ox[kSlotsB * kUnits], oy[kSlotsB * kUnits], oz[kSlotsB * kUnits];
     double val[kSlotsB][2][kEntFlat];     // [slot][y=50,60][survivor]
     double tun[2][kEntFlat];              // tunnel scale e per survivor and height
@@ -650,7 +656,7 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
     const int my_noise = c_slot_c[0][my_slot][0], my_sub = c_slot_c[0][my_slot][1], my_p = c_slot_c[0][my_slot][2];
     for (uint32_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const uint32_t ri = tile * kUnits + (uint32_t)rr;
-        perm_blocks_init<kUnits>(S.perm, kSlotsB * 64 * kUnits, tid, kThreadsB);
+        perm_blocks_init<kUnits, kPitch>(S.perm, kSlotsB, tid, kThreadsB);
         __syncthreads();
         uint32_t cnt = 0;
         if (ri < n_rec) {
@@ -669,7 +675,7 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
             if (cnt) {
                 Xr r = octave_rng(c_noise[my_noise], seed_fork_of(seed), my_sub, my_p);
                 double ox, oy, oz;
-                perlin_shuffle<kUnits>(S.perm + my_slot * (256 * kUnits) + rr, r, ox, oy, oz);
+                perlin_shuffle<kUnits>(S.perm + my_slot * kPitch + rr, r, ox, oy, oz);
                 const int o = my_slot * kUnits + rr;
                 S.ox[o] = ox;
                 S.oy[o] = oy;
@@ -782,73 +788,203 @@ void launch_entrance(const BatchArgs &a, int grid, cudaStream_t s) {
 
 // ------------------------------------------------------------------------------------
 // ladder kernel: the rest of lysh_phase1_check_ex for candidates past Entrance(60)
+//
+// One CTA per candidate.  After its 54 tables are built, every Perlin sample the remaining
+// ladder can read is computed in parallel (round 1: everything but spaghetti_3d_1/2; then the
+// tunnel scale per height; round 2: spaghetti_3d_1/2), and one thread walks lysh's ladder in order
+// over the stored samples.  Samples the ladder ends up not reading change nothing.
 // ------------------------------------------------------------------------------------
+constexpr int kLadderHeights = 12;   // maxHeight, the y <= 0 ladder (<= 6), y = 10..40
+constexpr int kFloodHeights = 16;
+
 struct LadderSmem {
-    uint8_t perm[kSlotsC * 256];
+    uint8_t perm[256 * kLadderStride];       // slot s, row k at k * kLadderStride + s
     double org[kSlotsC * 3];
+    double val[kSlotsC][kLadderHeights];     // [slot][height index]
+    double fval[2][kFloodHeights];           // floodedness samples
+    double tun[kLadderHeights];
+    int ys[kLadderHeights];
     uint32_t grad[kGradWords];
 };
 
+// Octave-sum of noise `noise` (slots base .. base + 2 np) over stored samples v[slot * stride].
+__device__ __forceinline__ double combine_vals(int noise, const double *v, int stride) {
+    const NoiseSpec &ns = c_noise[noise];
+    const int np = ns.npresent;
+    double a = 0.0, b = 0.0;
+    for (int p = 0; p < np; p++) a += (ns.amp[p] * v[p * stride]) * ns.per[p];
+    for (int p = 0; p < np; p++) b += (ns.amp[p] * v[(np + p) * stride]) * ns.per[p];
+    return (a + b) * ns.amplitude;
+}
+
 __global__ void __launch_bounds__(kThreadsC) ladder_kernel(BatchArgs a) {
     __shared__ __align__(16) LadderSmem S;
+    const int t = threadIdx.x;
     const int large = a.large_biomes ? 1 : 0;
+    const int cont_noise = large ? N_CONTINENTALNESS_LARGE : N_CONTINENTALNESS;
     if (a.counters[CNT_OVERFLOW]) return;
     const uint32_t n_deep = min(a.counters[CNT_DEEP], a.cap_deep);
-    fill_grad_table(S.grad, threadIdx.x);
+    fill_grad_table(S.grad, t);
     const SrcFlat src{S.perm, S.org, S.grad};
+    const int mh = a.max_height;
+    // heights: [0] maxHeight, then y = 0, -10, ... >= ladderFloor with maxHeight < y, then 10..40
+    int floor_y = (-40 < mh) ? -40 : mh;
+    if (floor_y < -50) floor_y = -50;
+    int nh = 0;
+    if (t == 0) S.ys[nh] = mh;
+    nh++;
+    for (int y = 0; y >= floor_y; y -= 10)
+        if (mh < y) {
+            if (t == 0) S.ys[nh] = y;
+            nh++;
+        }
+    const int first_pos = nh;
+    for (int y = 10; y <= 40; y += 10) {
+        if (t == 0) S.ys[nh] = y;
+        nh++;
+    }
+    const long long nf_ll = mh > 60 ? 0 : ((long long)60 - mh) / 10 + 1;
+    const int nf = nf_ll > kFloodHeights ? 0 : (int)nf_ll;   // more: sampled one by one at the end
+
     for (uint32_t q = blockIdx.x; q < n_deep; q += gridDim.x) {
         const uint32_t u = a.deep[2 * q], jr = a.deep[2 * q + 1];
         const uint64_t g = unit_seed_index(a, u);
         const uint64_t r = unit_window(a, u) * a.win + jr;
         const uint64_t seed = seed_value(a, g);
-        const int t = threadIdx.x;
+        int rx, rz, cx, cz;
+        region_xz(a, r, rx, rz);
+        hut_chunk(seed, rx, rz, a.salt, cx, cz);
+        const int hut_x = cx * 16, hut_z = cz * 16;
+        const int hx = hut_x + 3, hz = hut_z + 3;
+        perm_blocks_init<kLadderStride, 256 * kLadderStride>(S.perm, 1, t, kThreadsC);
+        __syncthreads();
         if (t < kSlotsC) {
             const int noise = c_slot_c[large][t][0], sub = c_slot_c[large][t][1], p = c_slot_c[large][t][2];
             Xr rng = octave_rng(c_noise[noise], seed_fork_of(seed), sub, p);
             double ox, oy, oz;
-            perlin_build_flat(S.perm + t * 256, rng, ox, oy, oz);
+            perlin_shuffle<kLadderStride>(S.perm + t, rng, ox, oy, oz);
             S.org[3 * t] = ox;
             S.org[3 * t + 1] = oy;
             S.org[3 * t + 2] = oz;
         }
         __syncthreads();
+        // round 1: per height, rarity .. rough minus spaghetti_3d_1/2 (8 slots), cave_layer and
+        // cave_cheese (16 slots); cave_entrance (6 slots) at y = 10..40; continentalness; flood
+        const int n_a = nh * 24, n_b = (nh - first_pos) * 6, n_c = 18, n_d = nf * 2;
+        for (int k = t; k < n_a + n_b + n_c + n_d; k += kThreadsC) {
+            int slot, hi = 0;
+            double px, py, pz;
+            if (k < n_a) {
+                hi = k / 24;
+                const int s24 = k % 24;
+                slot = s24 < 4 ? kBaseRarity + s24 : (s24 < 8 ? kBaseRmod + (s24 - 4) : kBaseLayer + (s24 - 8));
+                const int y = S.ys[hi];
+                if (slot < kBaseRmod || slot >= kBaseLayer) {
+                    if (slot < kBaseThickness) {   // rarity at (x*2, y, z*2)
+                        px = (double)(int)((uint32_t)hx * 2u); py = (double)y; pz = (double)(int)((uint32_t)hz * 2u);
+                    } else if (slot < kBaseSp1) {  // thickness
+                        px = (double)hx; py = (double)y; pz = (double)hz;
+                    } else if (slot < kBaseCheese) {   // cave_layer at (x, y*8, z)
+                        px = (double)hx; py = (double)(int)((uint32_t)y * 8u); pz = (double)hz;
+                    } else {                           // cave_cheese at (x, y*2/3, z)
+                        px = (double)hx; py = (double)y * 0.6666666666666666; pz = (double)hz;
+                    }
+                } else {                               // roughness modulator / roughness
+                    px = (double)hx; py = (double)y; pz = (double)hz;
+                }
+            } else if (k < n_a + n_b) {
+                const int kk = k - n_a;
+                hi = first_pos + kk / 6;
+                slot = kBaseEntrance + kk % 6;
+                const int y = S.ys[hi];
+                px = (double)hx * 0.75; py = (double)y * 0.5; pz = (double)hz * 0.75;
+            } else if (k < n_a + n_b + n_c) {
+                slot = kBaseCont + (k - n_a - n_b);
+                px = (hut_x + 8) / 4.0; py = 0.0; pz = (hut_z + 8) / 4.0;
+            } else {
+                const int kk = k - n_a - n_b - n_c;
+                hi = kk >> 1;
+                slot = kBaseFlood + (kk & 1);
+                px = (double)(hut_x + 3); py = (double)(mh + 10 * hi) * 0.67; pz = (double)(hut_z + 3);
+            }
+            const int noise = c_slot_c[large][slot][0], sub = c_slot_c[large][slot][1], p = c_slot_c[large][slot][2];
+            const double v = slot_sample(src, slot, sub, c_noise[noise].lac[p], px, py, pz);
+            if (slot >= kBaseFlood) S.fval[slot - kBaseFlood][hi] = v;
+            else S.val[slot][hi] = v;
+        }
+        __syncthreads();
+        if (t < nh) S.tun[t] = tunnel_scale(combine_vals(N_SPAGHETTI_RARITY, &S.val[kBaseRarity][t], kLadderHeights));
+        __syncthreads();
+        // round 2: spaghetti_3d_1 / _2 at (x/e, y/e, z/e)
+        for (int k = t; k < nh * 4; k += kThreadsC) {
+            const int hi = k >> 2, slot = kBaseSp1 + (k & 3);
+            const double e = S.tun[hi], y = (double)S.ys[hi];
+            const int noise = c_slot_c[large][slot][0], sub = c_slot_c[large][slot][1], p = c_slot_c[large][slot][2];
+            S.val[slot][hi] = slot_sample(src, slot, sub, c_noise[noise].lac[p], (double)hx / e, y / e, (double)hz / e);
+        }
+        __syncthreads();
         if (t == 0) {
-            int rx, rz, cx, cz;
-            region_xz(a, r, rx, rz);
-            hut_chunk(seed, rx, rz, a.salt, cx, cz);
-            const int hut_x = cx * 16, hut_z = cz * 16;
-            const int hx = hut_x + 3, hz = hut_z + 3, mh = a.max_height;
+            // lysh_phase1_check_ex from the cave at maxHeight on (phase1.c:149-199)
+            auto spag = [&](int hi) {
+                const double e = S.tun[hi];
+                const double tv = combine_vals(N_SPAGHETTI_THICKNESS, &S.val[kBaseThickness][hi], kLadderHeights);
+                const double h = lerp((tv - -1.0) / (1.0 - -1.0), 0.065, 0.088);
+                const double l = combine_vals(N_SPAGHETTI_1, &S.val[kBaseSp1][hi], kLadderHeights);
+                const double m = fabs(e * l) - h;
+                const double n = combine_vals(N_SPAGHETTI_2, &S.val[kBaseSp2][hi], kLadderHeights);
+                const double o = fabs(e * n) - h;
+                const double pp = clampd(jmax(m, o), -1.0, 1.0);
+                const double mod = combine_vals(N_ROUGHNESS_MODULATOR, &S.val[kBaseRmod][hi], kLadderHeights);
+                const double rgh = combine_vals(N_ROUGHNESS, &S.val[kBaseRough][hi], kLadderHeights);
+                const double qq = (-0.05 + (-0.05 * mod)) * (-0.4 + fabs(rgh));
+                return pp + qq;
+            };
+            auto chz = [&](int hi) {
+                const double layer = combine_vals(N_CAVE_LAYER, &S.val[kBaseLayer][hi], kLadderHeights);
+                const double av = 4.0 * layer * layer;
+                const double raw = combine_vals(N_CAVE_CHEESE, &S.val[kBaseCheese][hi], kLadderHeights);
+                return av + clampd(0.27 + raw, -1.0, 1.0);
+            };
             int code = P1_ACCEPT;
-            if (spaghetti(src, hx, mh, hz) >= 0 && cheese(src, hx, mh, hz) >= 0) code = P1_CAVE_AT_MAXH;
-            if (code == P1_ACCEPT) {
-                int floor_y = (-40 < mh) ? -40 : mh;
-                if (floor_y < -50) floor_y = -50;
-                for (int y = 0; y >= floor_y; y -= 10)
-                    if (mh < y && spaghetti(src, hx, y, hz) >= 0 && cheese(src, hx, y, hz) >= 0) {
+            if (spag(0) >= 0 && chz(0) >= 0) code = P1_CAVE_AT_MAXH;
+            if (code == P1_ACCEPT)
+                for (int hi = 1; hi < first_pos; hi++)
+                    if (spag(hi) >= 0 && chz(hi) >= 0) {
                         code = P1_LADDER_NEG;
                         break;
                     }
-            }
-            if (code == P1_ACCEPT) {
-                for (int y = 10; y <= 40; y += 10)
-                    if (entrance(src, hx, y, hz) >= 0 && cheese(src, hx, y, hz) >= 0) {
+            if (code == P1_ACCEPT)
+                for (int hi = first_pos; hi < nh; hi++) {
+                    const int y = S.ys[hi];
+                    const double ent = combine_vals(N_CAVE_ENTRANCE, &S.val[kBaseEntrance][hi], kLadderHeights);
+                    const double tt = (10.0 + (double)y) / 40.0;
+                    const double cl = tt < 0.0 ? 0.3 : (tt > 1.0 ? 0.0 : lerp(tt, 0.3, 0.0));
+                    const double cc = ent + 0.37 + cl;
+                    if (jmin(cc, spag(hi)) >= 0 && chz(hi) >= 0) {
                         code = P1_LADDER_POS;
                         break;
                     }
-            }
+                }
             if (code == P1_ACCEPT && !a.single_biome) {
-                // The y = 0 climate sample equals the 3-D sample at y = 0 bit for bit.
-                double c = dbl3d(src, large ? N_CONTINENTALNESS_LARGE : N_CONTINENTALNESS, kBaseCont,
-                                 (hut_x + 8) / 4.0, 0.0, (hut_z + 8) / 4.0);
+                // the y = 0 climate sample equals the 3-D sample at y = 0 bit for bit
+                const double c = combine_vals(cont_noise, &S.val[kBaseCont][0], kLadderHeights);
                 if (c < -0.11) code = P1_CONTINENTALNESS;
             }
             if (code == P1_ACCEPT) {
-                for (int y = mh; y <= 60; y += 10) {
-                    double f = dbl3d(src, N_FLOODEDNESS, kBaseFlood, (double)(hut_x + 3), (double)y * 0.67,
-                                     (double)(hut_z + 3));
-                    if (f > 0.41) {
-                        code = P1_FLOODEDNESS;
-                        break;
+                if (nf_ll <= kFloodHeights) {
+                    for (int fi = 0; fi < nf; fi++)
+                        if (combine_vals(N_FLOODEDNESS, &S.fval[0][fi], kFloodHeights) > 0.41) {
+                            code = P1_FLOODEDNESS;
+                            break;
+                        }
+                } else {
+                    for (long long y = mh; y <= 60; y += 10) {
+                        const double f = dbl3d(src, N_FLOODEDNESS, kBaseFlood, (double)(hut_x + 3),
+                                               (double)y * 0.67, (double)(hut_z + 3));
+                        if (f > 0.41) {
+                            code = P1_FLOODEDNESS;
+                            break;
+                        }
                     }
                 }
             }

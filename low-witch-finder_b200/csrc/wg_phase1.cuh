@@ -46,7 +46,7 @@ constexpr int kSlotsB = 18;         // cave_entrance 6 + six one-octave spaghett
 constexpr int kSlotsC = 54;         // kSlotsB + cave_layer 2 + cave_cheese 14 + continentalness 18 + floodedness 2
 constexpr int kThreadsA = kSlotsA * kUnits;   // one thread per (slot, unit) table
 constexpr int kThreadsB = kSlotsB * kUnits;
-constexpr int kThreadsC = 64;
+constexpr int kThreadsC = 128;
 constexpr int kRecordCap = 64;      // survivors held per unit record in the climate kernel
 constexpr int kChunk = 96;          // regions per unit whose hut positions are staged at a time
 constexpr int kClimateList = 128;   // erosion survivors per chunk finished in parallel (temperature, ridge)
