@@ -1,10 +1,13 @@
 // Seed Check phase-1 kernels; see wg_phase1.cuh for the pipeline.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "wg_device.cuh"
 #include "wg_phase1.cuh"
 
 namespace wg {
+
+namespace cg = cooperative_groups;
 
 __constant__ NoiseSpec c_noise[N_NOISE_COUNT];
 __constant__ ClimateStep c_steps[2][kClimateSteps];     // [large_biomes][step]
@@ -198,9 +201,10 @@ struct ClimateSmem {
     uint32_t n_tlist, t_next, n_clist, n_rlist;
     uint32_t surv[kUnits * kRecordCap];
     uint32_t cnt[kUnits];
-    uint32_t next[kUnits];                     // next window offset to hand out, per unit
     uint32_t end[kUnits];                      // end of the current chunk, per unit
-    uint64_t g[kUnits], rbase[kUnits];         // seed index and first region of each unit
+    uint64_t g[kUnits], rbase[kUnits], seed[kUnits];   // seed index, first region, world seed
+    uint32_t col0[kUnits];                     // column of the unit's first region in its rect row
+    int row0[kUnits];                          // rz of the unit's first region
     unsigned int hist[P1_KINDS + kTiers];
     uint32_t grad[kGradWords];
     ClimateSteps steps;
@@ -236,6 +240,27 @@ __device__ __forceinline__ void climate_reject(ClimateSmem &S, const BatchArgs &
     note_code(a, S.g[iu], S.rbase[iu] + j, code, tier);
 }
 
+// Erosion rejections are counted per thread in registers (16-bit fields, tiers 0-3 and 4-6) and
+// added to the histogram once at the end; a shared counter hit by most lanes of a warp at once
+// would serialise.  A field cannot overflow: per chunk a thread rejects at most 6 regions in the
+// tier-0 pass and at most kTierList (768) afterwards, over at most 43 chunks (4,096 / 96).
+struct TierCounts {
+    uint64_t lo = 0, hi = 0;
+    __device__ __forceinline__ void add(int tier) {
+        if (tier < 4) lo += 1ull << (16 * tier);
+        else hi += 1ull << (16 * (tier - 4));
+    }
+    __device__ __forceinline__ uint32_t get(int tier) const {
+        return (uint32_t)(((tier < 4 ? lo : hi) >> (16 * (tier & 3))) & 0xFFFFu);
+    }
+};
+
+__device__ __forceinline__ void erosion_reject(const ClimateSmem &S, const BatchArgs &a, TierCounts &tc, int iu,
+                                               uint32_t j, int tier) {
+    tc.add(tier);
+    note_code(a, S.g[iu], S.rbase[iu] + j, P1_EROSION, tier);
+}
+
 // One y = 0 Perlin sample of climate step k for unit iu at climate point (xc, zc).
 __device__ __forceinline__ double climate_sample(const ClimateSmem &S, int iu, int k, double xc, double zc) {
     const ClimateSteps &st = S.steps;
@@ -254,9 +279,10 @@ __device__ __forceinline__ void climate_point(const ClimateSmem &S, int iu, uint
 }
 
 // The erosion tiers from step k0 for one region (e = unit << 16 | offset in the chunk), one Perlin
-// sample per loop trip.  A region that passes the last tier is handed to the climate list; if the
-// list is full, this thread also runs its temperature and ridge steps.
-__device__ void climate_rest(ClimateSmem &S, const BatchArgs &a, uint32_t e, uint32_t c0, int k0, double sum,
+// sample per loop trip, run by one thread: the path for a tier-0 survivor that finds the tier list
+// full.  A region that passes the last tier is handed to the climate list; if that list is full
+// too, this thread also runs its temperature and ridge steps.
+__device__ void climate_rest(ClimateSmem &S, const BatchArgs &a, TierCounts &tc, uint32_t e, uint32_t c0, int k0, double sum,
                              double xc, double zc) {
     const ClimateSteps &st = S.steps;
     const int iu = (int)(e >> 16);
@@ -268,13 +294,13 @@ __device__ void climate_rest(ClimateSmem &S, const BatchArgs &a, uint32_t e, uin
         switch (st.act[k]) {
             case ACT_TIER:
                 if (sum * st.amp[k] < st.thr[k]) {
-                    climate_reject(S, a, iu, j, P1_EROSION, st.tier[k]);
+                    erosion_reject(S, a, tc, iu, j, st.tier[k]);
                     return;
                 }
                 break;
             case ACT_TIER_LAST:
                 if (sum * st.amp[k] < st.thr[k]) {
-                    climate_reject(S, a, iu, j, P1_EROSION, st.tier[k]);
+                    erosion_reject(S, a, tc, iu, j, st.tier[k]);
                     return;
                 } else {
                     const uint32_t q = atomicAdd(&S.n_clist, 1u);
@@ -346,10 +372,15 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
     const uint64_t seed = valid ? seed_value(a, g) : 0;
     const uint32_t len = valid ? window_len(a, w) : 0;
     if (tid < kUnits) {
+        const uint64_t rbase = w * a.win;
         S.cnt[tid] = 0;
         S.g[tid] = g;
-        S.rbase[tid] = w * a.win;
+        S.rbase[tid] = rbase;
+        S.seed[tid] = seed;
+        S.col0[tid] = (uint32_t)(rbase % (uint64_t)a.rw);
+        S.row0[tid] = a.rz0 + (int)(rbase / (uint64_t)a.rw);
     }
+    TierCounts tc;
 
     // ---- build: every thread shuffles one table ----
     if (!a.single_biome) {
@@ -381,22 +412,18 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
 
     for (uint32_t c0 = 0; c0 < cta_len; c0 += kChunk) {
         // ---- stage the hut chunks of this chunk of regions, all units at once ----
+        if (tid < kUnits) S.end[tid] = (valid && c0 < len) ? min(len, c0 + (uint32_t)kChunk) : c0;
+        __syncthreads();
         for (int q = tid; q < kChunk * kUnits; q += kThreadsA) {
-            const int qu = q % kUnits, qj = q / kUnits;
-            const uint32_t qunit = blockIdx.x * kUnits + (uint32_t)qu;
-            if (qunit >= a.n_units) continue;
-            const uint64_t qg = unit_seed_index(a, qunit), qw = unit_window(a, qunit);
-            const uint32_t j = c0 + (uint32_t)qj;
-            if (j >= window_len(a, qw)) continue;
-            const uint64_t qr = qw * a.win + j;
-            int rx, rz, cx, cz;
-            region_xz(a, qr, rx, rz);
-            hut_chunk(seed_value(a, qg), rx, rz, a.salt, cx, cz);
+            const int qu = q % kUnits;
+            const uint32_t j = c0 + (uint32_t)(q / kUnits);
+            if (j >= S.end[qu]) continue;
+            const uint32_t t = S.col0[qu] + j;   // region offset from the unit's first row start
+            const uint32_t rw = (uint32_t)a.rw;
+            const int rz = S.row0[qu] + (int)(t / rw), rx = a.rx0 + (int)(t % rw);
+            int cx, cz;
+            hut_chunk(S.seed[qu], rx, rz, a.salt, cx, cz);
             S.pos[q] = make_int2(cx, cz);
-        }
-        if (tid < kUnits) {
-            S.next[tid] = c0;
-            S.end[tid] = (valid && c0 < len) ? min(len, c0 + (uint32_t)kChunk) : c0;
         }
         if (tid == 0) {
             S.n_tlist = 0;
@@ -422,33 +449,91 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                 double sum = 0.0;
                 sum += (st.c1[0] * climate_sample(S, iu, 0, xc, zc)) * st.c2[0];
                 sum += (st.c1[1] * climate_sample(S, iu, 1, xc, zc)) * st.c2[1];
-                if (sum * st.amp[1] < st.thr[1]) {
-                    climate_reject(S, a, iu, j, P1_EROSION, st.tier[1]);
+                const bool pass = !(sum * st.amp[1] < st.thr[1]);
+                // warp-aggregated append of the survivors to the tier list
+                cg::coalesced_group grp = cg::coalesced_threads();
+                const unsigned m = grp.ballot(pass);
+                uint32_t base = 0;
+                if (grp.thread_rank() == 0 && m) base = atomicAdd(&S.n_tlist, (uint32_t)__popc(m));
+                base = grp.shfl(base, 0);
+                if (!pass) {
+                    erosion_reject(S, a, tc, iu, j, st.tier[1]);
                 } else {
-                    const uint32_t t = atomicAdd(&S.n_tlist, 1u);
+                    const uint32_t t = base + (uint32_t)__popc(m & ((1u << grp.thread_rank()) - 1u));
                     if (t < kTierList) {
                         S.tlist[t] = ((uint32_t)iu << 16) | jl;
                         S.tsum[t] = sum;
                     } else {
                         // list full: this thread walks the region through the rest itself
-                        uint32_t e = ((uint32_t)iu << 16) | jl;
-                        climate_rest(S, a, e, c0, 2, sum, xc, zc);
+                        climate_rest(S, a, tc, ((uint32_t)iu << 16) | jl, c0, 2, sum, xc, zc);
                     }
                 }
             }
         }
         __syncthreads();
 
-        // ---- the remaining erosion tiers for the tier-0 survivors, any thread any region ----
+        // ---- the remaining erosion tiers (and, past a full climate list, temperature and ridge)
+        // for the tier-0 survivors: one Perlin sample per loop trip, a thread whose region is done
+        // takes the next one from the shared list at once ----
         {
             const uint32_t n_t = min(S.n_tlist, (uint32_t)kTierList);
+            uint32_t e = 0, item = 0;
+            int iu = 0, k = 0;
+            bool have = false;
+            double xc = 0.0, zc = 0.0, sum = 0.0, sum_a = 0.0;
             for (;;) {
-                const uint32_t t = atomicAdd(&S.t_next, 1u);
-                if (t >= n_t) break;
-                const uint32_t e = S.tlist[t];
-                double xc, zc;
-                climate_point(S, (int)(e >> 16), e & 0xFFFFu, xc, zc);
-                climate_rest(S, a, e, c0, 2, S.tsum[t], xc, zc);
+                if (!have) {
+                    cg::coalesced_group grp = cg::coalesced_threads();
+                    uint32_t base = 0;
+                    if (grp.thread_rank() == 0) base = atomicAdd(&S.t_next, grp.size());
+                    item = grp.shfl(base, 0) + grp.thread_rank();
+                    if (item >= n_t) break;
+                    e = S.tlist[item];
+                    iu = (int)(e >> 16);
+                    climate_point(S, iu, e & 0xFFFFu, xc, zc);
+                    sum = S.tsum[item];
+                    k = 2;
+                    have = true;
+                }
+                const uint32_t j = c0 + (e & 0xFFFFu);
+                const double v = climate_sample(S, iu, k, xc, zc);
+                sum += (st.c1[k] * v) * st.c2[k];
+                const int act = st.act[k];
+                bool done = false;
+                if (act == ACT_TIER || act == ACT_TIER_LAST) {
+                    if (sum * st.amp[k] < st.thr[k]) {
+                        erosion_reject(S, a, tc, iu, j, st.tier[k]);
+                        done = true;
+                    } else if (act == ACT_TIER_LAST) {
+                        const uint32_t qq = atomicAdd(&S.n_clist, 1u);
+                        if (qq < kClimateList) {
+                            S.clist[qq] = e;
+                            done = true;
+                        } else {
+                            sum = 0.0;   // climate list full: finish it here
+                        }
+                    }
+                } else if (act == ACT_END_SUB_A) {
+                    sum_a = sum;
+                    sum = 0.0;
+                } else if (act == ACT_TEMPERATURE) {
+                    const double t = (sum_a + sum) * st.amp[k];
+                    const bool bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
+                    if (bad) {
+                        climate_reject(S, a, iu, j, P1_TEMPERATURE, -1);
+                        done = true;
+                    }
+                    sum = 0.0;
+                } else if (act == ACT_RIDGE) {
+                    const double rg = (sum_a + sum) * st.amp[k];
+                    if ((rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91))
+                        climate_reject(S, a, iu, j, P1_RIDGE, -1);
+                    else
+                        keep_survivor(S, a, iu, j);   // climate survivor, not yet a verdict
+                    done = true;
+                }
+                if (done) have = false;
+                else k++;
             }
         }
         __syncthreads();
@@ -513,6 +598,18 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
         }
         __syncthreads();
     }
+
+    // ---- erosion rejections counted in registers: one warp sum per tier ----
+    {
+        uint32_t total = 0;
+        for (int t = 0; t < kTiers; t++) {
+            const uint32_t v = __reduce_add_sync(0xFFFFFFFFu, tc.get(t));
+            total += v;
+            if ((tid & 31) == 0 && v) atomicAdd(&S.hist[P1_KINDS + t], v);
+        }
+        if ((tid & 31) == 0 && total) atomicAdd(&S.hist[P1_EROSION], total);
+    }
+    __syncthreads();
 
     // ---- one record per unit with survivors ----
     if (tid < kUnits && valid) {
