@@ -133,6 +133,75 @@ int wg_seed_check_noalloc(const int64_t *d_seeds, uint64_t gen_base, uint32_t n_
                           int rx0, int rx1, int rz0, int rz1,
                           wg_candidate *d_out, uint32_t cap, uint32_t *n_out, void *stream);
 
+/* ---------------- phase 2: confirmation of a hut (lysh_eval_hut) ---------------- */
+
+/* One confirmed (or rejected) hut: the fields of lysh_hut_result
+ * (engine/tools/lysh/src/eval.h:63-85), same meanings and units. */
+typedef struct {
+    int32_t hut_x, hut_z;        /* hut origin (block), = chunk * 16 */
+    int32_t rx, rz;              /* its region (floorDiv by 32 chunks) */
+    int32_t dir;                 /* orientation: 0 N, 1 E, 2 S, 3 W */
+    int32_t axis_z;              /* 1 -> footprint 7 (x) by 9 (z), 0 -> 9 by 7 */
+    int32_t size_x, size_z;
+    int32_t avg_y;               /* post-carver footprint height sum / 63 (truncated) */
+    int32_t wet_columns;         /* footprint columns with water above y = 62 */
+    int32_t flooded, all_dry;    /* wet_columns == 63 / == 0 */
+    int32_t ok;                  /* biome ok && !flooded && avg_y <= max_y */
+    int32_t reject;              /* 0 ok, 1 avg_y > max_y, 2 flooded, 3 biome */
+    int32_t biome_ok, biome_winner;
+    int32_t biome_qx, biome_qy, biome_qz, biome_occ_y;
+    int64_t sum_h;               /* footprint height sum (pre-carver when the flood short-circuit applied) */
+    int64_t biome_t[6];          /* quantized temperature, humidity, continentalness, erosion, depth, weirdness */
+} wg_hut_result;
+
+/* Phase 2 for n huts: hut i of world seed seeds[i] at block (hut_x[i], hut_z[i]) (the
+ * chunk origin of a phase-1 survivor), judged against max_y.  out[0..n) receives
+ * lysh_eval_hut's result for each (engine/tools/lysh/src/eval.c:121-242): orientation,
+ * the real biome gate at the chunk centre, the y = 62 aquifer flood test of the 63 footprint
+ * columns, the post-carver footprint heights.  The search context's version and preset come
+ * from opts (eval.c:70-107).  Replaces lysh_eval_hut and the `lysh hut` confirmations
+ * hunt.py spawns per candidate. */
+int wg_eval_huts(wg_engine *e, const int64_t *seeds, const int32_t *hut_x, const int32_t *hut_z, uint64_t n,
+                 const wg_opts *opts, int max_y, wg_hut_result *out);
+
+/* Counts of a graded scan: lysh_hut_grade (engine/tools/lysh/src/eval.h:100-114). */
+typedef struct {
+    int64_t scanned;             /* regions scanned */
+    int64_t evaluated;           /* phase-1 survivors judged by phase 2 */
+    int64_t accepted;
+    int64_t rejected_y, rejected_flood, rejected_biome;
+    int32_t hits_written;        /* rows written to hits */
+    double ms;                   /* wall time of the call */
+    double p2_ms;                /* of which phase 2 */
+} wg_hut_grade;
+
+#define WG_HUT_GRADE_INTS 12
+
+/* Phase 1 + phase 2 over [rx0,rx1) x [rz0,rz1) for one seed: lysh_grade_scan
+ * (engine/tools/lysh/src/eval.c:481-492, session band :405-477).  hits (may be NULL) receives
+ * up to hits_cap rows of WG_HUT_GRADE_INTS ints for the accepted huts, in region order
+ * (rz outer, rx inner): hutX, hutZ, rx, rz, dir, avg_y, flooded, ok, wet_columns, size_x,
+ * size_z, reject (eval.c:258-271). */
+int wg_grade_scan(wg_engine *e, int64_t seed, const wg_opts *opts, int max_height,
+                  int rx0, int rx1, int rz0, int rz1, int salt, int max_y,
+                  int32_t *hits, int32_t hits_cap, wg_hut_grade *grade);
+
+/* Phase-2 parity probes: out[i] = the value of `kind` at block (xyz[3i], xyz[3i+1],
+ * xyz[3i+2]) in world `seed` (y ignored where the quantity is per column).  Kinds and the
+ * reference function each one equals:
+ *   0 blended base noise                lysh_interp_calculate_noise_261   interp_noise.c:100
+ *   1 density before interpolation      lysh_phase2_density_raw_at        phase2.c:151
+ *   2 preliminary surface level         lysh_preliminary_surface_level    column_top.c:94
+ *   3/4/5 continentalness / erosion / weirdness at biome (x>>2, z>>2)     terrain.c:22
+ *   6/7/8 terrain offset / factor / peaks (26.1 ridges_folded)            spline.c:112
+ *   9 computeFluid: level * 4 + type (0 solid, 1 air, 2 water, 3 lava)    aquifer.c:327
+ *   10 interpolated final density       lysh_phase2_density_at            phase2.c:161
+ *   11 block state before carvers       lysh_phase2_block_at              phase2.c:309
+ *   12 surface height before carvers    lysh_phase2_height_pre_carver     phase2.c:318
+ *   13 surface height after carvers     lysh_phase2_height                phase2.c:438 */
+int wg_p2_probe(wg_engine *e, int64_t seed, const wg_opts *opts, int kind, const int32_t *xyz, uint64_t n,
+                double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,7 +58,29 @@ CANDIDATE_DTYPE = np.dtype([("seed_index", "<u8"), ("seed", "<i8"), ("rx", "<i4"
 
 # Every symbol include/witchgpu.h declares.
 EXPORTS = ("wg_engine_open", "wg_engine_close", "wg_engine_error", "wg_parse_version", "wg_parse_preset",
-           "wg_seed_check", "wg_seed_check_device", "wg_phase1_codes", "wg_seed_check_noalloc")
+           "wg_seed_check", "wg_seed_check_device", "wg_phase1_codes", "wg_seed_check_noalloc",
+           "wg_eval_huts", "wg_grade_scan", "wg_p2_probe")
+
+# wg_hut_result (lysh_hut_result's fields, engine/tools/lysh/src/eval.h:63-85).
+HUT_DTYPE = np.dtype([("hut_x", "<i4"), ("hut_z", "<i4"), ("rx", "<i4"), ("rz", "<i4"), ("dir", "<i4"),
+                      ("axis_z", "<i4"), ("size_x", "<i4"), ("size_z", "<i4"), ("avg_y", "<i4"),
+                      ("wet_columns", "<i4"), ("flooded", "<i4"), ("all_dry", "<i4"), ("ok", "<i4"),
+                      ("reject", "<i4"), ("biome_ok", "<i4"), ("biome_winner", "<i4"), ("biome_qx", "<i4"),
+                      ("biome_qy", "<i4"), ("biome_qz", "<i4"), ("biome_occ_y", "<i4"), ("sum_h", "<i8"),
+                      ("biome_t", "<i8", (6,))])
+HUT_REJECTS = ("ok", "avg_y > max_y", "flooded", "biome")
+GRADE_INTS = 12   # hutX, hutZ, rx, rz, dir, avg_y, flooded, ok, wet, size_x, size_z, reject
+
+# wg_p2_probe kinds (include/witchgpu.h).
+PROBE_KINDS = {"base_noise": 0, "density_raw": 1, "column_top": 2, "continentalness": 3, "erosion": 4,
+               "weirdness": 5, "offset": 6, "factor": 7, "peaks": 8, "fluid": 9, "density": 10, "block": 11,
+               "height_pre": 12, "height": 13}
+
+
+class HutGrade(C.Structure):
+    _fields_ = [("scanned", C.c_int64), ("evaluated", C.c_int64), ("accepted", C.c_int64),
+                ("rejected_y", C.c_int64), ("rejected_flood", C.c_int64), ("rejected_biome", C.c_int64),
+                ("hits_written", C.c_int32), ("ms", C.c_double), ("p2_ms", C.c_double)]
 
 _lib = None
 
@@ -89,6 +111,10 @@ def library() -> C.CDLL:
     lib.wg_phase1_codes.argtypes = common + [vp, vp]
     lib.wg_seed_check_noalloc.argtypes = [vp, u64, C.c_uint32, C.POINTER(Opts), i32, i32, i32, i32, i32, i32,
                                           vp, C.c_uint32, C.POINTER(C.c_uint32), vp]
+    lib.wg_eval_huts.argtypes = [vp, vp, vp, vp, u64, C.POINTER(Opts), i32, vp]
+    lib.wg_grade_scan.argtypes = [vp, i64, C.POINTER(Opts), i32, i32, i32, i32, i32, i32, i32, vp, C.c_int32,
+                                  C.POINTER(HutGrade)]
+    lib.wg_p2_probe.argtypes = [vp, i64, C.POINTER(Opts), i32, vp, u64, vp]
     _lib = lib
     return lib
 
@@ -208,6 +234,49 @@ class Engine:
         if rc != WG_OK:
             raise self._err(rc, "wg_phase1_codes")
         return codes, tiers
+
+    def eval_huts(self, seeds, hut_x, hut_z, max_y: int = -50, version: str = DEFAULT_VERSION,
+                  preset: str = "NORMAL", opts: Opts | None = None) -> np.ndarray:
+        """Phase 2 (lysh_eval_hut) for each (seed, hut_x, hut_z): a HUT_DTYPE array."""
+        s = as_seed_array(seeds)
+        hx = np.ascontiguousarray(hut_x, dtype=np.int32)
+        hz = np.ascontiguousarray(hut_z, dtype=np.int32)
+        if not (len(s) == len(hx) == len(hz)):
+            raise ValueError("seeds, hut_x and hut_z differ in length")
+        o = opts if opts is not None else make_opts(version, preset)
+        out = np.zeros(len(s), HUT_DTYPE)
+        rc = library().wg_eval_huts(self._h, s.ctypes.data, hx.ctypes.data, hz.ctypes.data, len(s), C.byref(o),
+                                    max_y, out.ctypes.data)
+        if rc != WG_OK:
+            raise self._err(rc, "wg_eval_huts")
+        return out
+
+    def grade_scan(self, seed: int, rect, max_height: int = -50, max_y: int = -50, version: str = DEFAULT_VERSION,
+                   preset: str = "NORMAL", salt: int = 0, cap: int = 4096,
+                   opts: Opts | None = None) -> tuple[np.ndarray, dict]:
+        """Phase 1 + phase 2 over rect for one seed (lysh_grade_scan): (hits [n, 12] int32, counts)."""
+        o = opts if opts is not None else make_opts(version, preset)
+        hits = np.zeros((cap, GRADE_INTS), np.int32)
+        g = HutGrade()
+        rc = library().wg_grade_scan(self._h, to_signed(int(seed)), C.byref(o), max_height, *rect, salt, max_y,
+                                     hits.ctypes.data, cap, C.byref(g))
+        if rc != WG_OK:
+            raise self._err(rc, "wg_grade_scan")
+        counts = {k: getattr(g, k) for k, _ in HutGrade._fields_}
+        return hits[:g.hits_written].copy(), counts
+
+    def p2_probe(self, seed: int, kind, xyz, version: str = DEFAULT_VERSION, preset: str = "NORMAL",
+                 opts: Opts | None = None) -> np.ndarray:
+        """Phase-2 parity probes (wg_p2_probe) at block points xyz [n, 3]."""
+        k = PROBE_KINDS[kind] if isinstance(kind, str) else int(kind)
+        pts = np.ascontiguousarray(np.asarray(xyz, dtype=np.int32).reshape(-1, 3))
+        o = opts if opts is not None else make_opts(version, preset)
+        out = np.zeros(len(pts), np.float64)
+        rc = library().wg_p2_probe(self._h, to_signed(int(seed)), C.byref(o), k, pts.ctypes.data, len(pts),
+                                   out.ctypes.data)
+        if rc != WG_OK:
+            raise self._err(rc, "wg_p2_probe")
+        return out
 
 
 def as_seed_array(seeds) -> np.ndarray:

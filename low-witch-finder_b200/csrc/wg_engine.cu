@@ -11,6 +11,7 @@
 
 #include "../../include/witchgpu.h"
 #include "wg_catalog.h"
+#include "wg_engine_impl.h"
 #include "wg_phase1.cuh"
 
 using namespace wg;
@@ -71,32 +72,6 @@ void wg::build_climate_steps(const NoiseSpec *specs, int erosion, int temperatur
         base += 2 * n.npresent;
     }
 }
-
-struct wg_engine {
-    int device = 0;
-    int sm_count = 148;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    std::string err;
-
-    uint32_t *rec_unit = nullptr, *rec_off = nullptr, *rec_cnt = nullptr, *surv = nullptr, *deep = nullptr;
-    Candidate *out = nullptr;
-    uint32_t *counters = nullptr;
-    unsigned long long *hist = nullptr;
-    uint32_t *h_counters = nullptr;         // pinned
-    unsigned long long *h_hist = nullptr;   // pinned
-    cudaEvent_t kev[4] = {nullptr, nullptr, nullptr, nullptr};   // around the three kernels of a batch
-    int64_t *d_seed_list = nullptr;
-    uint64_t d_seed_cap = 0;
-
-    int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
-        char buf[512];
-        if (e != cudaSuccess) std::snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
-        else std::snprintf(buf, sizeof buf, "%s", what);
-        err = buf;
-        return code;
-    }
-};
 
 #define WG_CUDA(call, what)                                        \
     do {                                                           \
@@ -368,6 +343,7 @@ void wg_engine_close(wg_engine *eng) {
     cudaFree(eng->counters);
     cudaFree(eng->hist);
     cudaFree(eng->d_seed_list);
+    p2_release(eng);
     cudaFreeHost(eng->h_counters);
     cudaFreeHost(eng->h_hist);
     if (eng->ev0) cudaEventDestroy(eng->ev0);

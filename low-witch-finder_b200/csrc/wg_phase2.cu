@@ -1,0 +1,1401 @@
+// Phase 2 kernels: see wg_phase2.cuh for the job structure.
+//
+// Every floating-point expression keeps the reference's operation order (the library is built
+// with -fmad=false, the reference with -ffp-contract=off), so densities, heights and verdicts
+// are bit-identical to lysh's.  Reference functions restated here, by file:
+//
+//   noise.c:200-290          Perlin / octave / DoublePerlin sampling, legacy octave creation
+//   interp_noise.c:100-139   the 26.1 blended base noise (old_blended_noise)
+//   terrain.c:22-44          terrain info at biome coordinates
+//   spline.c:10-131          float spline evaluation, normalized weirdness (1.18 and 26.1)
+//   column_top.c:1-130       preliminary surface level and overworld offset
+//   density.c:1-281          the non-interpolated density column, noodle children, squeeze
+//   phase2.c:44-194,318-456  interpolation grid, density / block / height queries
+//   aquifer.c:1-563          computeFluid / computeSubstance (26.1 NoiseBasedAquifer)
+//   carver.c:1-523           cave / canyon carvers over a target chunk
+//   biome.c:17-156           the biome R-tree search and the swamp-hut biome gate
+//   eval.c:41-242            orientation, wet columns, flood short-circuit, verdict
+#include <cuda_runtime.h>
+
+#include "wg_phase2.cuh"
+
+namespace wg {
+namespace {
+
+// ------------------------------------------------------------------------------------
+// Java-semantics helpers (mcmath.h)
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ double mc_clamp(double v, double lo, double hi) {
+    if (v < lo) return lo;
+    if (v > hi) return hi;
+    return v;
+}
+__device__ __forceinline__ double mc_lerp(double t, double a, double b) { return a + t * (b - a); }
+__device__ __forceinline__ double mc_clamped_lerp(double a, double b, double t) {
+    if (t < 0.0) return a;
+    if (t > 1.0) return b;
+    return mc_lerp(t, a, b);
+}
+__device__ __forceinline__ double mc_lerp_progress(double v, double a, double b) { return (v - a) / (b - a); }
+__device__ __forceinline__ double mc_lerp_from_progress(double v, double mn, double mx, double a, double b) {
+    return mc_lerp(mc_lerp_progress(v, mn, mx), a, b);
+}
+__device__ __forceinline__ int floor_div(int a, int b) {
+    int q = a / b, r = a % b;
+    if (r != 0 && ((r < 0) != (b < 0))) q--;
+    return q;
+}
+__device__ __forceinline__ double ygrad(double y, double from_y, double to_y, double from_v, double to_v) {
+    double t = mc_clamp((y - from_y) / (to_y - from_y), 0.0, 1.0);
+    return mc_lerp(t, from_v, to_v);
+}
+
+// x^3 rounded once (the reference calls pow(x, 3.0), which glibc rounds correctly): the exact
+// square as a double-double (Dekker's two-product, with the fused multiply-add used only to
+// recover the rounding error exactly), then the exact cube's leading parts summed once.
+__device__ __forceinline__ double cube_rn(double x) {
+    double s = x * x;
+    double se = __fma_rn(x, x, -s);          // x*x = s + se exactly
+    double c1 = s * x;
+    double c1e = __fma_rn(s, x, -c1);        // s*x = c1 + c1e exactly
+    double c2 = se * x;                      // tail of the cube (its own rounding is far below 1 ulp of c1)
+    return c1 + (c1e + c2);
+}
+
+// ------------------------------------------------------------------------------------
+// Perlin sampling (noise.c:200-290)
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ double gsel(uint32_t codes, int h) {
+    const uint32_t c = (codes >> (2 * h)) & 3u;
+    return c == 1u ? 1.0 : (c == 3u ? -1.0 : 0.0);
+}
+__device__ __forceinline__ double p2_grad(int hash, double x, double y, double z) {
+    const int h = hash & 15;
+    return gsel(kGradCodeX, h) * x + gsel(kGradCodeY, h) * y + gsel(kGradCodeZ, h) * z;
+}
+
+__device__ double p2_perlin_at(const P2Perlin &P, int i, int j, int k, double x, double y, double z,
+                               double fade_y_of) {
+    const uint8_t *pm = P.perm;
+    int a = pm[i & 255], b = pm[(i + 1) & 255];
+    int c = pm[(a + j) & 255], d = pm[(a + j + 1) & 255];
+    int e = pm[(b + j) & 255], f = pm[(b + j + 1) & 255];
+    double v000 = p2_grad(pm[(c + k) & 255], x, y, z);
+    double v100 = p2_grad(pm[(e + k) & 255], x - 1, y, z);
+    double v010 = p2_grad(pm[(d + k) & 255], x, y - 1, z);
+    double v110 = p2_grad(pm[(f + k) & 255], x - 1, y - 1, z);
+    double v001 = p2_grad(pm[(c + k + 1) & 255], x, y, z - 1);
+    double v101 = p2_grad(pm[(e + k + 1) & 255], x - 1, y, z - 1);
+    double v011 = p2_grad(pm[(d + k + 1) & 255], x, y - 1, z - 1);
+    double v111 = p2_grad(pm[(f + k + 1) & 255], x - 1, y - 1, z - 1);
+    double fx = fade(x), fy = fade(fade_y_of), fz = fade(z);
+    double x00 = lerp(fx, v000, v100), x10 = lerp(fx, v010, v110);
+    double x01 = lerp(fx, v001, v101), x11 = lerp(fx, v011, v111);
+    return lerp(fz, lerp(fy, x00, x10), lerp(fy, x01, x11));
+}
+
+// lysh_perlin_sample (noise.c:234-250): y_scale / y_max fold the y coordinate (legacy octaves).
+__device__ double p2_perlin(const P2Perlin &P, double x, double y, double z, double ys, double ymax) {
+    double d = x + P.ox, e = y + P.oy, f = z + P.oz;
+    int i = (int)floor(d), j = (int)floor(e), k = (int)floor(f);
+    double g = d - i, h = e - j, l = f - k;
+    double m;
+    if (ys != 0.0) {
+        double nn = (ymax >= 0.0 && ymax < h) ? ymax : h;
+        m = floor(nn / ys + 1.0000000116860974E-7) * ys;
+    } else {
+        m = 0.0;
+    }
+    return p2_perlin_at(P, i, j, k, g, h - m, l, h);
+}
+
+__device__ double p2_octaves(const P2World &W, const P2Spec &S, int sub, double x, double y, double z) {
+    double value = 0.0;
+    const P2Perlin *base = W.perl + S.first_slot + sub * S.npresent;
+    for (int p = 0; p < S.npresent; p++) {
+        const double lac = S.lac[p];
+        double v = p2_perlin(base[p], keep_precision(x * lac), keep_precision(y * lac), keep_precision(z * lac),
+                             0.0, 0.0);
+        value += (S.amp[p] * v) * S.per[p];
+    }
+    return value;
+}
+
+__device__ double p2_dbl(const P2Tables &T, const P2World &W, int q, double x, double y, double z) {
+    const P2Spec &S = T.spec[W.large][q];
+    return (p2_octaves(W, S, 0, x, y, z) + p2_octaves(W, S, 1, x * kDblScale, y * kDblScale, z * kDblScale)) *
+           S.amplitude;
+}
+
+// ------------------------------------------------------------------------------------
+// Splines and terrain (spline.c, terrain.c)
+// ------------------------------------------------------------------------------------
+__device__ int spline_lower_bound(const float *loc, int n, float v) {
+    int start = 0, len = n;
+    while (len > 0) {
+        int half = len / 2;
+        int mid = start + half;
+        if (v < loc[mid]) {
+            len = half;
+        } else {
+            start = mid + 1;
+            len -= half + 1;
+        }
+    }
+    return start;
+}
+__device__ __forceinline__ float lerpf(float t, float a, float b) { return a + t * (b - a); }
+
+__device__ __noinline__ float p2_spline(const P2Tables &T, int root, const float *pt) {
+    const SplineNode &n = T.nodes[root];
+    if (n.kind == 1) return n.constant;
+    const float f = pt[n.coord];
+    const float *loc = T.floats + n.loc;
+    const float *der = T.floats + n.der;
+    const int *ch = T.child + n.child;
+    const int i = spline_lower_bound(loc, n.n, f) - 1;
+    const int j = n.n - 1;
+    if (i < 0) return p2_spline(T, ch[0], pt) + der[0] * (f - loc[0]);
+    if (i == j) return p2_spline(T, ch[j], pt) + der[j] * (f - loc[j]);
+    const float g = loc[i], h = loc[i + 1];
+    const float k = (f - g) / (h - g);
+    const float l = p2_spline(T, ch[i], pt);
+    const float m = p2_spline(T, ch[i + 1], pt);
+    const float d1 = der[i], d2 = der[i + 1];
+    const float pp = d1 * (h - g) - (m - l);
+    const float qq = -d2 * (h - g) + (m - l);
+    return lerpf(k, l, m) + k * (1.0f - k) * lerpf(k, pp, qq);
+}
+
+__device__ __forceinline__ float normalized_weirdness_118(float w) {
+    float a = w < 0.0f ? -w : w;
+    float b = a - 0.6666667f;
+    float c = b < 0.0f ? -b : b;
+    float d = c - 0.33333334f;
+    return -d * 3.0f;
+}
+__device__ __forceinline__ float normalized_weirdness_261(double w) {
+    double a = fabs(w);
+    double b = -0.6666666666666666 + a;
+    double c = fabs(b);
+    double d = -0.3333333333333333 + c;
+    return (float)(-3.0 * d);
+}
+
+struct TerrainInfo {
+    double sx, sz;          // shifted coordinates
+    double c, w, e;         // continentalness, weirdness, erosion
+};
+
+__device__ void p2_terrain(const P2Tables &T, const P2World &W, int bx, int bz, TerrainInfo &ti) {
+    ti.sx = (double)bx + p2_dbl(T, W, Q_OFFSET, (double)bx, 0.0, (double)bz) * 4.0;
+    ti.sz = (double)bz + p2_dbl(T, W, Q_OFFSET, (double)bz, (double)bx, 0.0) * 4.0;
+    ti.c = p2_dbl(T, W, Q_CONT, ti.sx, 0.0, ti.sz);
+    ti.w = p2_dbl(T, W, Q_RIDGE, ti.sx, 0.0, ti.sz);
+    ti.e = p2_dbl(T, W, Q_EROSION, ti.sx, 0.0, ti.sz);
+}
+
+// TerrainNoisePoint with the 26.1 ridges_folded (spline.c:112-126).
+struct TerrainPoint {
+    float offset, factor, peaks;
+};
+__device__ TerrainPoint p2_point_261(const P2Tables &T, const TerrainInfo &ti) {
+    float pt[4] = {(float)ti.c, (float)ti.e, normalized_weirdness_261(ti.w), (float)ti.w};
+    TerrainPoint p;
+    p.offset = p2_spline(T, T.root_offset, pt) + (-0.50375f);
+    p.factor = p2_spline(T, T.root_factor, pt);
+    p.peaks = p2_spline(T, T.root_peak, pt);
+    return p;
+}
+
+// column_top.c ps_offset_factor: the density-function offset / factor in double.
+__device__ void p2_offset_factor(const P2Tables &T, const TerrainInfo &ti, double &offset, double &factor) {
+    const float w = (float)ti.w;
+    float pt[4] = {(float)ti.c, (float)ti.e, normalized_weirdness_118(w), w};
+    const double raw_offset = (double)p2_spline(T, T.root_offset, pt);
+    const double raw_factor = (double)p2_spline(T, T.root_factor, pt);
+    const double blend_alpha = 1.0, blend_offset = 0.0;
+    offset = blend_offset * (1.0 + -1.0 * blend_alpha) + (-0.5037500262260437 + raw_offset) * blend_alpha;
+    factor = 10.0 + blend_alpha * (-10.0 + raw_factor);
+}
+
+__device__ __forceinline__ double ps_density(double y, double offset, double factor) {
+    double depth = ygrad(y, -64.0, 320.0, 1.5, -1.5) + offset;
+    double v = depth * factor;
+    double cheese = 4.0 * (v > 0.0 ? v : v * 0.25);
+    double c = mc_clamp(-0.703125 + cheese, -64.0, 64.0);
+    double a1 = ygrad(y, 240.0, 256.0, 1.0, 0.0);
+    double a2 = ygrad(y, -64.0, -40.0, 0.0, 1.0);
+    return -0.390625 + (0.1171875 + a2 * (-0.1171875 + (-0.078125 + a1 * (0.078125 + c))));
+}
+
+// lysh_preliminary_surface_level (column_top.c:94-118), block coordinates.
+__device__ int p2_column_top(const P2Tables &T, const P2World &W, int x, int z) {
+    TerrainInfo ti;
+    p2_terrain(T, W, x >> 2, z >> 2, ti);
+    double offset, factor;
+    p2_offset_factor(T, ti, offset, factor);
+    double inv = 1.0 / factor;
+    double inner = inv * 0.2734375 + offset * -1.0;
+    double ub = mc_clamp(128.0 + -128.0 * inner, -40.0, 320.0);
+    int y = (int)(ub / 8.0) * 8;
+    if (y <= -64) return -64;
+    for (int i = y; i >= -64; i -= 8)
+        if (ps_density((double)i, offset, factor) > 0.0) return i;
+    return -64;
+}
+
+// ------------------------------------------------------------------------------------
+// Blended base noise (interp_noise.c:100-139)
+// ------------------------------------------------------------------------------------
+__device__ double p2_blended(const P2Tables &T, const P2World &W, int x, int y, int z) {
+    const P2Perlin *lower = W.perl + T.n_slots, *upper = lower + 16, *mainn = lower + 32;
+    const double xz_mult = 684.412 * 0.25, y_mult = 684.412 * 0.125;
+    const double xz_factor = 80.0, y_factor = 160.0, smear = 8.0;
+    double d = (double)x * xz_mult;
+    double e = (double)y * y_mult;
+    double f = (double)z * xz_mult;
+    double g = d / xz_factor;
+    double h = e / y_factor;
+    double i = f / xz_factor;
+    double j = y_mult * smear;
+    double k = j / y_factor;
+    double n = 0.0, q = 1.0;
+    for (int o = 0; o < 8; o++) {
+        n += p2_perlin(mainn[o], keep_precision(g * q), keep_precision(h * q), keep_precision(i * q), k * q, h * q) / q;
+        q /= 2.0;
+    }
+    double t = (n / 10.0 + 1.0) / 2.0;
+    const bool skip_min = (t >= 1.0), skip_max = (t <= 0.0);
+    double l = 0.0, m = 0.0;
+    q = 1.0;
+    for (int o = 0; o < 16; o++) {
+        double xx = keep_precision(d * q), yy = keep_precision(e * q), zz = keep_precision(f * q);
+        double ys = j * q, ymax = e * q;
+        if (!skip_min) l += p2_perlin(lower[o], xx, yy, zz, ys, ymax) / q;
+        if (!skip_max) m += p2_perlin(upper[o], xx, yy, zz, ys, ymax) / q;
+        q /= 2.0;
+    }
+    return mc_clamped_lerp(l / 512.0, m / 512.0, t) / 128.0;
+}
+
+// ------------------------------------------------------------------------------------
+// Density column (density.c)
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ double lfp(const P2Tables &T, const P2World &W, int q, double x, double y, double z,
+                                      double a, double b) {
+    return mc_lerp_from_progress(p2_dbl(T, W, q, x, y, z), -1.0, 1.0, a, b);
+}
+__device__ __forceinline__ double scale_tunnels(double v) {
+    if (v < -0.5) return 0.75;
+    if (v < 0.0) return 1.0;
+    if (v < 0.5) return 1.5;
+    return 2.0;
+}
+__device__ __forceinline__ double scale_caves(double v) {
+    if (v < -0.75) return 0.5;
+    if (v < -0.5) return 0.75;
+    if (v < 0.5) return 1.0;
+    if (v < 0.75) return 2.0;
+    return 3.0;
+}
+
+__device__ double p2_jagged(const P2Tables &T, const P2World &W, double peaks, int x, int z) {
+    if (peaks == 0.0) return 0.0;
+    double n = p2_dbl(T, W, Q_JAGGED, (double)x * 1500.0, 0.0, (double)z * 1500.0);
+    return n > 0.0 ? peaks * n : (peaks / 2.0) * n;
+}
+
+// lysh_sample_noise_column (density.c:226-281) with useJagged = 1, noNoiseCaves = 0; `jagged`
+// is the column's precomputed lysh_jagged value.
+__device__ double p2_noise_column(const P2Tables &T, const P2World &W, int x, int y, int z, const TerrainPoint &tp,
+                                  double jagged, double base_noise) {
+    const double X = (double)x, Y = (double)y, Z = (double)z;
+    double depth = (1.0 - Y / 128.0) + (double)tp.offset;
+    double dens = (depth + jagged) * (double)tp.factor;
+    dens = dens > 0.0 ? dens * 4.0 : dens;
+    double g = dens + base_noise;
+    double cheese, spaghetti, pillar;
+    if (g < -64.0) {
+        cheese = g;
+        spaghetti = 64.0;
+        pillar = -64.0;
+    } else {
+        double i = g - 1.5625;
+        const bool shallow = i < 0.0;
+        // cave entrance
+        double ce = p2_dbl(T, W, Q_ENTRANCE, X * 0.75, Y * 0.5, Z * 0.75);
+        double cave_entrance = ce + 0.37 + mc_clamped_lerp(0.3, 0.0, (10.0 + Y) / 40.0);
+        // spaghetti roughness
+        double rm = lfp(T, W, Q_ROUGH_MOD, X, Y, Z, 0.0, 0.1);
+        double rr = fabs(p2_dbl(T, W, Q_ROUGH, X, Y, Z));
+        double rough = (0.4 - rr) * rm;
+        // spaghetti 3d
+        double rarity = p2_dbl(T, W, Q_SP3D_RARITY, (double)(x * 2), Y, (double)(z * 2));
+        double e = scale_tunnels(rarity);
+        double h = lfp(T, W, Q_SP3D_THICK, X, Y, Z, 0.065, 0.088);
+        double l3 = p2_dbl(T, W, Q_SP3D_1, X / e, Y / e, Z / e);
+        double m3 = fabs(e * l3) - h;
+        double n3 = p2_dbl(T, W, Q_SP3D_2, X / e, Y / e, Z / e);
+        double o3 = fabs(e * n3) - h;
+        double sp3d = mc_clamp(jmax(m3, o3), -1.0, 1.0);
+        double m = jmin(cave_entrance, sp3d + rough);
+        if (shallow) {
+            cheese = g;
+            spaghetti = m * 5.0;
+            pillar = -64.0;
+        } else {
+            double lv = p2_dbl(T, W, Q_LAYER, X, (double)(y * 8), Z);
+            double layer = lv * lv * 4.0;
+            if (layer > 64.0) {
+                cheese = 64.0;
+            } else {
+                double raw = p2_dbl(T, W, Q_CHEESE, X, Y / 1.5, Z);
+                double p = mc_clamp(raw + 0.27, -1.0, 1.0);
+                double qv = i * 1.28;
+                cheese = p + mc_clamped_lerp(0.5, 0.0, qv) + layer;
+            }
+            // spaghetti 2d
+            double mod = p2_dbl(T, W, Q_SP2D_MOD, (double)(x * 2), Y, (double)(z * 2));
+            double s = scale_caves(mod);
+            double h2 = lfp(T, W, Q_SP2D_THICK, (double)(x * 2), Y, (double)(z * 2), 0.6, 1.3);
+            double v2 = p2_dbl(T, W, Q_SP2D, X / s, Y / s, Z / s);
+            double j2 = fabs(s * v2) - 0.083 * h2;
+            double l2 = lfp(T, W, Q_SP2D_ELEV, X, 0.0, Z, (double)-8, 8.0);
+            double m2 = fabs(l2 - Y / 8.0) - h2;
+            m2 = m2 * m2 * m2;
+            double sp2d = mc_clamp(jmax(m2, j2), -1.0, 1.0);
+            spaghetti = jmin(m, sp2d + rough);
+            // pillar
+            double rare = lfp(T, W, Q_PILLAR_RARE, X, Y, Z, 0.0, 2.0);
+            double thick = lfp(T, W, Q_PILLAR_THICK, X, Y, Z, 0.0, 1.1);
+            thick = cube_rn(thick);
+            double pf = p2_dbl(T, W, Q_PILLAR, X * 25.0, Y * 0.3, Z * 25.0);
+            double pg = thick * (pf * 2.0 - rare);
+            pillar = pg > 0.03 ? pg : -__longlong_as_double(0x7FF0000000000000LL);
+        }
+    }
+    double v = jmax(jmin(cheese, spaghetti), pillar);
+    // applySlides(v, y / 8) with C's truncating division
+    const int cell_y = y / 8;
+    const int iy = cell_y - (-8);
+    {
+        double dd = (double)((48 - iy) - 8) / (double)2;
+        v = mc_clamped_lerp(-0.078125, v, dd);
+    }
+    {
+        double dd = (double)(iy - 0) / (double)3;
+        v = mc_clamped_lerp(0.1171875, v, dd);
+    }
+    return mc_clamp(v, -64.0, 64.0);
+}
+
+__device__ __forceinline__ double squeeze(double v) {
+    double a = mc_clamp(v * 0.64, -1.0, 1.0);
+    return a / 2.0 - a * a * a / 24.0;
+}
+
+__device__ __forceinline__ bool noodle_y_in_range(int y) { return y >= -60 && y <= 320; }
+
+// lysh_noodle_child (density.c:185-205): which 0 = noodle, 1 = thickness, 2 = ridge a, 3 = ridge b.
+__device__ double p2_noodle_child(const P2Tables &T, const P2World &W, int which, int x, int y, int z) {
+    const double X = (double)x, Y = (double)y, Z = (double)z;
+    switch (which) {
+        case 0:
+            if (!noodle_y_in_range(y)) return -1.0;
+            return p2_dbl(T, W, Q_NOODLE, X, Y, Z);
+        case 1:
+            if (!noodle_y_in_range(y)) return 0.0;
+            return -0.07500000000000001 + -0.025 * p2_dbl(T, W, Q_NOODLE_THICK, X, Y, Z);
+        default:
+            if (!noodle_y_in_range(y)) return 0.0;
+            return p2_dbl(T, W, which == 2 ? Q_NOODLE_RA : Q_NOODLE_RB, X * 2.6666666666666665,
+                          Y * 2.6666666666666665, Z * 2.6666666666666665);
+    }
+}
+__device__ __forceinline__ double noodle_combine(double n, double thickness, double ra, double rb) {
+    if (n >= -1000000.0 && n < 0.0) return 64.0;
+    return thickness + 1.5 * jmax(fabs(ra), fabs(rb));
+}
+
+// lysh_phase2_density_raw_at (phase2.c:151-158)
+__device__ double p2_density_raw(const P2Tables &T, const P2World &W, int x, int y, int z) {
+    TerrainInfo ti;
+    p2_terrain(T, W, x >> 2, z >> 2, ti);
+    TerrainPoint tp = p2_point_261(T, ti);
+    double base = p2_blended(T, W, x, y, z);
+    double jag = p2_jagged(T, W, (double)tp.peaks, x, z);
+    return p2_noise_column(T, W, x, y, z, tp, jag, base);
+}
+
+// ------------------------------------------------------------------------------------
+// Interpolated density over the chunk grid (phase2.c:44-194)
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ double interp_grid(const double (*grid)[kGridYs], int cell_x, int cell_z, int rel_x,
+                                              int rel_y, int rel_z, int cy) {
+    const int gx = cell_x & 3, gz = cell_z & 3;
+    const double *c00 = grid[gx * 5 + gz];
+    const double *c10 = grid[(gx + 1) * 5 + gz];
+    const double *c01 = grid[gx * 5 + gz + 1];
+    const double *c11 = grid[(gx + 1) * 5 + gz + 1];
+    const double dx = (double)rel_x / 4.0, dy = (double)rel_y / 8.0, dz = (double)rel_z / 4.0;
+    double xz00 = mc_lerp(dy, c00[cy], c00[cy + 1]);
+    double xz10 = mc_lerp(dy, c10[cy], c10[cy + 1]);
+    double xz01 = mc_lerp(dy, c01[cy], c01[cy + 1]);
+    double xz11 = mc_lerp(dy, c11[cy], c11[cy + 1]);
+    double z0 = mc_lerp(dx, xz00, xz10);
+    double z1 = mc_lerp(dx, xz01, xz11);
+    return mc_lerp(dz, z0, z1);
+}
+
+// lysh_phase2_density_at for a block of the job's chunk.
+__device__ double p2_density_at(const P2Tables &T, const P2World &W, const P2Chunk &J, int x, int y, int z) {
+    const int y_off = y + 64;
+    if (y_off < 0 || y_off >= 384) return p2_density_raw(T, W, x, y, z);
+    const int cell_x = x >> 2, cell_z = z >> 2, rel_x = x & 3, rel_z = z & 3;
+    const int cy = y_off / 8, rel_y = y_off - cy * 8;
+    double v = interp_grid(J.main, cell_x, cell_z, rel_x, rel_y, rel_z, cy);
+    double sq = squeeze(v);
+    double nn = p2_noodle_child(T, W, 0, x, y, z);
+    double th = interp_grid(J.noodle[0], cell_x, cell_z, rel_x, rel_y, rel_z, cy);
+    double ra = interp_grid(J.noodle[1], cell_x, cell_z, rel_x, rel_y, rel_z, cy);
+    double rb = interp_grid(J.noodle[2], cell_x, cell_z, rel_x, rel_y, rel_z, cy);
+    return jmin(sq, noodle_combine(nn, th, ra, rb));
+}
+
+// ------------------------------------------------------------------------------------
+// Aquifer (aquifer.c, 26.1 NoiseBasedAquifer)
+// ------------------------------------------------------------------------------------
+constexpr int kNoFluidY = -32512;
+
+__device__ __forceinline__ void global_fluid(int y, int &level, int &type) {
+    if (y < -54) {
+        level = -54;
+        type = BS_LAVA;
+    } else {
+        level = 63;
+        type = BS_WATER;
+    }
+}
+__device__ __forceinline__ int level_block_at(int level, int type, int y) { return y < level ? type : BS_AIR; }
+
+__device__ bool deep_dark(const P2Tables &T, const P2World &W, int x, int y, int z) {
+    TerrainInfo ti;
+    p2_terrain(T, W, x >> 2, z >> 2, ti);
+    if (!(ti.e < -0.22499999403953552)) return false;
+    double offset, factor;
+    p2_offset_factor(T, ti, offset, factor);
+    double depth = ygrad((double)y, -64.0, 320.0, 1.5, -1.5) + offset;
+    return depth > 0.8999999761581421;
+}
+
+__device__ const int kSurfOffsets[13][2] = {{0, 0},   {-2, -1}, {-1, -1}, {0, -1}, {1, -1}, {-3, 0}, {-2, 0},
+                                           {-1, 0}, {1, 0},    {-2, 1},  {-1, 1}, {0, 1},  {1, 1}};
+
+// computeFluid (aquifer.c:327-376): level and type.
+__device__ void p2_compute_fluid(const P2Tables &T, const P2World &W, int x, int y, int z, int &out_level,
+                                 int &out_type) {
+    int glevel, gtype;
+    global_fluid(y, glevel, gtype);
+    int min_top = 0x7FFFFFFF;
+    bool has_above = false;
+    for (int i = 0; i < 13; i++) {
+        const int bx = x + kSurfOffsets[i][0] * 16, bz = z + kSurfOffsets[i][1] * 16;
+        const int top = p2_column_top(T, W, bx, bz);
+        const int top_adj = top + 8;
+        const bool center = (i == 0);
+        if (center && y - 12 > top_adj) {
+            out_level = glevel;
+            out_type = gtype;
+            return;
+        }
+        const bool above = y + 12 > top_adj;
+        if (above || center) {
+            int lvl, typ;
+            global_fluid(top_adj, lvl, typ);
+            if (level_block_at(lvl, typ, top_adj) != BS_AIR) {
+                if (center) has_above = true;
+                if (above) {
+                    out_level = lvl;
+                    out_type = typ;
+                    return;
+                }
+            }
+        }
+        if (top < min_top) min_top = top;
+    }
+    // computeSurfaceLevel
+    int level;
+    if (deep_dark(T, W, x, y, z)) {
+        level = kNoFluidY;
+    } else {
+        const int d = (min_top + 8) - y;
+        const double f = has_above ? mc_clamped_lerp(1.0, 0.0, mc_lerp_progress((double)d, 0.0, 64.0)) : 0.0;
+        const double high = mc_lerp_from_progress(f, 1.0, 0.0, -0.3, 0.8);
+        const double low = mc_lerp_from_progress(f, 1.0, 0.0, -0.8, 0.4);
+        const double flood = mc_clamp(p2_dbl(T, W, Q_AQ_FLOOD, (double)x, (double)y * 0.67, (double)z), -1.0, 1.0);
+        if (flood - high > 0.0) {
+            level = glevel;
+        } else if (flood - low > 0.0) {
+            const int fx = floor_div(x, 16), fy = floor_div(y, 40), fz = floor_div(z, 16);
+            const int base = fy * 40 + 20;
+            const double n = p2_dbl(T, W, Q_AQ_SPREAD, (double)fx, (double)fy * 0.7142857142857143, (double)fz) * 10.0;
+            const int q = (int)floor(n / 3.0) * 3;
+            const int lv = base + q;
+            level = min_top < lv ? min_top : lv;
+        } else {
+            level = kNoFluidY;
+        }
+    }
+    // computeFluidType
+    int type = gtype;
+    if (level <= -10 && level != kNoFluidY && gtype != BS_LAVA) {
+        const int bx = floor_div(x, 64), by = floor_div(y, 40), bz = floor_div(z, 64);
+        const double n = p2_dbl(T, W, Q_AQ_LAVA, (double)bx, (double)by, (double)bz);
+        if (fabs(n) > 0.3) type = BS_LAVA;
+    }
+    out_level = level;
+    out_type = type;
+}
+
+__device__ __forceinline__ int64_t mc_hash_code(int x, int y, int z) {
+    const int64_t xm = (int64_t)(int32_t)((uint32_t)x * 3129871u);
+    uint64_t i = (uint64_t)(xm ^ ((int64_t)z * 116129781LL) ^ (int64_t)y);
+    i = i * i * 42317861ULL + i * 11ULL;
+    return (int64_t)i >> 16;
+}
+
+__device__ __forceinline__ int aq_index(const P2Chunk &J, int gx, int gy, int gz) {
+    const int dx = gx - J.min_gx, dy = gy - J.min_gy, dz = gz - J.min_gz;
+    if (dx < 0 || dx >= kAqX || dy < 0 || dy >= kAqY || dz < 0 || dz >= kAqZ) return -1;
+    return (dy * kAqZ + dz) * kAqX + dx;
+}
+
+__device__ __forceinline__ double similarity(int a, int b) { return 1.0 - (double)(b - a) / 25.0; }
+
+__device__ double aq_pressure(const P2Tables &T, const P2World &W, int x, int y, int z, bool &have, double &acc,
+                              int la, int ta, int lb, int tb) {
+    const int sa = level_block_at(la, ta, y), sb = level_block_at(lb, tb, y);
+    if ((sa == BS_LAVA && sb == BS_WATER) || (sa == BS_WATER && sb == BS_LAVA)) return 2.0;
+    int dy = la - lb;
+    if (dy < 0) dy = -dy;
+    if (dy == 0) return 0.0;
+    const double mid = 0.5 * ((double)la + (double)lb);
+    const double f = ((double)y + 0.5) - mid;
+    const double half = (double)dy / 2.0;
+    const double n = half - fabs(f);
+    double o;
+    if (f > 0.0) {
+        const double p = 0.0 + n;
+        o = p > 0.0 ? p / 1.5 : p / 2.5;
+    } else {
+        const double p = 3.0 + n;
+        o = p > 0.0 ? p / 3.0 : p / 10.0;
+    }
+    double inner;
+    if (o < -2.0 || o > 2.0) {
+        inner = 0.0;
+    } else if (!have) {
+        acc = p2_dbl(T, W, Q_AQ_BARRIER, (double)x, (double)y * 0.5, (double)z);
+        have = true;
+        inner = acc;
+    } else {
+        inner = acc;
+    }
+    return 2.0 * (inner + o);
+}
+
+// Aquifer.computeSubstance (aquifer.c:438-563) on the job's precomputed cells; BS_SOLID = null.
+__device__ int p2_substance(const P2Tables &T, const P2World &W, const P2Chunk &J, int x, int y, int z,
+                            double density) {
+    if (density > 0.0) return BS_SOLID;
+    int glevel, gtype;
+    global_fluid(y, glevel, gtype);
+    if (y > J.skip_above) return level_block_at(glevel, gtype, y);
+    if (level_block_at(glevel, gtype, y) == BS_LAVA) return BS_LAVA;
+    const int gx = floor_div(x - 5, 16), gy = floor_div(y + 1, 12), gz = floor_div(z - 5, 16);
+    int d[4] = {0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF};
+    int slot[4] = {0, 0, 0, 0};
+    for (int i = 0; i <= 1; i++)
+        for (int j = -1; j <= 1; j++)
+            for (int k = 0; k <= 1; k++) {
+                const int idx = aq_index(J, gx + i, gy + j, gz + k);
+                if (idx < 0) continue;
+                const int64_t pk = J.aq_loc[idx];
+                const int px = (int)(pk >> 38), py = (int)((pk << 52) >> 52), pz = (int)((pk << 26) >> 38);
+                const int dx = px - x, dy = py - y, dz = pz - z;
+                const int dist = dx * dx + dy * dy + dz * dz;
+                if (dist <= d[0]) {
+                    d[3] = d[2]; d[2] = d[1]; d[1] = d[0]; d[0] = dist;
+                    slot[3] = slot[2]; slot[2] = slot[1]; slot[1] = slot[0]; slot[0] = idx;
+                } else if (dist <= d[1]) {
+                    d[3] = d[2]; d[2] = d[1]; d[1] = dist;
+                    slot[3] = slot[2]; slot[2] = slot[1]; slot[1] = idx;
+                } else if (dist <= d[2]) {
+                    d[3] = d[2]; d[2] = dist;
+                    slot[3] = slot[2]; slot[2] = idx;
+                } else if (dist <= d[3]) {
+                    d[3] = dist;
+                    slot[3] = idx;
+                }
+            }
+    const int l0 = J.aq_level[slot[0]], t0 = J.aq_type[slot[0]];
+    const double s01 = similarity(d[0], d[1]);
+    const int result = level_block_at(l0, t0, y);
+    if (!(s01 > 0.0)) return result;
+    {
+        int bl, bt;
+        global_fluid(y - 1, bl, bt);
+        if (result == BS_WATER && level_block_at(bl, bt, y - 1) == BS_LAVA) return result;
+    }
+    bool have = false;
+    double acc = 0.0;
+    const int l1 = J.aq_level[slot[1]], t1 = J.aq_type[slot[1]];
+    const double p1 = s01 * aq_pressure(T, W, x, y, z, have, acc, l0, t0, l1, t1);
+    if (density + p1 > 0.0) return BS_SOLID;
+    const int l2 = J.aq_level[slot[2]], t2 = J.aq_type[slot[2]];
+    const double s02 = similarity(d[0], d[2]);
+    if (s02 > 0.0) {
+        const double p2 = s01 * s02 * aq_pressure(T, W, x, y, z, have, acc, l0, t0, l2, t2);
+        if (density + p2 > 0.0) return BS_SOLID;
+    }
+    const double s12 = similarity(d[1], d[2]);
+    if (s12 > 0.0) {
+        const double p3 = s01 * s12 * aq_pressure(T, W, x, y, z, have, acc, l1, t1, l2, t2);
+        if (density + p3 > 0.0) return BS_SOLID;
+    }
+    return result;
+}
+
+// lysh_phase2_block_at: the pre-carver block state.
+__device__ __forceinline__ int p2_block_at(const P2Tables &T, const P2World &W, const P2Chunk &J, int x, int y,
+                                           int z) {
+    return p2_substance(T, W, J, x, y, z, p2_density_at(T, W, J, x, y, z));
+}
+
+__device__ __forceinline__ int carve_index(int lx, int y, int lz) { return ((lz & 15) << 4) | (lx & 15) | ((y + 64) << 8); }
+
+// Surface height (NOT_AIR predicate, y + 1; phase2.c:318-334 and :438-456).
+__device__ int p2_height(const P2Tables &T, const P2World &W, const P2Chunk &J, int x, int z, bool carved) {
+    for (int y = 319; y >= -64; y--) {
+        int st = BS_SOLID;
+        const uint8_t cv = carved ? J.cells[carve_index(x & 15, y, z & 15)] : (uint8_t)CV_UNCHANGED;
+        if (cv != CV_UNCHANGED) st = cv;   // CV_AIR / CV_WATER / CV_LAVA share the BS_* codes
+        else st = p2_block_at(T, W, J, x, y, z);
+        if (st != BS_AIR) return y + 1;
+    }
+    return -64;
+}
+
+// ------------------------------------------------------------------------------------
+// Kernels: world construction
+// ------------------------------------------------------------------------------------
+__device__ void walk_perlin(Xr &r) {
+    (void)xr_next(r);
+    (void)xr_next(r);
+    (void)xr_next(r);
+    for (int i = 0; i < 256; i++) (void)xr_bounded(r, (uint32_t)(256 - i));
+}
+
+// One thread per world: start states of the 40 legacy octaves (created in sequence from the
+// "minecraft:terrain" random, lower -> upper -> main; interp_noise.c:44-75, noise.c:205-250)
+// and the aquifer's positional random factory (aquifer.c:126-136).
+__global__ void p2_legacy_kernel(const P2Tables *__restrict__ Tp, P2World *worlds, int n_worlds) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= n_worlds) return;
+    const P2Tables &T = *Tp;
+    P2World &W = worlds[w];
+    const Xr fork = seed_fork_of(W.seed);
+    Xr r = xr_make(T.terrain_lo ^ fork.lo, T.terrain_hi ^ fork.hi);
+    for (int k = 0; k < kLegacyPerlins; k++) {
+        W.legacy_rng[k] = r;
+        walk_perlin(r);
+    }
+    Xr s = xr_from_seed(W.seed);
+    Xr base;
+    base.lo = xr_next(s);
+    base.hi = xr_next(s);
+    Xr aq = xr_make(T.aquifer_lo ^ base.lo, T.aquifer_hi ^ base.hi);
+    W.aq_rand_lo = xr_next(aq);
+    W.aq_rand_hi = xr_next(aq);
+}
+
+constexpr int kBuildThreads = 128;
+
+// One thread per Perlin table of one world.
+__global__ void __launch_bounds__(kBuildThreads) p2_build_kernel(const P2Tables *__restrict__ Tp, P2World *worlds) {
+    __shared__ uint8_t col[256 * kBuildThreads];
+    const P2Tables &T = *Tp;
+    P2World &W = worlds[blockIdx.y];
+    const int slot = blockIdx.x * kBuildThreads + threadIdx.x;
+    const int n_total = T.n_slots + kLegacyPerlins;
+    uint8_t *t = col + threadIdx.x;
+    for (int k = 0; k < 256; k++) t[k * kBuildThreads] = (uint8_t)k;
+    if (slot >= n_total) return;
+    Xr r;
+    if (slot < T.n_slots) {
+        const int q = T.slot_noise[slot], sub = T.slot_sub[slot], p = T.slot_oct[slot];
+        const P2Digest &D = T.digest[W.large][q];
+        const Xr fork = seed_fork_of(W.seed);
+        Xr noise = xr_make(D.name_lo ^ fork.lo, D.name_hi ^ fork.hi);
+        uint64_t a = xr_next(noise), b = xr_next(noise);
+        if (sub) {
+            a = xr_next(noise);
+            b = xr_next(noise);
+        }
+        const Xr sf = xr_make(a, b);
+        r = xr_make(D.oct_lo[p] ^ sf.lo, D.oct_hi[p] ^ sf.hi);
+    } else {
+        r = W.legacy_rng[slot - T.n_slots];
+    }
+    P2Perlin &P = W.perl[slot];
+    P.ox = xr_double(r) * 256.0;
+    P.oy = xr_double(r) * 256.0;
+    P.oz = xr_double(r) * 256.0;
+    for (int i = 0; i < 256; i++) {
+        const int j = i + xr_bounded(r, (uint32_t)(256 - i));
+        const uint8_t a = t[i * kBuildThreads], b = t[j * kBuildThreads];
+        t[i * kBuildThreads] = b;
+        t[j * kBuildThreads] = a;
+    }
+    uint32_t *out = reinterpret_cast<uint32_t *>(P.perm);
+    for (int k = 0; k < 64; k++)
+        out[k] = (uint32_t)t[(4 * k) * kBuildThreads] | ((uint32_t)t[(4 * k + 1) * kBuildThreads] << 8) |
+                 ((uint32_t)t[(4 * k + 2) * kBuildThreads] << 16) | ((uint32_t)t[(4 * k + 3) * kBuildThreads] << 24);
+}
+
+// ------------------------------------------------------------------------------------
+// Kernels: chunk grid and aquifer cells
+// ------------------------------------------------------------------------------------
+constexpr int kGridThreads = 256;
+
+// One CTA per job: the 25 corner columns' terrain points and jagged values, then 25 x 49 base
+// densities and 3 x 25 x 49 noodle children (phase2.c:73-116).
+__global__ void __launch_bounds__(kGridThreads) p2_grid_kernel(const P2Tables *__restrict__ Tp,
+                                                               const P2World *__restrict__ worlds, P2Chunk *jobs) {
+    __shared__ TerrainPoint tp[kGridCols];
+    __shared__ double jag[kGridCols];
+    const P2Tables &T = *Tp;
+    P2Chunk &J = jobs[blockIdx.x];
+    const P2World &W = worlds[J.world];
+    const int cx0 = J.chunk_x * 4, cz0 = J.chunk_z * 4;   // first cell of the chunk
+    for (int c = threadIdx.x; c < kGridCols; c += blockDim.x) {
+        const int cell_x = cx0 + c / 5, cell_z = cz0 + c % 5;
+        TerrainInfo ti;
+        p2_terrain(T, W, cell_x, cell_z, ti);
+        tp[c] = p2_point_261(T, ti);
+        jag[c] = p2_jagged(T, W, (double)tp[c].peaks, cell_x * 4, cell_z * 4);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < kGridCols * kGridYs; q += blockDim.x) {
+        const int c = q / kGridYs, i = q % kGridYs;
+        const int bx = (cx0 + c / 5) * 4, bz = (cz0 + c % 5) * 4, y = -64 + i * 8;
+        const double base = p2_blended(T, W, bx, y, bz);
+        J.main[c][i] = p2_noise_column(T, W, bx, y, bz, tp[c], jag[c], base);
+    }
+    for (int q = threadIdx.x; q < 3 * kGridCols * kGridYs; q += blockDim.x) {
+        const int which = q / (kGridCols * kGridYs), rem = q % (kGridCols * kGridYs);
+        const int c = rem / kGridYs, i = rem % kGridYs;
+        const int bx = (cx0 + c / 5) * 4, bz = (cz0 + c % 5) * 4, y = -64 + i * 8;
+        J.noodle[which][c][i] = p2_noodle_child(T, W, which + 1, bx, y, bz);
+    }
+}
+
+constexpr int kAqThreads = 128;
+
+// One CTA per job: skipSamplingAboveY from the column tops over the grid's x/z span, then
+// every aquifer cell's random anchor and fluid status (aquifer.c:158-196, 379-395, 481-501).
+__global__ void __launch_bounds__(kAqThreads) p2_aquifer_kernel(const P2Tables *__restrict__ Tp,
+                                                                const P2World *__restrict__ worlds, P2Chunk *jobs) {
+    __shared__ int max_psl;
+    const P2Tables &T = *Tp;
+    P2Chunk &J = jobs[blockIdx.x];
+    const P2World &W = worlds[J.world];
+    const int min_bx = J.chunk_x * 16, min_bz = J.chunk_z * 16;
+    const int min_gx = (min_bx - 5) >> 4, max_gx = ((min_bx + 15 - 5) >> 4) + 1;
+    const int min_gz = (min_bz - 5) >> 4, max_gz = ((min_bz + 15 - 5) >> 4) + 1;
+    const int min_gy = floor_div(-64 + 1, 12) - 1;
+    if (threadIdx.x == 0) {
+        max_psl = -0x7FFFFFFF - 1;
+        J.min_gx = min_gx;
+        J.min_gy = min_gy;
+        J.min_gz = min_gz;
+    }
+    __syncthreads();
+    const int x1 = min_gx * 16, z1 = min_gz * 16, x2 = max_gx * 16 + 9, z2 = max_gz * 16 + 9;
+    const int nxs = (x2 - x1) / 4 + 1, nzs = (z2 - z1) / 4 + 1;
+    for (int q = threadIdx.x; q < nxs * nzs; q += blockDim.x) {
+        const int x = x1 + (q % nxs) * 4, z = z1 + (q / nxs) * 4;
+        atomicMax(&max_psl, p2_column_top(T, W, x, z));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int g = floor_div((max_psl + 8) + 12, 12) + 1;
+        J.skip_above = g * 12 + 11 - 1;
+    }
+    const Xr factory{W.aq_rand_lo, W.aq_rand_hi};
+    for (int idx = threadIdx.x; idx < kAqCells; idx += blockDim.x) {
+        const int dx = idx % kAqX, dz = (idx / kAqX) % kAqZ, dy = idx / (kAqX * kAqZ);
+        const int cx = min_gx + dx, cy = min_gy + dy, cz = min_gz + dz;
+        Xr rnd = xr_make((uint64_t)mc_hash_code(cx, cy, cz) ^ factory.lo, factory.hi);
+        const int px = (cx << 4) + xr_bounded(rnd, 10);
+        const int py = cy * 12 + xr_bounded(rnd, 9);
+        const int pz = (cz << 4) + xr_bounded(rnd, 10);
+        const int64_t packed = ((int64_t)(px & 0x3FFFFFF) << 38) | ((int64_t)(pz & 0x3FFFFFF) << 12) |
+                               (int64_t)(py & 0xFFF);
+        J.aq_loc[idx] = packed;
+        int level, type;
+        p2_compute_fluid(T, W, (int)(packed >> 38), (int)((packed << 52) >> 52), (int)((packed << 26) >> 38), level,
+                         type);
+        J.aq_level[idx] = level;
+        J.aq_type[idx] = (uint8_t)type;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Carvers (carver.c), one warp per job
+// ------------------------------------------------------------------------------------
+constexpr int kCarveThreads = 32;
+constexpr int kMaskWords = kCarveCells / 32;
+
+struct CarveCtx {
+    const P2Tables *T;
+    const P2World *W;
+    const P2Chunk *J;
+    uint8_t *cells;
+    uint32_t *mask;
+    float *width;                 // canyon width factors (384)
+    int tmin_x, tmin_z;
+    double tmid_x, tmid_z;
+};
+
+__device__ __forceinline__ float mc_sin(const P2Tables &T, double a) {
+    return T.sin_table[(int)((long long)(a * 10430.378350470453) & 65535LL)];
+}
+__device__ __forceinline__ float mc_cos(const P2Tables &T, double a) {
+    return T.sin_table[(int)((long long)(a * 10430.378350470453 + 16384.0) & 65535LL)];
+}
+__device__ __forceinline__ float lcg_float(uint64_t &st) { return (float)lcg_bits(st, 24) * 5.9604645e-8f; }
+__device__ __forceinline__ float uniform_float(uint64_t &st, float lo, float hi) { return lcg_float(st) * (hi - lo) + lo; }
+__device__ __forceinline__ void lcg_set_seed(uint64_t &st, uint64_t s) { st = (s ^ kLcgMul) & kLcgMask; }
+__device__ __forceinline__ int jfloor(double d) { return (int)floor(d); }
+
+// setLargeFeatureSeed (structure.c:26-42)
+__device__ __forceinline__ uint64_t large_feature_state(uint64_t world_seed, int cx, int cz) {
+    uint64_t st;
+    lcg_set_seed(st, world_seed);
+    const uint64_t a = lcg_long(st), b = lcg_long(st);
+    const uint64_t s = (uint64_t)((int64_t)cx * (int64_t)a) ^ (uint64_t)((int64_t)cz * (int64_t)b) ^ world_seed;
+    lcg_set_seed(st, s);
+    return st;
+}
+
+// WorldCarver.carveEllipsoid (carver.c:165-214); the ellipsoid's cells are independent, so the
+// warp's lanes take them in turn.  kind 0 = cave (floor level), 1 = canyon (width factors).
+__device__ void carve_ellipsoid(CarveCtx &c, int kind, double floor_level, double x, double y, double z, double hr,
+                                double vr) {
+    const double reach = 16.0 + hr * 2.0;
+    if (fabs(x - c.tmid_x) > reach || fabs(z - c.tmid_z) > reach) return;
+    const int min_bx = c.tmin_x, min_bz = c.tmin_z;
+    const int i0 = max(jfloor(x - hr) - min_bx - 1, 0);
+    const int i1 = min(jfloor(x + hr) - min_bx, 15);
+    const int k0 = max(jfloor(y - vr) - 1, -64 + 1);
+    const int m0 = min(jfloor(y + vr) + 1, -64 + 384 - 1 - 7);
+    const int n0 = max(jfloor(z - hr) - min_bz - 1, 0);
+    const int o0 = min(jfloor(z + hr) - min_bz, 15);
+    const int nxp = i1 - i0 + 1, nzp = o0 - n0 + 1, nyp = m0 - k0;
+    if (nxp <= 0 || nzp <= 0 || nyp <= 0) return;
+    const int total = nxp * nzp * nyp;
+    const int lane = threadIdx.x & 31;
+    for (int q = lane; q < total; q += 32) {
+        const int p = i0 + q / (nzp * nyp);
+        const int s = n0 + (q / nyp) % nzp;
+        const int v = m0 - q % nyp;
+        const int bx = min_bx + p, bz = min_bz + s;
+        const double nx = ((double)bx + 0.5 - x) / hr;
+        const double nz = ((double)bz + 0.5 - z) / hr;
+        if (nx * nx + nz * nz >= 1.0) continue;
+        const double ny = ((double)v - 0.5 - y) / vr;
+        bool skip;
+        if (kind == 0) {
+            skip = (ny <= floor_level) || (nx * nx + ny * ny + nz * nz) >= 1.0;
+        } else {
+            const int idx = v - (-64) - 1;
+            skip = (nx * nx + nz * nz) * (double)c.width[idx] + ny * ny / 6.0 >= 1.0;
+        }
+        if (skip) continue;
+        const int ci = carve_index(p, v, s);
+        const uint32_t bit = 1u << (ci & 31);
+        const uint32_t old = atomicOr(&c.mask[ci >> 5], bit);
+        if (old & bit) continue;
+        // carveBlock
+        int st;
+        const uint8_t cv = c.cells[ci];
+        if (cv != CV_UNCHANGED) st = cv;
+        else st = p2_block_at(*c.T, *c.W, *c.J, bx, v, bz);
+        if (!(st == BS_SOLID || st == BS_WATER)) continue;
+        int cs;
+        if (v <= -56) {
+            cs = BS_LAVA;
+        } else {
+            cs = p2_substance(*c.T, *c.W, *c.J, bx, v, bz, 0.0);
+            if (cs == BS_SOLID) continue;
+        }
+        c.cells[ci] = (uint8_t)cs;
+    }
+    __syncwarp();
+}
+
+__device__ float cave_thickness(uint64_t &r) {
+    float f = lcg_float(r) * 2.0f + lcg_float(r);
+    if (lcg_int(r, 10) == 0) {
+        float a = lcg_float(r);
+        float b = lcg_float(r);
+        f = f * (a * b * 3.0f + 1.0f);
+    }
+    return f;
+}
+
+__device__ __noinline__ void cave_tunnel(CarveCtx &c, double floor_level, uint64_t seed, double x, double y, double z,
+                                         double d4, double d5, float thickness, float yaw, float pitch, int first_step,
+                                         int total_steps, double y_scale) {
+    const P2Tables &T = *c.T;
+    uint64_t r;
+    lcg_set_seed(r, seed);
+    const int branch_step = lcg_int(r, total_steps / 2) + total_steps / 4;
+    const bool wide = (lcg_int(r, 6) == 0);
+    float f30 = 0.0f, f31 = 0.0f;
+    for (int i = first_step; i < total_steps; i++) {
+        const float ang = (float)i * 3.1415927f / (float)total_steps;
+        const double radius = 1.5 + (double)(mc_sin(T, (double)ang) * thickness);
+        const double vert_base = radius * y_scale;
+        const float cos_pitch = mc_cos(T, (double)pitch);
+        x += (double)(mc_cos(T, (double)yaw) * cos_pitch);
+        y += (double)mc_sin(T, (double)pitch);
+        z += (double)(mc_sin(T, (double)yaw) * cos_pitch);
+        pitch *= wide ? 0.92f : 0.7f;
+        pitch += f31 * 0.1f;
+        yaw += f30 * 0.1f;
+        f31 *= 0.9f;
+        f30 *= 0.75f;
+        {
+            const float a1 = lcg_float(r), b1 = lcg_float(r), c1 = lcg_float(r);
+            f31 += (a1 - b1) * c1 * 2.0f;
+            const float a2 = lcg_float(r), b2 = lcg_float(r), c2 = lcg_float(r);
+            f30 += (a2 - b2) * c2 * 4.0f;
+        }
+        if (i == branch_step && thickness > 1.0f) {
+            const uint64_t s1 = lcg_long(r);
+            const float t1 = lcg_float(r) * 0.5f + 0.5f;
+            cave_tunnel(c, floor_level, s1, x, y, z, d4, d5, t1, yaw - 1.5707964f, pitch / 3.0f, i, total_steps, 1.0);
+            const uint64_t s2 = lcg_long(r);
+            const float t2 = lcg_float(r) * 0.5f + 0.5f;
+            cave_tunnel(c, floor_level, s2, x, y, z, d4, d5, t2, yaw + 1.5707964f, pitch / 3.0f, i, total_steps, 1.0);
+            return;
+        }
+        if (lcg_int(r, 4) == 0) continue;
+        {
+            const double dx = x - c.tmid_x, dz = z - c.tmid_z;
+            const double dy = (double)(total_steps - i);
+            const double rr = (double)(thickness + 2.0f + 16.0f);
+            if (!(dx * dx + dz * dz - dy * dy <= rr * rr)) return;
+        }
+        carve_ellipsoid(c, 0, floor_level, x, y, z, radius * d4, vert_base * d5);
+    }
+}
+
+__device__ void cave_carve(CarveCtx &c, uint64_t &r, int ocx, int ocz, int y_hi) {
+    const P2Tables &T = *c.T;
+    const int i10 = lcg_int(r, lcg_int(r, lcg_int(r, 15) + 1) + 1);
+    for (int k = 0; k < i10; k++) {
+        const int lx = lcg_int(r, 16);
+        const double x = (double)(ocx * 16 + lx);
+        const int y = lcg_int(r, y_hi - (-56) + 1) + (-56);
+        const int lz = lcg_int(r, 16);
+        const double z = (double)(ocz * 16 + lz);
+        const double hrm = (double)uniform_float(r, 0.7f, 1.4f);
+        const double vrm = (double)uniform_float(r, 0.8f, 1.3f);
+        const double floor_level = (double)uniform_float(r, -1.0f, -0.4f);
+        int tunnels = 1;
+        if (lcg_int(r, 4) == 0) {
+            const double room_y_scale = (double)uniform_float(r, 0.1f, 0.9f);
+            const float f28 = 1.0f + lcg_float(r) * 6.0f;
+            const float sf = mc_sin(T, 1.5707963705062866);
+            const double d17 = 1.5 + (double)(sf * f28);
+            const double d19 = d17 * room_y_scale;
+            carve_ellipsoid(c, 0, floor_level, x + 1.0, (double)y, z, d17, d19);
+            tunnels += lcg_int(r, 4);
+        }
+        for (int t = 0; t < tunnels; t++) {
+            const float yaw = lcg_float(r) * 6.2831855f;
+            const float pitch = (lcg_float(r) - 0.5f) / 4.0f;
+            const float thick = cave_thickness(r);
+            const int steps = 112 - lcg_int(r, 112 / 4);
+            const uint64_t seed = lcg_long(r);
+            cave_tunnel(c, floor_level, seed, x, (double)y, z, hrm, vrm, thick, yaw, pitch, 0, steps, 1.0);
+        }
+    }
+}
+
+__device__ void canyon_carve(CarveCtx &c, uint64_t &r0, int ocx, int ocz) {
+    const P2Tables &T = *c.T;
+    const int lx = lcg_int(r0, 16);
+    double x = (double)(ocx * 16 + lx);
+    const int yi = lcg_int(r0, 67 - 10 + 1) + 10;
+    const int lz = lcg_int(r0, 16);
+    double z = (double)(ocz * 16 + lz);
+    float yaw = lcg_float(r0) * 6.2831855f;
+    float pitch = uniform_float(r0, -0.125f, 0.125f);
+    const double y_scale = (double)3.0f;
+    float thickness;
+    {   // TrapezoidFloat(0, 6, plateau 2)
+        const float d = 6.0f - 0.0f;
+        const float e = (d - 2.0f) / 2.0f;
+        const float f = d - e;
+        const float a = lcg_float(r0) * f + 0.0f;
+        thickness = a + lcg_float(r0) * e;
+    }
+    const float dist = uniform_float(r0, 0.75f, 1.0f);
+    const int total_steps = (int)((float)112 * dist);
+    const uint64_t seed = lcg_long(r0);
+    // doCarve
+    uint64_t r;
+    lcg_set_seed(r, seed);
+    const int lane = threadIdx.x & 31;
+    {   // width factors: every lane draws the same sequence; lane 0 stores it
+        float f = 1.0f;
+        for (int i = 0; i < 384; i++) {
+            if (i == 0 || lcg_int(r, 3) == 0) {
+                const float a = lcg_float(r);
+                const float b = lcg_float(r);
+                f = 1.0f + a * b;
+            }
+            if (lane == 0) c.width[i] = f * f;
+        }
+        __syncwarp();
+    }
+    double y = (double)yi;
+    float yaw_drift = 0.0f, pitch_drift = 0.0f;
+    for (int i = 0; i < total_steps; i++) {
+        const float ang = (float)i * 3.1415927f / (float)total_steps;
+        double radius = 1.5 + (double)(mc_sin(T, (double)ang) * thickness);
+        double vert_radius = radius * y_scale;
+        radius *= (double)uniform_float(r, 0.75f, 1.0f);
+        {   // updateVerticalRadius
+            const float f1 = (float)total_steps, f2 = (float)i;
+            const float f7 = 1.0f - fabsf(0.5f - f2 / f1) * 2.0f;
+            const float f8 = 0.0f + 1.0f * f7;
+            const double base = (double)f8 * vert_radius;
+            vert_radius = base * (double)uniform_float(r, 0.75f, 1.0f);
+        }
+        const float cos_pitch = mc_cos(T, (double)pitch);
+        const float sin_pitch = mc_sin(T, (double)pitch);
+        x += (double)(mc_cos(T, (double)yaw) * cos_pitch);
+        y += (double)sin_pitch;
+        z += (double)(mc_sin(T, (double)yaw) * cos_pitch);
+        pitch *= 0.7f;
+        pitch += pitch_drift * 0.05f;
+        yaw += yaw_drift * 0.05f;
+        pitch_drift *= 0.8f;
+        yaw_drift *= 0.5f;
+        {
+            const float a1 = lcg_float(r), b1 = lcg_float(r), c1 = lcg_float(r);
+            pitch_drift += (a1 - b1) * c1 * 2.0f;
+            const float a2 = lcg_float(r), b2 = lcg_float(r), c2 = lcg_float(r);
+            yaw_drift += (a2 - b2) * c2 * 4.0f;
+        }
+        if (lcg_int(r, 4) == 0) continue;
+        {
+            const double dx = x - c.tmid_x, dz = z - c.tmid_z;
+            const double dy = (double)(total_steps - i);
+            const double rr = (double)(thickness + 2.0f + 16.0f);
+            if (!(dx * dx + dz * dz - dy * dy <= rr * rr)) return;
+        }
+        carve_ellipsoid(c, 1, 0.0, x, y, z, radius, vert_radius);
+    }
+}
+
+// applyCarvers for the job's chunk (carver.c:482-523): cells and mask in shared memory.
+__global__ void __launch_bounds__(kCarveThreads) p2_carve_kernel(const P2Tables *__restrict__ Tp,
+                                                                 const P2World *__restrict__ worlds, P2Chunk *jobs) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint8_t *cells = smem;
+    uint32_t *mask = reinterpret_cast<uint32_t *>(smem + kCarveCells);
+    float *width = reinterpret_cast<float *>(smem + kCarveCells + kMaskWords * 4);
+    P2Chunk &J = jobs[blockIdx.x];
+    const P2World &W = worlds[J.world];
+    for (int q = threadIdx.x; q < kCarveCells / 4; q += blockDim.x) reinterpret_cast<uint32_t *>(cells)[q] = 0u;
+    for (int q = threadIdx.x; q < kMaskWords; q += blockDim.x) mask[q] = 0u;
+    __syncwarp();
+    CarveCtx c;
+    c.T = Tp;
+    c.W = &W;
+    c.J = &J;
+    c.cells = cells;
+    c.mask = mask;
+    c.width = width;
+    c.tmin_x = J.chunk_x * 16;
+    c.tmin_z = J.chunk_z * 16;
+    c.tmid_x = (double)(c.tmin_x + 8);
+    c.tmid_z = (double)(c.tmin_z + 8);
+    for (int dx = -8; dx <= 8; dx++)
+        for (int dz = -8; dz <= 8; dz++) {
+            const int ox = J.chunk_x + dx, oz = J.chunk_z + dz;
+            for (int ci = 0; ci < 3; ci++) {
+                const float prob = ci == 0 ? 0.15f : (ci == 1 ? 0.07f : 0.01f);
+                uint64_t r = large_feature_state(W.seed + (uint64_t)ci, ox, oz);
+                const float f = lcg_float(r);
+                if (!(f <= prob)) continue;
+                if (ci == 1) cave_carve(c, r, ox, oz, 47);
+                else if (ci == 0) cave_carve(c, r, ox, oz, 180);
+                else canyon_carve(c, r, ox, oz);
+            }
+        }
+    __syncwarp();
+    for (int q = threadIdx.x; q < kCarveCells / 4; q += blockDim.x)
+        reinterpret_cast<uint32_t *>(J.cells)[q] = reinterpret_cast<const uint32_t *>(cells)[q];
+    if (threadIdx.x == 0) J.carved = 1;
+}
+
+// ------------------------------------------------------------------------------------
+// Biome gate (biome.c) and the verdict (eval.c)
+// ------------------------------------------------------------------------------------
+__device__ int64_t tree_dist(const BiomeTree &g, int i, const int64_t np[6]) {
+    int64_t ds = 0;
+    for (int k = 0; k < 6; k++) {
+        int64_t d = np[k] - g.range[12 * i + 2 * k + 1], e = (int64_t)g.range[12 * i + 2 * k] - np[k];
+        d = d > 0 ? d : (e > 0 ? e : 0);
+        ds += d * d;
+    }
+    return ds;
+}
+
+__device__ __noinline__ int tree_search(const BiomeTree &g, int node, const int64_t np[6], int leaf) {
+    if (g.kids[node] == 0) return node;
+    int64_t best = leaf < 0 ? 0x7FFFFFFFFFFFFFFFLL : tree_dist(g, leaf, np);
+    int result = leaf, c = node + 1;
+    for (int k = 0; k < g.kids[node]; k++, c = g.end[c]) {
+        const int64_t d = tree_dist(g, c, np);
+        if (best > d) {
+            const int l2 = tree_search(g, c, np, result);
+            const int64_t d2 = (l2 == c) ? d : tree_dist(g, l2, np);
+            if (best > d2) {
+                best = d2;
+                result = l2;
+            }
+        }
+    }
+    return result;
+}
+
+constexpr int kFinishThreads = 64;
+
+__global__ void __launch_bounds__(kFinishThreads) p2_finish_kernel(const P2Tables *__restrict__ Tp,
+                                                                   const P2World *__restrict__ worlds,
+                                                                   const P2Chunk *__restrict__ jobs,
+                                                                   const P2Hut *__restrict__ huts, int tree,
+                                                                   P2Result *out) {
+    __shared__ int pre_h[64], post_h[64], wet[64];
+    __shared__ int size_x, size_z;
+    const P2Tables &T = *Tp;
+    const P2Hut H = huts[blockIdx.x];
+    const P2Chunk &J = jobs[H.job];
+    const P2World &W = worlds[J.world];
+    P2Result &R = out[blockIdx.x];
+    const int t = threadIdx.x;
+    if (t == 0) {
+        const int dir = hut_dir(W.seed, H.hut_x, H.hut_z);
+        const int axis_z = (dir == 0 || dir == 2);
+        size_x = axis_z ? 7 : 9;
+        size_z = axis_z ? 9 : 7;
+        R.hut_x = H.hut_x;
+        R.hut_z = H.hut_z;
+        R.rx = floor_div(H.hut_x, 32);
+        R.rz = floor_div(H.hut_z, 32);
+        R.dir = dir;
+        R.axis_z = axis_z;
+        R.size_x = size_x;
+        R.size_z = size_z;
+    }
+    __syncthreads();
+    // footprint column t (dx outer, dz inner), and the chunk-centre column as t == 63
+    if (t < 63) {
+        const int dx = t / size_z, dz = t % size_z;
+        const int x = H.hut_x + dx, z = H.hut_z + dz;
+        int level, type;
+        p2_compute_fluid(T, W, x, 62, z, level, type);
+        wet[t] = (type == BS_WATER && 62 < level) ? 1 : 0;
+        pre_h[t] = p2_height(T, W, J, x, z, false);
+        post_h[t] = p2_height(T, W, J, x, z, true);
+    } else if (t == 63) {
+        const int mid_x = (H.hut_x >> 4) * 16 + 8, mid_z = (H.hut_z >> 4) * 16 + 8;
+        pre_h[63] = p2_height(T, W, J, mid_x, mid_z, false);
+    }
+    __syncthreads();
+    if (t != 0) return;
+    // biome gate at the chunk centre (biome.c:94-156)
+    {
+        const int mid_x = (H.hut_x >> 4) * 16 + 8, mid_z = (H.hut_z >> 4) * 16 + 8;
+        const int y = pre_h[63] - 1;
+        const int qx = mid_x >> 2, qy = y >> 2, qz = mid_z >> 2;
+        TerrainInfo ti;
+        p2_terrain(T, W, qx, qz, ti);
+        const double temperature = p2_dbl(T, W, Q_TEMPERATURE, ti.sx, 0.0, ti.sz);
+        const double humidity = p2_dbl(T, W, Q_VEGETATION, ti.sx, 0.0, ti.sz);
+        double offset, factor;
+        {
+            TerrainInfo t2;
+            p2_terrain(T, W, (qx * 4) >> 2, (qz * 4) >> 2, t2);
+            p2_offset_factor(T, t2, offset, factor);
+        }
+        const double yq = (double)(qy * 4);
+        const double depth = mc_lerp(mc_clamp((yq - -64.0) / (320.0 - -64.0), 0.0, 1.0), 1.5, -1.5) + offset;
+        int64_t np[6];
+        np[0] = (int64_t)((float)temperature * 10000.0f);
+        np[1] = (int64_t)((float)humidity * 10000.0f);
+        np[2] = (int64_t)((float)ti.c * 10000.0f);
+        np[3] = (int64_t)((float)ti.e * 10000.0f);
+        np[4] = (int64_t)((float)depth * 10000.0f);
+        np[5] = (int64_t)((float)ti.w * 10000.0f);
+        const BiomeTree &g = T.trees[tree];
+        const int winner = g.biome[tree_search(g, 0, np, -1)];
+        for (int a = 0; a < 6; a++) R.biome_t[a] = np[a];
+        R.biome_qx = qx;
+        R.biome_qy = qy;
+        R.biome_qz = qz;
+        R.biome_occ_y = y;
+        R.biome_winner = winner;
+        R.biome_ok = winner == 6 ? 1 : 0;
+    }
+    int nwet = 0;
+    for (int k = 0; k < 63; k++) nwet += wet[k];
+    R.wet_columns = nwet;
+    R.flooded = nwet == 63;
+    R.all_dry = nwet == 0;
+    long long sum = 0;
+    bool carve_skipped = false;
+    if (R.flooded) {
+        bool blocked = false;
+        long long sum_pre = 0;
+        for (int k = 0; k < 63 && !blocked; k++) {
+            sum_pre += pre_h[k];
+            if (pre_h[k] - 1 >= 64) blocked = true;
+        }
+        if (!blocked) {
+            sum = sum_pre;
+            carve_skipped = true;
+        }
+    }
+    if (!carve_skipped)
+        for (int k = 0; k < 63; k++) sum += post_h[k];
+    R.sum_h = sum;
+    R.avg_y = (int)(sum / 63);
+    if (!R.biome_ok) {
+        R.ok = 0;
+        R.reject = 3;
+    } else if (R.flooded) {
+        R.ok = 0;
+        R.reject = 2;
+    } else if (R.avg_y > H.max_y) {
+        R.ok = 0;
+        R.reject = 1;
+    } else {
+        R.ok = 1;
+        R.reject = 0;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Point probes
+// ------------------------------------------------------------------------------------
+__global__ void p2_probe_kernel(const P2Tables *__restrict__ Tp, const P2World *__restrict__ worlds,
+                                const P2Chunk *__restrict__ jobs, const int32_t *__restrict__ pts, int n, int kind,
+                                double *out) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const P2Tables &T = *Tp;
+    const int32_t *p = pts + 5 * q;
+    const P2World &W = worlds[p[0]];
+    const int x = p[1], y = p[2], z = p[3], job = p[4];
+    double v = 0.0;
+    switch (kind) {
+        case PR_BASE_NOISE: v = p2_blended(T, W, x, y, z); break;
+        case PR_DENSITY_RAW: v = p2_density_raw(T, W, x, y, z); break;
+        case PR_COLUMN_TOP: v = (double)p2_column_top(T, W, x, z); break;
+        case PR_CONTINENTALNESS:
+        case PR_EROSION:
+        case PR_WEIRDNESS: {
+            TerrainInfo ti;
+            p2_terrain(T, W, x >> 2, z >> 2, ti);
+            v = kind == PR_CONTINENTALNESS ? ti.c : (kind == PR_EROSION ? ti.e : ti.w);
+            break;
+        }
+        case PR_OFFSET_261:
+        case PR_FACTOR_261:
+        case PR_PEAKS_261: {
+            TerrainInfo ti;
+            p2_terrain(T, W, x >> 2, z >> 2, ti);
+            const TerrainPoint tp = p2_point_261(T, ti);
+            v = kind == PR_OFFSET_261 ? (double)tp.offset : (kind == PR_FACTOR_261 ? (double)tp.factor : (double)tp.peaks);
+            break;
+        }
+        case PR_FLUID: {
+            int level, type;
+            p2_compute_fluid(T, W, x, y, z, level, type);
+            v = (double)level * 4.0 + (double)type;
+            break;
+        }
+        case PR_DENSITY: v = p2_density_at(T, W, jobs[job], x, y, z); break;
+        case PR_BLOCK: v = (double)p2_block_at(T, W, jobs[job], x, y, z); break;
+        case PR_HEIGHT_PRE: v = (double)p2_height(T, W, jobs[job], x, z, false); break;
+        case PR_HEIGHT: v = (double)p2_height(T, W, jobs[job], x, z, true); break;
+        default: break;
+    }
+    out[q] = v;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------
+// Launchers
+// ------------------------------------------------------------------------------------
+void p2_launch_legacy(const P2Tables *T, P2World *worlds, int n_worlds, cudaStream_t s) {
+    p2_legacy_kernel<<<(n_worlds + 63) / 64, 64, 0, s>>>(T, worlds, n_worlds);
+}
+
+void p2_launch_build(const P2Tables *T, P2World *worlds, int n_worlds, cudaStream_t s) {
+    const dim3 grid((kWorldSlotsMax + kBuildThreads - 1) / kBuildThreads, n_worlds);
+    p2_build_kernel<<<grid, kBuildThreads, 0, s>>>(T, worlds);
+}
+
+void p2_launch_grid(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s) {
+    p2_grid_kernel<<<n_jobs, kGridThreads, 0, s>>>(T, worlds, jobs);
+}
+
+void p2_launch_aquifer(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s) {
+    p2_aquifer_kernel<<<n_jobs, kAqThreads, 0, s>>>(T, worlds, jobs);
+}
+
+void p2_launch_carve(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s) {
+    static unsigned long long done = 0;
+    const size_t smem = kCarveCells + kMaskWords * 4 + 384 * 4;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !((done >> dev) & 1ull)) {
+        cudaFuncSetAttribute(p2_carve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        done |= 1ull << dev;
+    }
+    p2_carve_kernel<<<n_jobs, kCarveThreads, smem, s>>>(T, worlds, jobs);
+}
+
+void p2_launch_finish(const P2Tables *T, const P2World *worlds, const P2Chunk *jobs, const P2Hut *huts, int n_huts,
+                      int tree, P2Result *out, cudaStream_t s) {
+    p2_finish_kernel<<<n_huts, kFinishThreads, 0, s>>>(T, worlds, jobs, huts, tree, out);
+}
+
+void p2_launch_probe(const P2Tables *T, const P2World *worlds, const P2Chunk *jobs, const int32_t *pts, int n_pts,
+                     int kind, double *out, cudaStream_t s) {
+    p2_probe_kernel<<<(n_pts + 127) / 128, 128, 0, s>>>(T, worlds, jobs, pts, n_pts, kind, out);
+}
+
+}  // namespace wg
