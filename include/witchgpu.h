@@ -198,7 +198,9 @@ int wg_grade_scan(wg_engine *e, int64_t seed, const wg_opts *opts, int max_heigh
  *   10 interpolated final density       lysh_phase2_density_at            phase2.c:161
  *   11 block state before carvers       lysh_phase2_block_at              phase2.c:309
  *   12 surface height before carvers    lysh_phase2_height_pre_carver     phase2.c:318
- *   13 surface height after carvers     lysh_phase2_height                phase2.c:438 */
+ *   13 surface height after carvers     lysh_phase2_height                phase2.c:438
+ *   14 the chunk's stored `interpolated` corner value for the cell holding the point, i.e.
+ *      kind 1 at ((x >> 2) * 4, -64 + 8 * ((y + 64) >> 3), (z >> 2) * 4)  phase2.c:73-96 */
 int wg_p2_probe(wg_engine *e, int64_t seed, const wg_opts *opts, int kind, const int32_t *xyz, uint64_t n,
                 double *out);
 

@@ -74,7 +74,7 @@ GRADE_INTS = 12   # hutX, hutZ, rx, rz, dir, avg_y, flooded, ok, wet, size_x, si
 # wg_p2_probe kinds (include/witchgpu.h).
 PROBE_KINDS = {"base_noise": 0, "density_raw": 1, "column_top": 2, "continentalness": 3, "erosion": 4,
                "weirdness": 5, "offset": 6, "factor": 7, "peaks": 8, "fluid": 9, "density": 10, "block": 11,
-               "height_pre": 12, "height": 13}
+               "height_pre": 12, "height": 13, "grid_main": 14}
 
 
 class HutGrade(C.Structure):

@@ -129,12 +129,33 @@ int upload(wg_engine *eng, const T *src, size_t count, const T **dst) {
     return WG_OK;
 }
 
+// Nesting depth of a spline node / an R-tree node (the device evaluators use fixed stacks).
+int spline_depth(const GameData &g, int node) {
+    const SplineNode &n = g.nodes[node];
+    if (n.kind == 1) return 1;
+    int d = 0;
+    for (int k = 0; k < n.n; k++) d = std::max(d, spline_depth(g, g.child[n.child + k]));
+    return d + 1;
+}
+int tree_depth(const BiomeTree &t, int node) {
+    if (t.kids[node] == 0) return 1;
+    int d = 0, c = node + 1;
+    for (int k = 0; k < t.kids[node]; k++, c = t.end[c]) d = std::max(d, tree_depth(t, c));
+    return d + 1;
+}
+
 int ensure_tables(wg_engine *eng) {
     if (eng->p2_tables) return WG_OK;
     const GameData &g = game_data();
     if (!g.available)
         return eng->fail(WG_ERR_ARG, "phase 2 needs the game data tables, which were not found when the library was "
                                      "built (set LYSH to the reference's engine/tools/lysh/src and rebuild)");
+    if (spline_depth(g, g.root_offset) > kSplineDepth || spline_depth(g, g.root_factor) > kSplineDepth ||
+        spline_depth(g, g.root_peak) > kSplineDepth)
+        return eng->fail(WG_ERR_ARG, "phase 2: terrain spline nests deeper than the device evaluator holds");
+    for (int k = 0; k < kBiomeTrees; k++)
+        if (tree_depth(g.trees[k], 0) > kTreeDepth)
+            return eng->fail(WG_ERR_ARG, "phase 2: biome tree nests deeper than the device search holds");
     std::vector<P2Tables> hv(1);
     P2Tables *h = hv.data();
     std::memset(h, 0, sizeof *h);

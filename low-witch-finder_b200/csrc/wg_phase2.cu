@@ -146,25 +146,62 @@ __device__ int spline_lower_bound(const float *loc, int n, float v) {
 }
 __device__ __forceinline__ float lerpf(float t, float a, float b) { return a + t * (b - a); }
 
-__device__ __noinline__ float p2_spline(const P2Tables &T, int root, const float *pt) {
-    const SplineNode &n = T.nodes[root];
-    if (n.kind == 1) return n.constant;
-    const float f = pt[n.coord];
-    const float *loc = T.floats + n.loc;
-    const float *der = T.floats + n.der;
-    const int *ch = T.child + n.child;
-    const int i = spline_lower_bound(loc, n.n, f) - 1;
-    const int j = n.n - 1;
-    if (i < 0) return p2_spline(T, ch[0], pt) + der[0] * (f - loc[0]);
-    if (i == j) return p2_spline(T, ch[j], pt) + der[j] * (f - loc[j]);
-    const float g = loc[i], h = loc[i + 1];
-    const float k = (f - g) / (h - g);
-    const float l = p2_spline(T, ch[i], pt);
-    const float m = p2_spline(T, ch[i + 1], pt);
-    const float d1 = der[i], d2 = der[i + 1];
-    const float pp = d1 * (h - g) - (m - l);
-    const float qq = -d2 * (h - g) + (m - l);
-    return lerpf(k, l, m) + k * (1.0f - k) * lerpf(k, pp, qq);
+// CubicSpline.apply over the nested spline table (spline.c:26-57), evaluated with an explicit
+// stack instead of recursion: each frame is one node waiting for its first and second child.
+// The host checks at upload that the table nests no deeper than kSplineDepth.
+__device__ float p2_spline(const P2Tables &T, int root, const float *pt) {
+    int node[kSplineDepth], stage[kSplineDepth];
+    float first[kSplineDepth];
+    int sp = 0;
+    node[0] = root;
+    stage[0] = 0;
+    float ret = 0.0f;
+    for (;;) {
+        const SplineNode &n = T.nodes[node[sp]];
+        float result;
+        if (n.kind == 1) {
+            result = n.constant;
+        } else {
+            const float f = pt[n.coord];
+            const float *loc = T.floats + n.loc;
+            const float *der = T.floats + n.der;
+            const int *ch = T.child + n.child;
+            const int i = spline_lower_bound(loc, n.n, f) - 1;
+            const int j = n.n - 1;
+            if (i < 0 || i == j) {   // outside the points: the end child plus a linear extension
+                const int k = i < 0 ? 0 : j;
+                if (stage[sp] == 0) {
+                    if (sp + 1 >= kSplineDepth) return __int_as_float(0x7FC00000);
+                    stage[sp] = 1;
+                    node[sp + 1] = ch[k];
+                    stage[sp + 1] = 0;
+                    sp++;
+                    continue;
+                }
+                result = ret + der[k] * (f - loc[k]);
+            } else {
+                if (stage[sp] < 2) {
+                    if (sp + 1 >= kSplineDepth) return __int_as_float(0x7FC00000);
+                    if (stage[sp] == 1) first[sp] = ret;
+                    node[sp + 1] = ch[i + stage[sp]];
+                    stage[sp]++;
+                    stage[sp + 1] = 0;
+                    sp++;
+                    continue;
+                }
+                const float g = loc[i], h = loc[i + 1];
+                const float k = (f - g) / (h - g);
+                const float l = first[sp], m = ret;
+                const float d1 = der[i], d2 = der[i + 1];
+                const float pp = d1 * (h - g) - (m - l);
+                const float qq = -d2 * (h - g) + (m - l);
+                result = lerpf(k, l, m) + k * (1.0f - k) * lerpf(k, pp, qq);
+            }
+        }
+        if (sp == 0) return result;
+        ret = result;
+        sp--;
+    }
 }
 
 __device__ __forceinline__ float normalized_weirdness_118(float w) {
@@ -956,6 +993,10 @@ __device__ float cave_thickness(uint64_t &r) {
     return f;
 }
 
+// createTunnel (carver.c:266-330).  A tunnel may split once into two thinner ones (thickness
+// <= 1, so they never split again); the split tunnels are the kBranch = false instantiation,
+// which keeps the call chain two levels deep without recursion.
+template <bool kBranch>
 __device__ __noinline__ void cave_tunnel(CarveCtx &c, double floor_level, uint64_t seed, double x, double y, double z,
                                          double d4, double d5, float thickness, float yaw, float pitch, int first_step,
                                          int total_steps, double y_scale) {
@@ -984,13 +1025,15 @@ __device__ __noinline__ void cave_tunnel(CarveCtx &c, double floor_level, uint64
             const float a2 = lcg_float(r), b2 = lcg_float(r), c2 = lcg_float(r);
             f30 += (a2 - b2) * c2 * 4.0f;
         }
-        if (i == branch_step && thickness > 1.0f) {
+        if (kBranch && i == branch_step && thickness > 1.0f) {
             const uint64_t s1 = lcg_long(r);
             const float t1 = lcg_float(r) * 0.5f + 0.5f;
-            cave_tunnel(c, floor_level, s1, x, y, z, d4, d5, t1, yaw - 1.5707964f, pitch / 3.0f, i, total_steps, 1.0);
+            cave_tunnel<false>(c, floor_level, s1, x, y, z, d4, d5, t1, yaw - 1.5707964f, pitch / 3.0f, i,
+                               total_steps, 1.0);
             const uint64_t s2 = lcg_long(r);
             const float t2 = lcg_float(r) * 0.5f + 0.5f;
-            cave_tunnel(c, floor_level, s2, x, y, z, d4, d5, t2, yaw + 1.5707964f, pitch / 3.0f, i, total_steps, 1.0);
+            cave_tunnel<false>(c, floor_level, s2, x, y, z, d4, d5, t2, yaw + 1.5707964f, pitch / 3.0f, i,
+                               total_steps, 1.0);
             return;
         }
         if (lcg_int(r, 4) == 0) continue;
@@ -1032,7 +1075,7 @@ __device__ void cave_carve(CarveCtx &c, uint64_t &r, int ocx, int ocz, int y_hi)
             const float thick = cave_thickness(r);
             const int steps = 112 - lcg_int(r, 112 / 4);
             const uint64_t seed = lcg_long(r);
-            cave_tunnel(c, floor_level, seed, x, (double)y, z, hrm, vrm, thick, yaw, pitch, 0, steps, 1.0);
+            cave_tunnel<true>(c, floor_level, seed, x, (double)y, z, hrm, vrm, thick, yaw, pitch, 0, steps, 1.0);
         }
     }
 }
@@ -1170,22 +1213,62 @@ __device__ int64_t tree_dist(const BiomeTree &g, int i, const int64_t np[6]) {
     return ds;
 }
 
-__device__ __noinline__ int tree_search(const BiomeTree &g, int node, const int64_t np[6], int leaf) {
-    if (g.kids[node] == 0) return node;
-    int64_t best = leaf < 0 ? 0x7FFFFFFFFFFFFFFFLL : tree_dist(g, leaf, np);
-    int result = leaf, c = node + 1;
-    for (int k = 0; k < g.kids[node]; k++, c = g.end[c]) {
-        const int64_t d = tree_dist(g, c, np);
-        if (best > d) {
-            const int l2 = tree_search(g, c, np, result);
-            const int64_t d2 = (l2 == c) ? d : tree_dist(g, l2, np);
-            if (best > d2) {
-                best = d2;
-                result = l2;
+// Climate.RTree.SubTree.search (biome.c:35-48) with an explicit stack instead of recursion:
+// a frame is one inner node scanning its children (k-th child at index c) with the best leaf
+// so far.  The host checks at upload that no tree nests deeper than kTreeDepth.
+__device__ int tree_search(const BiomeTree &g, const int64_t np[6]) {
+    int fnode[kTreeDepth], fk[kTreeDepth], fc[kTreeDepth], fres[kTreeDepth];
+    int64_t fbest[kTreeDepth], fd[kTreeDepth];
+    if (g.kids[0] == 0) return 0;
+    int sp = 0;
+    fnode[0] = 0;
+    fk[0] = 0;
+    fc[0] = 1;
+    fres[0] = -1;
+    fbest[0] = 0x7FFFFFFFFFFFFFFFLL;
+    int ret = -1;
+    bool returning = false;
+    for (;;) {
+        if (returning) {   // the search below child fc[sp] returned leaf `ret`
+            const int c = fc[sp];
+            const int64_t d2 = (ret == c) ? fd[sp] : tree_dist(g, ret, np);
+            if (fbest[sp] > d2) {
+                fbest[sp] = d2;
+                fres[sp] = ret;
             }
+            fk[sp]++;
+            fc[sp] = g.end[c];
+            returning = false;
         }
+        if (fk[sp] < g.kids[fnode[sp]]) {
+            const int c = fc[sp];
+            const int64_t d = tree_dist(g, c, np);
+            if (fbest[sp] > d) {
+                fd[sp] = d;
+                if (g.kids[c] == 0) {   // a leaf returns itself
+                    ret = c;
+                    returning = true;
+                    continue;
+                }
+                if (sp + 1 >= kTreeDepth) return -1;
+                const int leaf = fres[sp];
+                sp++;
+                fnode[sp] = c;
+                fk[sp] = 0;
+                fc[sp] = c + 1;
+                fres[sp] = leaf;
+                fbest[sp] = leaf < 0 ? 0x7FFFFFFFFFFFFFFFLL : tree_dist(g, leaf, np);
+                continue;
+            }
+            fk[sp]++;
+            fc[sp] = g.end[c];
+            continue;
+        }
+        ret = fres[sp];
+        if (sp == 0) return ret;
+        sp--;
+        returning = true;
     }
-    return result;
 }
 
 constexpr int kFinishThreads = 64;
@@ -1258,7 +1341,8 @@ __global__ void __launch_bounds__(kFinishThreads) p2_finish_kernel(const P2Table
         np[4] = (int64_t)((float)depth * 10000.0f);
         np[5] = (int64_t)((float)ti.w * 10000.0f);
         const BiomeTree &g = T.trees[tree];
-        const int winner = g.biome[tree_search(g, 0, np, -1)];
+        const int leaf = tree_search(g, np);
+        const int winner = leaf >= 0 ? g.biome[leaf] : -1;
         for (int a = 0; a < 6; a++) R.biome_t[a] = np[a];
         R.biome_qx = qx;
         R.biome_qy = qy;
@@ -1349,6 +1433,13 @@ __global__ void p2_probe_kernel(const P2Tables *__restrict__ Tp, const P2World *
         case PR_BLOCK: v = (double)p2_block_at(T, W, jobs[job], x, y, z); break;
         case PR_HEIGHT_PRE: v = (double)p2_height(T, W, jobs[job], x, z, false); break;
         case PR_HEIGHT: v = (double)p2_height(T, W, jobs[job], x, z, true); break;
+        case PR_GRID_MAIN: {
+            const P2Chunk &J = jobs[job];
+            const int c = ((x >> 2) - J.chunk_x * 4) * 5 + ((z >> 2) - J.chunk_z * 4);
+            const int i = (y + 64) >> 3;
+            v = (c >= 0 && c < kGridCols && i >= 0 && i < kGridYs) ? J.main[c][i] : -1.0e300;
+            break;
+        }
         default: break;
     }
     out[q] = v;

@@ -22,6 +22,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstdint>
 
 #include "wg_device.cuh"
@@ -108,6 +109,8 @@ struct P2Tables {
 };
 
 constexpr int kWorldSlotsMax = 192;
+constexpr int kSplineDepth = 8;   // deepest spline nesting the evaluator holds (the game's is 5)
+constexpr int kTreeDepth = 16;    // deepest biome R-tree the search holds
 
 // One seed's phase-2 noise state.
 struct P2World {
@@ -139,8 +142,10 @@ struct P2Chunk {
     int64_t aq_loc[kAqCells];
     int32_t aq_level[kAqCells];
     uint8_t aq_type[kAqCells];
-    uint8_t cells[kCarveCells];    // CV_* per block of the chunk, index (lz << 4 | lx) | (y + 64) << 8
+    alignas(16) uint8_t cells[kCarveCells];   // CV_* per block, index (lz << 4 | lx) | (y + 64) << 8; copied as words
 };
+static_assert(offsetof(P2Chunk, cells) % 16 == 0, "carve cells are copied as 32-bit words");
+static_assert(offsetof(P2Perlin, perm) % 4 == 0, "tables are written as 32-bit words");
 
 // One hut to confirm and its result (the fields of lysh_hut_result, engine/tools/lysh/src/eval.h:63-85).
 struct P2Hut {
@@ -173,6 +178,7 @@ enum : int {
     PR_BLOCK,            // lysh_phase2_block_at   (chunk job)
     PR_HEIGHT_PRE,       // lysh_phase2_height_pre_carver (chunk job)
     PR_HEIGHT,           // lysh_phase2_height (chunk job, carved)
+    PR_GRID_MAIN,        // the chunk grid's stored corner value at the cell holding (x, y, z)
     PR_KINDS
 };
 

@@ -154,7 +154,8 @@ class Ref:
         lib.refh_ctx_density.restype = C.c_double
         lib.refh_ctx_density.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
         lib.refh_ctx_block.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
-        lib.refh_grade_scan.argtypes = [C.c_uint64] + [C.c_int] * 14 + [C.c_void_p, C.c_int, C.c_void_p]
+        lib.refh_grade_scan.argtypes = [C.c_uint64] + [C.c_int] * 13 + [C.c_void_p, C.c_int, C.c_void_p]
+        lib.refh_ctx_probe.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_longlong, C.c_void_p]
         lib.refh_phase1_seeds.restype = C.c_double
         lib.refh_phase1_seeds.argtypes = [C.c_void_p, C.c_longlong] + [C.c_int] * 12 + [C.c_void_p]
         lib.refh_cpu_count.restype = C.c_int
@@ -187,6 +188,20 @@ class Ref:
                                  org.ctypes.data, pm.ctypes.data)
         return h, pr, org, pm
 
+    def ctx(self, seed: int, r: dict, max_height: int = -50, tree: int = 0) -> "RefCtx":
+        """One lysh_search_ctx (phase 1 + phase 2 state of a seed; eval.c:70-107)."""
+        return RefCtx(self, seed, r, max_height, tree)
+
+    def grade_scan(self, seed: int, r: dict, max_height: int, rect, max_y: int, threads: int = 0, salt: int = 0,
+                   tree: int = 0, cap: int = 4096):
+        """lysh_grade_scan -> (hits [n, 12] int32, stats [7])."""
+        hits = np.zeros((cap, 12), np.int32)
+        st = np.zeros(7, np.int64)
+        self.lib.refh_grade_scan(seed & 0xFFFFFFFFFFFFFFFF, r["mc_1_18_2"], r["pre_26_2"], r["large_biomes"],
+                                 r["single_biome"], tree, max_height, *rect, salt, threads, max_y,
+                                 hits.ctypes.data, cap, st.ctypes.data)
+        return hits[:st[6]].copy(), st
+
     def phase1_seeds(self, seeds, r: dict, max_height: int, rect, threads: int = 0, salt: int = 0):
         """Times lysh's own phase-1 scan over many seeds; returns (seconds, accepted per seed)."""
         arr = as_u64(seeds)
@@ -198,3 +213,40 @@ class Ref:
 
     def cpu_count(self) -> int:
         return int(self.lib.refh_cpu_count())
+
+
+# lysh_hut_result fields in refh_ctx_eval's output order (ref_harness.c).
+EVAL_FIELDS = ("dir", "size_x", "size_z", "avg_y", "sum_h", "wet_columns", "flooded", "ok", "reject", "biome_ok",
+               "biome_winner", "biome_qx", "biome_qy", "biome_qz", "biome_occ_y", "t0", "t1", "t2", "t3", "t4", "t5",
+               "rx", "rz", "all_dry")
+
+
+class RefCtx:
+    """A lysh search context of the compiled reference: phase-2 probes and lysh_eval_hut."""
+
+    def __init__(self, ref: Ref, seed: int, r: dict, max_height: int, tree: int):
+        self.ref = ref
+        self.h = ref.lib.refh_ctx_new(seed & 0xFFFFFFFFFFFFFFFF, r["mc_1_18_2"], r["pre_26_2"], r["large_biomes"],
+                                      r["single_biome"], tree, max_height)
+
+    def probe(self, kind: int, xyz) -> np.ndarray:
+        pts = np.ascontiguousarray(np.asarray(xyz, dtype=np.int32).reshape(-1, 3))
+        out = np.zeros(len(pts))
+        self.ref.lib.refh_ctx_probe(self.h, kind, pts.ctypes.data, len(pts), out.ctypes.data)
+        return out
+
+    def eval_hut(self, hut_x: int, hut_z: int, max_y: int) -> dict:
+        out = np.zeros(24, np.int64)
+        self.ref.lib.refh_ctx_eval(self.h, hut_x, hut_z, max_y, out.ctypes.data)
+        return dict(zip(EVAL_FIELDS, (int(v) for v in out)))
+
+    def close(self) -> None:
+        if self.h:
+            self.ref.lib.refh_ctx_free(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -18,6 +18,7 @@
 #include <time.h>
 
 #include "biome.h"
+#include "column_top.h"
 #include "eval.h"
 #include "noise.h"
 #include "phase1.h"
@@ -186,6 +187,44 @@ double refh_ctx_density(void *h, int x, int y, int z) {
 int refh_ctx_block(void *h, int x, int y, int z) {
     lysh_search_ctx *c = (lysh_search_ctx *)h;
     return (int)lysh_phase2_block_at(&c->p2, x, y, z);
+}
+
+/* Phase-2 probes, kind for kind the ones the GPU engine's wg_p2_probe answers:
+ *   0 lysh_interp_calculate_noise_261 (interp_noise.c:100)   1 lysh_phase2_density_raw_at (phase2.c:151)
+ *   2 lysh_preliminary_surface_level (column_top.c:94)       3/4/5 terrain info cont / erosion / weirdness
+ *   6/7/8 terrain point offset / factor / peaks (26.1)        9 computeFluid: level * 4 + type (aquifer.c:327)
+ *   10 lysh_phase2_density_at  11 lysh_phase2_block_at  12 height before carvers  13 height after carvers */
+void refh_ctx_probe(void *h, int kind, const int *xyz, long long n, double *out) {
+    lysh_search_ctx *c = (lysh_search_ctx *)h;
+    for (long long i = 0; i < n; i++) {
+        const int x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+        double v = 0.0;
+        lysh_terrain_info ti;
+        switch (kind) {
+            case 0: v = lysh_interp_calculate_noise_261(&c->p2.interp, x, y, z); break;
+            case 1: v = lysh_phase2_density_raw_at(&c->p2, x, y, z); break;
+            case 2: v = (double)lysh_preliminary_surface_level(&c->p2.terrain, x, z); break;
+            case 3: case 4: case 5: case 6: case 7: case 8:
+                lysh_terrain_info_at(&c->p2.terrain, x >> 2, z >> 2, &ti);
+                v = kind == 3 ? ti.continentalness : kind == 4 ? ti.erosion : kind == 5 ? ti.weirdness
+                  : kind == 6 ? (double)ti.point.offset : kind == 7 ? (double)ti.point.factor
+                  : (double)ti.point.peaks;
+                break;
+            case 9: {
+                int level;
+                lysh_block_state type;
+                lysh_aquifer_compute_fluid(&c->p2.aquifer, x, y, z, &level, &type);
+                v = (double)level * 4.0 + (double)type;
+                break;
+            }
+            case 10: v = lysh_phase2_density_at(&c->p2, x, y, z); break;
+            case 11: v = (double)lysh_phase2_block_at(&c->p2, x, y, z); break;
+            case 12: v = (double)lysh_phase2_height_pre_carver(&c->p2, x, z); break;
+            case 13: v = (double)lysh_phase2_height(&c->p2, x, z); break;
+            default: break;
+        }
+        out[i] = v;
+    }
 }
 
 /* lysh_grade_scan: phase 1 + phase 2 over a rect for one seed.  stats[0..6] =
