@@ -149,6 +149,43 @@ def cpu_baseline(n_sample: int) -> dict:
                       f"(lysh_scan_rect per seed, one seed per thread)", "seconds": secs}
 
 
+def phase2_measure(eng, cands, opts, cpu: bool) -> dict:
+    """Phase 2 (lysh_eval_hut: biome gate, aquifer flood, carvers, footprint heights) of the step's
+    phase-1 survivors through wg_eval_huts, host buffers in and out (wall clock, 3 timed calls
+    after one warm-up); beside it the reference lysh on one host core for the same huts."""
+    if len(cands) == 0:
+        return {"huts": 0}
+    seeds = cands["seed"]
+    hx = cands["chunk_x"].astype(np.int64) * 16
+    hz = cands["chunk_z"].astype(np.int64) * 16
+    eng.eval_huts(seeds[:8], hx[:8], hz[:8], max_y=MAX_HEIGHT, opts=opts)
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        res = eng.eval_huts(seeds, hx, hz, max_y=MAX_HEIGHT, opts=opts)
+        times.append(time.perf_counter() - t0)
+    secs = statistics.median(times)
+    out = {"huts": int(len(cands)), "unit": "huts/s", "value": len(cands) / secs, "ms": 1e3 * secs,
+           "accepted": int(res["ok"].sum()), "rejected_biome": int((res["reject"] == 3).sum()),
+           "rejected_flood": int((res["reject"] == 2).sum()), "rejected_y": int((res["reject"] == 1).sum()),
+           "timing": "wall clock around wg_eval_huts (host arrays in and out), median of 3"}
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import bind
+        if os.path.exists(bind.REF_LIB):
+            ref = bind.Ref()
+            r = bind.rules(VERSION)
+            n = min(64, len(cands))
+            t0 = time.perf_counter()
+            for i in range(n):
+                with ref.ctx(int(seeds[i]), r, MAX_HEIGHT, 0) as ctx:
+                    ctx.eval_hut(int(hx[i]), int(hz[i]), MAX_HEIGHT)
+            dt = time.perf_counter() - t0
+            out["cpu_baseline"] = {"value": n / dt, "unit": "huts/s", "cores": 1, "kind": "reference",
+                                   "sample": f"first {n} huts: lysh_search_ctx_init + lysh_eval_hut per hut"}
+    return out
+
+
 def run_reference(args) -> None:
     """--impl reference: the reference's CPU scanner on the host cores, same metric."""
     rank = int(os.environ.get("RANK", "0"))
@@ -312,6 +349,7 @@ def main() -> None:
             },
             "clocks": cs,
         }
+        line["phase2"] = phase2_measure(eng, res.candidates, opts, cpu=(world == 1 and not args.no_cpu_baseline))
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(1 << 19)
         print(json.dumps(line), flush=True)
