@@ -186,6 +186,30 @@ def phase2_measure(eng, cands, opts, cpu: bool) -> dict:
     return out
 
 
+def deep_measure(eng, opts) -> dict:
+    """Deep Dive: the region walk (structure seeds x regions -> huts on mineshaft start chunks)
+    and the terrain stage (each spot's 65,536 upper-bit world seeds through phase 1 at -54),
+    wall clock around the public calls after one warm-up."""
+    rect = (-2048, 2048, -2048, 2048)
+    n_s48 = 16
+    eng.deep_starts(base=1, count=1, rect=(-64, 64, -64, 64))
+    t0 = time.perf_counter()
+    hits = eng.deep_starts(base=0x5EED0000, count=n_s48, rect=rect)
+    walk_s = time.perf_counter() - t0
+    regions = n_s48 * (rect[1] - rect[0]) * (rect[3] - rect[2])
+    spots = hits[:64]
+    eng.deep_spots(spots["s48"][:2], spots["chunk_x"][:2], spots["chunk_z"][:2], max_height=-54, opts=opts)
+    t0 = time.perf_counter()
+    surv, bad = eng.deep_spots(spots["s48"], spots["chunk_x"], spots["chunk_z"], max_height=-54, opts=opts)
+    spot_s = time.perf_counter() - t0
+    return {"walk": {"structure_seeds": n_s48, "regions": regions, "starts": int(len(hits)),
+                     "regions_per_s": regions / walk_s, "ms": 1e3 * walk_s},
+            "terrain": {"spots": int(len(spots)), "world_seeds": int(len(spots)) << 16,
+                        "world_seeds_per_s": (len(spots) << 16) / spot_s, "ms": 1e3 * spot_s,
+                        "survivors": int(len(surv)), "max_height": -54},
+            "timing": "wall clock around wg_deep_starts / wg_deep_spots (host buffers in and out)"}
+
+
 def run_reference(args) -> None:
     """--impl reference: the reference's CPU scanner on the host cores, same metric."""
     rank = int(os.environ.get("RANK", "0"))
@@ -350,6 +374,7 @@ def main() -> None:
             "clocks": cs,
         }
         line["phase2"] = phase2_measure(eng, res.candidates, opts, cpu=(world == 1 and not args.no_cpu_baseline))
+        line["deep_dive"] = deep_measure(eng, opts)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(1 << 19)
         print(json.dumps(line), flush=True)

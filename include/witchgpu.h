@@ -204,6 +204,38 @@ int wg_grade_scan(wg_engine *e, int64_t seed, const wg_opts *opts, int max_heigh
 int wg_p2_probe(wg_engine *e, int64_t seed, const wg_opts *opts, int kind, const int32_t *xyz, uint64_t n,
                 double *out);
 
+/* ---------------- Deep Dive: mineshaft starts under swamp huts ---------------- */
+
+/* A swamp hut whose chunk is also a mineshaft start chunk, for a 48-bit structure seed. */
+typedef struct {
+    uint64_t seed_index;         /* index of the structure seed in the request (list position / base offset) */
+    int64_t s48;                 /* structure seed (the world seed's low 48 bits) */
+    int32_t rx, rz;              /* hut region */
+    int32_t chunk_x, chunk_z;    /* hut chunk = mineshaft start chunk */
+    int64_t carver;              /* setLargeFeatureSeed state of that chunk (48 bits) */
+} wg_deep_start;
+
+/* The region walk of the Deep Dive solver: for every structure seed s48[0..n) (or, when s48 is
+ * NULL, s48_base + i) and every region of [rx0,rx1) x [rz0,rz1), the region's swamp-hut chunk
+ * and whether a mineshaft starts there (setLargeFeatureSeed + nextDouble() < 0.004).  Writes up
+ * to cap hits to out (host), sorted by (seed_index, rz, rx); *n_out = the number found.  Replaces the
+ * room walk of hut_lookup_v4 (rcWalkStep / walkStepCarver / rcIsStartS0,
+ * engine/gpu/room_core.h:40-175, engine/gpu/hut_lookup_v4_source.cu:47-75); the layout-catalog
+ * lookup and the solver's inversion tables are not part of it. */
+int wg_deep_starts(wg_engine *e, const int64_t *s48, int64_t s48_base, uint64_t n,
+                   int rx0, int rx1, int rz0, int rz1, wg_deep_start *out, uint64_t cap, uint64_t *n_out);
+
+/* The Deep Dive terrain stage (hut_lookup_v4 --spots, engine/gpu/hut_lookup_v4_source.cu:1262-1290):
+ * for each spot (s48[i], chunk_x[i], chunk_z[i]), the 65,536 world seeds (u << 48) | s48[i],
+ * u = 0..65535, through the phase-1 gates (lysh_phase1_check_ex at max_height) at the spot's
+ * region.  Writes the surviving (seed, region) of every spot whose hut lies in the spot chunk to
+ * out (host, up to cap, sorted; seed_index = i * 65536 + u); *n_out = the number found.  Spots
+ * that are not mineshaft start chunks are skipped and counted in *not_start (may be NULL), as
+ * hut_lookup_v4 reports them. */
+int wg_deep_spots(wg_engine *e, const int64_t *s48, const int32_t *chunk_x, const int32_t *chunk_z, uint64_t n_spots,
+                  const wg_opts *opts, int max_height, wg_candidate *out, uint64_t cap, uint64_t *n_out,
+                  uint64_t *not_start);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,7 +59,11 @@ CANDIDATE_DTYPE = np.dtype([("seed_index", "<u8"), ("seed", "<i8"), ("rx", "<i4"
 # Every symbol include/witchgpu.h declares.
 EXPORTS = ("wg_engine_open", "wg_engine_close", "wg_engine_error", "wg_parse_version", "wg_parse_preset",
            "wg_seed_check", "wg_seed_check_device", "wg_phase1_codes", "wg_seed_check_noalloc",
-           "wg_eval_huts", "wg_grade_scan", "wg_p2_probe")
+           "wg_eval_huts", "wg_grade_scan", "wg_p2_probe", "wg_deep_starts", "wg_deep_spots")
+
+# wg_deep_start: a swamp hut whose chunk is a mineshaft start chunk.
+DEEP_START_DTYPE = np.dtype([("seed_index", "<u8"), ("s48", "<i8"), ("rx", "<i4"), ("rz", "<i4"), ("chunk_x", "<i4"), ("chunk_z", "<i4"),
+                             ("carver", "<i8")])
 
 # wg_hut_result (lysh_hut_result's fields, engine/tools/lysh/src/eval.h:63-85).
 HUT_DTYPE = np.dtype([("hut_x", "<i4"), ("hut_z", "<i4"), ("rx", "<i4"), ("rz", "<i4"), ("dir", "<i4"),
@@ -115,6 +119,9 @@ def library() -> C.CDLL:
     lib.wg_grade_scan.argtypes = [vp, i64, C.POINTER(Opts), i32, i32, i32, i32, i32, i32, i32, vp, C.c_int32,
                                   C.POINTER(HutGrade)]
     lib.wg_p2_probe.argtypes = [vp, i64, C.POINTER(Opts), i32, vp, u64, vp]
+    lib.wg_deep_starts.argtypes = [vp, vp, i64, u64, i32, i32, i32, i32, vp, u64, C.POINTER(u64)]
+    lib.wg_deep_spots.argtypes = [vp, vp, vp, vp, u64, C.POINTER(Opts), i32, vp, u64, C.POINTER(u64),
+                                  C.POINTER(u64)]
     _lib = lib
     return lib
 
@@ -264,6 +271,45 @@ class Engine:
             raise self._err(rc, "wg_grade_scan")
         counts = {k: getattr(g, k) for k, _ in HutGrade._fields_}
         return hits[:g.hits_written].copy(), counts
+
+    def deep_starts(self, s48=None, base: int = 0, count: int = 0, rect=(-64, 64, -64, 64)) -> np.ndarray:
+        """Deep Dive region walk: huts on mineshaft start chunks (DEEP_START_DTYPE, sorted by
+        (seed_index, rz, rx))."""
+        if s48 is not None:
+            arr = np.ascontiguousarray(np.asarray([int(v) & 0xFFFFFFFFFFFF for v in s48], dtype=np.int64))
+            ptr, n = arr.ctypes.data, len(arr)
+        else:
+            arr, ptr, n = None, None, int(count)
+        cap = 1 << 12
+        while True:
+            out = np.zeros(cap, DEEP_START_DTYPE)
+            found = C.c_uint64()
+            rc = library().wg_deep_starts(self._h, ptr, int(base), n, *rect, out.ctypes.data, cap, C.byref(found))
+            if rc != WG_OK:
+                raise self._err(rc, "wg_deep_starts")
+            if found.value <= cap:
+                return out[:found.value].copy()
+            cap = int(found.value)
+
+    def deep_spots(self, s48, chunk_x, chunk_z, max_height: int = -54, version: str = DEFAULT_VERSION,
+                   preset: str = "NORMAL", opts: Opts | None = None) -> tuple[np.ndarray, int]:
+        """Deep Dive terrain stage: (survivors CANDIDATE_DTYPE with seed_index = spot * 65536 + u,
+        number of spots that are not mineshaft start chunks)."""
+        s = np.ascontiguousarray(np.asarray([int(v) & 0xFFFFFFFFFFFF for v in s48], dtype=np.int64))
+        cx = np.ascontiguousarray(chunk_x, dtype=np.int32)
+        cz = np.ascontiguousarray(chunk_z, dtype=np.int32)
+        o = opts if opts is not None else make_opts(version, preset)
+        cap = 1 << 12
+        while True:
+            out = np.zeros(cap, CANDIDATE_DTYPE)
+            found, bad = C.c_uint64(), C.c_uint64()
+            rc = library().wg_deep_spots(self._h, s.ctypes.data, cx.ctypes.data, cz.ctypes.data, len(s), C.byref(o),
+                                         max_height, out.ctypes.data, cap, C.byref(found), C.byref(bad))
+            if rc != WG_OK:
+                raise self._err(rc, "wg_deep_spots")
+            if found.value <= cap:
+                return out[:found.value].copy(), int(bad.value)
+            cap = int(found.value)
 
     def p2_probe(self, seed: int, kind, xyz, version: str = DEFAULT_VERSION, preset: str = "NORMAL",
                  opts: Opts | None = None) -> np.ndarray:

@@ -11,6 +11,7 @@
 
 #include "../../include/witchgpu.h"
 #include "wg_catalog.h"
+#include "wg_deep.cuh"
 #include "wg_engine_impl.h"
 #include "wg_phase1.cuh"
 
@@ -89,6 +90,8 @@ struct Request {
     int max_height, salt;
     int rx0, rx1, rz0, rz1;
     int8_t *d_codes, *d_tiers;   // optional per-region verdicts (device)
+    const int64_t *d_spot_s48;   // optional spots mode (BatchArgs::spot_s48 and the spot regions)
+    const int32_t *d_spot_rx, *d_spot_rz;
 };
 
 struct Sink {            // where phase-1 survivors go after each batch
@@ -197,6 +200,9 @@ int run_request(wg_engine *eng, const Request &rq, Sink &sink, wg_scan_stats &st
     a.hist = eng->hist;
     a.codes = rq.d_codes;
     a.tiers = rq.d_tiers;
+    a.spot_s48 = rq.d_spot_s48;
+    a.spot_rx = rq.d_spot_rx;
+    a.spot_rz = rq.d_spot_rz;
 
     uint64_t per_batch = std::min<uint64_t>(kMaxUnits, std::max<uint64_t>(32, kWorkPerBatch / win));
     if (rq.opts.single_biome)  // every region survives the climate stage
@@ -466,6 +472,82 @@ int wg_phase1_codes(wg_engine *eng, const int64_t *seeds, uint64_t gen_base, uin
     cudaFree(dc);
     cudaFree(dt);
     return rc;
+}
+
+int wg_deep_spots(wg_engine *eng, const int64_t *s48, const int32_t *chunk_x, const int32_t *chunk_z,
+                  uint64_t n_spots, const wg_opts *opts, int max_height, wg_candidate *out, uint64_t cap,
+                  uint64_t *n_out, uint64_t *not_start) {
+    if (!eng || (n_spots && (!s48 || !chunk_x || !chunk_z)) || (cap && !out)) return WG_ERR_ARG;
+    if (n_spots > (1ull << 16)) return WG_ERR_CAPACITY;   // 2^32 world seeds per call at most
+    WG_CUDA(cudaSetDevice(eng->device), "cudaSetDevice");
+    // keep the spots that are mineshaft start chunks (hut_lookup_v4 --spots skips the others)
+    std::vector<int64_t> ks;
+    std::vector<int32_t> krx, krz;
+    std::vector<uint64_t> kidx;
+    uint64_t bad = 0;
+    for (uint64_t i = 0; i < n_spots; i++) {
+        const DeepCtx c = deep_ctx((uint64_t)s48[i]);
+        if (!deep_is_start(deep_carver(c, chunk_x[i], chunk_z[i]))) {
+            bad++;
+            continue;
+        }
+        ks.push_back((int64_t)c.s48);
+        krx.push_back(chunk_x[i] >> 5);   // floorDiv by 32 chunks
+        krz.push_back(chunk_z[i] >> 5);
+        kidx.push_back(i);
+    }
+    if (not_start) *not_start = bad;
+    if (n_out) *n_out = 0;
+    if (ks.empty()) return WG_OK;
+    const uint64_t nk = ks.size();
+    int64_t *d_s = nullptr;
+    int32_t *d_x = nullptr, *d_z = nullptr;
+    cudaError_t e = cudaMalloc(&d_s, sizeof(int64_t) * nk);
+    if (e == cudaSuccess) e = cudaMalloc(&d_x, sizeof(int32_t) * nk);
+    if (e == cudaSuccess) e = cudaMalloc(&d_z, sizeof(int32_t) * nk);
+    if (e == cudaSuccess) e = cudaMemcpy(d_s, ks.data(), sizeof(int64_t) * nk, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_x, krx.data(), sizeof(int32_t) * nk, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_z, krz.data(), sizeof(int32_t) * nk, cudaMemcpyHostToDevice);
+    int rc = WG_OK;
+    std::vector<Candidate> found;
+    if (e != cudaSuccess) {
+        rc = eng->fail(WG_ERR_CUDA, "deep spots upload", e);
+    } else {
+        Request rq = make_request(opts, 0, nk << 16, max_height, 0, 0, 1, 0, 1);
+        rq.d_spot_s48 = d_s;
+        rq.d_spot_rx = d_x;
+        rq.d_spot_rz = d_z;
+        wg_scan_stats st;
+        std::memset(&st, 0, sizeof st);
+        Sink sink;
+        sink.host = &found;
+        rc = run_request(eng, rq, sink, st);
+    }
+    cudaFree(d_s);
+    cudaFree(d_x);
+    cudaFree(d_z);
+    if (rc) return rc;
+    // survivors whose hut is the spot chunk, renumbered by the caller's spot index
+    std::vector<wg_candidate> keep;
+    for (const Candidate &c : found) {
+        const uint64_t k = c.seed_index >> 16, u = c.seed_index & 0xFFFF;
+        const uint64_t i = kidx[k];
+        if (c.chunk_x != chunk_x[i] || c.chunk_z != chunk_z[i]) continue;
+        wg_candidate w;
+        w.seed_index = (i << 16) | u;
+        w.seed = c.seed;
+        w.rx = c.rx;
+        w.rz = c.rz;
+        w.chunk_x = c.chunk_x;
+        w.chunk_z = c.chunk_z;
+        keep.push_back(w);
+    }
+    std::sort(keep.begin(), keep.end(),
+              [](const wg_candidate &x, const wg_candidate &y) { return x.seed_index < y.seed_index; });
+    const uint64_t nw = std::min<uint64_t>(cap, keep.size());
+    for (uint64_t i = 0; i < nw; i++) out[i] = keep[i];
+    if (n_out) *n_out = keep.size();
+    return WG_OK;
 }
 
 }  // extern "C"

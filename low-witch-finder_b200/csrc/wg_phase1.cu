@@ -62,8 +62,12 @@ void upload_tables(const NoiseSpec *specs, const ClimateStep *steps_normal, cons
 __device__ __forceinline__ uint64_t unit_seed_index(const BatchArgs &a, uint32_t u) { return (a.unit0 + u) / a.n_win; }
 __device__ __forceinline__ uint64_t unit_window(const BatchArgs &a, uint32_t u) { return (a.unit0 + u) % a.n_win; }
 __device__ __forceinline__ uint64_t seed_value(const BatchArgs &a, uint64_t g) {
+    if (a.spot_s48) return ((g & 0xFFFFull) << 48) | ((uint64_t)a.spot_s48[g >> 16] & 0xFFFFFFFFFFFFull);
     return a.seeds ? (uint64_t)a.seeds[g] : splitmix64(a.gen_base + g);
 }
+// Rect origin of seed g (shifted to the seed's spot region in spots mode).
+__device__ __forceinline__ int rect_x0(const BatchArgs &a, uint64_t g) { return a.spot_rx ? a.rx0 + a.spot_rx[g >> 16] : a.rx0; }
+__device__ __forceinline__ int rect_z0(const BatchArgs &a, uint64_t g) { return a.spot_rz ? a.rz0 + a.spot_rz[g >> 16] : a.rz0; }
 // Number of regions in a unit's window.
 __device__ __forceinline__ uint32_t window_len(const BatchArgs &a, uint64_t w) {
     uint64_t start = w * a.win;
@@ -71,9 +75,9 @@ __device__ __forceinline__ uint32_t window_len(const BatchArgs &a, uint64_t w) {
     return (uint32_t)(left < a.win ? left : a.win);
 }
 // Region (rx, rz) of global region index r (rz outer, rx inner: search.c:148-149).
-__device__ __forceinline__ void region_xz(const BatchArgs &a, uint64_t r, int &rx, int &rz) {
-    rz = a.rz0 + (int)(r / (uint64_t)a.rw);
-    rx = a.rx0 + (int)(r % (uint64_t)a.rw);
+__device__ __forceinline__ void region_xz(const BatchArgs &a, uint64_t g, uint64_t r, int &rx, int &rz) {
+    rz = rect_z0(a, g) + (int)(r / (uint64_t)a.rw);
+    rx = rect_x0(a, g) + (int)(r % (uint64_t)a.rw);
 }
 
 __device__ __forceinline__ void note_code(const BatchArgs &a, uint64_t g, uint64_t r, int code, int tier) {
@@ -205,6 +209,7 @@ struct ClimateSmem {
     uint64_t g[kUnits], rbase[kUnits], seed[kUnits];   // seed index, first region, world seed
     uint32_t col0[kUnits];                     // column of the unit's first region in its rect row
     int row0[kUnits];                          // rz of the unit's first region
+    int rx0u[kUnits];                          // rect x origin of the unit's seed
     unsigned int hist[P1_KINDS + kTiers];
     uint32_t grad[kGradWords];
     ClimateSteps steps;
@@ -378,7 +383,8 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
         S.rbase[tid] = rbase;
         S.seed[tid] = seed;
         S.col0[tid] = (uint32_t)(rbase % (uint64_t)a.rw);
-        S.row0[tid] = a.rz0 + (int)(rbase / (uint64_t)a.rw);
+        S.row0[tid] = rect_z0(a, g) + (int)(rbase / (uint64_t)a.rw);
+        S.rx0u[tid] = rect_x0(a, g);
     }
     TierCounts tc;
 
@@ -420,7 +426,7 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
             if (j >= S.end[qu]) continue;
             const uint32_t t = S.col0[qu] + j;   // region offset from the unit's first row start
             const uint32_t rw = (uint32_t)a.rw;
-            const int rz = S.row0[qu] + (int)(t / rw), rx = a.rx0 + (int)(t % rw);
+            const int rz = S.row0[qu] + (int)(t / rw), rx = S.rx0u[qu] + (int)(t % rw);
             int cx, cz;
             hut_chunk(S.seed[qu], rx, rz, a.salt, cx, cz);
             S.pos[q] = make_int2(cx, cz);
@@ -795,7 +801,7 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
                 const int r2 = (int)(em >> 16);
                 const uint32_t jr = a.surv_region[S.roff[r2] + (em & 0xFFFFu)];
                 int rx, rz, cx, cz;
-                region_xz(a, S.rbase[r2] + jr, rx, rz);
+                region_xz(a, S.rg[r2], S.rbase[r2] + jr, rx, rz);
                 hut_chunk(S.rseed[r2], rx, rz, a.salt, cx, cz);
                 S.hx[e] = cx * 16 + 3;
                 S.hz[e] = cz * 16 + 3;
@@ -949,7 +955,7 @@ __global__ void __launch_bounds__(kThreadsC) ladder_kernel(BatchArgs a) {
         const uint64_t r = unit_window(a, u) * a.win + jr;
         const uint64_t seed = seed_value(a, g);
         int rx, rz, cx, cz;
-        region_xz(a, r, rx, rz);
+        region_xz(a, g, r, rx, rz);
         hut_chunk(seed, rx, rz, a.salt, cx, cz);
         const int hut_x = cx * 16, hut_z = cz * 16;
         const int hx = hut_x + 3, hz = hut_z + 3;

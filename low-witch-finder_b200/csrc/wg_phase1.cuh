@@ -99,6 +99,12 @@ struct BatchArgs {
     unsigned long long *hist;     // [P1_KINDS + kTiers] funnel + erosion tier histogram, zeroed per batch
     int8_t *codes;                // optional [n_seeds * n_regions] reject code per (seed, region)
     int8_t *tiers;                // optional, same shape: erosion tier (-1 if none)
+
+    // Optional spots mode (the Deep Dive terrain stage): seed g is the world seed
+    // (g & 0xFFFF) << 48 | spot_s48[g >> 16], one of the 65,536 upper-bit variants of a 48-bit
+    // structure seed, and its rect is shifted by the spot's region (spot_rx, spot_rz)[g >> 16].
+    const int64_t *spot_s48 = nullptr;
+    const int32_t *spot_rx = nullptr, *spot_rz = nullptr;
 };
 
 // One evaluation step of the climate state machine (a single y=0 Perlin sample).

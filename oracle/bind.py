@@ -73,7 +73,23 @@ class Port:
         lib.wo_scan_seeds.restype = C.c_longlong
         lib.wo_scan_seeds.argtypes = [C.c_void_p, C.c_uint64, C.c_longlong, C.POINTER(WoOpts)] + [C.c_int] * 7 + \
             [C.c_void_p, C.c_longlong, C.c_void_p]
+        lib.wo_mineshaft_start.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_void_p]
+        lib.wo_deep_starts.restype = C.c_longlong
+        lib.wo_deep_starts.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                       C.c_longlong]
         self.lib = lib
+
+    def mineshaft_start(self, s48: int, cx: int, cz: int) -> tuple[bool, int]:
+        carver = C.c_uint64()
+        ok = self.lib.wo_mineshaft_start(s48 & 0xFFFFFFFFFFFF, cx, cz, C.byref(carver))
+        return bool(ok), carver.value
+
+    def deep_starts(self, s48s, rect, cap: int = 1 << 16) -> np.ndarray:
+        """Rows (s48, rx, rz, cx, cz, carver) of hut chunks that are mineshaft starts."""
+        s = np.ascontiguousarray(np.asarray([int(v) & 0xFFFFFFFFFFFF for v in s48s], dtype=np.uint64))
+        out = np.zeros((cap, 6), np.int64)
+        n = self.lib.wo_deep_starts(s.ctypes.data, len(s), *rect, out.ctypes.data, cap)
+        return out[:min(n, cap)].copy()
 
     @staticmethod
     def _o(r: dict) -> WoOpts:
@@ -130,6 +146,33 @@ class Port:
         out = out[:found]
         out.sort(order=["seed_index", "rz", "rx"])
         return out, hist
+
+
+ROOM_LIB = os.path.join(HERE, "_ref", "libroom_ref.so")
+
+
+class RoomRef:
+    """The reference's own Deep Dive room walk (engine/gpu/room_core.h), compiled into oracle/_ref/."""
+
+    def __init__(self, path: str = ROOM_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is missing (make -C oracle ref needs the reference sources)")
+        lib = C.CDLL(path)
+        lib.roomh_is_start.argtypes = [C.c_int64, C.c_int, C.c_int]
+        lib.roomh_walk.restype = C.c_longlong
+        lib.roomh_walk.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                   C.c_longlong]
+        self.lib = lib
+
+    def is_start(self, s48: int, cx: int, cz: int) -> bool:
+        return bool(self.lib.roomh_is_start(C.c_int64(s48 & 0xFFFFFFFFFFFF), cx, cz))
+
+    def walk(self, s48s, rect, cap: int = 1 << 16) -> np.ndarray:
+        """Rows (s48, rx, rz, cx, cz) of hut chunks that are mineshaft starts."""
+        s = np.ascontiguousarray(np.asarray([int(v) & 0xFFFFFFFFFFFF for v in s48s], dtype=np.int64))
+        out = np.zeros((cap, 5), np.int64)
+        n = self.lib.roomh_walk(s.ctypes.data, len(s), *rect, out.ctypes.data, cap)
+        return out[:min(n, cap)].copy()
 
 
 class Ref:

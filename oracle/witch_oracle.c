@@ -645,3 +645,43 @@ long long wo_scan_seeds(const uint64_t *seeds, uint64_t gen_base, long long n, c
     if (reject_hist) memcpy(reject_hist, j.hist, sizeof(j.hist));
     return j.found;
 }
+
+/* ------------------------------------------------------------------ */
+/* Deep Dive: mineshaft start chunks under swamp huts                  */
+/* engine/gpu/room_core.h:34-73 (setLargeFeatureSeed + nextDouble()    */
+/* < 0.004), :146-175 (the region walk)                                */
+/* ------------------------------------------------------------------ */
+int wo_mineshaft_start(uint64_t s48, int cx, int cz, uint64_t *carver_out) {
+    const uint64_t S = s48 & LCG_MASK;
+    uint64_t st = (S ^ LCG_MUL) & LCG_MASK;
+    const uint64_t a = lcg_long(&st);
+    const uint64_t b = lcg_long(&st);
+    const uint64_t carver =
+        ((uint64_t)((int64_t)cx * (int64_t)a) ^ (uint64_t)((int64_t)cz * (int64_t)b) ^ S) & LCG_MASK;
+    if (carver_out) *carver_out = carver;
+    st = (carver ^ LCG_MUL) & LCG_MASK;
+    const int64_t hi = (int64_t)(uint32_t)lcg_bits(&st, 26);
+    const int64_t lo = (int64_t)(uint32_t)lcg_bits(&st, 27);
+    return (double)((hi << 27) + lo) * 1.1102230246251565404e-16 < 0.004;
+}
+
+long long wo_deep_starts(const uint64_t *s48s, long long n, int rx0, int rx1, int rz0, int rz1, int64_t *out,
+                         long long cap) {
+    long long found = 0;
+    for (long long i = 0; i < n; i++) {
+        const uint64_t S = s48s[i] & LCG_MASK;
+        for (int rz = rz0; rz < rz1; rz++)
+            for (int rx = rx0; rx < rx1; rx++) {
+                int cx, cz;
+                uint64_t carver;
+                wo_hut_in_region(S, rx, rz, 14357620, &cx, &cz);
+                if (!wo_mineshaft_start(S, cx, cz, &carver)) continue;
+                if (found < cap) {
+                    int64_t *o = out + 6 * found;
+                    o[0] = (int64_t)S; o[1] = rx; o[2] = rz; o[3] = cx; o[4] = cz; o[5] = (int64_t)carver;
+                }
+                found++;
+            }
+    }
+    return found;
+}

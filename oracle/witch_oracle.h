@@ -47,6 +47,13 @@ long long wo_phase1_rect(uint64_t seed, const wo_opts *o, int max_height, int sa
                          signed char *codes, signed char *tiers, int *cx, int *cz);
 
 /* The 38 fixed-order probe doubles. */
+/* Deep Dive (engine/gpu/room_core.h): is chunk (cx, cz) a mineshaft start of structure seed
+ * s48; and every region of a rect whose swamp-hut chunk is one, as rows (s48, rx, rz, cx, cz,
+ * carver), seed-major, rz outer, rx inner.  Returns the number found (rows beyond cap unwritten). */
+int wo_mineshaft_start(uint64_t s48, int cx, int cz, uint64_t *carver_out);
+long long wo_deep_starts(const uint64_t *s48s, long long n, int rx0, int rx1, int rz0, int rz1, int64_t *out,
+                         long long cap);
+
 int wo_probe(uint64_t seed, const wo_opts *o, int hut_x, int hut_z, int max_height, double *out);
 
 /* Phase-1 survivors of many seeds over one rect (threads <= 0: all cores).  Seeds are

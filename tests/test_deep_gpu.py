@@ -1,0 +1,47 @@
+"""GPU: the Deep Dive entry points against the reference's own values.
+
+wg_deep_starts (the region walk) must return exactly the rows of the reference's room walker
+(tests/golden/deep_starts.npz) with the oracle's carver state; wg_deep_spots (the terrain stage
+over the 65,536 upper-bit variants) must keep exactly the variants lysh's phase 1 keeps
+(tests/golden/deep_spots.npz) — for hunt.py's TERRAIN_REFERENCE spots, the known seeds.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_deep_starts_match_reference(engine, port):
+    d = np.load(os.path.join(GOLDEN, "deep_starts.npz"))
+    for k, rect in enumerate(d["rects"]):
+        got = engine.deep_starts(s48=d["s48"], rect=tuple(int(v) for v in rect))
+        rows = np.stack([got["s48"], got["rx"], got["rz"], got["chunk_x"], got["chunk_z"]], 1).astype(np.int64)
+        assert np.array_equal(rows, d[f"rows{k}"]), k
+        want = port.deep_starts(d["s48"], tuple(int(v) for v in rect))
+        assert np.array_equal(got["carver"], want[:, 5]), k
+
+
+def test_deep_starts_generator_and_capacity(engine, port):
+    got = engine.deep_starts(base=12345, count=6, rect=(-300, 300, -200, 200))
+    want = port.deep_starts([12345 + i for i in range(6)], (-300, 300, -200, 200), cap=1 << 15)
+    assert len(got) == len(want) > 4096   # exercises the capacity retry
+    assert np.array_equal(np.stack([got["s48"], got["rx"], got["rz"]], 1), want[:, :3])
+
+
+def test_deep_spots_match_reference(engine):
+    d = np.load(os.path.join(GOLDEN, "deep_spots.npz"))
+    surv, bad = engine.deep_spots(d["s48"], d["chunk_x"], d["chunk_z"], max_height=int(d["max_height"]))
+    assert bad == int((d["start"] == 0).sum())
+    off = np.concatenate([[0], np.cumsum(d["counts"])])
+    want = [(i << 16) | int(u) for i in range(len(d["s48"])) for u in d["passed"][off[i]:off[i + 1]]]
+    assert surv["seed_index"].tolist() == want
+    for row in surv:
+        i, u = int(row["seed_index"]) >> 16, int(row["seed_index"]) & 0xFFFF
+        assert (int(row["seed"]) & ((1 << 64) - 1)) == (u << 48) | int(d["s48"][i])
+        assert (row["chunk_x"], row["chunk_z"]) == (d["chunk_x"][i], d["chunk_z"][i])
