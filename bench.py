@@ -210,6 +210,80 @@ def deep_measure(eng, opts) -> dict:
             "timing": "wall clock around wg_deep_starts / wg_deep_spots (host buffers in and out)"}
 
 
+def jobs_measure(wg, eng, n_jobs: int = 65536) -> dict:
+    """Uneven batched jobs: the 65,536 jobs of the splitmix64(3) job stream (1..4,096 seeds,
+    radius 1..64, floors -50..-54) through one wg_seed_check_jobs call, host seed lists in and
+    survivors out (wall clock; device time from the call's own CUDA events), after a warm-up on
+    the first 64 jobs."""
+    jobs = wg.uneven_jobs(n_jobs=n_jobs)
+    eng.seed_check_jobs(jobs[:64])
+    t0 = time.perf_counter()
+    got, st = eng.seed_check_jobs(jobs)
+    secs = time.perf_counter() - t0
+    seeds = sum(len(j["seeds"]) for j in jobs)
+    return {"jobs": n_jobs, "seeds": seeds, "checks": st["scanned"], "survivors": st["accepted"],
+            "seeds_per_s": seeds / secs, "checks_per_s": st["scanned"] / secs, "ms": 1e3 * secs,
+            "gpu_ms": st["gpu_ms"], "kernel_ms": st["kernel_ms"], "batches": st["batches"],
+            "gpu_launches": sum(st["kernel_launches"]),
+            "timing": "wall clock around wg_seed_check_jobs (host seed lists in, survivors out)"}
+
+
+def serving_measure(wg, n_req: int = 200) -> dict:
+    """Serving: one wg_server; the request stream of serving_requests (1..10^6 seeds as splitmix64
+    generators, radius 1..32, floors -50..-54).  Peak = all requests submitted at once (checks/s
+    over the makespan); then the same requests with Poisson arrivals at 30 %, 70 % and 100 % of
+    that peak, p50 / p99 of submit-to-done latency and the seeds/s delivered."""
+    import threading
+    base_reqs = wg.serving_requests(n_req, rate_per_s=1.0)
+    work = [q["gen"][1] * (q["rect"][1] - q["rect"][0]) * (q["rect"][3] - q["rect"][2]) for q in base_reqs]
+    out = {"requests": n_req, "seeds": int(sum(q["gen"][1] for q in base_reqs)), "checks": int(sum(work))}
+    with wg.Server(0) as srv:
+        for q in base_reqs[:8]:   # warm-up
+            srv.wait(srv.submit(gen=q["gen"], rect=q["rect"], max_height=q["max_height"]))
+        t0 = time.perf_counter()
+        ids = [srv.submit(gen=q["gen"], rect=q["rect"], max_height=q["max_height"]) for q in base_reqs]
+        for j in ids:
+            srv.wait(j)
+            srv.take(j)
+        peak_s = time.perf_counter() - t0
+        peak = sum(work) / peak_s
+        out["peak"] = {"checks_per_s": peak, "seeds_per_s": out["seeds"] / peak_s, "ms": 1e3 * peak_s}
+        loads = []
+        for frac in (0.3, 0.7, 1.0):
+            rate = frac * peak / (sum(work) / n_req)
+            reqs = wg.serving_requests(n_req, rate_per_s=rate)
+            ids = [None] * n_req
+
+            def feed():
+                t_start = time.perf_counter()
+                for i, q in enumerate(reqs):
+                    delay = q["t"] - (time.perf_counter() - t_start)
+                    if delay > 0:
+                        time.sleep(delay)
+                    ids[i] = srv.submit(gen=q["gen"], rect=q["rect"], max_height=q["max_height"])
+
+            t0 = time.perf_counter()
+            th = threading.Thread(target=feed)
+            th.start()
+            th.join()
+            lat = []
+            for j in ids:
+                st = srv.wait(j)
+                srv.take(j)
+                lat.append(st["latency_ms"])
+            secs = time.perf_counter() - t0
+            lat = np.array(lat)
+            loads.append({"offered": frac, "rate_per_s": rate, "p50_ms": float(np.percentile(lat, 50)),
+                          "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat.max()),
+                          "seeds_per_s": out["seeds"] / secs, "checks_per_s": sum(work) / secs})
+        out["loads"] = loads
+        st = srv.stats()
+        out["gpu_launches"] = sum(st["kernel_launches"])
+    out["timing"] = ("wall clock; latency = submit to done inside the library (steady clock); requests "
+                     "are generator jobs (seed lists made on the host at submit)")
+    return out
+
+
 def run_reference(args) -> None:
     """--impl reference: the reference's CPU scanner on the host cores, same metric."""
     rank = int(os.environ.get("RANK", "0"))
@@ -239,6 +313,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-jobs", action="store_true", help="skip the batched-jobs and serving measurements")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -375,6 +450,9 @@ def main() -> None:
         }
         line["phase2"] = phase2_measure(eng, res.candidates, opts, cpu=(world == 1 and not args.no_cpu_baseline))
         line["deep_dive"] = deep_measure(eng, opts)
+        if world == 1 and not args.no_jobs:
+            line["jobs"] = jobs_measure(wg, eng)
+            line["serving"] = serving_measure(wg)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(1 << 19)
         print(json.dumps(line), flush=True)

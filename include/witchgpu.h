@@ -236,6 +236,68 @@ int wg_deep_spots(wg_engine *e, const int64_t *s48, const int32_t *chunk_x, cons
                   const wg_opts *opts, int max_height, wg_candidate *out, uint64_t cap, uint64_t *n_out,
                   uint64_t *not_start);
 
+/* ---------------- job server: batched and streamed Seed Check jobs ---------------- */
+
+/* One Seed Check job: seeds[0..n_seeds) (copied at submit) or, when seeds is NULL,
+ * splitmix64(gen_base + i); every seed x every region of [rx0,rx1) x [rz0,rz1) at max_height. */
+typedef struct {
+    const int64_t *seeds;
+    uint64_t gen_base;
+    uint64_t n_seeds;
+    int rx0, rx1, rz0, rz1;
+    int max_height;
+    int salt;                    /* 0 = the swamp-hut salt */
+    wg_opts opts;
+} wg_job;
+
+typedef struct {
+    int32_t done;                /* 1 when the job's survivors are ready */
+    int32_t status;              /* WG_OK, or the error the job ended with */
+    uint64_t found;              /* phase-1 survivors */
+    double queue_ms;             /* submit -> start of the batch that ran it */
+    double latency_ms;           /* submit -> done */
+    uint64_t batch_jobs;         /* jobs flattened into that batch (the job included) */
+} wg_job_status;
+
+/* Many Seed Check jobs at once (uneven seed counts, rects and floors), flattened into shared
+ * device batches: every batch covers slices of several jobs through the kernels' job table.
+ * Survivors are written job by job (job order, then seed_index, rz, rx; seed_index is the seed's
+ * position in its job); job_found[i] (if not NULL) = job i's count; *n_out = all, at most cap
+ * written.  Each job's survivors equal wg_seed_check on that job alone.  The reference has one
+ * job per phase1_scan request (engine/gpu/low54/phase1_scan.cu:1328-1387). */
+int wg_seed_check_jobs(wg_engine *e, const wg_job *jobs, uint64_t n_jobs, wg_candidate *out, uint64_t cap,
+                       uint64_t *n_out, uint64_t *job_found, wg_scan_stats *stats);
+
+typedef struct wg_server wg_server;
+
+/* A job server on CUDA device `device`: one worker thread with its own engine takes the queued
+ * jobs, flattens every queued job with the same rect, max_height, salt and rules into one
+ * request (their seed lists concatenated), runs it, and hands each job its survivors.  Seeds
+ * of queued jobs stay in host memory until their batch runs (max_queued_seeds bounds them;
+ * submit returns WG_ERR_CAPACITY beyond it).  The reference has no job server; lysh's
+ * session API (engine/tools/lysh/src/eval.h:180-205) and hunt.py's worker protocol
+ * (hunt.py:1276-1332) are the interfaces it batches. */
+int wg_server_open(int device, uint64_t max_queued_seeds, wg_server **out);
+
+/* Queue a job; *job_id identifies it.  Non-blocking. */
+int wg_server_submit(wg_server *s, const wg_job *job, uint64_t *job_id);
+
+/* The job's status; when wait_ms > 0, waits up to that long for it to finish. */
+int wg_server_poll(wg_server *s, uint64_t job_id, int wait_ms, wg_job_status *st);
+
+/* A finished job's survivors (sorted by seed_index within the job, then rz, rx; seed_index is
+ * the seed's position in the job); *n_out = all of them, at most cap written.  The job's
+ * results are released once they have all been taken. */
+int wg_server_take(wg_server *s, uint64_t job_id, wg_candidate *out, uint64_t cap, uint64_t *n_out);
+
+/* The server's totals so far: batches, kernel launches and device times, (seed, region) checks
+ * and survivors of the finished jobs. */
+int wg_server_stats(wg_server *s, wg_scan_stats *st);
+
+/* Stop the worker (finishing the batch in flight) and release everything; jobs not finished
+ * are dropped. */
+void wg_server_close(wg_server *s);
+
 #ifdef __cplusplus
 }
 #endif

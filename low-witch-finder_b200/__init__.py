@@ -13,6 +13,7 @@ bench.py and tests/conftest.py do.
 from __future__ import annotations
 
 import ctypes as C
+import functools
 import os
 
 import numpy as np
@@ -59,7 +60,9 @@ CANDIDATE_DTYPE = np.dtype([("seed_index", "<u8"), ("seed", "<i8"), ("rx", "<i4"
 # Every symbol include/witchgpu.h declares.
 EXPORTS = ("wg_engine_open", "wg_engine_close", "wg_engine_error", "wg_parse_version", "wg_parse_preset",
            "wg_seed_check", "wg_seed_check_device", "wg_phase1_codes", "wg_seed_check_noalloc",
-           "wg_eval_huts", "wg_grade_scan", "wg_p2_probe", "wg_deep_starts", "wg_deep_spots")
+           "wg_eval_huts", "wg_grade_scan", "wg_p2_probe", "wg_deep_starts", "wg_deep_spots",
+           "wg_seed_check_jobs", "wg_server_open", "wg_server_submit", "wg_server_poll", "wg_server_take",
+           "wg_server_stats", "wg_server_close")
 
 # wg_deep_start: a swamp hut whose chunk is a mineshaft start chunk.
 DEEP_START_DTYPE = np.dtype([("seed_index", "<u8"), ("s48", "<i8"), ("rx", "<i4"), ("rz", "<i4"), ("chunk_x", "<i4"), ("chunk_z", "<i4"),
@@ -85,6 +88,19 @@ class HutGrade(C.Structure):
     _fields_ = [("scanned", C.c_int64), ("evaluated", C.c_int64), ("accepted", C.c_int64),
                 ("rejected_y", C.c_int64), ("rejected_flood", C.c_int64), ("rejected_biome", C.c_int64),
                 ("hits_written", C.c_int32), ("ms", C.c_double), ("p2_ms", C.c_double)]
+
+
+
+class Job(C.Structure):
+    """wg_job: one Seed Check job (seeds or a splitmix64 generator, rect, floor, rules)."""
+    _fields_ = [("seeds", C.c_void_p), ("gen_base", C.c_uint64), ("n_seeds", C.c_uint64), ("rx0", C.c_int),
+                ("rx1", C.c_int), ("rz0", C.c_int), ("rz1", C.c_int), ("max_height", C.c_int), ("salt", C.c_int),
+                ("opts", Opts)]
+
+
+class JobStatus(C.Structure):
+    _fields_ = [("done", C.c_int32), ("status", C.c_int32), ("found", C.c_uint64), ("queue_ms", C.c_double),
+                ("latency_ms", C.c_double), ("batch_jobs", C.c_uint64)]
 
 _lib = None
 
@@ -122,6 +138,14 @@ def library() -> C.CDLL:
     lib.wg_deep_starts.argtypes = [vp, vp, i64, u64, i32, i32, i32, i32, vp, u64, C.POINTER(u64)]
     lib.wg_deep_spots.argtypes = [vp, vp, vp, vp, u64, C.POINTER(Opts), i32, vp, u64, C.POINTER(u64),
                                   C.POINTER(u64)]
+    lib.wg_seed_check_jobs.argtypes = [vp, C.POINTER(Job), u64, vp, u64, C.POINTER(u64), vp, C.POINTER(Stats)]
+    lib.wg_server_open.argtypes = [i32, u64, C.POINTER(vp)]
+    lib.wg_server_submit.argtypes = [vp, C.POINTER(Job), C.POINTER(u64)]
+    lib.wg_server_poll.argtypes = [vp, u64, i32, C.POINTER(JobStatus)]
+    lib.wg_server_take.argtypes = [vp, u64, vp, u64, C.POINTER(u64)]
+    lib.wg_server_stats.argtypes = [vp, C.POINTER(Stats)]
+    lib.wg_server_close.argtypes = [vp]
+    lib.wg_server_close.restype = None
     _lib = lib
     return lib
 
@@ -201,7 +225,8 @@ class Engine:
         """Phase-1 survivors of every seed x every region of rect = (rx0, rx1, rz0, rz1)."""
         keep, ptr, base, n = self._seeds(seeds, gen)
         o = opts if opts is not None else make_opts(version, preset)
-        cap = 1 << 12
+        # one survivor per 65,536 checks fits the usual floors; a fuller result re-runs once
+        cap = min(1 << 26, max(1 << 12, (n * max(0, rect[1] - rect[0]) * max(0, rect[3] - rect[2])) >> 16))
         while True:
             out = np.zeros(cap, CANDIDATE_DTYPE)
             found = C.c_uint64()
@@ -291,6 +316,33 @@ class Engine:
                 return out[:found.value].copy()
             cap = int(found.value)
 
+    def seed_check_jobs(self, jobs) -> tuple[list[np.ndarray], dict]:
+        """wg_seed_check_jobs: many jobs (dicts with seeds= or gen=(base, count), rect=, max_height=,
+        and version= / preset= / opts= / salt=) flattened into shared batches.  Returns each job's
+        survivors (CANDIDATE_DTYPE, seed_index = position in the job) and the funnel."""
+        arr = (Job * max(len(jobs), 1))()
+        keep = [_fill_job(arr[i], j) for i, j in enumerate(jobs)]
+        per = np.zeros(max(len(jobs), 1), np.uint64)
+        # room for one survivor per 65,536 checks (about 500 x the rate at floor -50), so the
+        # call normally runs once; a fuller result re-runs it with the exact size
+        checks = sum(int(arr[i].n_seeds) * (arr[i].rx1 - arr[i].rx0) * (arr[i].rz1 - arr[i].rz0)
+                     for i in range(len(jobs)))
+        cap = min(1 << 26, max(1 << 12, checks >> 16))
+        while True:
+            out = np.zeros(cap, CANDIDATE_DTYPE)
+            found = C.c_uint64()
+            st = Stats()
+            rc = library().wg_seed_check_jobs(self._h, arr, len(jobs), out.ctypes.data, cap, C.byref(found),
+                                              per.ctypes.data, C.byref(st))
+            if rc != WG_OK:
+                raise self._err(rc, "wg_seed_check_jobs")
+            if found.value <= cap:
+                break
+            cap = int(found.value)
+        del keep
+        bounds = np.concatenate([[0], np.cumsum(per[:len(jobs)].astype(np.int64))])
+        return [out[bounds[i]:bounds[i + 1]].copy() for i in range(len(jobs))], st.as_dict()
+
     def deep_spots(self, s48, chunk_x, chunk_z, max_height: int = -54, version: str = DEFAULT_VERSION,
                    preset: str = "NORMAL", opts: Opts | None = None) -> tuple[np.ndarray, int]:
         """Deep Dive terrain stage: (survivors CANDIDATE_DTYPE with seed_index = spot * 65536 + u,
@@ -366,3 +418,157 @@ def seed_check_noalloc(d_seeds_ptr, gen_base: int, n_seeds: int, rect, max_heigh
     if rc != WG_OK:
         raise EngineError(f"wg_seed_check_noalloc failed with status {rc}")
     return int(n.value)
+
+
+@functools.lru_cache(maxsize=64)
+def _cached_opts(version: str, preset: str) -> Opts:
+    return make_opts(version, preset)
+
+
+def _fill_job(dst: Job, job: dict):
+    """Fills a wg_job from a job dict; returns the seed array the struct points into."""
+    keep, ptr, base, n = Engine._seeds(job.get("seeds"), job.get("gen"))
+    rect = job.get("rect", (-4, 5, -4, 5))
+    o = job.get("opts") or _cached_opts(job.get("version", DEFAULT_VERSION), job.get("preset", "NORMAL"))
+    dst.seeds = ptr
+    dst.gen_base = base
+    dst.n_seeds = n
+    dst.rx0, dst.rx1, dst.rz0, dst.rz1 = (int(v) for v in rect)
+    dst.max_height = int(job.get("max_height", -50))
+    dst.salt = int(job.get("salt", 0))
+    dst.opts = o
+    return keep
+
+
+class Server:
+    """wg_server: a job server on one device.  submit() queues a job and returns at once; the
+    library's worker thread admits queued jobs as device seed slots free up and runs them in
+    shared batches; poll() / take() return a job's status and survivors."""
+
+    def __init__(self, device: int = 0, max_queued_seeds: int = 0):
+        lib = library()
+        h = C.c_void_p()
+        rc = lib.wg_server_open(device, max_queued_seeds, C.byref(h))
+        if rc != WG_OK:
+            raise EngineError(f"wg_server_open(device={device}) failed with status {rc}")
+        self._h = h
+
+    def submit(self, **job) -> int:
+        j = Job()
+        keep = _fill_job(j, job)
+        jid = C.c_uint64()
+        rc = library().wg_server_submit(self._h, C.byref(j), C.byref(jid))
+        del keep
+        if rc != WG_OK:
+            raise EngineError(f"wg_server_submit failed with status {rc}")
+        return int(jid.value)
+
+    def poll(self, job_id: int, wait_ms: int = 0) -> dict:
+        st = JobStatus()
+        rc = library().wg_server_poll(self._h, job_id, wait_ms, C.byref(st))
+        if rc != WG_OK:
+            raise EngineError(f"wg_server_poll({job_id}) failed with status {rc}")
+        return {"done": bool(st.done), "status": st.status, "found": st.found, "queue_ms": st.queue_ms,
+                "latency_ms": st.latency_ms, "batch_jobs": st.batch_jobs}
+
+    def wait(self, job_id: int, timeout_s: float = 600.0) -> dict:
+        import time
+        end = time.monotonic() + timeout_s
+        while True:
+            st = self.poll(job_id, 200)
+            if st["done"]:
+                return st
+            if time.monotonic() > end:
+                raise EngineError(f"job {job_id} not done after {timeout_s} s")
+
+    def take(self, job_id: int) -> np.ndarray:
+        cap = 1 << 10
+        while True:
+            out = np.zeros(cap, CANDIDATE_DTYPE)
+            n = C.c_uint64()
+            rc = library().wg_server_take(self._h, job_id, out.ctypes.data, cap, C.byref(n))
+            if rc != WG_OK:
+                raise EngineError(f"wg_server_take({job_id}) failed with status {rc}")
+            if n.value <= cap:
+                return out[:n.value].copy()
+            cap = int(n.value)
+
+    def stats(self) -> dict:
+        st = Stats()
+        rc = library().wg_server_stats(self._h, C.byref(st))
+        if rc != WG_OK:
+            raise EngineError(f"wg_server_stats failed with status {rc}")
+        return st.as_dict()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            library().wg_server_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------------------------
+# Synthetic job streams (the reference measures on no public dataset).  Every draw is one step
+# of the splitmix64 stream x_k = splitmix64(base + k), k = 0, 1, 2, ...; U(x) = (x >> 11) * 2^-53.
+# ---------------------------------------------------------------------------------------------
+
+def _u01(x: int) -> float:
+    return (x >> 11) * (1.0 / (1 << 53))
+
+
+def splitmix64_array(base: int, count: int) -> np.ndarray:
+    """splitmix64(base + i) for i < count, vectorised (uint64 wrap-around arithmetic)."""
+    with np.errstate(over="ignore"):
+        x = (np.uint64(base & 0xFFFFFFFFFFFFFFFF) + np.arange(count, dtype=np.uint64)) + np.uint64(0x9E3779B97F4A7C15)
+        z = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return (z ^ (z >> np.uint64(31))).view(np.int64)
+
+
+def uneven_jobs(n_jobs: int = 65536, base: int = 3, max_seeds: int = 4096, max_radius: int = 64) -> list[dict]:
+    """The uneven batched-jobs workload.  Per job, four draws then its seeds:
+    n = floor((max_seeds + 1) ** U) seeds (log-uniform 1..max_seeds), radius r = floor((max_radius + 1) ** U)
+    (1..max_radius, rect [-r, r + 1)^2), floor g = -50 - (x mod 5), mode = x & 1 (1 = "or lower",
+    0 = "exactly": phase 1 gates on maxHeight = g in both modes), then the n seeds are the next n
+    values of the stream."""
+    jobs = []
+    k = 0
+    for _ in range(n_jobs):
+        x = [splitmix64(base + k + i) for i in range(4)]
+        k += 4
+        n = max(1, min(max_seeds, int((max_seeds + 1) ** _u01(x[0]))))
+        r = max(1, min(max_radius, int((max_radius + 1) ** _u01(x[1]))))
+        g = -50 - (x[2] % 5)
+        jobs.append({"seeds": splitmix64_array(base + k, n), "rect": (-r, r + 1, -r, r + 1), "max_height": g,
+                     "mode": "or_lower" if x[3] & 1 else "exactly"})
+        k += n
+    return jobs
+
+
+def serving_requests(n_req: int, rate_per_s: float, base: int = 5, max_seeds: int = 10 ** 6,
+                     max_radius: int = 32) -> list[dict]:
+    """The serving workload: Poisson arrivals at rate_per_s.  Per request, four draws: the
+    inter-arrival gap -ln(1 - U) / rate, n = floor((max_seeds + 1) ** U) seeds, radius
+    r = floor((max_radius + 1) ** U), floor g = -50 - (x mod 5); the seeds are
+    splitmix64(gen_base + i) with gen_base the request's last draw (a generator job)."""
+    import math
+    reqs = []
+    t = 0.0
+    for i in range(n_req):
+        x = [splitmix64(base + 4 * i + q) for q in range(4)]
+        t += -math.log(1.0 - _u01(x[0])) / rate_per_s
+        n = max(1, min(max_seeds, int((max_seeds + 1) ** _u01(x[1]))))
+        r = max(1, min(max_radius, int((max_radius + 1) ** _u01(x[2]))))
+        reqs.append({"t": t, "gen": (x[3], n), "rect": (-r, r + 1, -r, r + 1), "max_height": -50 - (x[3] % 5)})
+    return reqs

@@ -17,20 +17,8 @@
 
 using namespace wg;
 
-namespace {
-
-// Per-batch work budget: (seed, region) checks per batch and units per batch.
-constexpr uint64_t kWorkPerBatch = 1ull << 27;
-constexpr uint32_t kMaxUnits = 1u << 20;
-constexpr uint32_t kCapRec = kMaxUnits + (1u << 16);
-constexpr uint32_t kCapSurv = 1u << 23;
-constexpr uint32_t kCapDeep = 1u << 20;
-constexpr uint32_t kCapOut = 1u << 20;
-
 // Regions per unit window: a whole seed when its rect is small, else 2048-region windows.
-uint32_t window_for(uint64_t n_regions) { return n_regions <= 4096 ? (uint32_t)n_regions : 2048u; }
-
-}  // namespace
+uint32_t wg::window_for(uint64_t n_regions) { return n_regions <= 4096 ? (uint32_t)n_regions : 2048u; }
 
 // Climate evaluation steps (see ClimateStep): the tiered erosion sequence
 // (engine/tools/lysh/src/noise.c:387-459) followed by plain y=0 DoublePerlin samples of
@@ -80,29 +68,10 @@ void wg::build_climate_steps(const NoiseSpec *specs, int erosion, int temperatur
         if (e_ != cudaSuccess) return eng->fail(WG_ERR_CUDA, what, e_); \
     } while (0)
 
-namespace {
+namespace wg {
 
-struct Request {
-    const int64_t *d_seeds;   // device seeds or nullptr (generator)
-    uint64_t gen_base;
-    uint64_t n_seeds;
-    wg_opts opts;
-    int max_height, salt;
-    int rx0, rx1, rz0, rz1;
-    int8_t *d_codes, *d_tiers;   // optional per-region verdicts (device)
-    const int64_t *d_spot_s48;   // optional spots mode (BatchArgs::spot_s48 and the spot regions)
-    const int32_t *d_spot_rx, *d_spot_rz;
-};
-
-struct Sink {            // where phase-1 survivors go after each batch
-    std::vector<Candidate> *host = nullptr;
-    Candidate *dev = nullptr;
-    uint64_t dev_cap = 0;
-    uint64_t found = 0;
-};
-
-int run_batch(wg_engine *eng, const Request &rq, const BatchArgs &proto, uint64_t unit0, uint32_t n_units,
-              Sink &sink, wg_scan_stats &st) {
+int run_batch(wg_engine *eng, const BatchArgs &proto, uint64_t unit0, uint32_t n_units, Sink &sink,
+              wg_scan_stats &st) {
     BatchArgs a = proto;
     a.unit0 = unit0;
     a.n_units = n_units;
@@ -135,9 +104,9 @@ int run_batch(wg_engine *eng, const Request &rq, const BatchArgs &proto, uint64_
         if (n_units <= 32) return eng->fail(WG_ERR_CAPACITY, "phase-1 work list full even for 32 units");
         st.retries++;
         uint32_t half = n_units / 2;
-        int rc = run_batch(eng, rq, proto, unit0, half, sink, st);
+        int rc = run_batch(eng, proto, unit0, half, sink, st);
         if (rc) return rc;
-        return run_batch(eng, rq, proto, unit0 + half, n_units - half, sink, st);
+        return run_batch(eng, proto, unit0 + half, n_units - half, sink, st);
     }
     for (int i = 0; i < P1_KINDS; i++) st.reject_hist[i] += (int64_t)eng->h_hist[i];
     for (int i = 0; i < kTiers; i++) st.tier_hist[i] += (int64_t)eng->h_hist[P1_KINDS + i];
@@ -161,31 +130,14 @@ int run_batch(wg_engine *eng, const Request &rq, const BatchArgs &proto, uint64_
     return WG_OK;
 }
 
-int run_request(wg_engine *eng, const Request &rq, Sink &sink, wg_scan_stats &st) {
-    if (rq.rx1 <= rq.rx0 || rq.rz1 <= rq.rz0 || rq.n_seeds == 0) return eng->fail(WG_ERR_ARG, "empty request");
-    const uint64_t rw = (uint64_t)((int64_t)rq.rx1 - rq.rx0), rh = (uint64_t)((int64_t)rq.rz1 - rq.rz0);
-    const uint64_t n_regions = rw * rh;
-    const uint32_t win = window_for(n_regions);
-    const uint64_t n_win = (n_regions + win - 1) / win;
-    const uint64_t units = rq.n_seeds * n_win;
-
+BatchArgs base_args(wg_engine *eng, const wg_opts &opts, int salt) {
     BatchArgs a;
     std::memset(&a, 0, sizeof a);
-    a.seeds = rq.d_seeds;
-    a.gen_base = rq.gen_base;
-    a.win = win;
-    a.n_win = n_win;
-    a.n_regions = n_regions;
-    a.rx0 = rq.rx0;
-    a.rz0 = rq.rz0;
-    a.rw = (int)rw;
-    a.rh = (int)rh;
-    a.salt = rq.salt ? rq.salt : 14357620;
-    a.max_height = rq.max_height;
-    a.mc_1_18_2 = rq.opts.mc_1_18_2;
-    a.pre_26_2 = rq.opts.pre_26_2;
-    a.single_biome = rq.opts.single_biome;
-    a.large_biomes = rq.opts.large_biomes;
+    a.salt = salt ? salt : 14357620;
+    a.mc_1_18_2 = opts.mc_1_18_2;
+    a.pre_26_2 = opts.pre_26_2;
+    a.single_biome = opts.single_biome;
+    a.large_biomes = opts.large_biomes;
     a.rec_unit = eng->rec_unit;
     a.rec_off = eng->rec_off;
     a.rec_cnt = eng->rec_cnt;
@@ -198,6 +150,28 @@ int run_request(wg_engine *eng, const Request &rq, Sink &sink, wg_scan_stats &st
     a.cap_out = kCapOut;
     a.counters = eng->counters;
     a.hist = eng->hist;
+    return a;
+}
+
+int run_request(wg_engine *eng, const Request &rq, Sink &sink, wg_scan_stats &st) {
+    if (rq.rx1 <= rq.rx0 || rq.rz1 <= rq.rz0 || rq.n_seeds == 0) return eng->fail(WG_ERR_ARG, "empty request");
+    const uint64_t rw = (uint64_t)((int64_t)rq.rx1 - rq.rx0), rh = (uint64_t)((int64_t)rq.rz1 - rq.rz0);
+    const uint64_t n_regions = rw * rh;
+    const uint32_t win = window_for(n_regions);
+    const uint64_t n_win = (n_regions + win - 1) / win;
+    const uint64_t units = rq.n_seeds * n_win;
+
+    BatchArgs a = base_args(eng, rq.opts, rq.salt);
+    a.seeds = rq.d_seeds;
+    a.gen_base = rq.gen_base;
+    a.win = win;
+    a.n_win = n_win;
+    a.n_regions = n_regions;
+    a.rx0 = rq.rx0;
+    a.rz0 = rq.rz0;
+    a.rw = (int)rw;
+    a.rh = (int)rh;
+    a.max_height = rq.max_height;
     a.codes = rq.d_codes;
     a.tiers = rq.d_tiers;
     a.spot_s48 = rq.d_spot_s48;
@@ -210,12 +184,16 @@ int run_request(wg_engine *eng, const Request &rq, Sink &sink, wg_scan_stats &st
     st.scanned = (int64_t)(rq.n_seeds * n_regions);
     for (uint64_t u0 = 0; u0 < units; u0 += per_batch) {
         uint32_t n = (uint32_t)std::min<uint64_t>(per_batch, units - u0);
-        int rc = run_batch(eng, rq, a, u0, n, sink, st);
+        int rc = run_batch(eng, a, u0, n, sink, st);
         if (rc) return rc;
     }
     st.accepted = (int64_t)sink.found;
     return WG_OK;
 }
+
+}  // namespace wg
+
+namespace {
 
 int stage_seeds(wg_engine *eng, const int64_t *seeds, uint64_t n, const int64_t **d_seeds) {
     *d_seeds = nullptr;

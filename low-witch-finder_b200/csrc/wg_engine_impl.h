@@ -7,6 +7,7 @@
 #include <string>
 #include <vector>
 
+#include "../../include/witchgpu.h"
 #include "wg_phase1.cuh"
 
 namespace wg {
@@ -56,3 +57,46 @@ struct wg_engine {
 
 // Frees the phase-2 state of an engine (called by wg_engine_close).
 void p2_release(wg_engine *eng);
+
+namespace wg {
+
+// Per-batch work budget: (seed, region) checks per batch and units per batch, and the sizes of
+// the engine's phase-1 work lists.
+constexpr uint64_t kWorkPerBatch = 1ull << 27;
+constexpr uint32_t kMaxUnits = 1u << 20;
+constexpr uint32_t kCapRec = kMaxUnits + (1u << 16);
+constexpr uint32_t kCapSurv = 1u << 23;
+constexpr uint32_t kCapDeep = 1u << 20;
+constexpr uint32_t kCapOut = 1u << 20;
+
+// Regions per unit window: a whole seed when its rect is small, else 2048-region windows.
+uint32_t window_for(uint64_t n_regions);
+
+// One phase-1 request over one rect (wg_engine.cu).
+struct Request {
+    const int64_t *d_seeds;   // device seeds or nullptr (generator)
+    uint64_t gen_base;
+    uint64_t n_seeds;
+    wg_opts opts;
+    int max_height, salt;
+    int rx0, rx1, rz0, rz1;
+    int8_t *d_codes, *d_tiers;   // optional per-region verdicts (device)
+    const int64_t *d_spot_s48;   // optional spots mode (BatchArgs::spot_s48 and the spot regions)
+    const int32_t *d_spot_rx, *d_spot_rz;
+};
+
+struct Sink {            // where phase-1 survivors go after each batch
+    std::vector<Candidate> *host = nullptr;
+    Candidate *dev = nullptr;
+    uint64_t dev_cap = 0;
+    uint64_t found = 0;
+};
+
+// The BatchArgs fields every batch of an engine shares (work lists, counters, rules, salt).
+BatchArgs base_args(wg_engine *eng, const wg_opts &opts, int salt);
+// Runs units [unit0, unit0 + n_units) of `proto` (three kernels, one sync), halving on overflow.
+int run_batch(wg_engine *eng, const BatchArgs &proto, uint64_t unit0, uint32_t n_units, Sink &sink,
+              wg_scan_stats &st);
+int run_request(wg_engine *eng, const Request &rq, Sink &sink, wg_scan_stats &st);
+
+}  // namespace wg

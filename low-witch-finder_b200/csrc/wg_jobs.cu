@@ -1,0 +1,526 @@
+// Batched and streamed Seed Check jobs: the scheduler that flattens jobs with different seed
+// counts, rects and floors into shared phase-1 batches (wg_seed_check_jobs), and the job server
+// built on it (wg_server_*: a worker thread with its own engine, continuous batching).
+//
+// The reference runs one job per process invocation (phase1_scan --worker, one request line at a
+// time: engine/gpu/low54/phase1_scan.cu:1328-1387) or one lysh session per seed
+// (engine/tools/lysh/src/eval.h:180-205); the results per job are the same as there.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+#include "../../include/witchgpu.h"
+#include "wg_device.cuh"
+#include "wg_jobs.h"
+
+namespace wg {
+
+namespace {
+
+constexpr uint64_t kMaxRectSide = 1ull << 24;
+constexpr uint64_t kStageSeeds = 1ull << 21;   // pinned staging for the seeds of small jobs (16 MiB)
+
+bool same_rules(const SchedJob &x, const SchedJob &y) {
+    return x.salt == y.salt && x.opts.mc_1_18_2 == y.opts.mc_1_18_2 && x.opts.single_biome == y.opts.single_biome &&
+           x.opts.pre_26_2 == y.opts.pre_26_2 && x.opts.large_biomes == y.opts.large_biomes;
+}
+
+bool candidate_order(const Candidate &x, const Candidate &y) {
+    if (x.seed_index != y.seed_index) return x.seed_index < y.seed_index;
+    if (x.rz != y.rz) return x.rz < y.rz;
+    return x.rx < y.rx;
+}
+
+}  // namespace
+
+int sched_job_init(SchedJob &j, const wg_job &spec) {
+    if (spec.n_seeds == 0 || spec.rx1 <= spec.rx0 || spec.rz1 <= spec.rz0) return WG_ERR_ARG;
+    const uint64_t rw = (uint64_t)((int64_t)spec.rx1 - spec.rx0), rh = (uint64_t)((int64_t)spec.rz1 - spec.rz0);
+    if (rw > kMaxRectSide || rh > kMaxRectSide) return WG_ERR_ARG;
+    j.opts = spec.opts;
+    j.salt = spec.salt ? spec.salt : 14357620;
+    j.max_height = spec.max_height;
+    j.rx0 = spec.rx0;
+    j.rz0 = spec.rz0;
+    j.rw = (int)rw;
+    j.n_regions = rw * rh;
+    j.win = window_for(j.n_regions);
+    j.n_win = (j.n_regions + j.win - 1) / j.win;
+    if (spec.n_seeds > ~0ull / j.n_win) return WG_ERR_ARG;
+    j.units = spec.n_seeds * j.n_win;
+    try {
+        j.seeds.resize(spec.n_seeds);
+    } catch (...) {
+        return WG_ERR_NOMEM;
+    }
+    if (spec.seeds) std::memcpy(j.seeds.data(), spec.seeds, sizeof(int64_t) * spec.n_seeds);
+    else
+        for (uint64_t i = 0; i < spec.n_seeds; i++) j.seeds[i] = (int64_t)splitmix64(spec.gen_base + i);
+    return WG_OK;
+}
+
+Scheduler::Scheduler(wg_engine *eng, uint64_t arena_seeds, uint64_t step_work)
+    : eng_(eng), arena_cap_(std::max<uint64_t>(arena_seeds, 1)), step_work_(std::max<uint64_t>(step_work, 1)) {}
+
+Scheduler::~Scheduler() {
+    cudaFree(d_arena_);
+    cudaFree(d_table_);
+    cudaFreeHost(h_table_);
+    cudaFreeHost(h_stage_);
+}
+
+int Scheduler::init() {
+    cudaError_t e = cudaMalloc(&d_arena_, sizeof(int64_t) * arena_cap_);
+    if (e != cudaSuccess) return eng_->fail(WG_ERR_NOMEM, "job seed arena", e);
+    stage_cap_ = std::min<uint64_t>(arena_cap_, kStageSeeds);
+    e = cudaMallocHost(&h_stage_, sizeof(int64_t) * stage_cap_);
+    if (e != cudaSuccess) return eng_->fail(WG_ERR_NOMEM, "seed staging buffer", e);
+    free_.clear();
+    free_[0] = arena_cap_;
+    return WG_OK;
+}
+
+uint64_t Scheduler::alloc(uint64_t n) {
+    for (auto it = free_.begin(); it != free_.end(); ++it) {   // first fit
+        if (it->second < n) continue;
+        const uint64_t off = it->first, len = it->second;
+        free_.erase(it);
+        if (len > n) free_[off + n] = len - n;
+        return off;
+    }
+    return ~0ull;
+}
+
+void Scheduler::release(uint64_t off, uint64_t n) {
+    auto it = free_.emplace(off, n).first;
+    auto next = std::next(it);
+    if (next != free_.end() && it->first + it->second == next->first) {   // merge with the next range
+        it->second += next->second;
+        free_.erase(next);
+    }
+    if (it != free_.begin()) {   // and with the previous one
+        auto prev = std::prev(it);
+        if (prev->first + prev->second == it->first) {
+            prev->second += it->second;
+            free_.erase(it);
+        }
+    }
+}
+
+int Scheduler::flush_uploads() {
+    // runs that continue each other in both buffers go up as one copy
+    size_t i = 0;
+    while (i < runs_.size()) {
+        Run r = runs_[i++];
+        while (i < runs_.size() && runs_[i].arena_off == r.arena_off + r.n && runs_[i].stage_off == r.stage_off + r.n)
+            r.n += runs_[i++].n;
+        cudaError_t e = cudaMemcpyAsync(d_arena_ + r.arena_off, h_stage_ + r.stage_off, sizeof(int64_t) * r.n,
+                                        cudaMemcpyHostToDevice, eng_->stream);
+        if (e != cudaSuccess) return eng_->fail(WG_ERR_CUDA, "upload job seeds", e);
+    }
+    runs_.clear();
+    return WG_OK;
+}
+
+bool Scheduler::admit(SchedJob *j, int *rc) {
+    *rc = WG_OK;
+    const uint64_t n = j->seeds.size();
+    const uint64_t off = alloc(n);
+    if (off == ~0ull) return false;
+    cudaError_t e = cudaSuccess;
+    if (n > stage_cap_ / 4) {
+        // a large job goes straight from its (pageable) host copy, read before the call returns
+        e = cudaMemcpyAsync(d_arena_ + off, j->seeds.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice,
+                            eng_->stream);
+    } else {
+        if (stage_used_ + n > stage_cap_) {   // staging full: send what it holds and reuse it
+            *rc = flush_uploads();
+            if (*rc == WG_OK) e = cudaStreamSynchronize(eng_->stream);
+            stage_used_ = 0;
+        }
+        if (*rc == WG_OK && e == cudaSuccess) {
+            std::memcpy(h_stage_ + stage_used_, j->seeds.data(), sizeof(int64_t) * n);
+            runs_.push_back(Run{off, stage_used_, n});
+            stage_used_ += n;
+        }
+    }
+    if (*rc == WG_OK && e != cudaSuccess) *rc = eng_->fail(WG_ERR_CUDA, "upload job seeds", e);
+    if (*rc) {
+        release(off, n);
+        return false;
+    }
+    j->arena_off = off;
+    order_.insert(j);
+    return true;
+}
+
+int Scheduler::step(std::vector<SchedJob *> &finished, std::vector<SchedJob *> &members) {
+    members.clear();
+    if (order_.empty()) return WG_OK;
+    int rc = flush_uploads();   // the staged seeds of newly admitted jobs
+    if (rc) return rc;
+    const SchedJob &lead = **order_.begin();
+    uint64_t budget = step_work_;
+    if (lead.opts.single_biome)   // every region survives the climate stage
+        budget = std::min<uint64_t>(budget, kCapSurv / 2);
+    std::vector<JobGeom> &table = table_;
+    table.clear();
+    std::vector<uint64_t> took;
+    uint64_t units = 0;
+    int misses = 0;   // consecutive jobs whose windows no longer fit the budget
+    for (SchedJob *j : order_) {
+        if (units >= kMaxUnits || budget == 0 || misses >= 64) break;
+        if (!same_rules(*j, lead)) continue;
+        uint64_t k = std::min<uint64_t>(j->units - j->dispatched, kMaxUnits - units);
+        uint64_t kb = budget / j->win;
+        if (kb == 0) {
+            if (units) {
+                misses++;
+                continue;
+            }
+            kb = 1;
+        }
+        misses = 0;
+        k = std::min(k, kb);
+        JobGeom g;
+        std::memset(&g, 0, sizeof g);
+        g.unit0 = units;
+        g.first = j->dispatched;
+        g.seed0 = j->arena_off;
+        g.n_win = j->n_win;
+        g.n_regions = j->n_regions;
+        g.win = j->win;
+        g.rx0 = j->rx0;
+        g.rz0 = j->rz0;
+        g.rw = j->rw;
+        g.max_height = j->max_height;
+        table.push_back(g);
+        took.push_back(k);
+        members.push_back(j);
+        units += k;
+        budget -= std::min(budget, k * (uint64_t)j->win);
+    }
+    // the table: pinned host copy (rewritten only after the batch's closing sync) -> device
+    if (table.size() > table_cap_) {
+        cudaFree(d_table_);
+        cudaFreeHost(h_table_);
+        d_table_ = nullptr;
+        h_table_ = nullptr;
+        table_cap_ = 0;
+        const uint32_t cap = (uint32_t)std::max<size_t>(table.size() * 2, 256);
+        cudaError_t e = cudaMalloc(&d_table_, sizeof(JobGeom) * cap);
+        if (e == cudaSuccess) e = cudaMallocHost(&h_table_, sizeof(JobGeom) * cap);
+        if (e != cudaSuccess) return eng_->fail(WG_ERR_NOMEM, "job table", e);
+        table_cap_ = cap;
+    }
+    std::memcpy(h_table_, table.data(), sizeof(JobGeom) * table.size());
+    cudaError_t e = cudaMemcpyAsync(d_table_, h_table_, sizeof(JobGeom) * table.size(), cudaMemcpyHostToDevice,
+                                    eng_->stream);
+    if (e != cudaSuccess) return eng_->fail(WG_ERR_CUDA, "upload job table", e);
+
+    BatchArgs a = base_args(eng_, lead.opts, lead.salt);
+    a.seeds = d_arena_;
+    a.jobs = d_table_;
+    a.n_jobs = (uint32_t)table.size();
+    found_.clear();
+    Sink sink;
+    sink.host = &found_;
+    rc = run_batch(eng_, a, 0, (uint32_t)units, sink, stats);
+    stage_used_ = 0;   // the batch's closing sync also ended the staged copies
+    if (rc) return rc;
+
+    // survivors back to their jobs: seed_index is an arena slot until here
+    std::vector<std::pair<uint64_t, size_t>> by_off(members.size());
+    for (size_t i = 0; i < members.size(); i++) by_off[i] = {members[i]->arena_off, i};
+    std::sort(by_off.begin(), by_off.end());
+    for (Candidate c : found_) {
+        auto it = std::upper_bound(by_off.begin(), by_off.end(), std::make_pair(c.seed_index, ~(size_t)0));
+        if (it == by_off.begin()) continue;   // not reachable: every slot belongs to a member
+        --it;
+        SchedJob *j = members[it->second];
+        c.seed_index -= j->arena_off;
+        if (c.seed_index >= j->seeds.size()) continue;
+        j->found.push_back(c);
+    }
+    for (size_t i = 0; i < members.size(); i++) {
+        SchedJob *j = members[i];
+        order_.erase(j);   // its key changes
+        j->dispatched += took[i];
+        if (j->dispatched < j->units) {
+            order_.insert(j);
+            continue;
+        }
+        std::sort(j->found.begin(), j->found.end(), candidate_order);
+        release(j->arena_off, j->seeds.size());
+        stats.scanned += (int64_t)(j->seeds.size() * j->n_regions);
+        stats.accepted += (int64_t)j->found.size();
+        finished.push_back(j);
+    }
+    return WG_OK;
+}
+
+void Scheduler::fail_all(int rc, std::vector<SchedJob *> &finished) {
+    cudaStreamSynchronize(eng_->stream);   // no staged copy may still read the staging buffer
+    for (SchedJob *j : order_) {
+        j->status = rc;
+        release(j->arena_off, j->seeds.size());
+        finished.push_back(j);
+    }
+    order_.clear();
+    runs_.clear();
+    stage_used_ = 0;
+}
+
+}  // namespace wg
+
+using namespace wg;
+
+extern "C" int wg_seed_check_jobs(wg_engine *eng, const wg_job *jobs, uint64_t n_jobs, wg_candidate *out,
+                                  uint64_t cap, uint64_t *n_out, uint64_t *job_found, wg_scan_stats *stats) {
+    if (!eng || (n_jobs && !jobs) || (cap && !out)) return WG_ERR_ARG;
+    const auto t0 = Clock::now();
+    cudaError_t e = cudaSetDevice(eng->device);
+    if (e != cudaSuccess) return eng->fail(WG_ERR_CUDA, "cudaSetDevice", e);
+    std::vector<SchedJob> js(n_jobs);
+    uint64_t total = 0, largest = 0;
+    for (uint64_t i = 0; i < n_jobs; i++) {
+        const int rc = sched_job_init(js[i], jobs[i]);
+        if (rc) return eng->fail(rc, rc == WG_ERR_NOMEM ? "job seeds" : "job: empty or oversized");
+        js[i].id = i;
+        total += js[i].seeds.size();
+        largest = std::max<uint64_t>(largest, js[i].seeds.size());
+    }
+    // seeds resident on the device at once: all of them, up to 2^27 (1 GiB), and the largest job
+    Scheduler sched(eng, std::min<uint64_t>(std::max<uint64_t>(total, 1), std::max<uint64_t>(largest, 1ull << 27)),
+                    kWorkPerBatch);
+    int rc = sched.init();
+    if (rc) return rc;
+    e = cudaEventRecord(eng->ev0, eng->stream);
+    if (e != cudaSuccess) return eng->fail(WG_ERR_CUDA, "event", e);
+    std::vector<SchedJob *> finished, members;
+    uint64_t next = 0, n_done = 0;
+    while (n_done < n_jobs) {
+        while (next < n_jobs && sched.admit(&js[next], &rc)) next++;
+        if (rc) return rc;
+        rc = sched.step(finished, members);
+        if (rc) return rc;
+        n_done += finished.size();
+        finished.clear();
+        if (sched.idle() && next < n_jobs && n_done < n_jobs && members.empty())
+            return eng->fail(WG_ERR_CAPACITY, "job does not fit the seed arena");
+    }
+    e = cudaEventRecord(eng->ev1, eng->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(eng->ev1);
+    if (e != cudaSuccess) return eng->fail(WG_ERR_CUDA, "event", e);
+    uint64_t w = 0, all = 0;
+    for (uint64_t i = 0; i < n_jobs; i++) {
+        if (job_found) job_found[i] = js[i].found.size();
+        for (const Candidate &c : js[i].found) {
+            if (w < cap) std::memcpy(&out[w++], &c, sizeof c);
+            all++;
+        }
+    }
+    if (n_out) *n_out = all;
+    if (stats) {
+        wg_scan_stats st = sched.stats;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, eng->ev0, eng->ev1);
+        st.gpu_ms = ms;
+        st.wall_ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+        *stats = st;
+    }
+    return WG_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Job server: submitters queue jobs; one worker thread admits them into the scheduler as seed
+// slots free up (FIFO) and runs batch after batch, so jobs that arrive while others are on the
+// device join the next batch.  Fields of a job that poll/take read are written under the lock.
+// ---------------------------------------------------------------------------------------------
+struct wg_server {
+    int device = 0;
+    wg_engine *eng = nullptr;
+    std::unique_ptr<Scheduler> sched;
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<SchedJob *> queue;
+    std::unordered_map<uint64_t, std::unique_ptr<SchedJob>> jobs;
+    uint64_t next_id = 1, queued_seeds = 0, max_queued = 0;
+    bool stop = false;
+    wg_scan_stats stats{};
+};
+
+namespace {
+
+void server_loop(wg_server *s) {
+    cudaSetDevice(s->device);
+    Scheduler &sched = *s->sched;
+    std::vector<SchedJob *> finished, members;
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty() || !sched.idle(); });
+            if (s->stop) return;
+        }
+        // admit in arrival order while the seed arena has room (only this thread pops the queue)
+        int rc = WG_OK;
+        for (;;) {
+            SchedJob *j = nullptr;
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                if (s->queue.empty()) break;
+                j = s->queue.front();
+            }
+            if (!sched.admit(j, &rc)) break;
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->queue.pop_front();
+            s->queued_seeds -= j->seeds.size();
+        }
+        const auto t_step = Clock::now();
+        if (rc == WG_OK) rc = sched.step(finished, members);
+        if (rc) sched.fail_all(rc, finished);
+        const auto t_end = Clock::now();
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (SchedJob *j : members) {
+            if (!j->started) {
+                j->started = true;
+                j->t_start = t_step;
+            }
+            j->batch_jobs = std::max<uint64_t>(j->batch_jobs, members.size());
+        }
+        for (SchedJob *j : finished) {
+            if (!j->started) {
+                j->started = true;
+                j->t_start = t_step;
+            }
+            j->t_done = t_end;
+            j->done = true;
+            std::vector<int64_t>().swap(j->seeds);
+        }
+        if (rc) {   // a failed batch also fails the jobs still queued behind it
+            for (SchedJob *j : s->queue) {
+                j->status = rc;
+                j->t_start = j->t_done = t_end;
+                j->started = j->done = true;
+            }
+            s->queue.clear();
+            s->queued_seeds = 0;
+        }
+        s->stats = sched.stats;
+        finished.clear();
+        s->cv_done.notify_all();
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int wg_server_open(int device, uint64_t max_queued_seeds, wg_server **out) {
+    if (!out) return WG_ERR_ARG;
+    *out = nullptr;
+    auto s = std::make_unique<wg_server>();
+    s->device = device;
+    int rc = wg_engine_open(device, &s->eng);
+    if (rc) return rc;
+    // seeds resident on the device: a quarter of the free HBM, at most 2^28 (2 GiB)
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 1ull << 30;
+    const uint64_t arena = std::max<uint64_t>(1ull << 20, std::min<uint64_t>(free_b / 4 / sizeof(int64_t), 1ull << 28));
+    s->max_queued = max_queued_seeds ? max_queued_seeds : (1ull << 30);
+    // small batches keep a short job's wait behind the batch in flight short
+    s->sched = std::make_unique<Scheduler>(s->eng, arena, kWorkPerBatch / 4);
+    rc = s->sched->init();
+    if (rc) {
+        s->sched.reset();
+        wg_engine_close(s->eng);
+        return rc;
+    }
+    s->worker = std::thread(server_loop, s.get());
+    *out = s.release();
+    return WG_OK;
+}
+
+int wg_server_submit(wg_server *s, const wg_job *job, uint64_t *job_id) {
+    if (!s || !job) return WG_ERR_ARG;
+    const auto t = Clock::now();
+    auto j = std::make_unique<SchedJob>();
+    int rc = sched_job_init(*j, *job);
+    if (rc) return rc;
+    if (j->seeds.size() > s->sched->arena_seeds()) return WG_ERR_CAPACITY;
+    j->t_submit = t;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return WG_ERR_ARG;
+    if (s->queued_seeds + j->seeds.size() > s->max_queued) return WG_ERR_CAPACITY;
+    j->id = s->next_id++;
+    if (job_id) *job_id = j->id;
+    s->queued_seeds += j->seeds.size();
+    s->queue.push_back(j.get());
+    s->jobs.emplace(j->id, std::move(j));
+    s->cv_work.notify_one();
+    return WG_OK;
+}
+
+int wg_server_poll(wg_server *s, uint64_t job_id, int wait_ms, wg_job_status *st) {
+    if (!s || !st) return WG_ERR_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(job_id);
+    if (it == s->jobs.end()) return WG_ERR_ARG;
+    SchedJob *j = it->second.get();
+    if (wait_ms > 0 && !j->done)
+        s->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), [&] { return j->done; });
+    std::memset(st, 0, sizeof *st);
+    st->done = j->done ? 1 : 0;
+    st->status = j->status;
+    st->batch_jobs = j->batch_jobs;
+    if (j->started) st->queue_ms = std::chrono::duration<double, std::milli>(j->t_start - j->t_submit).count();
+    if (j->done) {
+        st->found = j->found.size();
+        st->latency_ms = std::chrono::duration<double, std::milli>(j->t_done - j->t_submit).count();
+    }
+    return WG_OK;
+}
+
+int wg_server_take(wg_server *s, uint64_t job_id, wg_candidate *out, uint64_t cap, uint64_t *n_out) {
+    if (!s || (cap && !out)) return WG_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->jobs.find(job_id);
+    if (it == s->jobs.end() || !it->second->done) return WG_ERR_ARG;
+    SchedJob *j = it->second.get();
+    if (j->status) return j->status;
+    const uint64_t n = j->found.size(), w = std::min<uint64_t>(n, cap);
+    if (w) std::memcpy(out, j->found.data(), sizeof(Candidate) * w);
+    if (n_out) *n_out = n;
+    if (w == n) s->jobs.erase(it);
+    return WG_OK;
+}
+
+int wg_server_stats(wg_server *s, wg_scan_stats *st) {
+    if (!s || !st) return WG_ERR_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    *st = s->stats;
+    return WG_OK;
+}
+
+void wg_server_close(wg_server *s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    s->sched.reset();
+    wg_engine_close(s->eng);
+    delete s;
+}
+
+}  // extern "C"

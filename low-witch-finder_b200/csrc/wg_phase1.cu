@@ -68,16 +68,51 @@ __device__ __forceinline__ uint64_t seed_value(const BatchArgs &a, uint64_t g) {
 // Rect origin of seed g (shifted to the seed's spot region in spots mode).
 __device__ __forceinline__ int rect_x0(const BatchArgs &a, uint64_t g) { return a.spot_rx ? a.rx0 + a.spot_rx[g >> 16] : a.rx0; }
 __device__ __forceinline__ int rect_z0(const BatchArgs &a, uint64_t g) { return a.spot_rz ? a.rz0 + a.spot_rz[g >> 16] : a.rz0; }
-// Number of regions in a unit's window.
-__device__ __forceinline__ uint32_t window_len(const BatchArgs &a, uint64_t w) {
-    uint64_t start = w * a.win;
-    uint64_t left = a.n_regions - start;
-    return (uint32_t)(left < a.win ? left : a.win);
+// Everything about a batch-local unit: its seed, its window and the rect it walks.
+struct UnitPos {
+    uint64_t g;        // global seed index
+    uint64_t rbase;    // first region of the window (index into the rect, rz outer, rx inner)
+    uint32_t len;      // regions in the window
+    int rx0, rz0, rw;  // the rect the window lies in
+    int max_height;
+};
+__device__ __forceinline__ UnitPos unit_pos(const BatchArgs &a, uint32_t u) {
+    UnitPos p;
+    if (a.jobs) {
+        // the last table entry whose first global unit is <= this unit
+        const uint64_t ul = a.unit0 + u;
+        uint32_t lo = 0, hi = a.n_jobs - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (a.jobs[mid].unit0 <= ul) lo = mid;
+            else hi = mid - 1;
+        }
+        const JobGeom &j = a.jobs[lo];
+        const uint64_t loc = ul - j.unit0 + j.first;
+        p.g = j.seed0 + loc / j.n_win;
+        p.rbase = (loc % j.n_win) * j.win;
+        const uint64_t left = j.n_regions - p.rbase;
+        p.len = (uint32_t)(left < j.win ? left : j.win);
+        p.rx0 = j.rx0;
+        p.rz0 = j.rz0;
+        p.rw = j.rw;
+        p.max_height = j.max_height;
+        return p;
+    }
+    p.g = unit_seed_index(a, u);
+    p.rbase = unit_window(a, u) * a.win;
+    const uint64_t left = a.n_regions - p.rbase;
+    p.len = (uint32_t)(left < a.win ? left : a.win);
+    p.rx0 = rect_x0(a, p.g);
+    p.rz0 = rect_z0(a, p.g);
+    p.rw = a.rw;
+    p.max_height = a.max_height;
+    return p;
 }
-// Region (rx, rz) of global region index r (rz outer, rx inner: search.c:148-149).
-__device__ __forceinline__ void region_xz(const BatchArgs &a, uint64_t g, uint64_t r, int &rx, int &rz) {
-    rz = rect_z0(a, g) + (int)(r / (uint64_t)a.rw);
-    rx = rect_x0(a, g) + (int)(r % (uint64_t)a.rw);
+// Region (rx, rz) of region index r of a unit's rect (rz outer, rx inner: search.c:148-149).
+__device__ __forceinline__ void unit_region_xz(const UnitPos &p, uint64_t r, int &rx, int &rz) {
+    rz = p.rz0 + (int)(r / (uint64_t)p.rw);
+    rx = p.rx0 + (int)(r % (uint64_t)p.rw);
 }
 
 __device__ __forceinline__ void note_code(const BatchArgs &a, uint64_t g, uint64_t r, int code, int tier) {
@@ -210,6 +245,7 @@ struct ClimateSmem {
     uint32_t col0[kUnits];                     // column of the unit's first region in its rect row
     int row0[kUnits];                          // rz of the unit's first region
     int rx0u[kUnits];                          // rect x origin of the unit's seed
+    uint32_t rwu[kUnits];                      // rect width of the unit's job
     unsigned int hist[P1_KINDS + kTiers];
     uint32_t grad[kGradWords];
     ClimateSteps steps;
@@ -372,19 +408,21 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
 
     const uint32_t u = blockIdx.x * kUnits + (uint32_t)uu;
     const bool valid = u < a.n_units;
-    const uint64_t g = valid ? unit_seed_index(a, u) : 0;
-    const uint64_t w = valid ? unit_window(a, u) : 0;
+    UnitPos up{};
+    up.rw = 1;
+    if (valid) up = unit_pos(a, u);
+    const uint64_t g = up.g;
     const uint64_t seed = valid ? seed_value(a, g) : 0;
-    const uint32_t len = valid ? window_len(a, w) : 0;
+    const uint32_t len = valid ? up.len : 0;
     if (tid < kUnits) {
-        const uint64_t rbase = w * a.win;
         S.cnt[tid] = 0;
         S.g[tid] = g;
-        S.rbase[tid] = rbase;
+        S.rbase[tid] = up.rbase;
         S.seed[tid] = seed;
-        S.col0[tid] = (uint32_t)(rbase % (uint64_t)a.rw);
-        S.row0[tid] = rect_z0(a, g) + (int)(rbase / (uint64_t)a.rw);
-        S.rx0u[tid] = rect_x0(a, g);
+        S.col0[tid] = (uint32_t)(up.rbase % (uint64_t)up.rw);
+        S.row0[tid] = up.rz0 + (int)(up.rbase / (uint64_t)up.rw);
+        S.rx0u[tid] = up.rx0;
+        S.rwu[tid] = (uint32_t)up.rw;
     }
     TierCounts tc;
 
@@ -425,7 +463,7 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
             const uint32_t j = c0 + (uint32_t)(q / kUnits);
             if (j >= S.end[qu]) continue;
             const uint32_t t = S.col0[qu] + j;   // region offset from the unit's first row start
-            const uint32_t rw = (uint32_t)a.rw;
+            const uint32_t rw = S.rwu[qu];
             const int rz = S.row0[qu] + (int)(t / rw), rx = S.rx0u[qu] + (int)(t % rw);
             int cx, cz;
             hut_chunk(S.seed[qu], rx, rz, a.salt, cx, cz);
@@ -677,6 +715,7 @@ struct EntranceSmem {
     uint32_t emap[kEntList];              // tile survivor list: record << 16 | index in its record
     uint64_t rseed[kUnits], rg[kUnits], rbase[kUnits];
     uint32_t runit[kUnits], roff[kUnits];
+    int rrx0[kUnits], rrz0[kUnits], rrw[kUnits];   // rect of each record's unit
     unsigned int hist[P1_KINDS];
     unsigned int n_list;
     uint32_t grad[kGradWords];
@@ -766,14 +805,18 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
             const uint32_t u = a.rec_unit[ri], off = a.rec_off[ri];
             cnt = a.rec_cnt[ri];
             if (u >= a.n_units || off >= a.cap_surv || cnt > a.cap_surv - off || cnt > kRecordCap) cnt = 0;
-            const uint64_t g = unit_seed_index(a, u);
+            const UnitPos up = unit_pos(a, u);
+            const uint64_t g = up.g;
             const uint64_t seed = seed_value(a, g);
             if (my_slot == 0) {
                 S.rseed[rr] = seed;
                 S.rg[rr] = g;
-                S.rbase[rr] = unit_window(a, u) * a.win;
+                S.rbase[rr] = up.rbase;
                 S.runit[rr] = u;
                 S.roff[rr] = off;
+                S.rrx0[rr] = up.rx0;
+                S.rrz0[rr] = up.rz0;
+                S.rrw[rr] = up.rw;
             }
             if (cnt) {
                 Xr r = octave_rng(c_noise[my_noise], seed_fork_of(seed), my_sub, my_p);
@@ -800,8 +843,10 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
                 const uint32_t em = S.emap[e0 + e];
                 const int r2 = (int)(em >> 16);
                 const uint32_t jr = a.surv_region[S.roff[r2] + (em & 0xFFFFu)];
-                int rx, rz, cx, cz;
-                region_xz(a, S.rg[r2], S.rbase[r2] + jr, rx, rz);
+                const uint64_t reg = S.rbase[r2] + jr;
+                const int rz = S.rrz0[r2] + (int)(reg / (uint64_t)S.rrw[r2]);
+                const int rx = S.rrx0[r2] + (int)(reg % (uint64_t)S.rrw[r2]);
+                int cx, cz;
                 hut_chunk(S.rseed[r2], rx, rz, a.salt, cx, cz);
                 S.hx[e] = cx * 16 + 3;
                 S.hz[e] = cz * 16 + 3;
@@ -929,34 +974,36 @@ __global__ void __launch_bounds__(kThreadsC) ladder_kernel(BatchArgs a) {
     const uint32_t n_deep = min(a.counters[CNT_DEEP], a.cap_deep);
     fill_grad_table(S.grad, t);
     const SrcFlat src{S.perm, S.org, S.grad};
-    const int mh = a.max_height;
-    // heights: [0] maxHeight, then y = 0, -10, ... >= ladderFloor with maxHeight < y, then 10..40
-    int floor_y = (-40 < mh) ? -40 : mh;
-    if (floor_y < -50) floor_y = -50;
-    int nh = 0;
-    if (t == 0) S.ys[nh] = mh;
-    nh++;
-    for (int y = 0; y >= floor_y; y -= 10)
-        if (mh < y) {
-            if (t == 0) S.ys[nh] = y;
-            nh++;
-        }
-    const int first_pos = nh;
-    for (int y = 10; y <= 40; y += 10) {
-        if (t == 0) S.ys[nh] = y;
-        nh++;
-    }
-    const long long nf_ll = mh > 60 ? 0 : ((long long)60 - mh) / 10 + 1;
-    const int nf = nf_ll > kFloodHeights ? 0 : (int)nf_ll;   // more: sampled one by one at the end
 
     for (uint32_t q = blockIdx.x; q < n_deep; q += gridDim.x) {
         const uint32_t u = a.deep[2 * q], jr = a.deep[2 * q + 1];
-        const uint64_t g = unit_seed_index(a, u);
-        const uint64_t r = unit_window(a, u) * a.win + jr;
+        const UnitPos up = unit_pos(a, u);
+        const uint64_t g = up.g;
+        const uint64_t r = up.rbase + jr;
         const uint64_t seed = seed_value(a, g);
         int rx, rz, cx, cz;
-        region_xz(a, g, r, rx, rz);
+        unit_region_xz(up, r, rx, rz);
         hut_chunk(seed, rx, rz, a.salt, cx, cz);
+        // heights: [0] maxHeight, then y = 0, -10, ... >= ladderFloor with maxHeight < y, then
+        // 10..40 (S.ys is rewritten only after the previous candidate's closing barrier)
+        const int mh = up.max_height;
+        int floor_y = (-40 < mh) ? -40 : mh;
+        if (floor_y < -50) floor_y = -50;
+        int nh = 0;
+        if (t == 0) S.ys[nh] = mh;
+        nh++;
+        for (int y = 0; y >= floor_y; y -= 10)
+            if (mh < y) {
+                if (t == 0) S.ys[nh] = y;
+                nh++;
+            }
+        const int first_pos = nh;
+        for (int y = 10; y <= 40; y += 10) {
+            if (t == 0) S.ys[nh] = y;
+            nh++;
+        }
+        const long long nf_ll = mh > 60 ? 0 : ((long long)60 - mh) / 10 + 1;
+        const int nf = nf_ll > kFloodHeights ? 0 : (int)nf_ll;   // more: sampled one by one at the end
         const int hut_x = cx * 16, hut_z = cz * 16;
         const int hx = hut_x + 3, hz = hut_z + 3;
         perm_blocks_init<kLadderStride, 256 * kLadderStride>(S.perm, 1, t, kThreadsC);

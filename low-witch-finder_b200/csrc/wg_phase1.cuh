@@ -74,6 +74,23 @@ struct Candidate {
 // u % n_win); a window is `win` consecutive regions of the rect (rz outer, rx inner).  One
 // lane of the climate kernel owns one unit, so a request with few seeds and a huge rect
 // (a whole-world scan of one seed) fills the GPU as well as many seeds x 9x9 regions.
+//
+// Jobs mode flattens many Seed Check jobs, each with its own rect and floor, into one batch:
+// entry k of the job table covers the global units [unit0, next entry's unit0) and maps them
+// to units first, first + 1, ... of one job (so a batch can take any slice of a job).
+struct JobGeom {
+    uint64_t unit0;        // first global unit of this entry (entries sorted by unit0, none empty)
+    uint64_t first;        // the job's unit index of that first unit
+    uint64_t seed0;        // global seed index of the job's seed 0 (index into BatchArgs::seeds)
+    uint64_t n_win;        // windows per seed of the job
+    uint64_t n_regions;    // regions per seed (rw * rh)
+    uint32_t win;          // regions per window
+    int32_t rx0, rz0, rw;  // the job's region rect origin and width
+    int32_t max_height;    // the job's gate floor
+    int32_t pad;
+};
+static_assert(sizeof(JobGeom) == 64, "job table entry layout");
+
 // Everything a phase-1 batch needs (device pointers only).
 struct BatchArgs {
     const int64_t *seeds;         // all request seeds (global seed index), or nullptr: splitmix64(gen_base + i)
@@ -105,6 +122,11 @@ struct BatchArgs {
     // structure seed, and its rect is shifted by the spot's region (spot_rx, spot_rz)[g >> 16].
     const int64_t *spot_s48 = nullptr;
     const int32_t *spot_rx = nullptr, *spot_rz = nullptr;
+
+    // Optional jobs mode: the batch's units are resolved through this table (rect, window and
+    // max_height per job; seeds from `seeds`); unit0 .. unit0 + n_units are global units of it.
+    const JobGeom *jobs = nullptr;
+    uint32_t n_jobs = 0;
 };
 
 // One evaluation step of the climate state machine (a single y=0 Perlin sample).

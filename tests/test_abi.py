@@ -34,6 +34,33 @@ def test_struct_layouts(wg):
     assert C.sizeof(wg.Stats) == 8 * (4 + 11 + 7 + 2 + 3) + 8 * 3 + 16
 
 
+def test_job_struct_layouts_match_the_header(wg, tmp_path):
+    """wg_job / wg_job_status as the C compiler lays them out = the ctypes mirrors."""
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stddef.h>\n#include <stdio.h>\n#include "witchgpu.h"\n'
+        'int main(void) { printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(wg_job), offsetof(wg_job, n_seeds),'
+        ' offsetof(wg_job, max_height), offsetof(wg_job, opts), sizeof(wg_job_status),'
+        ' offsetof(wg_job_status, queue_ms), offsetof(wg_job_status, batch_jobs)); return 0; }\n')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.dirname(wg.HEADER_PATH), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [C.sizeof(wg.Job), wg.Job.n_seeds.offset, wg.Job.max_height.offset, wg.Job.opts.offset,
+            C.sizeof(wg.JobStatus), wg.JobStatus.queue_ms.offset, wg.JobStatus.batch_jobs.offset]
+    assert got == want
+
+
+def test_server_without_gpu_fails_loudly(wg):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    with pytest.raises(wg.EngineError, match="status 5"):
+        wg.Server(0)
+
+
 @pytest.mark.parametrize("name,mc,pre,tree", [("1.19.x~26.1", 0, 1, 0), ("26.2", 0, 0, 7), ("26.2~26.3", 0, 0, 0),
                                               ("1.18.2", 1, 1, 1), ("1.18.x", 1, 1, 0), ("1.21", 0, 1, 4),
                                               ("1.21.5", 0, 1, 6), ("26.3", 0, 0, 8), ("1.20.1", 0, 1, 4)])
