@@ -236,6 +236,50 @@ int wg_deep_spots(wg_engine *e, const int64_t *s48, const int32_t *chunk_x, cons
                   const wg_opts *opts, int max_height, wg_candidate *out, uint64_t cap, uint64_t *n_out,
                   uint64_t *not_start);
 
+/* ---------------- Deep Dive solver: structure seeds for a mineshaft layout ---------------- */
+
+/* One plan line (the reference's plan.txt: "X regime class ..."): the setLargeFeatureSeed state
+ * wanted at the hut chunk (a catalogued mineshaft layout), the region regime on each axis
+ * (0: |r| <= 16383, 1: 16384..32767, 2: 32768..58593, both signs) and the chunk-offset class
+ * (1 "odd": one offset odd; 2 "u2": both even, 2-adic valuations differ; 3 "eq": equal
+ * valuations, not both 0). */
+typedef struct {
+    uint64_t layout;
+    int32_t regime_x, regime_z;
+    int32_t tier;
+    int32_t pad;
+} wg_solve_bundle;
+
+/* A structure seed whose swamp hut (chunk_x, chunk_z) has that layout's carver state. */
+typedef struct {
+    uint64_t s48;
+    int32_t chunk_x, chunk_z;
+    uint64_t layout;
+    uint64_t group;          /* the group it was found in (bundle << 20 | group within the bundle) */
+} wg_solve_hit;
+
+typedef struct {
+    uint64_t groups, regions, tasks;
+    uint64_t candidates;     /* low-20-bit candidates lifted (sum over tasks of their list length) */
+    uint64_t hits;
+    uint64_t host_check_failures;   /* hits dropped by the host's forward check (expected 0) */
+    double gpu_ms, wall_ms;
+} wg_solve_stats;
+
+/* Groups [first_group, first_group + n_groups) of the bundles (group g: bundle g >> 20, residue
+ * class scramble(g & 0xFFFFF) of the region constant's low 20 bits): every (region, chunk offset)
+ * task of the group solved for all structure seeds.  Hits sorted by (group, s48, chunk_x, chunk_z);
+ * *n_out = all, at most cap written.  Replaces hut_lookup_v4 --solve-only --solve5 --plan
+ * (engine/gpu/hut_lookup_v4_source.cu:1293-1380; equations solver_kernels.cuh, solver_fused.cuh;
+ * task space taskspace.h). */
+int wg_deep_solve(wg_engine *e, const wg_solve_bundle *bundles, uint64_t n_bundles, uint64_t first_group,
+                  uint64_t n_groups, wg_solve_hit *out, uint64_t cap, uint64_t *n_out, wg_solve_stats *stats);
+
+/* The same solve for explicit tasks: region (rx[i], rz[i]) with chunk offsets (ox[i], oz[i]) in
+ * 0..23, not both 0; hits' group = the task index.  hut_lookup_v4 --solve --tasks-file. */
+int wg_deep_solve_tasks(wg_engine *e, uint64_t layout, const int32_t *rx, const int32_t *rz, const int32_t *ox,
+                        const int32_t *oz, uint64_t n, wg_solve_hit *out, uint64_t cap, uint64_t *n_out);
+
 /* ---------------- job server: batched and streamed Seed Check jobs ---------------- */
 
 /* One Seed Check job: seeds[0..n_seeds) (copied at submit) or, when seeds is NULL,

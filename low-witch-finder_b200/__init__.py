@@ -61,7 +61,7 @@ CANDIDATE_DTYPE = np.dtype([("seed_index", "<u8"), ("seed", "<i8"), ("rx", "<i4"
 EXPORTS = ("wg_engine_open", "wg_engine_close", "wg_engine_error", "wg_parse_version", "wg_parse_preset",
            "wg_seed_check", "wg_seed_check_device", "wg_phase1_codes", "wg_seed_check_noalloc",
            "wg_eval_huts", "wg_grade_scan", "wg_p2_probe", "wg_deep_starts", "wg_deep_spots",
-           "wg_seed_check_jobs", "wg_server_open", "wg_server_submit", "wg_server_poll", "wg_server_take",
+           "wg_deep_solve", "wg_deep_solve_tasks", "wg_seed_check_jobs", "wg_server_open", "wg_server_submit", "wg_server_poll", "wg_server_take",
            "wg_server_stats", "wg_server_close")
 
 # wg_deep_start: a swamp hut whose chunk is a mineshaft start chunk.
@@ -89,6 +89,24 @@ class HutGrade(C.Structure):
                 ("rejected_y", C.c_int64), ("rejected_flood", C.c_int64), ("rejected_biome", C.c_int64),
                 ("hits_written", C.c_int32), ("ms", C.c_double), ("p2_ms", C.c_double)]
 
+
+
+class SolveBundle(C.Structure):
+    """wg_solve_bundle: one plan line (layout, regime per axis, offset class)."""
+    _fields_ = [("layout", C.c_uint64), ("regime_x", C.c_int32), ("regime_z", C.c_int32), ("tier", C.c_int32),
+                ("pad", C.c_int32)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("groups", C.c_uint64), ("regions", C.c_uint64), ("tasks", C.c_uint64), ("candidates", C.c_uint64),
+                ("hits", C.c_uint64), ("host_check_failures", C.c_uint64), ("gpu_ms", C.c_double),
+                ("wall_ms", C.c_double)]
+
+
+# wg_solve_hit: a structure seed whose hut chunk has the layout's carver state.
+SOLVE_HIT_DTYPE = np.dtype([("s48", "<u8"), ("chunk_x", "<i4"), ("chunk_z", "<i4"), ("layout", "<u8"),
+                            ("group", "<u8")])
+SOLVE_TIERS = {"odd": 1, "u2": 2, "eq": 3}
 
 
 class Job(C.Structure):
@@ -138,6 +156,9 @@ def library() -> C.CDLL:
     lib.wg_deep_starts.argtypes = [vp, vp, i64, u64, i32, i32, i32, i32, vp, u64, C.POINTER(u64)]
     lib.wg_deep_spots.argtypes = [vp, vp, vp, vp, u64, C.POINTER(Opts), i32, vp, u64, C.POINTER(u64),
                                   C.POINTER(u64)]
+    lib.wg_deep_solve.argtypes = [vp, C.POINTER(SolveBundle), u64, u64, u64, vp, u64, C.POINTER(u64),
+                                  C.POINTER(SolveStats)]
+    lib.wg_deep_solve_tasks.argtypes = [vp, u64, vp, vp, vp, vp, u64, vp, u64, C.POINTER(u64)]
     lib.wg_seed_check_jobs.argtypes = [vp, C.POINTER(Job), u64, vp, u64, C.POINTER(u64), vp, C.POINTER(Stats)]
     lib.wg_server_open.argtypes = [i32, u64, C.POINTER(vp)]
     lib.wg_server_submit.argtypes = [vp, C.POINTER(Job), C.POINTER(u64)]
@@ -315,6 +336,42 @@ class Engine:
             if found.value <= cap:
                 return out[:found.value].copy()
             cap = int(found.value)
+
+    def deep_solve(self, bundles, first_group: int, n_groups: int) -> tuple[np.ndarray, dict]:
+        """wg_deep_solve: bundles = [(layout, "XZ" regime digits or (rx, rz), "odd" | "u2" | "eq"), ...]
+        (plan lines); the hits of groups [first_group, first_group + n_groups)."""
+        arr = (SolveBundle * len(bundles))()
+        for i, (x, regime, tier) in enumerate(bundles):
+            rg = (int(regime[0]), int(regime[1]))
+            arr[i] = SolveBundle(int(x) & 0xFFFFFFFFFFFF, rg[0], rg[1], SOLVE_TIERS.get(tier, tier) if isinstance(tier, str) else int(tier), 0)
+        cap = max(1 << 12, 2048 * n_groups)
+        while True:
+            out = np.zeros(cap, SOLVE_HIT_DTYPE)
+            n = C.c_uint64()
+            st = SolveStats()
+            rc = library().wg_deep_solve(self._h, arr, len(bundles), first_group, n_groups, out.ctypes.data, cap,
+                                         C.byref(n), C.byref(st))
+            if rc != WG_OK:
+                raise self._err(rc, "wg_deep_solve")
+            if n.value <= cap:
+                return out[:n.value].copy(), {k: getattr(st, k) for k, _ in SolveStats._fields_}
+            cap = int(n.value)
+
+    def deep_solve_tasks(self, layout: int, rx, rz, ox, oz) -> np.ndarray:
+        """wg_deep_solve_tasks: hits of explicit (region, chunk offset) tasks; group = task index."""
+        a = [np.ascontiguousarray(np.asarray(v, dtype=np.int32)) for v in (rx, rz, ox, oz)]
+        n = len(a[0])
+        cap = max(1 << 10, 4 * n)
+        while True:
+            out = np.zeros(cap, SOLVE_HIT_DTYPE)
+            got = C.c_uint64()
+            rc = library().wg_deep_solve_tasks(self._h, int(layout) & 0xFFFFFFFFFFFF, *(v.ctypes.data for v in a), n,
+                                               out.ctypes.data, cap, C.byref(got))
+            if rc != WG_OK:
+                raise self._err(rc, "wg_deep_solve_tasks")
+            if got.value <= cap:
+                return out[:got.value].copy()
+            cap = int(got.value)
 
     def seed_check_jobs(self, jobs) -> tuple[list[np.ndarray], dict]:
         """wg_seed_check_jobs: many jobs (dicts with seeds= or gen=(base, count), rect=, max_height=,

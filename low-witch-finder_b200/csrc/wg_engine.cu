@@ -328,6 +328,7 @@ void wg_engine_close(wg_engine *eng) {
     cudaFree(eng->hist);
     cudaFree(eng->d_seed_list);
     p2_release(eng);
+    solve_release(eng);
     cudaFreeHost(eng->h_counters);
     cudaFreeHost(eng->h_hist);
     if (eng->ev0) cudaEventDestroy(eng->ev0);

@@ -44,6 +44,9 @@ struct wg_engine {
     wg::P2Result *p2_results = nullptr;
     int32_t *p2_pts = nullptr;
     double *p2_vals = nullptr;
+    // Deep Dive solver (wg_solve.cu): its device tables and work buffers
+    struct SolveState *solve = nullptr;
+
     int p2_world_cap = 0, p2_job_cap = 0, p2_hut_cap = 0, p2_result_cap = 0, p2_pt_cap = 0, p2_val_cap = 0;
 
     int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
@@ -57,6 +60,8 @@ struct wg_engine {
 
 // Frees the phase-2 state of an engine (called by wg_engine_close).
 void p2_release(wg_engine *eng);
+// Frees the Deep Dive solver state of an engine (called by wg_engine_close).
+void solve_release(wg_engine *eng);
 
 namespace wg {
 

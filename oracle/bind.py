@@ -77,7 +77,35 @@ class Port:
         lib.wo_deep_starts.restype = C.c_longlong
         lib.wo_deep_starts.argtypes = [C.c_void_p, C.c_longlong, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                        C.c_longlong]
+        lib.wo_region_const.restype = C.c_uint64
+        lib.wo_region_const.argtypes = [C.c_int, C.c_int]
+        lib.wo_perm_group.restype = C.c_uint32
+        lib.wo_perm_group.argtypes = [C.c_uint32]
+        lib.wo_group_regions.restype = C.c_longlong
+        lib.wo_group_regions.argtypes = [C.c_uint32, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_longlong]
+        lib.wo_solve_task.restype = C.c_longlong
+        lib.wo_solve_task.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_longlong]
         self.lib = lib
+
+    def region_const(self, rx: int, rz: int) -> int:
+        return int(self.lib.wo_region_const(rx, rz))
+
+    def perm_group(self, g: int) -> int:
+        return int(self.lib.wo_perm_group(g & 0xFFFFF))
+
+    def group_regions(self, c20: int, regime_x: int, regime_z: int, cap: int = 1 << 14) -> np.ndarray:
+        """(rx, rz) rows of the regime's regions whose region constant has low 20 bits c20."""
+        rx = np.zeros(cap, np.int32)
+        rz = np.zeros(cap, np.int32)
+        n = self.lib.wo_group_regions(c20, regime_x, regime_z, rx.ctypes.data, rz.ctypes.data, cap)
+        return np.stack([rx[:min(n, cap)], rz[:min(n, cap)]], axis=1)
+
+    def solve_task(self, X: int, rx: int, rz: int, ox: int, oz: int, cap: int = 64) -> list[int]:
+        """Structure seeds S whose hut in (rx, rz) is at offsets (ox, oz) and whose carver state at
+        that chunk is X (sorted)."""
+        out = np.zeros(cap, np.uint64)
+        n = self.lib.wo_solve_task(X & 0xFFFFFFFFFFFF, rx, rz, ox, oz, out.ctypes.data, cap)
+        return sorted(int(v) for v in out[:min(n, cap)])
 
     def mineshaft_start(self, s48: int, cx: int, cz: int) -> tuple[bool, int]:
         carver = C.c_uint64()

@@ -685,3 +685,146 @@ long long wo_deep_starts(const uint64_t *s48s, long long n, int rx0, int rx1, in
     }
     return found;
 }
+
+/* ------------------------------------------------------------------ */
+/* Deep Dive solver: the structure seeds S (48 bits) whose swamp hut   */
+/* in region (rx, rz) lies at chunk offsets (ox, oz) and whose         */
+/* setLargeFeatureSeed state at that chunk equals a layout value X.    */
+/* Equations: engine/gpu/solver_kernels.cuh:15-115; task space:        */
+/* engine/gpu/taskspace.h.  Restated independently: the low 20 bits of */
+/* the LCG state t = S ^ 0x5DEECE66D by exhaustion (pruned by the hut  */
+/* offsets' low 3 bits and the equation's low bits), the upper 28 by a */
+/* bit-serial lifting of the low-32-bit equation, then a full check.   */
+/* ------------------------------------------------------------------ */
+#define SOLVE_C0 14357620ULL
+#define SOLVE_C1 341873128712ULL
+#define SOLVE_C2 132897987541ULL
+#define M20 0xFFFFFULL
+
+uint64_t wo_region_const(int rx, int rz) {
+    return (SOLVE_C0 + (uint64_t)(int64_t)rx * SOLVE_C1 + (uint64_t)(int64_t)rz * SOLVE_C2) & LCG_MASK;
+}
+
+/* taskspace.h:27: the 20-bit group scramble (the group -> residue map hunt.py's ranges name) */
+uint32_t wo_perm_group(uint32_t p) {
+    uint32_t x = (uint32_t)((p * 0x9E3779B1u) & 0xFFFFFu);
+    x ^= x >> 9;
+    x = (x * 0x85EBCA6Bu) & 0xFFFFFu;
+    x ^= x >> 7;
+    return x & 0xFFFFFu;
+}
+
+/* taskspace.h:12-18: the rx / rz ranges of a regime (both signs for 1 and 2) */
+static int regime_ranges(int regime, int64_t lo[2], int64_t hi[2]) {
+    if (regime == 0) { lo[0] = -16384; hi[0] = 16383; return 1; }
+    if (regime == 1) { lo[0] = -32768; hi[0] = -16385; lo[1] = 16384; hi[1] = 32767; return 2; }
+    lo[0] = -58593; hi[0] = -32769; lo[1] = 32768; hi[1] = 58593; return 2;
+}
+
+/* Regions of a regime whose region constant has low 20 bits c20 (taskspace.h:29-39), by
+ * scanning rz for every rx (no modular inverse: an independent check of the GPU's). */
+long long wo_group_regions(uint32_t c20, int regime_x, int regime_z, int32_t *rx_out, int32_t *rz_out, long long cap) {
+    int64_t xl[2], xh[2], zl[2], zh[2];
+    const int nx = regime_ranges(regime_x, xl, xh), nz = regime_ranges(regime_z, zl, zh);
+    long long n = 0;
+    for (int a = 0; a < nx; a++)
+        for (int64_t rx = xl[a]; rx <= xh[a]; rx++) {
+            const uint64_t base = (SOLVE_C0 + (uint64_t)rx * SOLVE_C1) & M20;
+            for (int b = 0; b < nz; b++)
+                for (int64_t rz = zl[b]; rz <= zh[b]; rz++) {
+                    if (((base + (uint64_t)rz * SOLVE_C2) & M20) != c20) continue;
+                    if (n < cap) { rx_out[n] = (int32_t)rx; rz_out[n] = (int32_t)rz; }
+                    n++;
+                }
+        }
+    return n;
+}
+
+/* The hut offsets of region constant creg under structure seed S (nextInt(24) twice, with the
+ * JDK rejection): rcHutExact, engine/gpu/room_core.h:78-96. */
+static void hut_offsets(uint64_t S, uint64_t creg, int *ox, int *oz) {
+    uint64_t st = ((S + creg) ^ LCG_MUL) & LCG_MASK;
+    *ox = lcg_int(&st, 24);
+    *oz = lcg_int(&st, 24);
+}
+
+static uint64_t carver_state(uint64_t S, int cx, int cz) {
+    uint64_t st = (S ^ LCG_MUL) & LCG_MASK;
+    const uint64_t a = lcg_long(&st);
+    const uint64_t b = lcg_long(&st);
+    return ((uint64_t)((int64_t)cx * (int64_t)a) ^ (uint64_t)((int64_t)cz * (int64_t)b) ^ S) & LCG_MASK;
+}
+
+typedef struct {
+    uint64_t X, creg, a2, k2, a4, k4;
+    int cx, cz, ox, oz, m;
+    uint64_t *out;
+    long long n, cap;
+} solve_ctx;
+
+/* low 32 bits of (cx * a) ^ (cz * b) ^ S ^ X for the state t (only bits of t below 48 - 16
+ * reach them): a and b agree with (A^2 t + K2) >> 16 and (A^4 t + K4) >> 16 in their low words */
+static uint32_t eq_low(const solve_ctx *c, uint64_t t) {
+    const uint32_t h2 = (uint32_t)((((c->a2 * t) + c->k2) & LCG_MASK) >> 16);
+    const uint32_t h4 = (uint32_t)((((c->a4 * t) + c->k4) & LCG_MASK) >> 16);
+    return ((uint32_t)c->cx * h2) ^ ((uint32_t)c->cz * h4) ^ (uint32_t)((t ^ LCG_MUL) & 0xFFFFFFFFu) ^ (uint32_t)c->X;
+}
+
+static void solve_verify(solve_ctx *c, uint64_t t) {
+    const uint64_t S = (t ^ LCG_MUL) & LCG_MASK;
+    if (carver_state(S, c->cx, c->cz) != c->X) return;
+    int ox, oz;
+    hut_offsets(S, c->creg, &ox, &oz);
+    if (ox != c->ox || oz != c->oz) return;
+    if (c->n < c->cap) c->out[c->n] = S;
+    c->n++;
+}
+
+/* Bits of t below j are chosen and equation bits below j - 16 + m are zero.  Choosing bit j
+ * settles equation bit j - 16 + m (the lowest bit the new term cx * A^2 * 2^(j-16) or
+ * cz * A^4 * 2^(j-16) can reach); past bit 31 the remaining bits are free. */
+static void solve_lift(solve_ctx *c, uint64_t t, int j) {
+    const int kb = j - 16 + c->m;
+    if (kb > 31) {
+        for (uint64_t f = 0; f < (1ULL << (48 - j)); f++) solve_verify(c, t | (f << j));
+        return;
+    }
+    for (uint64_t x = 0; x < 2; x++) {
+        const uint64_t t1 = t | (x << j);
+        if (!((eq_low(c, t1) >> kb) & 1u)) solve_lift(c, t1, j + 1);
+    }
+}
+
+static int v2(uint32_t v) { int k = 0; if (!v) return 40; while (!(v & 1u)) { v >>= 1; k++; } return k; }
+
+long long wo_solve_task(uint64_t X, int rx, int rz, int ox, int oz, uint64_t *out, long long cap) {
+    solve_ctx c;
+    memset(&c, 0, sizeof c);
+    c.X = X & LCG_MASK;
+    c.creg = wo_region_const(rx, rz);
+    c.a2 = (LCG_MUL * LCG_MUL) & LCG_MASK;
+    c.k2 = (0xBULL * (LCG_MUL + 1)) & LCG_MASK;
+    c.a4 = (c.a2 * c.a2) & LCG_MASK;
+    c.k4 = (0xBULL * (LCG_MUL * LCG_MUL * LCG_MUL + LCG_MUL * LCG_MUL + LCG_MUL + 1)) & LCG_MASK;
+    c.cx = rx * 32 + ox;
+    c.cz = rz * 32 + oz;
+    c.ox = ox;
+    c.oz = oz;
+    const int vx = v2((uint32_t)c.cx), vz = v2((uint32_t)c.cz);
+    c.m = vx < vz ? vx : vz;
+    if (c.m > 8) return 0;   /* both offsets 0: no class (the reference's tiers leave it out) */
+    c.out = out;
+    c.cap = cap;
+    const uint32_t low = (1u << (4 + c.m)) - 1u;
+    for (uint64_t t20 = 0; t20 <= M20; t20++) {
+        /* the hut offsets' low 3 bits come from state bits 17..19 of the region's first two draws */
+        const uint64_t q0 = ((((t20 ^ LCG_MUL) & M20) + c.creg) ^ LCG_MUL) & M20;
+        const uint64_t q1 = (q0 * LCG_MUL + 0xBULL) & M20;
+        if ((int)(q1 >> 17) != (ox & 7)) continue;
+        const uint64_t q2 = (q1 * LCG_MUL + 0xBULL) & M20;
+        if ((int)(q2 >> 17) != (oz & 7)) continue;
+        if (eq_low(&c, t20) & low) continue;
+        solve_lift(&c, t20, 20);
+    }
+    return c.n;
+}

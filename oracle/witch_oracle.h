@@ -64,6 +64,13 @@ long long wo_scan_seeds(const uint64_t *seeds, uint64_t gen_base, long long n, c
                         int max_height, int salt, int rx0, int rx1, int rz0, int rz1, int threads,
                         wo_candidate *out, long long cap, long long *reject_hist);
 
+
+/* Deep Dive solver (engine/gpu/solver_kernels.cuh, taskspace.h) */
+uint64_t wo_region_const(int rx, int rz);
+uint32_t wo_perm_group(uint32_t p);
+long long wo_group_regions(uint32_t c20, int regime_x, int regime_z, int32_t *rx_out, int32_t *rz_out, long long cap);
+long long wo_solve_task(uint64_t X, int rx, int rz, int ox, int oz, uint64_t *out, long long cap);
+
 #ifdef __cplusplus
 }
 #endif

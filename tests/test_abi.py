@@ -104,3 +104,16 @@ def test_shard_partition(wg):
             assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
             sizes = [hi - lo for lo, hi in spans]
             assert max(sizes) - min(sizes) <= 1
+
+
+def test_solver_struct_layouts_match_the_header(wg, tmp_path):
+    src = tmp_path / "solve_layout.c"
+    src.write_text(
+        '#include <stddef.h>\n#include <stdio.h>\n#include "witchgpu.h"\n'
+        'int main(void) { printf("%zu %zu %zu %zu %zu\\n", sizeof(wg_solve_bundle), offsetof(wg_solve_bundle, tier),'
+        ' sizeof(wg_solve_hit), offsetof(wg_solve_hit, layout), sizeof(wg_solve_stats)); return 0; }\n')
+    exe = tmp_path / "solve_layout"
+    subprocess.run(["gcc", "-I", os.path.dirname(wg.HEADER_PATH), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got == [C.sizeof(wg.SolveBundle), wg.SolveBundle.tier.offset, wg.SOLVE_HIT_DTYPE.itemsize,
+                   wg.SOLVE_HIT_DTYPE.fields["layout"][1], C.sizeof(wg.SolveStats)]
