@@ -202,12 +202,24 @@ def deep_measure(eng, opts) -> dict:
     t0 = time.perf_counter()
     surv, bad = eng.deep_spots(spots["s48"], spots["chunk_x"], spots["chunk_z"], max_height=-54, opts=opts)
     spot_s = time.perf_counter() - t0
-    return {"walk": {"structure_seeds": n_s48, "regions": regions, "starts": int(len(hits)),
+    # the solver on the -58 plan line (layout 231564844655014, regime 22, class odd: data/hunt/58)
+    plan = [(231564844655014, (2, 2), "odd")]
+    eng.deep_solve(plan, 0, 2)
+    t0 = time.perf_counter()
+    shits, sst = eng.deep_solve(plan, 4096, 64)
+    solve_s = time.perf_counter() - t0
+    return {"solver": {"plan": "231564844655014 22 odd", "groups": sst["groups"], "regions": sst["regions"],
+                       "tasks": sst["tasks"], "candidates": sst["candidates"], "hits": sst["hits"],
+                       "tasks_per_s": sst["tasks"] / solve_s, "groups_per_s": sst["groups"] / solve_s,
+                       "device_tasks_per_s": sst["tasks"] / (sst["gpu_ms"] / 1e3), "ms": 1e3 * solve_s,
+                       "gpu_ms": sst["gpu_ms"]},
+            "walk": {"structure_seeds": n_s48, "regions": regions, "starts": int(len(hits)),
                      "regions_per_s": regions / walk_s, "ms": 1e3 * walk_s},
             "terrain": {"spots": int(len(spots)), "world_seeds": int(len(spots)) << 16,
                         "world_seeds_per_s": (len(spots) << 16) / spot_s, "ms": 1e3 * spot_s,
                         "survivors": int(len(surv)), "max_height": -54},
-            "timing": "wall clock around wg_deep_starts / wg_deep_spots (host buffers in and out)"}
+            "timing": "wall clock around wg_deep_solve / wg_deep_starts / wg_deep_spots (host buffers in and "
+                      "out); device time of the solver from its CUDA events"}
 
 
 def jobs_measure(wg, eng, n_jobs: int = 65536) -> dict:

@@ -21,6 +21,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libwitchgpu.so")
 WORKER_PATH = os.path.join(HERE, "phase1_scan")
+HUT_LOOKUP_PATH = os.path.join(HERE, "hut_lookup")
 HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "witchgpu.h")
 
 WG_OK, WG_ERR_ARG, WG_ERR_CUDA, WG_ERR_NOMEM, WG_ERR_CAPACITY, WG_ERR_NODEV = 0, 1, 2, 3, 4, 5
@@ -326,7 +327,9 @@ class Engine:
             ptr, n = arr.ctypes.data, len(arr)
         else:
             arr, ptr, n = None, None, int(count)
-        cap = 1 << 12
+        # about 0.4 % of hut chunks are start chunks: room for 1 in 200 avoids a second walk
+        regions = max(0, rect[1] - rect[0]) * max(0, rect[3] - rect[2])
+        cap = min(1 << 24, max(1 << 12, n * regions // 200))
         while True:
             out = np.zeros(cap, DEEP_START_DTYPE)
             found = C.c_uint64()

@@ -1,0 +1,257 @@
+// hut_lookup: drop-in for the two Deep Dive commands hunt.py runs through the reference's GPU
+// engine (hut_lookup_v4, engine/gpu/hut_lookup_v4_source.cu:777-841 flags), on top of
+// libwitchgpu.so:
+//
+//   solver   --catalog C --solve-only --solve5 --plan P --first-index F --count N
+//            [--regime XZ] [--dump-hits H] [--out O] [--quiet]          (hunt.py:947-952)
+//            hits "S,chunkX,chunkZ,layoutX,1" to H; the summary line "solve: ..." on stdout
+//            (:1373-1380); exit 1 when a hit fails the host's forward check, as there
+//   terrain  --catalog C --spots SP [--max-height -54] --out O [--batch B] [--quiet]
+//            (hunt.py:954-957): "S chunkX chunkZ" lines; the world seeds (u << 48) | S48 that
+//            pass the phase-1 gates at the spot region whose hut is the spot chunk, as
+//            "seed,chunkX,chunkZ,layoutX,airHi,airLo" rows appended to O (header when empty);
+//            exit 1 when a spot is not a mineshaft start chunk (:1262-1290)
+//
+// The tuning flags of the reference (--fused-*, --task-batch, --ero-*, --batch, --u-*) are
+// accepted and change nothing: the solver and the gates here are exact.  The terrain gates are
+// lysh's phase 1 (lysh_phase1_check_ex) at --max-height with the hunt driver's version
+// (1.19.x~26.1), the same rule the spot fixtures pin.
+#include <cinttypes>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <algorithm>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/witchgpu.h"
+
+namespace {
+
+bool read_catalog(const char *path, std::map<uint64_t, std::pair<unsigned, unsigned>> &cat) {
+    FILE *f = std::fopen(path, "r");
+    if (!f) return false;
+    char ln[1024];
+    while (std::fgets(ln, sizeof ln, f)) {
+        if (ln[0] == '#' || ln[0] == '\n') continue;
+        unsigned long long x;
+        double hi, lo;
+        if (std::sscanf(ln, "%llu %lf %lf", &x, &hi, &lo) != 3) continue;
+        cat[x & 0xFFFFFFFFFFFFull] = {(unsigned)hi & 0x3FF, (unsigned)lo & 0x3FF};
+    }
+    std::fclose(f);
+    return true;
+}
+
+// The spot's setLargeFeatureSeed state, the reference's layoutX column for a spot: setSeed(S),
+// a = nextLong(), b = nextLong(), (cx a) ^ (cz b) ^ S (room_core.h:55-58).
+uint64_t carver_state(uint64_t s48, int cx, int cz) {
+    const uint64_t A = 0x5DEECE66Dull, M = 0xFFFFFFFFFFFFull;
+    uint64_t s = (s48 ^ A) & M;
+    int32_t h[4];
+    for (int k = 0; k < 4; k++) {
+        s = (s * A + 0xBull) & M;
+        h[k] = (int32_t)(s >> 16);
+    }
+    const uint64_t a = ((uint64_t)(int64_t)h[0] << 32) + (uint64_t)(int64_t)h[1];
+    const uint64_t b = ((uint64_t)(int64_t)h[2] << 32) + (uint64_t)(int64_t)h[3];
+    return ((uint64_t)((int64_t)cx * (int64_t)a) ^ (uint64_t)((int64_t)cz * (int64_t)b) ^ s48) & M;
+}
+
+int tier_of(const char *cls) {
+    if (!std::strcmp(cls, "odd")) return 1;
+    if (!std::strcmp(cls, "u2")) return 2;
+    if (!std::strcmp(cls, "eq")) return 3;
+    return 0;
+}
+
+int fail(const char *msg) {
+    std::fprintf(stderr, "%s\n", msg);
+    return 2;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    const char *cat_path = nullptr, *plan_path = nullptr, *spots_path = nullptr, *hits_path = nullptr;
+    const char *out_path = "hut_lookup_out.csv";
+    long long first = 0, count = 1;
+    int regx = -1, regz = -1, max_h = -54;
+    bool solve5 = false, quiet = false;
+    for (int i = 1; i < argc; i++) {
+        const char *a = argv[i];
+        auto val = [&]() -> const char * { return i + 1 < argc ? argv[++i] : nullptr; };
+        if (!std::strcmp(a, "--catalog")) cat_path = val();
+        else if (!std::strcmp(a, "--plan")) plan_path = val();
+        else if (!std::strcmp(a, "--spots")) spots_path = val();
+        else if (!std::strcmp(a, "--dump-hits")) hits_path = val();
+        else if (!std::strcmp(a, "--out")) out_path = val();
+        else if (!std::strcmp(a, "--first-index")) { const char *v = val(); if (v) first = std::atoll(v); }
+        else if (!std::strcmp(a, "--count")) { const char *v = val(); if (v) count = std::atoll(v); }
+        else if (!std::strcmp(a, "--max-height")) { const char *v = val(); if (v) max_h = std::atoi(v); }
+        else if (!std::strcmp(a, "--regime")) {
+            const char *v = val();
+            if (!v || std::strlen(v) != 2 || v[0] < '0' || v[0] > '2' || v[1] < '0' || v[1] > '2')
+                return fail("--regime XZ: two digits 0 (exact), 1 (mid), 2 (far)");
+            regx = v[0] - '0';
+            regz = v[1] - '0';
+        } else if (!std::strcmp(a, "--far")) regx = regz = 2;
+        else if (!std::strcmp(a, "--solve5")) solve5 = true;
+        else if (!std::strcmp(a, "--quiet")) quiet = true;
+        else if (!std::strcmp(a, "--solve-only") || !std::strcmp(a, "--solve") || !std::strcmp(a, "--ero-split") ||
+                 !std::strcmp(a, "--timing") || !std::strcmp(a, "--no-async"))
+            ;
+        else if (!std::strncmp(a, "--fused-", 8) || !std::strncmp(a, "--ero-", 6) || !std::strcmp(a, "--task-batch") ||
+                 !std::strcmp(a, "--batch") || !std::strcmp(a, "--u-lo") || !std::strcmp(a, "--u-hi") ||
+                 !std::strcmp(a, "--u-batch") || !std::strcmp(a, "--min-air") || !std::strcmp(a, "--cols")) {
+            if (!val()) return fail("missing value");
+        } else {
+            std::fprintf(stderr, "unknown arg %s\n", a);
+            return 2;
+        }
+    }
+    if (!cat_path) return fail("usage: hut_lookup --catalog cat.txt (--solve-only --solve5 --plan P | --spots S) ...");
+    std::map<uint64_t, std::pair<unsigned, unsigned>> cat;
+    if (!read_catalog(cat_path, cat)) { std::fprintf(stderr, "cannot read %s\n", cat_path); return 1; }
+
+    wg_engine *eng = nullptr;
+    int rc = wg_engine_open(0, &eng);
+    if (rc) { std::fprintf(stderr, "no GPU engine (status %d)\n", rc); return 1; }
+
+    if (spots_path) {
+        FILE *sf = std::fopen(spots_path, "r");
+        if (!sf) { std::fprintf(stderr, "cannot read %s\n", spots_path); wg_engine_close(eng); return 1; }
+        std::vector<int64_t> s48;
+        std::vector<int32_t> cx, cz;
+        char ln[512];
+        while (std::fgets(ln, sizeof ln, sf)) {
+            long long S;
+            int x, z;
+            if (ln[0] == '#' || std::sscanf(ln, "%lld %d %d", &S, &x, &z) != 3) continue;
+            s48.push_back((int64_t)((uint64_t)S & 0xFFFFFFFFFFFFull));
+            cx.push_back(x);
+            cz.push_back(z);
+        }
+        std::fclose(sf);
+        FILE *out = std::fopen(out_path, "a");
+        if (!out) { std::fprintf(stderr, "cannot write %s\n", out_path); wg_engine_close(eng); return 1; }
+        std::fseek(out, 0, SEEK_END);
+        if (std::ftell(out) == 0) std::fprintf(out, "seed,chunkX,chunkZ,layoutX,airHi,airLo\n");
+        wg_opts o{};   // wg_parse_version sets the version bits only; NORMAL preset
+        wg_parse_version("1.19.x~26.1", &o);
+        uint64_t total = 0, bad_all = 0;
+        for (size_t i0 = 0; i0 < s48.size(); i0 += 4096) {
+            const size_t n = std::min<size_t>(4096, s48.size() - i0);
+            std::vector<wg_candidate> c(1 << 16);
+            uint64_t got = 0, bad = 0;
+            for (;;) {
+                rc = wg_deep_spots(eng, s48.data() + i0, cx.data() + i0, cz.data() + i0, n, &o, max_h, c.data(),
+                                   c.size(), &got, &bad);
+                if (rc || got <= c.size()) break;
+                c.resize(got);
+            }
+            if (rc) { std::fprintf(stderr, "terrain stage failed: %s\n", wg_engine_error(eng)); break; }
+            bad_all += bad;
+            for (uint64_t k = 0; k < got; k++) {
+                const size_t spot = i0 + (size_t)(c[k].seed_index >> 16);
+                std::fprintf(out, "%lld,%d,%d,%llu,0,0\n", (long long)c[k].seed, cx[spot], cz[spot],
+                             (unsigned long long)carver_state((uint64_t)s48[spot], cx[spot], cz[spot]));
+                total++;
+            }
+        }
+        std::fclose(out);
+        if (bad_all) std::fprintf(stderr, "*** %llu spots are not mineshaft start chunks\n", (unsigned long long)bad_all);
+        std::printf("spots: %zu spots (%llu not a start), %llu terrain survivors -> %s\n", s48.size(),
+                    (unsigned long long)bad_all, (unsigned long long)total, out_path);
+        wg_engine_close(eng);
+        return rc ? 1 : (bad_all ? 1 : 0);
+    }
+
+    if (!solve5) { wg_engine_close(eng); return fail("only --solve5 and --spots are supported"); }
+    std::vector<wg_solve_bundle> bundles;
+    if (plan_path) {
+        FILE *pf = std::fopen(plan_path, "r");
+        if (!pf) { std::fprintf(stderr, "cannot read plan %s\n", plan_path); wg_engine_close(eng); return 1; }
+        char ln[1024];
+        while (std::fgets(ln, sizeof ln, pf)) {
+            if (ln[0] == '#' || ln[0] == '\n') continue;
+            unsigned long long x;
+            char rg[8], cls[16] = "odd";
+            if (std::sscanf(ln, "%llu %7s %15s", &x, rg, cls) < 2 || std::strlen(rg) != 2 || rg[0] < '0' || rg[0] > '2' ||
+                rg[1] < '0' || rg[1] > '2') {
+                std::fprintf(stderr, "bad plan line: %s", ln);
+                std::fclose(pf);
+                wg_engine_close(eng);
+                return 2;
+            }
+            const int t = tier_of(cls);
+            if (!t) { std::fprintf(stderr, "plan class '%s' unknown (odd | u2 | eq)\n", cls); std::fclose(pf); wg_engine_close(eng); return 2; }
+            wg_solve_bundle b;
+            std::memset(&b, 0, sizeof b);
+            b.layout = x & 0xFFFFFFFFFFFFull;
+            b.regime_x = rg[0] - '0';
+            b.regime_z = rg[1] - '0';
+            b.tier = t;
+            bundles.push_back(b);
+        }
+        std::fclose(pf);
+    } else {
+        if (regx < 0) { wg_engine_close(eng); return fail("--solve5 needs --regime XZ (or --plan)"); }
+        for (const auto &kv : cat) {
+            wg_solve_bundle b;
+            std::memset(&b, 0, sizeof b);
+            b.layout = kv.first;
+            b.regime_x = regx;
+            b.regime_z = regz;
+            b.tier = 1;
+            bundles.push_back(b);
+        }
+    }
+    if (bundles.empty()) { wg_engine_close(eng); return fail("no bundles"); }
+    if (first < 0 || count < 1 || (unsigned long long)(first + count) > ((unsigned long long)bundles.size() << 20)) {
+        std::fprintf(stderr, "group range %lld..%lld outside the %zu bundles x 2^20 groups\n", first, first + count,
+                     bundles.size());
+        wg_engine_close(eng);
+        return 2;
+    }
+    FILE *hf = hits_path ? std::fopen(hits_path, "w") : nullptr;
+    if (hits_path && !hf) { std::fprintf(stderr, "cannot write %s\n", hits_path); wg_engine_close(eng); return 1; }
+    wg_solve_stats tot;
+    std::memset(&tot, 0, sizeof tot);
+    std::vector<wg_solve_hit> hits(1 << 16);
+    for (long long g = first; g < first + count && rc == WG_OK;) {
+        const long long n = std::min<long long>(256, first + count - g);
+        wg_solve_stats st;
+        uint64_t got = 0;
+        for (;;) {
+            rc = wg_deep_solve(eng, bundles.data(), bundles.size(), (uint64_t)g, (uint64_t)n, hits.data(), hits.size(),
+                               &got, &st);
+            if (rc || got <= hits.size()) break;
+            hits.resize(got);
+        }
+        if (rc) { std::fprintf(stderr, "solver failed: %s\n", wg_engine_error(eng)); break; }
+        for (uint64_t k = 0; k < got && hf; k++)
+            std::fprintf(hf, "%llu,%d,%d,%llu,1\n", (unsigned long long)hits[k].s48, hits[k].chunk_x, hits[k].chunk_z,
+                         (unsigned long long)hits[k].layout);
+        tot.groups += st.groups;
+        tot.tasks += st.tasks;
+        tot.hits += st.hits;
+        tot.host_check_failures += st.host_check_failures;
+        tot.gpu_ms += st.gpu_ms;
+        tot.wall_ms += st.wall_ms;
+        if (!quiet)
+            std::fprintf(stderr, "groups %lld..%lld: %llu hits | %.1f s\n", first, g + n,
+                         (unsigned long long)tot.hits, tot.wall_ms / 1e3);
+        g += n;
+    }
+    if (hf) std::fclose(hf);
+    std::printf("solve: %llu tasks in %llu groups, %llu hits (%.4f per task), host-check failures %llu\n",
+                (unsigned long long)tot.tasks, (unsigned long long)tot.groups, (unsigned long long)tot.hits,
+                tot.tasks ? (double)tot.hits / (double)tot.tasks : 0.0, (unsigned long long)tot.host_check_failures);
+    std::printf("solve times: device %.3f s; wall %.3f s (%.4f us per task wall)\n", tot.gpu_ms / 1e3,
+                tot.wall_ms / 1e3, tot.tasks ? 1e3 * tot.wall_ms / (double)tot.tasks : 0.0);
+    wg_engine_close(eng);
+    if (rc) return 1;
+    return tot.host_check_failures ? 1 : 0;
+}

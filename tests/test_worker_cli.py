@@ -38,3 +38,24 @@ def test_no_gpu_worker_fails_loudly(wg):
     r = run(wg, "--worker", stdin="--seed 1 --out x.csv\n")
     assert r.returncode == 1 and "cannot open the GPU engine" in r.stderr
     assert "WORKER_READY" not in r.stdout
+
+
+def test_hut_lookup_usage_errors(wg, tmp_path):
+    """The Deep Dive worker refuses bad command lines with exit 2 before touching a GPU, and without
+    a GPU fails loudly (exit 1)."""
+    r = subprocess.run([wg.HUT_LOOKUP_PATH, "--bogus"], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 2 and "unknown arg" in r.stderr
+    r = subprocess.run([wg.HUT_LOOKUP_PATH, "--regime", "33"], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 2
+    r = subprocess.run([wg.HUT_LOOKUP_PATH, "--solve5"], capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 2 and "usage" in r.stderr
+    (tmp_path / "cat.txt").write_text("231564844655014 331 331\n")
+    try:
+        import torch
+        if torch.cuda.is_available():
+            return
+    except ImportError:
+        pass
+    r = subprocess.run([wg.HUT_LOOKUP_PATH, "--catalog", "cat.txt", "--solve5", "--regime", "22"],
+                       capture_output=True, text=True, cwd=tmp_path)
+    assert r.returncode == 1 and "no GPU" in r.stderr
