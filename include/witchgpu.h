@@ -220,8 +220,8 @@ typedef struct {
  * and whether a mineshaft starts there (setLargeFeatureSeed + nextDouble() < 0.004).  Writes up
  * to cap hits to out (host), sorted by (seed_index, rz, rx); *n_out = the number found.  Replaces the
  * room walk of hut_lookup_v4 (rcWalkStep / walkStepCarver / rcIsStartS0,
- * engine/gpu/room_core.h:40-175, engine/gpu/hut_lookup_v4_source.cu:47-75); the layout-catalog
- * lookup and the solver's inversion tables are not part of it. */
+ * engine/gpu/room_core.h:40-175, engine/gpu/hut_lookup_v4_source.cu:47-75): the forward
+ * direction; the layout-catalogue direction is wg_deep_solve. */
 int wg_deep_starts(wg_engine *e, const int64_t *s48, int64_t s48_base, uint64_t n,
                    int rx0, int rx1, int rz0, int rz1, wg_deep_start *out, uint64_t cap, uint64_t *n_out);
 
