@@ -236,6 +236,22 @@ int wg_deep_spots(wg_engine *e, const int64_t *s48, const int32_t *chunk_x, cons
                   const wg_opts *opts, int max_height, wg_candidate *out, uint64_t cap, uint64_t *n_out,
                   uint64_t *not_start);
 
+/* ---------------- biome map ---------------- */
+
+/* biome_map's raster (engine/tools/mineshaft/biome_map.c): w x h bytes (z outer, x inner; w, h
+ * <= 4096), cell (i, j) = the blocks [x0 + i step, x0 + (i+1) step) x [z0 + j step, ...); each of
+ * its ss x ss sample points (ss 1..4) gives the biome at the middle of the chunk holding it with the
+ * surface at y + 1 (lysh_swamp_hut_biome_ok); the cell is the dominant biome, a swamp winning at a
+ * quarter of the samples.  opts selects the biome tree (wg_parse_version). */
+int wg_biome_map(wg_engine *e, int64_t seed, const wg_opts *opts, int64_t x0, int64_t z0, int w, int h, int step,
+                 int ss, int y, uint8_t *out);
+
+/* biome_map --stdin: the biome the witch-hut test sees at each chunk (cx[i], cz[i]): the middle
+ * column at six fixed surface heights, and where they disagree about a swamp, at the chunk's
+ * real pre-carver surface (biome_map.c:38-52). */
+int wg_biome_chunks(wg_engine *e, int64_t seed, const wg_opts *opts, const int32_t *cx, const int32_t *cz,
+                    uint64_t n, uint8_t *out);
+
 /* ---------------- Deep Dive solver: structure seeds for a mineshaft layout ---------------- */
 
 /* One plan line (the reference's plan.txt: "X regime class ..."): the setLargeFeatureSeed state

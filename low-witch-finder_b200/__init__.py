@@ -22,6 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libwitchgpu.so")
 WORKER_PATH = os.path.join(HERE, "phase1_scan")
 HUT_LOOKUP_PATH = os.path.join(HERE, "hut_lookup")
+BIOME_MAP_PATH = os.path.join(HERE, "biome_map")
 HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "witchgpu.h")
 
 WG_OK, WG_ERR_ARG, WG_ERR_CUDA, WG_ERR_NOMEM, WG_ERR_CAPACITY, WG_ERR_NODEV = 0, 1, 2, 3, 4, 5
@@ -62,7 +63,7 @@ CANDIDATE_DTYPE = np.dtype([("seed_index", "<u8"), ("seed", "<i8"), ("rx", "<i4"
 EXPORTS = ("wg_engine_open", "wg_engine_close", "wg_engine_error", "wg_parse_version", "wg_parse_preset",
            "wg_seed_check", "wg_seed_check_device", "wg_phase1_codes", "wg_seed_check_noalloc",
            "wg_eval_huts", "wg_grade_scan", "wg_p2_probe", "wg_deep_starts", "wg_deep_spots",
-           "wg_deep_solve", "wg_deep_solve_tasks", "wg_seed_check_jobs", "wg_server_open", "wg_server_submit", "wg_server_poll", "wg_server_take",
+           "wg_biome_map", "wg_biome_chunks", "wg_deep_solve", "wg_deep_solve_tasks", "wg_seed_check_jobs", "wg_server_open", "wg_server_submit", "wg_server_poll", "wg_server_take",
            "wg_server_stats", "wg_server_close")
 
 # wg_deep_start: a swamp hut whose chunk is a mineshaft start chunk.
@@ -157,6 +158,8 @@ def library() -> C.CDLL:
     lib.wg_deep_starts.argtypes = [vp, vp, i64, u64, i32, i32, i32, i32, vp, u64, C.POINTER(u64)]
     lib.wg_deep_spots.argtypes = [vp, vp, vp, vp, u64, C.POINTER(Opts), i32, vp, u64, C.POINTER(u64),
                                   C.POINTER(u64)]
+    lib.wg_biome_map.argtypes = [vp, i64, C.POINTER(Opts), i64, i64, i32, i32, i32, i32, i32, vp]
+    lib.wg_biome_chunks.argtypes = [vp, i64, C.POINTER(Opts), vp, vp, u64, vp]
     lib.wg_deep_solve.argtypes = [vp, C.POINTER(SolveBundle), u64, u64, u64, vp, u64, C.POINTER(u64),
                                   C.POINTER(SolveStats)]
     lib.wg_deep_solve_tasks.argtypes = [vp, u64, vp, vp, vp, vp, u64, vp, u64, C.POINTER(u64)]
@@ -339,6 +342,32 @@ class Engine:
             if found.value <= cap:
                 return out[:found.value].copy()
             cap = int(found.value)
+
+    def biome_map(self, seed: int, x0: int, z0: int, w: int, h: int, step: int = 16, ss: int = 1,
+                  version: str = "26.3", y: int = 63) -> np.ndarray:
+        """wg_biome_map: (h, w) biome ids, as biome_map --seed ... writes them."""
+        o = Opts()
+        if library().wg_parse_version(version.encode(), C.byref(o)) != WG_OK:
+            raise ValueError(f"unknown version {version!r}")
+        out = np.zeros((h, w), np.uint8)
+        rc = library().wg_biome_map(self._h, to_signed(seed), C.byref(o), x0, z0, w, h, step, ss, y, out.ctypes.data)
+        if rc != WG_OK:
+            raise self._err(rc, "wg_biome_map")
+        return out
+
+    def biome_chunks(self, seed: int, cx, cz, version: str = "26.3") -> np.ndarray:
+        """wg_biome_chunks: the witch-hut test's biome at each chunk (biome_map --stdin)."""
+        o = Opts()
+        if library().wg_parse_version(version.encode(), C.byref(o)) != WG_OK:
+            raise ValueError(f"unknown version {version!r}")
+        x = np.ascontiguousarray(np.asarray(cx, dtype=np.int32))
+        z = np.ascontiguousarray(np.asarray(cz, dtype=np.int32))
+        out = np.zeros(len(x), np.uint8)
+        rc = library().wg_biome_chunks(self._h, to_signed(seed), C.byref(o), x.ctypes.data, z.ctypes.data, len(x),
+                                       out.ctypes.data)
+        if rc != WG_OK:
+            raise self._err(rc, "wg_biome_chunks")
+        return out
 
     def deep_solve(self, bundles, first_group: int, n_groups: int) -> tuple[np.ndarray, dict]:
         """wg_deep_solve: bundles = [(layout, "XZ" regime digits or (rx, rz), "odd" | "u2" | "eq"), ...]

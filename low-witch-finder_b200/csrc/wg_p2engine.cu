@@ -499,4 +499,79 @@ int wg_p2_probe(wg_engine *eng, int64_t seed, const wg_opts *opts, int kind, con
     return WG_OK;
 }
 
+int wg_biome_map(wg_engine *eng, int64_t seed, const wg_opts *opts, int64_t x0, int64_t z0, int w, int h, int step,
+                 int ss, int y, uint8_t *out) {
+    if (!eng || !out || w <= 0 || h <= 0 || w > 4096 || h > 4096 || step < 1 || ss < 1 || ss > 4) return WG_ERR_ARG;
+    P2_CUDA(cudaSetDevice(eng->device), "cudaSetDevice");
+    wg_opts o;
+    std::memset(&o, 0, sizeof o);
+    if (opts) o = *opts;
+    int rc = ensure_tables(eng);
+    if (rc) return rc;
+    rc = prepare(eng, std::vector<uint64_t>{(uint64_t)seed}, o.large_biomes ? 1 : 0, std::vector<JobKey>{}, false);
+    if (rc) return rc;
+    const size_t cells = (size_t)w * (size_t)h;
+    uint8_t *d_out = nullptr;
+    P2_CUDA(cudaMalloc(&d_out, cells), "biome map buffer");
+    p2_launch_biome_map(eng->p2_tables, eng->p2_worlds, tree_for(o), x0, z0, w, h, step, ss, y, d_out, eng->stream);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, cells, cudaMemcpyDeviceToHost, eng->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(eng->stream);
+    cudaFree(d_out);
+    if (e != cudaSuccess) return eng->fail(WG_ERR_CUDA, "biome map", e);
+    return WG_OK;
+}
+
+int wg_biome_chunks(wg_engine *eng, int64_t seed, const wg_opts *opts, const int32_t *cx, const int32_t *cz,
+                    uint64_t n, uint8_t *out) {
+    if (!eng || (n && (!cx || !cz || !out))) return WG_ERR_ARG;
+    if (n == 0) return WG_OK;
+    if (n > (1u << 24)) return WG_ERR_CAPACITY;
+    P2_CUDA(cudaSetDevice(eng->device), "cudaSetDevice");
+    wg_opts o;
+    std::memset(&o, 0, sizeof o);
+    if (opts) o = *opts;
+    int rc = ensure_tables(eng);
+    if (rc) return rc;
+    rc = prepare(eng, std::vector<uint64_t>{(uint64_t)seed}, o.large_biomes ? 1 : 0, std::vector<JobKey>{}, false);
+    if (rc) return rc;
+    int32_t *d_xz = nullptr;
+    uint8_t *d_out = nullptr;
+    std::vector<uint8_t> need(n);
+    cudaError_t e = cudaMalloc(&d_xz, sizeof(int32_t) * 2 * n);
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, 2 * n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_xz, cx, sizeof(int32_t) * n, cudaMemcpyHostToDevice, eng->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_xz + n, cz, sizeof(int32_t) * n, cudaMemcpyHostToDevice, eng->stream);
+    if (e == cudaSuccess) {
+        p2_launch_biome_chunks(eng->p2_tables, eng->p2_worlds, tree_for(o), d_xz, d_xz + n, (int)n, d_out, d_out + n,
+                               eng->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, n, cudaMemcpyDeviceToHost, eng->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(need.data(), d_out + n, n, cudaMemcpyDeviceToHost, eng->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(eng->stream);
+    cudaFree(d_xz);
+    cudaFree(d_out);
+    if (e != cudaSuccess) return eng->fail(WG_ERR_CUDA, "biome chunks", e);
+    // chunks on a swamp's edge: the biome with the real (pre-carver) surface of the chunk's middle,
+    // which the phase-2 path computes for a hut at the chunk origin
+    std::vector<int64_t> seeds;
+    std::vector<int32_t> hx, hz;
+    std::vector<uint64_t> at;
+    for (uint64_t k = 0; k < n; k++)
+        if (need[k]) {
+            seeds.push_back(seed);
+            hx.push_back(cx[k] * 16);
+            hz.push_back(cz[k] * 16);
+            at.push_back(k);
+        }
+    if (!at.empty()) {
+        std::vector<wg_hut_result> r(at.size());
+        rc = eval_huts(eng, seeds.data(), hx.data(), hz.data(), at.size(), o, -64, r.data());
+        if (rc) return rc;
+        for (size_t q = 0; q < at.size(); q++) out[at[q]] = (uint8_t)(r[q].biome_winner & 0xFF);
+    }
+    return WG_OK;
+}
+
 }  // extern "C"

@@ -1271,6 +1271,94 @@ __device__ int tree_search(const BiomeTree &g, const int64_t np[6]) {
     }
 }
 
+// The biome lysh_swamp_hut_biome_ok reports at a chunk's middle column (mid_x, mid_z) when the
+// surface there is at y + 1 (biome.c:94-156): the six climate parameters at quart
+// (mid_x >> 2, y >> 2, mid_z >> 2), quantised through float, and the nearest leaf of the tree.
+// The offset spline is evaluated at the same quart column (the reference asks for block
+// (qx * 4, qz * 4) >> 2, which is qx, qz again).
+__device__ int p2_biome_params(const P2Tables &T, const P2World &W, int tree, int mid_x, int mid_z, int y,
+                               int64_t np[6]) {
+    const int qx = mid_x >> 2, qy = y >> 2, qz = mid_z >> 2;
+    TerrainInfo ti;
+    p2_terrain(T, W, qx, qz, ti);
+    const double temperature = p2_dbl(T, W, Q_TEMPERATURE, ti.sx, 0.0, ti.sz);
+    const double humidity = p2_dbl(T, W, Q_VEGETATION, ti.sx, 0.0, ti.sz);
+    double offset, factor;
+    p2_offset_factor(T, ti, offset, factor);
+    const double yq = (double)(qy * 4);
+    const double depth = mc_lerp(mc_clamp((yq - -64.0) / (320.0 - -64.0), 0.0, 1.0), 1.5, -1.5) + offset;
+    np[0] = (int64_t)((float)temperature * 10000.0f);
+    np[1] = (int64_t)((float)humidity * 10000.0f);
+    np[2] = (int64_t)((float)ti.c * 10000.0f);
+    np[3] = (int64_t)((float)ti.e * 10000.0f);
+    np[4] = (int64_t)((float)depth * 10000.0f);
+    np[5] = (int64_t)((float)ti.w * 10000.0f);
+    const BiomeTree &g = T.trees[tree];
+    const int leaf = tree_search(g, np);
+    return leaf >= 0 ? g.biome[leaf] : -1;
+}
+
+__device__ __forceinline__ int64_t floor_div16(int64_t v) { return v >= 0 ? v / 16 : -((-v + 15) / 16); }
+
+// biome_map's raster (engine/tools/mineshaft/biome_map.c:105-127): cell (i, j) samples ss x ss
+// points, each the biome at the middle of the chunk holding it with the surface at y + 1; the
+// first id to reach the highest count wins, and a swamp that fills a quarter of the samples wins.
+__global__ void __launch_bounds__(128) p2_biome_map_kernel(const P2Tables *__restrict__ Tp, const P2World *__restrict__ worlds,
+                                                           int tree, int64_t x0, int64_t z0, int w, int h, int step,
+                                                           int ss, int y, uint8_t *out) {
+    const int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= (int64_t)w * h) return;
+    const P2Tables &T = *Tp;
+    const P2World &W = worlds[0];
+    const int i = (int)(cell % w), j = (int)(cell / w);
+    uint8_t ids[16];
+    int n = 0;
+    for (int b = 0; b < ss; b++) {
+        const int64_t Z = z0 + (int64_t)j * step + ((2LL * b + 1) * step) / (2LL * ss);
+        for (int a = 0; a < ss; a++) {
+            const int64_t X = x0 + (int64_t)i * step + ((2LL * a + 1) * step) / (2LL * ss);
+            const int cx = (int)floor_div16(X), cz = (int)floor_div16(Z);
+            int64_t np[6];
+            ids[n++] = (uint8_t)(p2_biome_params(T, W, tree, cx * 16 + 8, cz * 16 + 8, y, np) & 0xFF);
+        }
+    }
+    int best = -1, best_n = 0, swamps = 0;
+    for (int k = 0; k < n; k++) {
+        int c = 0;
+        for (int q = 0; q <= k; q++) c += ids[q] == ids[k];
+        if (c > best_n) {
+            best_n = c;
+            best = ids[k];
+        }
+        swamps += ids[k] == 6;
+    }
+    if (swamps * 4 >= n && swamps > 0) best = 6;
+    out[cell] = (uint8_t)best;
+}
+
+// biome_map --stdin's first pass (biome_map.c:38-52): the biome at each chunk's middle with the
+// surface at y + 1 for y = 40, 48, ..., 80; all swamp or no swamp settles it (the answer is the
+// swamp, or the y = 64 biome), a disagreement needs the real surface height (need[i] = 1).
+__global__ void __launch_bounds__(128) p2_biome_chunks_kernel(const P2Tables *__restrict__ Tp,
+                                                              const P2World *__restrict__ worlds, int tree,
+                                                              const int32_t *__restrict__ cx, const int32_t *__restrict__ cz,
+                                                              int n, uint8_t *out, uint8_t *need) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const P2Tables &T = *Tp;
+    const P2World &W = worlds[0];
+    int swamps = 0, first = 0;
+    for (int q = 0; q < 6; q++) {
+        int64_t np[6];
+        const int id = p2_biome_params(T, W, tree, cx[k] * 16 + 8, cz[k] * 16 + 8, 40 + 8 * q, np) & 0xFF;
+        if (q == 3) first = id;
+        swamps += id == 6;
+    }
+    const bool settled = swamps == 0 || swamps == 6;
+    out[k] = (uint8_t)(settled ? (swamps ? 6 : first) : 0);
+    need[k] = settled ? 0 : 1;
+}
+
 constexpr int kFinishThreads = 64;
 
 __global__ void __launch_bounds__(kFinishThreads) p2_finish_kernel(const P2Tables *__restrict__ Tp,
@@ -1320,33 +1408,12 @@ __global__ void __launch_bounds__(kFinishThreads) p2_finish_kernel(const P2Table
     {
         const int mid_x = (H.hut_x >> 4) * 16 + 8, mid_z = (H.hut_z >> 4) * 16 + 8;
         const int y = pre_h[63] - 1;
-        const int qx = mid_x >> 2, qy = y >> 2, qz = mid_z >> 2;
-        TerrainInfo ti;
-        p2_terrain(T, W, qx, qz, ti);
-        const double temperature = p2_dbl(T, W, Q_TEMPERATURE, ti.sx, 0.0, ti.sz);
-        const double humidity = p2_dbl(T, W, Q_VEGETATION, ti.sx, 0.0, ti.sz);
-        double offset, factor;
-        {
-            TerrainInfo t2;
-            p2_terrain(T, W, (qx * 4) >> 2, (qz * 4) >> 2, t2);
-            p2_offset_factor(T, t2, offset, factor);
-        }
-        const double yq = (double)(qy * 4);
-        const double depth = mc_lerp(mc_clamp((yq - -64.0) / (320.0 - -64.0), 0.0, 1.0), 1.5, -1.5) + offset;
         int64_t np[6];
-        np[0] = (int64_t)((float)temperature * 10000.0f);
-        np[1] = (int64_t)((float)humidity * 10000.0f);
-        np[2] = (int64_t)((float)ti.c * 10000.0f);
-        np[3] = (int64_t)((float)ti.e * 10000.0f);
-        np[4] = (int64_t)((float)depth * 10000.0f);
-        np[5] = (int64_t)((float)ti.w * 10000.0f);
-        const BiomeTree &g = T.trees[tree];
-        const int leaf = tree_search(g, np);
-        const int winner = leaf >= 0 ? g.biome[leaf] : -1;
+        const int winner = p2_biome_params(T, W, tree, mid_x, mid_z, y, np);
         for (int a = 0; a < 6; a++) R.biome_t[a] = np[a];
-        R.biome_qx = qx;
-        R.biome_qy = qy;
-        R.biome_qz = qz;
+        R.biome_qx = mid_x >> 2;
+        R.biome_qy = y >> 2;
+        R.biome_qz = mid_z >> 2;
         R.biome_occ_y = y;
         R.biome_winner = winner;
         R.biome_ok = winner == 6 ? 1 : 0;
@@ -1477,6 +1544,17 @@ void p2_launch_carve(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, in
         done |= 1ull << dev;
     }
     p2_carve_kernel<<<n_jobs, kCarveThreads, smem, s>>>(T, worlds, jobs);
+}
+
+void p2_launch_biome_map(const P2Tables *T, const P2World *worlds, int tree, int64_t x0, int64_t z0, int w, int h,
+                         int step, int ss, int y, uint8_t *out, cudaStream_t s) {
+    const int64_t cells = (int64_t)w * h;
+    p2_biome_map_kernel<<<(unsigned)((cells + 127) / 128), 128, 0, s>>>(T, worlds, tree, x0, z0, w, h, step, ss, y, out);
+}
+
+void p2_launch_biome_chunks(const P2Tables *T, const P2World *worlds, int tree, const int32_t *cx, const int32_t *cz,
+                            int n, uint8_t *out, uint8_t *need, cudaStream_t s) {
+    p2_biome_chunks_kernel<<<(n + 127) / 128, 128, 0, s>>>(T, worlds, tree, cx, cz, n, out, need);
 }
 
 void p2_launch_finish(const P2Tables *T, const P2World *worlds, const P2Chunk *jobs, const P2Hut *huts, int n_huts,

@@ -193,4 +193,10 @@ void p2_launch_finish(const P2Tables *T, const P2World *worlds, const P2Chunk *j
 void p2_launch_probe(const P2Tables *T, const P2World *worlds, const P2Chunk *jobs, const int32_t *pts,
                      int n_pts, int kind, double *out, cudaStream_t s);
 
+// biome_map raster and chunk-list passes (one world: worlds[0]).
+void p2_launch_biome_map(const P2Tables *T, const P2World *worlds, int tree, int64_t x0, int64_t z0, int w, int h,
+                         int step, int ss, int y, uint8_t *out, cudaStream_t s);
+void p2_launch_biome_chunks(const P2Tables *T, const P2World *worlds, int tree, const int32_t *cx, const int32_t *cz,
+                            int n, uint8_t *out, uint8_t *need, cudaStream_t s);
+
 }  // namespace wg
