@@ -14,7 +14,7 @@
 //     0 .. 3 + m are already zero; key = (cx, cz) mod 2^(4+m), which fixes those bits;
 //   * chain: per task (region, offset) one warp, each lane lifts the upper 28 state bits of one
 //     list entry.  When v2(cx) != v2(cz) each equation bit has one solution and the lift runs
-//     four bits per step (lift_nibbles); when v2(cx) == v2(cz) state bit j does not reach
+//     four bits per step (lift_chunks); when v2(cx) == v2(cz) state bit j does not reach
 //     equation bit j - 16 + m, so bit j branches and the lift is a bit-serial depth-first search
 //     (lift_branch).  Past equation bit 31 the remaining 2^m (2^(m+1)) top bits are enumerated
 //     and every completion is checked in full (48-bit carver state, hut offsets with the JDK
@@ -37,12 +37,15 @@ constexpr uint64_t kA2 = (kA * kA) & kM48;
 constexpr uint64_t kK2 = (kC * (kA + 1)) & kM48;
 constexpr uint64_t kA4 = (kA2 * kA2) & kM48;
 constexpr uint64_t kK4 = (kC * (kA * kA * kA + kA * kA + kA + 1)) & kM48;
+constexpr uint64_t kA3 = (kA2 * kA) & kM48;
+constexpr uint64_t kK3 = (kC * (kA * kA + kA + 1)) & kM48;
 constexpr uint64_t kSalt = 14357620ull, kRX = 341873128712ull, kRZ = 132897987541ull;
 constexpr int kRadius = 58593;
 constexpr uint32_t kListCap = 1536;     // t20 entries per (group, key) list (mean 1,024 at m = 0)
 constexpr uint32_t kGroupsPerBatch = 16;
 constexpr uint32_t kHitCap = 1u << 20;
 constexpr int kChainThreads = 256;
+constexpr int kLiftTable = 8 * 16 * 16;    // nibble lift table (bytes)
 
 // One group slot of a batch: its regions, offsets, key table and first task.
 struct SolveSlot {
@@ -146,7 +149,7 @@ __device__ __forceinline__ void leaf(const ChainTask &T, uint64_t t, int j, Solv
 // holds u only as V << 16 (bits known from lower nibbles), is triangular in z nibble by nibble:
 // nibble k solves zk ^ ((Aq_k + rho zk) mod 16) = Y_k, Aq = Kq + rho z<k, one lookup in a
 // 2,048-entry table [rho mod 16 / 2][Aq_k][Y_k].  The top m bits of u are free.
-struct NibbleTask {
+struct ChunkTask {
     uint32_t inv, rho, coef_o_x;   // 1 / odd multiplier, rho, 1 if the odd term is cx h2
     const uint8_t *row;            // table row for rho mod 16
 };
@@ -158,7 +161,7 @@ __device__ __forceinline__ uint32_t inverse_u32(uint32_t a) {   // a odd
     return x;
 }
 
-__device__ void lift_nibbles(const ChainTask &T, const NibbleTask &N, uint32_t t20, SolveHitDev *hits, uint32_t cap,
+__device__ void lift_chunks(const ChainTask &T, const ChunkTask &N, uint32_t t20, SolveHitDev *hits, uint32_t cap,
                              unsigned long long *cnt) {
     const uint32_t cx = (uint32_t)T.cx, cz = (uint32_t)T.cz, m = (uint32_t)T.m;
     const uint32_t h2 = (uint32_t)((((kA2 * t20) + kK2) & kM48) >> 16);
@@ -177,8 +180,20 @@ __device__ void lift_nibbles(const ChainTask &T, const NibbleTask &N, uint32_t t
     }
     const uint32_t u0 = (((z - o0) * N.inv) >> 4) & ((1u << (28 - m)) - 1u);
     for (uint32_t f = 0; f < (1u << m); f++) {
-        const uint64_t t = (uint64_t)t20 | ((uint64_t)(u0 | (f << (28 - m))) << 20);
-        const uint64_t S = (t ^ kA) & kM48;
+        // the 48-bit carver state of t = t20 | u << 20 from 32-bit words: the draws' low words
+        // h2, h4 move by (A^2 << 4) u and (A^4 << 4) u; only the low 16 bits of the high words
+        // h1, h3 reach bit 47 of a, b, and those are bits 16..31 of A t + C, A^3 t + K3, which the
+        // state's low word alone decides
+        const uint32_t u = u0 | (f << (28 - m)), t32 = t20 | (u << 20);
+        const uint32_t h2u = h2 + (uint32_t)(kA2 << 4) * u, h4u = h4 + (uint32_t)(kA4 << 4) * u;
+        const uint32_t h1lo = (((uint32_t)kA * t32 + (uint32_t)kC) >> 16) & 0xFFFFu;
+        const uint32_t h3lo = (((uint32_t)kA3 * t32 + (uint32_t)kK3) >> 16) & 0xFFFFu;
+        const uint64_t a = ((uint64_t)h1lo << 32) + (uint64_t)(int64_t)(int32_t)h2u;
+        const uint64_t b = ((uint64_t)h3lo << 32) + (uint64_t)(int64_t)(int32_t)h4u;
+        const uint64_t S = ((((uint64_t)(u >> 12)) << 32) | t32) ^ (kA & kM48);
+        const uint64_t carver =
+            ((uint64_t)((int64_t)T.cx * (int64_t)a) ^ (uint64_t)((int64_t)T.cz * (int64_t)b) ^ S) & kM48;
+        if (carver != T.X) continue;
         if (solve_check(S, T.cx, T.cz, T.X, T.creg, T.ox, T.oz)) emit_hit(T, S, hits, cap, cnt);
     }
 }
@@ -249,8 +264,8 @@ __global__ void __launch_bounds__(kChainThreads) solve_chain_kernel(
     const int2 *__restrict__ offsets, const uint32_t *__restrict__ keymap, const uint32_t *__restrict__ lists,
     const uint32_t *__restrict__ counts, const uint8_t *__restrict__ nib, uint64_t X, SolveHitDev *hits,
     uint32_t hit_cap, unsigned long long *cnt) {
-    __shared__ uint8_t tab[2048];
-    for (int i = threadIdx.x; i < 2048 / 4; i += kChainThreads) ((uint32_t *)tab)[i] = ((const uint32_t *)nib)[i];
+    __shared__ __align__(16) uint8_t tab[kLiftTable];
+    for (int i = threadIdx.x; i < kLiftTable / 16; i += kChainThreads) ((uint4 *)tab)[i] = ((const uint4 *)nib)[i];
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const uint64_t warps = (uint64_t)gridDim.x * (kChainThreads / 32);
@@ -285,14 +300,14 @@ __global__ void __launch_bounds__(kChainThreads) solve_chain_kernel(
         if (T.eq) {
             for (uint32_t i = lane; i < n; i += 32) lift_branch(T, list[i], hits, hit_cap, cnt);
         } else {
-            NibbleTask N;
+            ChunkTask N;
             const uint32_t cxa = (uint32_t)T.cx * (uint32_t)kA2, cza = (uint32_t)T.cz * (uint32_t)kA4;
             N.coef_o_x = vx < vz ? 1u : 0u;
             const uint32_t co = (N.coef_o_x ? cxa : cza) >> T.m, ce = (N.coef_o_x ? cza : cxa) >> T.m;
             N.inv = inverse_u32(co);
             N.rho = ce * N.inv;
             N.row = tab + ((N.rho & 15u) >> 1) * 256;
-            for (uint32_t i = lane; i < n; i += 32) lift_nibbles(T, N, list[i], hits, hit_cap, cnt);
+            for (uint32_t i = lane; i < n; i += 32) lift_chunks(T, N, list[i], hits, hit_cap, cnt);
         }
     }
     if (lane == 0 && lifted) atomicAdd(&cnt[SCNT_CANDIDATES], lifted);
@@ -368,12 +383,12 @@ int solve_state(wg_engine *eng, SolveState **out) {
         SOLVE_CUDA(cudaMemcpy(s->hq, list.data(), sizeof(uint32_t) << 20, cudaMemcpyHostToDevice), "solver tables");
         SOLVE_CUDA(cudaMemcpy(s->hq_off, off.data(), sizeof(uint32_t) * 65, cudaMemcpyHostToDevice), "solver tables");
         // the nibble step's solutions, by search: x ^ ((a + 2r x) mod 16) is a bijection of x
-        std::vector<uint8_t> nib(2048, 0);
+        std::vector<uint8_t> nib(kLiftTable, 0);
         for (int r = 0; r < 8; r++)
             for (int a = 0; a < 16; a++)
                 for (int x = 0; x < 16; x++) nib[r * 256 + a * 16 + (x ^ ((a + 2 * r * x) & 15))] = (uint8_t)x;
-        SOLVE_CUDA(cudaMalloc(&s->nib, 2048), "solver tables");
-        SOLVE_CUDA(cudaMemcpy(s->nib, nib.data(), 2048, cudaMemcpyHostToDevice), "solver tables");
+        SOLVE_CUDA(cudaMalloc(&s->nib, kLiftTable), "solver tables");
+        SOLVE_CUDA(cudaMemcpy(s->nib, nib.data(), kLiftTable, cudaMemcpyHostToDevice), "solver tables");
     }
     *out = eng->solve;
     return WG_OK;
