@@ -222,6 +222,18 @@ def deep_measure(eng, opts) -> dict:
                       "out); device time of the solver from its CUDA events"}
 
 
+def biome_measure(eng) -> dict:
+    """The map tab's biome raster (wg_biome_map): 2,048 x 2,048 cells of one chunk each (ss 1) around
+    the SCAN_REFERENCE hut, wall clock around the call (world build included), after a warm-up."""
+    seed = 1473884015873122059
+    eng.biome_map(seed, -16384, -17408, 64, 64, 16)
+    t0 = time.perf_counter()
+    m = eng.biome_map(seed, -16384 - 16 * 1024, -17408 - 16 * 1024, 2048, 2048, 16)
+    secs = time.perf_counter() - t0
+    return {"cells": int(m.size), "cells_per_s": m.size / secs, "ms": 1e3 * secs, "swamp_cells": int((m == 6).sum()),
+            "timing": "wall clock around wg_biome_map (one world build, raster back to the host)"}
+
+
 def jobs_measure(wg, eng, n_jobs: int = 65536) -> dict:
     """Uneven batched jobs: the 65,536 jobs of the splitmix64(3) job stream (1..4,096 seeds,
     radius 1..64, floors -50..-54) through one wg_seed_check_jobs call, host seed lists in and
@@ -462,6 +474,7 @@ def main() -> None:
         }
         line["phase2"] = phase2_measure(eng, res.candidates, opts, cpu=(world == 1 and not args.no_cpu_baseline))
         line["deep_dive"] = deep_measure(eng, opts)
+        line["biome_map"] = biome_measure(eng)
         if world == 1 and not args.no_jobs:
             line["jobs"] = jobs_measure(wg, eng)
             line["serving"] = serving_measure(wg)
