@@ -238,6 +238,7 @@ struct ClimateSmem {
     uint32_t clist[kClimateList];              // erosion survivors of the chunk
     uint32_t rlist[kClimateList];              // ... that also passed temperature
     uint32_t n_tlist, t_next, n_clist, n_rlist;
+    uint32_t tcount[2];                        // list lengths of the breadth-first tier steps (ping-pong)
     uint32_t surv[kUnits * kRecordCap];
     uint32_t cnt[kUnits];
     uint32_t end[kUnits];                      // end of the current chunk, per unit
@@ -516,68 +517,71 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
         }
         __syncthreads();
 
-        // ---- the remaining erosion tiers (and, past a full climate list, temperature and ridge)
-        // for the tier-0 survivors: one Perlin sample per loop trip, a thread whose region is done
-        // takes the next one from the shared list at once ----
+        // ---- the remaining erosion tiers, breadth first: every listed region takes erosion step k
+        // (one sample with the step's slot and constants, the same for all), its tier check, and
+        // the survivors are compacted for step k + 1 (items held in registers between the two
+        // barriers, so the list is rewritten in place); past the last tier they go to the climate
+        // list, or, when it is full, through temperature and ridge by the thread itself ----
         {
-            const uint32_t n_t = min(S.n_tlist, (uint32_t)kTierList);
-            uint32_t e = 0, item = 0;
-            int iu = 0, k = 0;
-            bool have = false;
-            double xc = 0.0, zc = 0.0, sum = 0.0, sum_a = 0.0;
-            for (;;) {
-                if (!have) {
-                    cg::coalesced_group grp = cg::coalesced_threads();
-                    uint32_t base = 0;
-                    if (grp.thread_rank() == 0) base = atomicAdd(&S.t_next, grp.size());
-                    item = grp.shfl(base, 0) + grp.thread_rank();
-                    if (item >= n_t) break;
-                    e = S.tlist[item];
-                    iu = (int)(e >> 16);
-                    climate_point(S, iu, e & 0xFFFFu, xc, zc);
-                    sum = S.tsum[item];
-                    k = 2;
-                    have = true;
-                }
-                const uint32_t j = c0 + (e & 0xFFFFu);
-                const double v = climate_sample(S, iu, k, xc, zc);
-                sum += (st.c1[k] * v) * st.c2[k];
-                const int act = st.act[k];
-                bool done = false;
-                if (act == ACT_TIER || act == ACT_TIER_LAST) {
-                    if (sum * st.amp[k] < st.thr[k]) {
-                        erosion_reject(S, a, tc, iu, j, st.tier[k]);
-                        done = true;
-                    } else if (act == ACT_TIER_LAST) {
-                        const uint32_t qq = atomicAdd(&S.n_clist, 1u);
-                        if (qq < kClimateList) {
-                            S.clist[qq] = e;
-                            done = true;
+            constexpr int kPer = (kTierList + kThreadsA - 1) / kThreadsA;
+            if (tid == 0) S.tcount[1] = min(S.n_tlist, (uint32_t)kTierList);
+            __syncthreads();
+#pragma unroll 1
+            for (int k = 2; k < kClimateSteps && st.act[k] != ACT_NONE && st.act[k] <= ACT_TIER_LAST; k++) {
+                const uint32_t n_t = S.tcount[(k - 1) & 1];
+                if (tid == 0) S.tcount[k & 1] = 0;
+                const double c1 = st.c1[k], c2 = st.c2[k], amp = st.amp[k], thr = st.thr[k];
+                const int tier = st.tier[k];
+                const bool last = st.act[k] == ACT_TIER_LAST;
+                uint32_t ke[kPer];
+                double ks[kPer];
+#pragma unroll
+                for (int r = 0; r < kPer; r++) {
+                    const uint32_t q = (uint32_t)tid + (uint32_t)(r * kThreadsA);
+                    ke[r] = 0xFFFFFFFFu;
+                    ks[r] = 0.0;
+                    if (q < n_t) {
+                        const uint32_t e = S.tlist[q];
+                        const int iu = (int)(e >> 16);
+                        double xc, zc;
+                        climate_point(S, iu, e & 0xFFFFu, xc, zc);
+                        double sum = S.tsum[q];
+                        sum += (c1 * climate_sample(S, iu, k, xc, zc)) * c2;
+                        if (sum * amp < thr) {
+                            erosion_reject(S, a, tc, iu, c0 + (e & 0xFFFFu), tier);
                         } else {
-                            sum = 0.0;   // climate list full: finish it here
+                            ke[r] = e;
+                            ks[r] = sum;
                         }
                     }
-                } else if (act == ACT_END_SUB_A) {
-                    sum_a = sum;
-                    sum = 0.0;
-                } else if (act == ACT_TEMPERATURE) {
-                    const double t = (sum_a + sum) * st.amp[k];
-                    const bool bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
-                    if (bad) {
-                        climate_reject(S, a, iu, j, P1_TEMPERATURE, -1);
-                        done = true;
-                    }
-                    sum = 0.0;
-                } else if (act == ACT_RIDGE) {
-                    const double rg = (sum_a + sum) * st.amp[k];
-                    if ((rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91))
-                        climate_reject(S, a, iu, j, P1_RIDGE, -1);
-                    else
-                        keep_survivor(S, a, iu, j);   // climate survivor, not yet a verdict
-                    done = true;
                 }
-                if (done) have = false;
-                else k++;
+                __syncthreads();   // every read of this step's list is done
+#pragma unroll
+                for (int r = 0; r < kPer; r++) {
+                    const bool keep = ke[r] != 0xFFFFFFFFu;
+                    if (!last) {
+                        cg::coalesced_group grp = cg::coalesced_threads();
+                        const unsigned m = grp.ballot(keep);
+                        uint32_t base = 0;
+                        if (grp.thread_rank() == 0 && m) base = atomicAdd(&S.tcount[k & 1], (uint32_t)__popc(m));
+                        base = grp.shfl(base, 0);
+                        if (keep) {
+                            const uint32_t at = base + (uint32_t)__popc(m & ((1u << grp.thread_rank()) - 1u));
+                            S.tlist[at] = ke[r];
+                            S.tsum[at] = ks[r];
+                        }
+                    } else if (keep) {
+                        const uint32_t qq = atomicAdd(&S.n_clist, 1u);
+                        if (qq < kClimateList) {
+                            S.clist[qq] = ke[r];
+                        } else {   // climate list full: temperature and ridge here
+                            double xc, zc;
+                            climate_point(S, (int)(ke[r] >> 16), ke[r] & 0xFFFFu, xc, zc);
+                            climate_rest(S, a, tc, ke[r], c0, k + 1, 0.0, xc, zc);
+                        }
+                    }
+                }
+                __syncthreads();   // the compacted list is complete
             }
         }
         __syncthreads();
