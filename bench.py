@@ -197,7 +197,7 @@ def deep_measure(eng, opts) -> dict:
     hits = eng.deep_starts(base=0x5EED0000, count=n_s48, rect=rect)
     walk_s = time.perf_counter() - t0
     regions = n_s48 * (rect[1] - rect[0]) * (rect[3] - rect[2])
-    spots = hits[:64]
+    spots = hits[:256]
     eng.deep_spots(spots["s48"][:2], spots["chunk_x"][:2], spots["chunk_z"][:2], max_height=-54, opts=opts)
     t0 = time.perf_counter()
     surv, bad = eng.deep_spots(spots["s48"], spots["chunk_x"], spots["chunk_z"], max_height=-54, opts=opts)

@@ -21,6 +21,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <chrono>
 #include <map>
 #include <string>
 #include <vector>
@@ -141,6 +142,7 @@ int main(int argc, char **argv) {
         wg_opts o{};   // wg_parse_version sets the version bits only; NORMAL preset
         wg_parse_version("1.19.x~26.1", &o);
         uint64_t total = 0, bad_all = 0;
+        const auto t0 = std::chrono::steady_clock::now();
         for (size_t i0 = 0; i0 < s48.size(); i0 += 4096) {
             const size_t n = std::min<size_t>(4096, s48.size() - i0);
             std::vector<wg_candidate> c(1 << 16);
@@ -162,8 +164,10 @@ int main(int argc, char **argv) {
         }
         std::fclose(out);
         if (bad_all) std::fprintf(stderr, "*** %llu spots are not mineshaft start chunks\n", (unsigned long long)bad_all);
-        std::printf("spots: %zu spots (%llu not a start), %llu terrain survivors -> %s\n", s48.size(),
-                    (unsigned long long)bad_all, (unsigned long long)total, out_path);
+        const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::printf("spots: %zu spots (%llu not a start), %llu terrain survivors -> %s; terrain %.3f s (%.1f ms per spot)\n",
+                    s48.size(), (unsigned long long)bad_all, (unsigned long long)total, out_path, secs,
+                    s48.empty() ? 0.0 : 1e3 * secs / (double)s48.size());
         wg_engine_close(eng);
         return rc ? 1 : (bad_all ? 1 : 0);
     }

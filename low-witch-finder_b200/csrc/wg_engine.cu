@@ -79,7 +79,18 @@ int run_batch(wg_engine *eng, const BatchArgs &proto, uint64_t unit0, uint32_t n
     WG_CUDA(cudaMemsetAsync(eng->hist, 0, sizeof(unsigned long long) * (P1_KINDS + kTiers), eng->stream),
             "memset hist");
     WG_CUDA(cudaEventRecord(eng->kev[0], eng->stream), "event");
-    launch_climate(a, eng->stream);
+    // one region per unit: the climate tables are built lazily, breadth first
+    if (!a.jobs && a.win == 1 && !a.codes && !a.single_biome) {
+        if (!eng->spot_counts) {
+            WG_CUDA(cudaMalloc(&eng->spot_items[0], sizeof(SpotItem) * kMaxUnits), "alloc");
+            WG_CUDA(cudaMalloc(&eng->spot_items[1], sizeof(SpotItem) * kMaxUnits), "alloc");
+            WG_CUDA(cudaMalloc(&eng->spot_counts, sizeof(uint32_t) * 2), "alloc");
+        }
+        launch_spot_climate(a, eng->spot_items[0], eng->spot_items[1], eng->spot_counts, kMaxUnits, eng->sm_count,
+                            eng->stream);
+    } else {
+        launch_climate(a, eng->stream);
+    }
     WG_CUDA(cudaEventRecord(eng->kev[1], eng->stream), "event");
     launch_entrance(a, eng->sm_count * 2, eng->stream);
     WG_CUDA(cudaEventRecord(eng->kev[2], eng->stream), "event");
@@ -327,6 +338,9 @@ void wg_engine_close(wg_engine *eng) {
     cudaFree(eng->counters);
     cudaFree(eng->hist);
     cudaFree(eng->d_seed_list);
+    cudaFree(eng->spot_items[0]);
+    cudaFree(eng->spot_items[1]);
+    cudaFree(eng->spot_counts);
     p2_release(eng);
     solve_release(eng);
     cudaFreeHost(eng->h_counters);

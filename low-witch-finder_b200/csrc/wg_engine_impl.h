@@ -34,6 +34,9 @@ struct wg_engine {
     cudaEvent_t kev[4] = {nullptr, nullptr, nullptr, nullptr};   // around the three kernels of a batch
     int64_t *d_seed_list = nullptr;
     uint64_t d_seed_cap = 0;
+    // breadth-first climate stage of one-region batches: two item lists and their counts
+    wg::SpotItem *spot_items[2] = {nullptr, nullptr};
+    uint32_t *spot_counts = nullptr;
 
     // phase 2 (wg_p2engine.cu): device tables, grow-only work buffers
     wg::P2Tables *p2_tables = nullptr;

@@ -697,6 +697,220 @@ void launch_climate(const BatchArgs &a, cudaStream_t s) {
 }
 
 // ------------------------------------------------------------------------------------
+// Climate stage for one-region units (the Deep Dive terrain stage: 65,536 upper-bit variants of
+// a spot, each a different world seed over one region).  The climate kernel builds all 18 climate
+// tables of a unit because a 9 x 9 unit needs nearly all of them; a one-region unit needs the two
+// tier-0 tables and then one more per erosion step it reaches (about 3.2 of 18 on average), and
+// each step samples only its own octave.  So the stage runs breadth first over lists in HBM:
+// tier 0 for every unit, then one kernel per erosion step over the survivors of the step before
+// (one table per item, the partial sum carried in the item), then temperature and ridge for the
+// erosion survivors; ridge survivors become unit records for the entrance kernel as usual.
+// A thread owns one byte column of its block's table area and builds one table at a time there.
+// ------------------------------------------------------------------------------------
+constexpr int kSpotThreads = 256;
+constexpr int kSpotStride = kSpotThreads + 16;   // bytes per table row: one column per thread
+
+struct SpotSmem {
+    uint8_t perm[256 * kSpotStride];
+    uint32_t grad[kGradWords];
+};
+
+// Builds, in this thread's column, the table of climate step k of `seed` and samples it at the
+// unit's climate point (xc, zc) (climate_sample for a single table).
+__device__ double spot_sample(SpotSmem &S, int large, int k, uint64_t seed, double xc, double zc) {
+    const ClimateStep &cs = c_steps[large][k];
+    const int slot = cs.slot;
+    uint8_t *col = S.perm + threadIdx.x;
+    for (int i = 0; i < 256; i++) col[i * kSpotStride] = (uint8_t)i;
+    Xr r = octave_rng(c_noise[c_slot_a[large][slot][0]], seed_fork_of(seed), c_slot_a[large][slot][1],
+                      c_slot_a[large][slot][2]);
+    double ox, oy, oz;
+    perlin_shuffle<kSpotStride>(col, r, ox, oy, oz);
+    const int jy = (int)floor(oy);
+    const double hy = oy - jy;
+    const ColTable<kSpotStride> T{col, S.grad};
+    return perlin_y0(T, ox, oz, jy, hy, fade(hy), keep_precision((xc * cs.sc) * cs.lac),
+                     keep_precision((zc * cs.sc) * cs.lac));
+}
+
+// The unit's world seed and climate point (its only region's hut chunk middle).
+__device__ __forceinline__ uint64_t spot_point(const BatchArgs &a, uint32_t u, double &xc, double &zc) {
+    const UnitPos up = unit_pos(a, u);
+    const uint64_t seed = seed_value(a, up.g);
+    int cx, cz;
+    hut_chunk(seed, up.rx0, up.rz0, a.salt, cx, cz);
+    xc = (cx * 16 + 8) / 4.0;
+    zc = (cz * 16 + 8) / 4.0;
+    return seed;
+}
+
+__device__ __forceinline__ void spot_append(SpotItem *out, uint32_t *out_n, uint32_t cap, bool keep, const SpotItem &it,
+                                            uint32_t *overflow) {
+    cg::coalesced_group grp = cg::coalesced_threads();
+    const unsigned m = grp.ballot(keep);
+    uint32_t base = 0;
+    if (grp.thread_rank() == 0 && m) base = atomicAdd(out_n, (uint32_t)__popc(m));
+    base = grp.shfl(base, 0);
+    if (keep) {
+        const uint32_t at = base + (uint32_t)__popc(m & ((1u << grp.thread_rank()) - 1u));
+        if (at < cap) out[at] = it;
+        else atomicOr(overflow, 1u);
+    }
+}
+
+__device__ __forceinline__ void spot_count(unsigned long long *hist, int idx, uint32_t n) {
+    const uint32_t tot = __reduce_add_sync(0xFFFFFFFFu, n);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&hist[idx], (unsigned long long)tot);
+}
+
+// Tier 0: lanes 2i and 2i+1 build octaves 0A and 0B of one unit; the even lane sums them in the
+// reference's order and applies the tier-0 threshold.
+__global__ void __launch_bounds__(kSpotThreads) spot_tier0_kernel(BatchArgs a, SpotItem *out, uint32_t *out_n,
+                                                                  uint32_t cap) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    SpotSmem &S = *reinterpret_cast<SpotSmem *>(smem_raw);
+    fill_grad_table(S.grad, threadIdx.x);
+    __syncthreads();
+    const int large = a.large_biomes ? 1 : 0;
+    const ClimateStep &s0 = c_steps[large][0], &s1 = c_steps[large][1];
+    uint32_t rejected = 0;
+    const uint64_t tasks = 2ull * a.n_units;
+    for (uint64_t base = (uint64_t)blockIdx.x * kSpotThreads; base < tasks; base += (uint64_t)gridDim.x * kSpotThreads) {
+        const uint64_t task = base + threadIdx.x;
+        const bool valid = task < tasks;
+        const uint32_t u = (uint32_t)(task >> 1);
+        double v = 0.0;
+        if (valid) {
+            double xc, zc;
+            const uint64_t seed = spot_point(a, u, xc, zc);
+            v = spot_sample(S, large, (int)(task & 1), seed, xc, zc);
+        }
+        const double v1 = __shfl_down_sync(0xFFFFFFFFu, v, 1);
+        bool keep = false;
+        SpotItem it{u, 0u, 0.0, 0.0};
+        if (valid && !(task & 1)) {
+            double sum = 0.0;
+            sum += (s0.c1 * v) * s0.c2;
+            sum += (s1.c1 * v1) * s1.c2;
+            if (sum * s1.amp < s1.thr) rejected++;
+            else {
+                keep = true;
+                it.sum = sum;
+            }
+        }
+        spot_append(out, out_n, cap, keep, it, &a.counters[CNT_OVERFLOW]);
+    }
+    spot_count(a.hist, P1_KINDS + s1.tier, rejected);
+    spot_count(a.hist, P1_EROSION, rejected);
+}
+
+// Climate steps [k0, k1) for every listed item, one table at a time per item, in the state
+// machine's order (erosion tier checks, the A/B split, temperature, ridge).  Items that pass the
+// last erosion tier or temperature go to `out` for the next stage; ridge survivors become unit
+// records (CNT_RECORDS / CNT_SURVIVORS, one region each) for the entrance kernel.
+__global__ void __launch_bounds__(kSpotThreads) spot_steps_kernel(BatchArgs a, int k0, int k1, const SpotItem *in,
+                                                                  const uint32_t *in_n, SpotItem *out, uint32_t *out_n,
+                                                                  uint32_t cap) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    SpotSmem &S = *reinterpret_cast<SpotSmem *>(smem_raw);
+    fill_grad_table(S.grad, threadIdx.x);
+    __syncthreads();
+    const int large = a.large_biomes ? 1 : 0;
+    const uint32_t n = min(*in_n, cap);
+    uint32_t rej_tier = 0, rej_temp = 0, rej_ridge = 0;
+    for (uint32_t base = blockIdx.x * kSpotThreads; base < n; base += gridDim.x * kSpotThreads) {
+        const uint32_t e = base + threadIdx.x;
+        bool keep = false;
+        SpotItem it{0u, 0u, 0.0, 0.0};
+        if (e < n) {
+            it = in[e];
+            double xc, zc;
+            const uint64_t seed = spot_point(a, it.unit, xc, zc);
+            double sum = it.sum, sum_a = it.sum_a;
+            bool alive = true;
+            for (int k = k0; k < k1 && alive; k++) {
+                const ClimateStep &cs = c_steps[large][k];
+                sum += (cs.c1 * spot_sample(S, large, k, seed, xc, zc)) * cs.c2;
+                switch (cs.act) {
+                    case ACT_TIER:
+                    case ACT_TIER_LAST:
+                        if (sum * cs.amp < cs.thr) {
+                            alive = false;
+                            rej_tier++;
+                        } else if (cs.act == ACT_TIER_LAST) {
+                            sum = 0.0;
+                        }
+                        break;
+                    case ACT_END_SUB_A:
+                        sum_a = sum;
+                        sum = 0.0;
+                        break;
+                    case ACT_TEMPERATURE: {
+                        const double t = (sum_a + sum) * cs.amp;
+                        const bool bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
+                        if (bad) {
+                            alive = false;
+                            rej_temp++;
+                        }
+                        sum = 0.0;
+                        sum_a = 0.0;
+                        break;
+                    }
+                    case ACT_RIDGE: {
+                        const double rg = (sum_a + sum) * cs.amp;
+                        if ((rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91)) {
+                            alive = false;
+                            rej_ridge++;
+                        } else {
+                            emit_single(a, it.unit, 0u);   // climate survivor: a record of one region
+                        }
+                        alive = false;   // ridge is the last climate step
+                        break;
+                    }
+                    default:
+                        break;
+                }
+            }
+            if (alive) {
+                keep = true;
+                it.sum = sum;
+                it.sum_a = sum_a;
+            }
+        }
+        spot_append(out, out_n, cap, keep, it, &a.counters[CNT_OVERFLOW]);
+    }
+    // a step kernel over erosion steps checks one tier (the caller runs one step per launch there)
+    if (k1 <= 8) {
+        spot_count(a.hist, P1_KINDS + (k1 - 2), rej_tier);
+        spot_count(a.hist, P1_EROSION, rej_tier);
+    }
+    spot_count(a.hist, P1_TEMPERATURE, rej_temp);
+    spot_count(a.hist, P1_RIDGE, rej_ridge);
+}
+
+size_t spot_smem_bytes() { return sizeof(SpotSmem); }
+
+void launch_spot_climate(const BatchArgs &a, SpotItem *list0, SpotItem *list1, uint32_t *counts, uint32_t cap,
+                         int sm_count, cudaStream_t s) {
+    static unsigned long long done0 = 0, done1 = 0;
+    allow_dynamic_smem(spot_tier0_kernel, sizeof(SpotSmem), done0);
+    allow_dynamic_smem(spot_steps_kernel, sizeof(SpotSmem), done1);
+    const int grid = sm_count * 3;   // three 70 KB blocks per SM
+    SpotItem *lists[2] = {list0, list1};
+    cudaMemsetAsync(counts, 0, sizeof(uint32_t) * 2, s);
+    spot_tier0_kernel<<<grid, kSpotThreads, sizeof(SpotSmem), s>>>(a, lists[0], &counts[0], cap);
+    int cur = 0;
+    // erosion steps 2..7, one launch each; then temperature (8..11) and ridge (12..17)
+    const int bounds[][2] = {{2, 3}, {3, 4}, {4, 5}, {5, 6}, {6, 7}, {7, 8}, {8, 12}, {12, 18}};
+    for (const auto &b : bounds) {
+        cudaMemsetAsync(&counts[cur ^ 1], 0, sizeof(uint32_t), s);
+        spot_steps_kernel<<<grid, kSpotThreads, sizeof(SpotSmem), s>>>(a, b[0], b[1], lists[cur], &counts[cur],
+                                                                       lists[cur ^ 1], &counts[cur ^ 1], cap);
+        cur ^= 1;
+    }
+}
+
+// ------------------------------------------------------------------------------------
 // entrance kernel: Entrance(50) / Entrance(60) for every climate survivor
 //
 // Thread t builds table (slot t / kUnits, record t % kUnits).  Afterwards it samples only that

@@ -140,12 +140,23 @@ constexpr int kClimateSteps = kSlotsA;
 // Host: the 18-step climate sequence for one preset (wg_engine.cu).
 void build_climate_steps(const NoiseSpec *specs, int erosion, int temperature, ClimateStep *steps);
 
+// An item of the breadth-first climate stage for one-region units: the unit, its partial sums.
+struct SpotItem {
+    uint32_t unit, pad;
+    double sum, sum_a;
+};
+
 // Launchers (wg_phase1.cu).
 void upload_tables(const NoiseSpec *specs, const ClimateStep *steps_normal, const ClimateStep *steps_large);
 void launch_climate(const BatchArgs &a, cudaStream_t s);
 void launch_entrance(const BatchArgs &a, int grid, cudaStream_t s);
 void launch_ladder(const BatchArgs &a, int grid, cudaStream_t s);
 size_t climate_smem_bytes();
+// The climate stage of a batch whose units have one region each (spots mode), breadth first over
+// two item lists of `cap` entries (counts: 2 words, device); climate survivors become records.
+void launch_spot_climate(const BatchArgs &a, SpotItem *list0, SpotItem *list1, uint32_t *counts, uint32_t cap,
+                         int sm_count, cudaStream_t s);
+size_t spot_smem_bytes();
 size_t entrance_smem_bytes();
 
 }  // namespace wg
