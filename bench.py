@@ -465,7 +465,9 @@ def main() -> None:
                 "peak_source": f"nominal INT32/FP32 issue rate: {sm_count} SMs x 128 lanes x {max_mhz:.0f} MHz "
                                "(sm_max_mhz of MEASURED_PEAKS.json); the kernel is not HBM- or tensor-bound",
                 "ops_per_launch": ops_per_launch, "launch_ms": launch_ms,
-                "traffic": None,
+                # dram__bytes_read.sum + dram__bytes_write.sum of one climate launch of 2^20 seeds x 9x9
+                # (profiles/climate_kernel_2p20_seeds.md): every table and list stays on chip
+                "traffic": 82e3, "traffic_unit": "bytes per launch",
                 "hbm": {"achieved_gbs": bytes_per_launch / (launch_ms / 1e3) / 1e9, "peak_gbs": hbm_peak,
                         "frac": bytes_per_launch / (launch_ms / 1e3) / 1e9 / hbm_peak,
                         "peak_source": "hbm_gbs of MEASURED_PEAKS.json"},
