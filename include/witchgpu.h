@@ -75,7 +75,9 @@ void wg_engine_close(wg_engine *e);
 const char *wg_engine_error(const wg_engine *e);
 
 /* lysh's --version / --preset names -> option bits
- * (engine/tools/lysh/src/main.c:104-132).  0 on success, WG_ERR_ARG if unknown. */
+ * (engine/tools/lysh/src/main.c:104-132).  0 on success, WG_ERR_ARG if unknown.  Each sets only
+ * its own fields (version: mc_1_18_2, pre_26_2, biome_tree; preset: single_biome, large_biomes),
+ * so start from a zeroed wg_opts. */
 int wg_parse_version(const char *name, wg_opts *opts);
 int wg_parse_preset(const char *name, wg_opts *opts);
 

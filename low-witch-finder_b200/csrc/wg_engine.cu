@@ -94,7 +94,7 @@ int run_batch(wg_engine *eng, const BatchArgs &proto, uint64_t unit0, uint32_t n
     WG_CUDA(cudaEventRecord(eng->kev[1], eng->stream), "event");
     launch_entrance(a, eng->sm_count * 2, eng->stream);
     WG_CUDA(cudaEventRecord(eng->kev[2], eng->stream), "event");
-    launch_ladder(a, eng->sm_count * 8, eng->stream);
+    launch_ladder(a, 0, eng->stream);
     WG_CUDA(cudaEventRecord(eng->kev[3], eng->stream), "event");
     WG_CUDA(cudaGetLastError(), "kernel launch");
     WG_CUDA(cudaMemcpyAsync(eng->h_counters, eng->counters, sizeof(uint32_t) * CNT_WORDS, cudaMemcpyDeviceToHost,

@@ -1378,6 +1378,21 @@ __global__ void __launch_bounds__(kThreadsC) ladder_kernel(BatchArgs a) {
     }
 }
 
-void launch_ladder(const BatchArgs &a, int grid, cudaStream_t s) { ladder_kernel<<<grid, kThreadsC, 0, s>>>(a); }
+// grid <= 0: as many blocks as are resident at once (the kernel loops over candidates, so blocks
+// beyond the resident count would only form a second, mostly idle wave)
+void launch_ladder(const BatchArgs &a, int grid, cudaStream_t s) {
+    if (grid <= 0) {
+        static int per_sm = 0, sms = 0;
+        if (!per_sm) {
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ladder_kernel, kThreadsC, 0);
+            if (per_sm < 1) per_sm = 1;
+        }
+        grid = sms * per_sm;
+    }
+    ladder_kernel<<<grid, kThreadsC, 0, s>>>(a);
+}
 
 }  // namespace wg

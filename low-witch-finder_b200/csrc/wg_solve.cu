@@ -554,8 +554,15 @@ int run_solve_batch(wg_engine *eng, SolveState *st, uint64_t X, const std::vecto
     solve_lists_kernel<<<dim3(max_keys, (unsigned)slots.size()), 256, 0, s>>>(st->slots, st->keys, st->hq, st->hq_off, X,
                                                                              st->lists, st->counts, st->cnt);
     if (n_tasks) {
+        // as many blocks as are resident at once: the kernel loops over tasks, so more would only
+        // form a second, mostly idle wave
+        static int per_sm = 0;
+        if (!per_sm) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solve_chain_kernel, kChainThreads, 0);
+            if (per_sm < 1) per_sm = 1;
+        }
         const uint64_t blocks = std::min<uint64_t>((n_tasks + (kChainThreads / 32) - 1) / (kChainThreads / 32),
-                                                   (uint64_t)eng->sm_count * 8);
+                                                   (uint64_t)eng->sm_count * per_sm);
         solve_chain_kernel<<<(unsigned)blocks, kChainThreads, 0, s>>>(
             st->slots, (uint32_t)slots.size(), n_tasks, st->regions, st->offsets, st->keymap, st->lists, st->counts,
             st->nib, X, st->hits, kHitCap, st->cnt);
