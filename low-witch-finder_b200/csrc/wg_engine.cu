@@ -80,13 +80,13 @@ int run_batch(wg_engine *eng, const BatchArgs &proto, uint64_t unit0, uint32_t n
             "memset hist");
     WG_CUDA(cudaEventRecord(eng->kev[0], eng->stream), "event");
     // one region per unit: the climate tables are built lazily, breadth first
-    if (!a.jobs && a.win == 1 && !a.codes && !a.single_biome) {
+    if (spot_path(a.jobs != nullptr, a.win, a.codes != nullptr, a.single_biome != 0)) {
         if (!eng->spot_counts) {
-            WG_CUDA(cudaMalloc(&eng->spot_items[0], sizeof(SpotItem) * kMaxUnits), "alloc");
-            WG_CUDA(cudaMalloc(&eng->spot_items[1], sizeof(SpotItem) * kMaxUnits), "alloc");
+            WG_CUDA(cudaMalloc(&eng->spot_items[0], sizeof(SpotItem) * kSpotUnits), "alloc");
+            WG_CUDA(cudaMalloc(&eng->spot_items[1], sizeof(SpotItem) * kSpotUnits), "alloc");
             WG_CUDA(cudaMalloc(&eng->spot_counts, sizeof(uint32_t) * 2), "alloc");
         }
-        launch_spot_climate(a, eng->spot_items[0], eng->spot_items[1], eng->spot_counts, kMaxUnits, eng->sm_count,
+        launch_spot_climate(a, eng->spot_items[0], eng->spot_items[1], eng->spot_counts, kSpotUnits, eng->sm_count,
                             eng->stream);
     } else {
         launch_climate(a, eng->stream);
@@ -192,6 +192,7 @@ int run_request(wg_engine *eng, const Request &rq, Sink &sink, wg_scan_stats &st
     uint64_t per_batch = std::min<uint64_t>(kMaxUnits, std::max<uint64_t>(32, kWorkPerBatch / win));
     if (rq.opts.single_biome)  // every region survives the climate stage
         per_batch = std::min<uint64_t>(per_batch, std::max<uint64_t>(32, kCapSurv / 2 / win));
+    if (spot_path(false, win, rq.d_codes != nullptr, rq.opts.single_biome != 0)) per_batch = kSpotUnits;
     st.scanned = (int64_t)(rq.n_seeds * n_regions);
     for (uint64_t u0 = 0; u0 < units; u0 += per_batch) {
         uint32_t n = (uint32_t)std::min<uint64_t>(per_batch, units - u0);

@@ -76,6 +76,14 @@ constexpr uint32_t kCapRec = kMaxUnits + (1u << 16);
 constexpr uint32_t kCapSurv = 1u << 23;
 constexpr uint32_t kCapDeep = 1u << 20;
 constexpr uint32_t kCapOut = 1u << 20;
+// Units per batch of the breadth-first one-region climate stage (its item lists are this long;
+// its climate survivors, ~1.7 %, stay far below the record capacity).
+constexpr uint32_t kSpotUnits = 1u << 22;
+
+// Whether a batch takes the breadth-first one-region climate stage.
+inline bool spot_path(bool jobs, uint64_t win, bool codes, bool single_biome) {
+    return !jobs && win == 1 && !codes && !single_biome;
+}
 
 // Regions per unit window: a whole seed when its rect is small, else 2048-region windows.
 uint32_t window_for(uint64_t n_regions);
