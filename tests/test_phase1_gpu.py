@@ -187,13 +187,16 @@ def test_repeat_is_deterministic(engine):
     assert np.array_equal(a.candidates, b.candidates) and a.stats["reject_hist"] == b.stats["reject_hist"]
 
 
-@pytest.mark.parametrize("rect,mh,version", [((3, 4, -2, -1), -50, "1.19.x~26.1"), ((-40000, -39999, 17, 18), 100, "26.2"),
-                                           ((0, 1, 0, 1), 0, "1.18.2")])
-def test_one_region_requests_vs_oracle(engine, port, bind_mod, rect, mh, version):
+@pytest.mark.parametrize("rect,mh,version,preset,salt", [((3, 4, -2, -1), -50, "1.19.x~26.1", "NORMAL", 0),
+                                                         ((-40000, -39999, 17, 18), 100, "26.2", "NORMAL", 0),
+                                                         ((0, 1, 0, 1), 0, "1.18.2", "NORMAL", 0),
+                                                         ((5, 6, 5, 6), 0, "1.19.x~26.1", "LARGE_BIOMES", 0),
+                                                         ((-7, -6, 2, 3), 100, "1.19.x~26.1", "NORMAL", 10387312)])
+def test_one_region_requests_vs_oracle(engine, port, bind_mod, rect, mh, version, preset, salt):
     """One-region units take the breadth-first climate stage (tables built per erosion step):
     survivors and the whole reject histogram must equal the oracle's."""
-    r = bind_mod.rules(version)
-    res = engine.seed_check(gen=(17, 300000), rect=rect, max_height=mh, version=version)
-    want, hist = port.scan_seeds(r, mh, rect, gen=(17, 300000))
+    r = bind_mod.rules(version, preset)
+    res = engine.seed_check(gen=(17, 300000), rect=rect, max_height=mh, version=version, preset=preset, salt=salt)
+    want, hist = port.scan_seeds(r, mh, rect, gen=(17, 300000), salt=salt)
     assert np.array_equal(res.candidates, want)
     assert res.stats["reject_hist"] == hist.tolist()
