@@ -12,9 +12,18 @@
 //   * --version / --preset take lysh's names (default 1.19.x~26.1, the hunt driver's);
 //     --v26-2 selects the 26.2 ridge rule as before.
 //   * The 6th CSV column (gpuEst) is "nan": the reference's prefilter estimate does not exist.
-//   * --quad-bases / --require-all-regions / --max-hut-dist / --gate-center-* are refused
-//     with a clear error (not part of the Seed Check path).
+//   * --quad-bases sweeps (base, high 16 bits) as the reference does (:64-86, :700-724):
+//     index i of the request is the seed bases[g >> 16] | (g & 0xffff) << 48 with
+//     g = offset * 65536 + i; the seeds are expanded on the host in slices.  Combining it
+//     with --seed / --seed-list / --seed-gen is an error here (the reference ignores them).
+//   * --max-hut-dist D (with --gate-center-x / -z) keeps the candidates whose reported
+//     position (16 chunkX, 16 chunkZ) lies within D blocks of the centre (:241-292, :340-349);
+//     D < 0 (the default) turns the gate off.
+//   * --require-all-regions keeps a seed's candidates only when every region of the rect
+//     passes the three climate gates (:145-181) -- here lysh's erosion / temperature / ridge
+//     verdicts, so the SINGLE_BIOME and 1.18.2 rules follow lysh.
 #include <cctype>
+#include <algorithm>
 #include <chrono>
 #include <cinttypes>
 #include <cstdio>
@@ -39,7 +48,45 @@ struct Params {
     int max_height = -40;
     wg_opts opts{};
     std::string out_path;
+    std::string quad_path;              // --quad-bases
+    std::vector<uint64_t> quad_bases;
+    long long quad_offset = 0, quad_limit = 0;
+    long long max_hut_dist = -1;        // --max-hut-dist; < 0 = no position gate
+    int gate_x = 0, gate_z = 0;
+    bool require_all = false;
 };
+
+// Seeds of a --quad-bases request: request index i -> bases[g >> 16] | (g & 0xffff) << 48,
+// g = offset * 65536 + i (phase1_scan.cu:79-86).
+int64_t quad_seed(const Params &p, uint64_t i) {
+    const uint64_t g = (uint64_t)p.quad_offset * 65536ull + i;
+    return (int64_t)(p.quad_bases[g >> 16] | ((g & 0xFFFFull) << 48));
+}
+
+bool load_quad_bases(Params &p) {
+    std::ifstream f(p.quad_path);
+    if (!f) {
+        std::fprintf(stderr, "cannot open --quad-bases %s\n", p.quad_path.c_str());
+        return false;
+    }
+    unsigned long long v;
+    while (f >> v) p.quad_bases.push_back(v);
+    if (p.quad_bases.empty()) {
+        std::fprintf(stderr, "--quad-bases file had no seeds\n");
+        return false;
+    }
+    if (p.quad_offset < 0 || (size_t)p.quad_offset >= p.quad_bases.size()) {
+        std::fprintf(stderr, "--quad-base-offset out of range\n");
+        return false;
+    }
+    const long long avail = (long long)p.quad_bases.size() - p.quad_offset;
+    if (p.quad_limit <= 0 || p.quad_limit > avail) p.quad_limit = avail;
+    if (p.quad_limit > 32767) {   // the reference's per-request cap (2^31 seeds)
+        std::fprintf(stderr, "--quad-base-limit capped at 32767\n");
+        p.quad_limit = 32767;
+    }
+    return true;
+}
 
 bool read_seed_list(const char *path, std::vector<int64_t> &out) {
     FILE *f = std::fopen(path, "rb");
@@ -114,17 +161,26 @@ bool parse(const std::vector<std::string> &t, Params &p) {
         else if (a == "--block") (void)next(a.c_str());
         else if (a == "--self-test" || a == "--no-density-prefilter" || a == "--climate-gate" ||
                  a == "--no-climate-gate" || a == "--worker") {
-        } else if (a == "--quad-bases" || a == "--quad-base-offset" || a == "--quad-base-limit" ||
-                   a == "--require-all-regions" || a == "--max-hut-dist" || a == "--gate-center-x" ||
-                   a == "--gate-center-z") {
-            std::fprintf(stderr, "unsupported option %s (not part of the Seed Check path)\n", a.c_str());
-            ok = false;
-        } else {
+        } else if (a == "--quad-bases") p.quad_path = next(a.c_str());
+        else if (a == "--quad-base-offset") p.quad_offset = std::atoll(next(a.c_str()).c_str());
+        else if (a == "--quad-base-limit") p.quad_limit = std::atoll(next(a.c_str()).c_str());
+        else if (a == "--max-hut-dist") p.max_hut_dist = std::atoll(next(a.c_str()).c_str());
+        else if (a == "--gate-center-x") p.gate_x = std::atoi(next(a.c_str()).c_str());
+        else if (a == "--gate-center-z") p.gate_z = std::atoi(next(a.c_str()).c_str());
+        else if (a == "--require-all-regions") p.require_all = true;
+        else {
             std::fprintf(stderr, "unknown argument: %s\n", a.c_str());
             ok = false;
         }
     }
     if (!ok) return false;
+    if (!p.quad_path.empty()) {
+        if (p.gen || !p.seeds.empty()) {
+            std::fprintf(stderr, "--quad-bases cannot be combined with --seed/--seed-list/--seed-gen\n");
+            return false;
+        }
+        if (!load_quad_bases(p)) return false;
+    }
     if (p.gen && !p.seeds.empty()) {
         std::fprintf(stderr, "--seed-gen cannot be combined with --seed/--seed-list\n");
         return false;
@@ -133,7 +189,7 @@ bool parse(const std::vector<std::string> &t, Params &p) {
         std::fprintf(stderr, "--seed-gen count must be positive\n");
         return false;
     }
-    if (!p.gen && p.seeds.empty()) {
+    if (!p.gen && p.seeds.empty() && p.quad_bases.empty()) {
         std::fprintf(stderr, "no seeds given\n");
         return false;
     }
@@ -145,27 +201,104 @@ bool parse(const std::vector<std::string> &t, Params &p) {
     return true;
 }
 
-int run_scan(wg_engine *eng, const Params &p) {
-    uint64_t n = p.gen ? (uint64_t)p.gen_count : p.seeds.size();
-    std::vector<wg_candidate> out;
+// One wg_seed_check call; the output grows until it holds every candidate.  The candidates
+// are appended to `out` with their seed_index shifted by `index0`.
+bool check_seeds(wg_engine *eng, const Params &p, const int64_t *seeds, uint64_t gen_base, uint64_t n,
+                 uint64_t index0, std::vector<wg_candidate> &out, int64_t &scanned) {
+    std::vector<wg_candidate> buf;
     uint64_t cap = 1u << 16, found = 0;
     wg_scan_stats st{};
-    auto t0 = std::chrono::steady_clock::now();
     for (;;) {
-        out.resize(cap);
-        int rc = wg_seed_check(eng, p.gen ? nullptr : p.seeds.data(), p.gen_base, n, &p.opts, p.max_height, 0,
-                               p.min_rx, p.max_rx, p.min_rz, p.max_rz, out.data(), cap, &found, &st);
+        buf.resize(cap);
+        int rc = wg_seed_check(eng, seeds, gen_base, n, &p.opts, p.max_height, 0, p.min_rx, p.max_rx, p.min_rz,
+                               p.max_rz, buf.data(), cap, &found, &st);
         if (rc) {
             std::fprintf(stderr, "scan failed (%d): %s\n", rc, wg_engine_error(eng));
-            return 1;
+            return false;
         }
         if (found <= cap) break;
         cap = found;
     }
-    out.resize(found);
+    for (uint64_t k = 0; k < found; k++) {
+        buf[k].seed_index += index0;
+        out.push_back(buf[k]);
+    }
+    scanned += st.scanned;
+    return true;
+}
+
+// --max-hut-dist: the reported position (16 chunkX, 16 chunkZ) within D blocks of the centre
+// (phase1_scan.cu:340-349).
+bool within_gate(const Params &p, const wg_candidate &c) {
+    if (p.max_hut_dist < 0) return true;
+    const long long dx = 16LL * c.chunk_x - p.gate_x, dz = 16LL * c.chunk_z - p.gate_z;
+    return dx * dx + dz * dz <= p.max_hut_dist * p.max_hut_dist;
+}
+
+// --require-all-regions: keeps the candidates of the seeds whose every region of the rect
+// passes erosion, temperature and ridge (phase1_scan.cu:145-181).  Only seeds that have a
+// candidate can qualify, so only those are re-checked, region by region, through
+// wg_phase1_codes (codes 0..2 are the three climate rejections).
+bool all_regions_filter(wg_engine *eng, const Params &p, std::vector<wg_candidate> &cands) {
+    std::vector<int64_t> seeds;
+    for (const wg_candidate &c : cands) seeds.push_back(c.seed);
+    std::sort(seeds.begin(), seeds.end());
+    seeds.erase(std::unique(seeds.begin(), seeds.end()), seeds.end());
+    const uint64_t R = (uint64_t)(p.max_rx - p.min_rx) * (uint64_t)(p.max_rz - p.min_rz);
+    const uint64_t per = std::max<uint64_t>(1, (1ull << 26) / R);
+    std::vector<char> good(seeds.size(), 0);
+    std::vector<int8_t> codes, tiers;
+    for (uint64_t k0 = 0; k0 < seeds.size(); k0 += per) {
+        const uint64_t n = std::min<uint64_t>(per, seeds.size() - k0);
+        codes.assign(n * R, -1);
+        tiers.assign(n * R, -1);
+        int rc = wg_phase1_codes(eng, seeds.data() + k0, 0, n, &p.opts, p.max_height, 0, p.min_rx, p.max_rx,
+                                 p.min_rz, p.max_rz, codes.data(), tiers.data());
+        if (rc) {
+            std::fprintf(stderr, "all-regions check failed (%d): %s\n", rc, wg_engine_error(eng));
+            return false;
+        }
+        for (uint64_t i = 0; i < n; i++) {
+            const int8_t *c = codes.data() + i * R;
+            good[k0 + i] = std::all_of(c, c + R, [](int8_t v) { return v > 2; });
+        }
+    }
+    std::vector<wg_candidate> kept;
+    for (const wg_candidate &c : cands) {
+        const size_t at = (size_t)(std::lower_bound(seeds.begin(), seeds.end(), c.seed) - seeds.begin());
+        if (good[at]) kept.push_back(c);
+    }
+    cands.swap(kept);
+    return true;
+}
+
+int run_scan(wg_engine *eng, const Params &p) {
+    const bool quad = !p.quad_bases.empty();
+    const uint64_t n = quad ? (uint64_t)p.quad_limit * 65536ull : p.gen ? (uint64_t)p.gen_count : p.seeds.size();
+    std::vector<wg_candidate> out;
+    int64_t scanned = 0;
+    auto t0 = std::chrono::steady_clock::now();
+    if (quad) {
+        // 2^31 seeds at most per request: expanded and checked in slices of 2^22
+        constexpr uint64_t kSlice = 1ull << 22;
+        std::vector<int64_t> slice;
+        for (uint64_t i0 = 0; i0 < n; i0 += kSlice) {
+            const uint64_t m = std::min(kSlice, n - i0);
+            slice.resize(m);
+            for (uint64_t i = 0; i < m; i++) slice[i] = quad_seed(p, i0 + i);
+            if (!check_seeds(eng, p, slice.data(), 0, m, i0, out, scanned)) return 1;
+        }
+    } else if (!check_seeds(eng, p, p.gen ? nullptr : p.seeds.data(), p.gen_base, n, 0, out, scanned)) {
+        return 1;
+    }
+    if (p.max_hut_dist >= 0)
+        out.erase(std::remove_if(out.begin(), out.end(), [&](const wg_candidate &c) { return !within_gate(p, c); }),
+                  out.end());
+    if (p.require_all && !out.empty() && !all_regions_filter(eng, p, out)) return 1;
+    const uint64_t found = out.size();
     double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     std::printf("kernel: %.3f s  candidates=%" PRIu64 "  (%.2f M region-seed-checks/s across %" PRIu64 " seed(s))\n",
-                secs, found, secs > 0 ? (double)st.scanned / secs / 1e6 : 0.0, n);
+                secs, found, secs > 0 ? (double)scanned / secs / 1e6 : 0.0, n);
     if (!p.out_path.empty()) {
         FILE *f = std::fopen(p.out_path.c_str(), "w");
         if (!f) {
@@ -203,6 +336,10 @@ void usage() {
         "  --version <v>        lysh version name (default 1.19.x~26.1); --v26-2 = 26.2 ridge rule\n"
         "  --preset <p>         NORMAL | LARGE_BIOMES | SINGLE_BIOME\n"
         "  --out <file>         CSV seed,chunkX,chunkZ,blockX,blockZ,gpuEst\n"
+        "  --quad-bases <file>  sweep every base x its 65,536 high-16-bit variants\n"
+        "  --quad-base-offset <n> / --quad-base-limit <n>  slice of the base list (limit <= 32767)\n"
+        "  --max-hut-dist <d>   keep huts within d blocks of --gate-center-x/--gate-center-z\n"
+        "  --require-all-regions  a seed needs every region to pass the climate gates\n"
         "  --device <n>         CUDA device (default 0)\n"
         "  --worker             read one request per stdin line; ===WORKER_READY===, ===SCAN_DONE rc=N===\n");
 }

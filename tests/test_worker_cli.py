@@ -59,3 +59,22 @@ def test_hut_lookup_usage_errors(wg, tmp_path):
     r = subprocess.run([wg.HUT_LOOKUP_PATH, "--catalog", "cat.txt", "--solve5", "--regime", "22"],
                        capture_output=True, text=True, cwd=tmp_path)
     assert r.returncode == 1 and "no GPU" in r.stderr
+
+
+def test_quad_option_errors(wg, tmp_path):
+    """--quad-bases follows the reference's checks (phase1_scan.cu:705-724): an unreadable or
+    empty base list, an offset outside it, or a second seed source is refused with exit 2."""
+    (tmp_path / "empty.txt").write_text("\n")
+    (tmp_path / "two.txt").write_text("20015998343868 5\n")
+    rect = ["--min-region-x", "0", "--max-region-x", "1", "--min-region-z", "0", "--max-region-z", "1"]
+    cases = [(["--quad-bases", str(tmp_path / "missing.txt")], "cannot open"),
+             (["--quad-bases", str(tmp_path / "empty.txt")], "no seeds"),
+             (["--quad-bases", str(tmp_path / "two.txt"), "--quad-base-offset", "2"], "out of range"),
+             (["--quad-bases", str(tmp_path / "two.txt"), "--quad-base-offset", "-1"], "out of range"),
+             (["--quad-bases", str(tmp_path / "two.txt"), "--seed-gen", "1", "5"], "cannot be combined"),
+             (["--quad-bases", str(tmp_path / "two.txt"), "--seed", "3"], "cannot be combined"),
+             (["--max-hut-dist"], "missing value")]
+    for args, msg in cases:
+        r = run(wg, *rect, *args)
+        assert r.returncode == 2, args
+        assert msg in r.stderr, (args, r.stderr)

@@ -69,3 +69,56 @@ def test_single_shot_cli(wg, engine, tmp_path):
     g = np.load(os.path.join(os.path.dirname(__file__), "golden", "c2_4m_survivors.npz"))["survivors"]
     assert rows == [(int(c["seed"]), int(c["chunk_x"]), int(c["chunk_z"]), int(c["chunk_x"]) * 16,
                      int(c["chunk_z"]) * 16) for c in g]
+
+
+def _rows(cands):
+    return [(int(c["seed"]), int(c["chunk_x"]), int(c["chunk_z"]), int(c["chunk_x"]) * 16, int(c["chunk_z"]) * 16)
+            for c in cands]
+
+
+def _scan(wg, tmp_path, *args, out="q.csv"):
+    r = subprocess.run([wg.WORKER_PATH, *args, "--out", out], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    return read_csv(tmp_path / out)
+
+
+def test_quad_bases_and_position_gate(wg, port, bind_mod, tmp_path):
+    """--quad-bases: the request's seeds are one base's 65,536 high-16-bit variants
+    (phase1_scan.cu:79-86); the survivors equal the oracle's over the same expanded seeds, and
+    --max-hut-dist keeps those whose reported position is within the distance of the centre."""
+    base = 0x0000123456789ABC
+    (tmp_path / "bases.txt").write_text(f"999\n{base}\n5\n")
+    rect = ["--min-region-x", "-3", "--max-region-x", "3", "--min-region-z", "-3", "--max-region-z", "3",
+            "--max-height", "100"]
+    seeds = np.array([base | (h << 48) for h in range(65536)], dtype=np.uint64).view(np.int64)
+    want, _ = port.scan_seeds(bind_mod.rules("1.19.x~26.1"), 100, (-3, 3, -3, 3), seeds=seeds)
+    want_rows = _rows(want)
+    assert [(r[1], r[2]) for r in want_rows] == [(8, -22), (2, -84)]
+    got = _scan(wg, tmp_path, "--quad-bases", "bases.txt", "--quad-base-offset", "1", "--quad-base-limit", "1",
+                *rect)
+    assert got == want_rows
+    gated = _scan(wg, tmp_path, "--quad-bases", "bases.txt", "--quad-base-offset", "1", "--quad-base-limit", "1",
+                  *rect, "--max-hut-dist", "300", "--gate-center-x", "100", "--gate-center-z", "-300")
+    assert gated == [r for r in want_rows if (r[3] - 100) ** 2 + (r[4] + 300) ** 2 <= 300 ** 2]
+    assert len(gated) == 1
+
+
+def test_require_all_regions(wg, engine, port, bind_mod, tmp_path):
+    """--require-all-regions keeps a seed's candidates only when every region of the rect passes
+    the climate gates (phase1_scan.cu:145-181); the kept rows equal the oracle's per-region
+    verdicts (codes 0..2 = erosion / temperature / ridge rejections) over the plain scan's seeds."""
+    rect = ["--min-region-x", "0", "--max-region-x", "2", "--min-region-z", "0", "--max-region-z", "1",
+            "--max-height", "100"]
+    gen = ["--seed-gen", "77", str(1 << 24)]
+    plain = _scan(wg, tmp_path, *gen, *rect, out="p.csv")
+    assert plain == _rows(engine.seed_check(gen=(77, 1 << 24), rect=(0, 2, 0, 1), max_height=100).candidates)
+    assert len(plain) == 28
+    r = bind_mod.rules("1.19.x~26.1")
+    want = [row for row in plain if (port.phase1_rect(row[0], r, 100, (0, 2, 0, 1))[0] > 2).all()]
+    assert [(w[1], w[2]) for w in want] == [(12, 18), (8, 11), (19, 1), (50, 1)]
+    assert _scan(wg, tmp_path, *gen, *rect, "--require-all-regions", out="a.csv") == want
+    both = _scan(wg, tmp_path, *gen, *rect, "--require-all-regions", "--max-hut-dist", "150", "--gate-center-x",
+                 "200", "--gate-center-z", "100", out="b.csv")
+    assert both == [w for w in want if (w[3] - 200) ** 2 + (w[4] - 100) ** 2 <= 150 ** 2]
+    assert len(both) == 2
