@@ -209,7 +209,7 @@ __device__ __forceinline__ void perlin_shuffle(uint8_t *t, Xr r, double &ox, dou
     oy = xr_double(r) * 256.0;
     oz = xr_double(r) * 256.0;
     Xr32 q(r);
-#pragma unroll 8
+#pragma unroll 4
     for (int i = 0; i < 256; i++) {
         const int k = i + (int)q.bounded((uint32_t)(256 - i));
         uint8_t a = t[i * STRIDE], b = t[k * STRIDE];
