@@ -15,10 +15,10 @@
 //   * chain: per task (region, offset) one warp, each lane lifts the upper 28 state bits of one
 //     list entry.  When v2(cx) != v2(cz) each equation bit has one solution and the lift runs
 //     four bits per step (lift_chunks); when v2(cx) == v2(cz) state bit j does not reach
-//     equation bit j - 16 + m, so bit j branches and the lift is a bit-serial depth-first search
-//     (lift_branch).  Past equation bit 31 the remaining 2^m (2^(m+1)) top bits are enumerated
-//     and every completion is checked in full (48-bit carver state, hut offsets with the JDK
-//     rejection).
+//     equation bit j - 16 + m, so a nibble of the equation has 0 to 16 solutions and the lift is
+//     a depth-first search over nibbles (lift_eq).  Past equation bit 31 the remaining top bits
+//     are enumerated and every completion is checked in full (48-bit carver state, hut offsets
+//     with the JDK rejection).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -46,6 +46,7 @@ constexpr uint32_t kGroupsPerBatch = 16;
 constexpr uint32_t kHitCap = 1u << 20;
 constexpr int kChainThreads = 256;
 constexpr int kLiftTable = 8 * 16 * 16;    // nibble lift table (bytes)
+constexpr int kEqTable = 8 * 16 * 16 * 2;  // nibble solution masks of the v2(cx) == v2(cz) lift (bytes)
 
 // One group slot of a batch: its regions, offsets, key table and first task.
 struct SolveSlot {
@@ -132,15 +133,6 @@ __device__ __forceinline__ void emit_hit(const ChainTask &T, uint64_t S, SolveHi
     else atomicOr(&cnt[SCNT_OVERFLOW], 2ull);
 }
 
-// Checks the 2^(48 - j) completions of state prefix t (bits >= j free).
-__device__ __forceinline__ void leaf(const ChainTask &T, uint64_t t, int j, SolveHitDev *hits, uint32_t cap,
-                                     unsigned long long *cnt) {
-    for (uint64_t f = 0; f < (1ull << (48 - j)); f++) {
-        const uint64_t S = ((t | (f << j)) ^ kA) & kM48;
-        if (solve_check(S, T.cx, T.cz, T.X, T.creg, T.ox, T.oz)) emit_hit(T, S, hits, cap, cnt);
-    }
-}
-
 // v2(cx) != v2(cz), four state bits per step.  Divide the equation by 2^m and call "o" the term
 // whose multiplier is odd after that (cx h2 if v2(cx) = m, else cz h4) and "e" the other.  With
 // z = o (the odd term's value) as the unknown instead of the upper state bits u: 16 u =
@@ -161,6 +153,25 @@ __device__ __forceinline__ uint32_t inverse_u32(uint32_t a) {   // a odd
     return x;
 }
 
+// Full check of t = t20 | u << 20 (u: 28 bits).  The 48-bit carver state from 32-bit words: the
+// draws' low words h2, h4 move by (A^2 << 4) u and (A^4 << 4) u; only the low 16 bits of the high
+// words h1, h3 reach bit 47 of a, b, and those are bits 16..31 of A t + C, A^3 t + K3, which the
+// state's low word alone decides.
+__device__ __forceinline__ void check_u(const ChainTask &T, uint32_t t20, uint32_t h2, uint32_t h4, uint32_t u,
+                                        SolveHitDev *hits, uint32_t cap, unsigned long long *cnt) {
+    const uint32_t t32 = t20 | (u << 20);
+    const uint32_t h2u = h2 + (uint32_t)(kA2 << 4) * u, h4u = h4 + (uint32_t)(kA4 << 4) * u;
+    const uint32_t h1lo = (((uint32_t)kA * t32 + (uint32_t)kC) >> 16) & 0xFFFFu;
+    const uint32_t h3lo = (((uint32_t)kA3 * t32 + (uint32_t)kK3) >> 16) & 0xFFFFu;
+    const uint64_t a = ((uint64_t)h1lo << 32) + (uint64_t)(int64_t)(int32_t)h2u;
+    const uint64_t b = ((uint64_t)h3lo << 32) + (uint64_t)(int64_t)(int32_t)h4u;
+    const uint64_t S = ((((uint64_t)(u >> 12)) << 32) | t32) ^ (kA & kM48);
+    const uint64_t carver =
+        ((uint64_t)((int64_t)T.cx * (int64_t)a) ^ (uint64_t)((int64_t)T.cz * (int64_t)b) ^ S) & kM48;
+    if (carver != T.X) return;
+    if (solve_check(S, T.cx, T.cz, T.X, T.creg, T.ox, T.oz)) emit_hit(T, S, hits, cap, cnt);
+}
+
 __device__ void lift_chunks(const ChainTask &T, const ChunkTask &N, uint32_t t20, SolveHitDev *hits, uint32_t cap,
                              unsigned long long *cnt) {
     const uint32_t cx = (uint32_t)T.cx, cz = (uint32_t)T.cz, m = (uint32_t)T.m;
@@ -179,50 +190,59 @@ __device__ void lift_chunks(const ChainTask &T, const ChunkTask &N, uint32_t t20
         z |= (uint32_t)N.row[(((Aq >> k) & 15u) << 4) | ((Y >> k) & 15u)] << k;
     }
     const uint32_t u0 = (((z - o0) * N.inv) >> 4) & ((1u << (28 - m)) - 1u);
-    for (uint32_t f = 0; f < (1u << m); f++) {
-        // the 48-bit carver state of t = t20 | u << 20 from 32-bit words: the draws' low words
-        // h2, h4 move by (A^2 << 4) u and (A^4 << 4) u; only the low 16 bits of the high words
-        // h1, h3 reach bit 47 of a, b, and those are bits 16..31 of A t + C, A^3 t + K3, which the
-        // state's low word alone decides
-        const uint32_t u = u0 | (f << (28 - m)), t32 = t20 | (u << 20);
-        const uint32_t h2u = h2 + (uint32_t)(kA2 << 4) * u, h4u = h4 + (uint32_t)(kA4 << 4) * u;
-        const uint32_t h1lo = (((uint32_t)kA * t32 + (uint32_t)kC) >> 16) & 0xFFFFu;
-        const uint32_t h3lo = (((uint32_t)kA3 * t32 + (uint32_t)kK3) >> 16) & 0xFFFFu;
-        const uint64_t a = ((uint64_t)h1lo << 32) + (uint64_t)(int64_t)(int32_t)h2u;
-        const uint64_t b = ((uint64_t)h3lo << 32) + (uint64_t)(int64_t)(int32_t)h4u;
-        const uint64_t S = ((((uint64_t)(u >> 12)) << 32) | t32) ^ (kA & kM48);
-        const uint64_t carver =
-            ((uint64_t)((int64_t)T.cx * (int64_t)a) ^ (uint64_t)((int64_t)T.cz * (int64_t)b) ^ S) & kM48;
-        if (carver != T.X) continue;
-        if (solve_check(S, T.cx, T.cz, T.X, T.creg, T.ox, T.oz)) emit_hit(T, S, hits, cap, cnt);
-    }
+    for (uint32_t f = 0; f < (1u << m); f++) check_u(T, t20, h2, h4, u0 | (f << (28 - m)), hits, cap, cnt);
 }
 
-// v2(cx) == v2(cz): state bit j does not reach equation bit j - 16 + m (both terms flip it), so
-// that bit is a check on the prefix and bit j branches; pending alternatives live in a bit mask.
-__device__ void lift_branch(const ChainTask &T, uint32_t t20, SolveHitDev *hits, uint32_t cap,
-                            unsigned long long *cnt) {
-    const uint32_t cx = (uint32_t)T.cx, cz = (uint32_t)T.cz, xs = (uint32_t)(T.X ^ kA);
-    const int m = T.m, last = 47 - m;   // last level with an equation bit (bit 31)
-    uint64_t t = t20;
-    uint32_t pend = 0;                  // bit (j - 20): value 1 at level j still to try
-    int j = 20;
+// v2(cx) == v2(cz): the same substitution with o = cx h2 leaves rho = (cz A^4) / (cx A^2) odd, and
+// then z ^ ((Aq + rho z) mod 16) no longer determines z's nibble: its bit 0 equals Aq's (a check on
+// the lower nibbles) and its bits 1..3 constrain the nibble's bits 0..2, so a nibble has 0 to 16
+// solutions.  They come as a 16-bit mask from a 4 KB table [rho mod 16 / 2][Aq_k][Y_k], and the
+// seven nibbles above the list's are searched depth first with one mask per level.  Equation bits
+// past 31 - m do not exist: at the top nibble the mask is the union over them, so every remaining
+// u is enumerated there.
+__device__ __forceinline__ uint32_t eq_mask(const uint16_t *row, uint32_t Aq, uint32_t Y, int k, int valid) {
+    const uint32_t a = (Aq >> k) & 15u, y = (Y >> k) & 15u;
+    if (valid >= 4) return row[(a << 4) | y];
+    uint32_t mk = 0;   // union over the equation bits that do not exist
+    const uint32_t keep = (1u << valid) - 1u;
+    for (uint32_t yy = 0; yy < 16; yy++)
+        if (((yy ^ y) & keep) == 0) mk |= row[(a << 4) | yy];
+    return mk;
+}
+
+__device__ void lift_eq(const ChainTask &T, const ChunkTask &N, const uint16_t *row, uint32_t t20, SolveHitDev *hits,
+                        uint32_t cap, unsigned long long *cnt) {
+    const uint32_t cx = (uint32_t)T.cx, cz = (uint32_t)T.cz, m = (uint32_t)T.m;
+    const uint32_t h2 = (uint32_t)((((kA2 * t20) + kK2) & kM48) >> 16);
+    const uint32_t h4 = (uint32_t)((((kA4 * t20) + kK4) & kM48) >> 16);
+    const uint32_t o0 = (cx * h2) >> m, e0 = (cz * h4) >> m;
+    const uint32_t s0 = t20 ^ (uint32_t)kA, x32 = (uint32_t)T.X;
+    const uint32_t kq = e0 - N.rho * o0;
+    const int top = 32 - (int)m;   // equation bits 0 .. top - 1 exist
+    uint32_t z = o0 & 15u;         // nibble 0: the list's
+    uint32_t masks[7];
+    int L = 0;
+    {
+        const uint32_t V = (z - o0) * N.inv;
+        masks[0] = eq_mask(row, kq + N.rho * z, ((s0 ^ (V << 16)) ^ x32) >> m, 4, top - 4);
+    }
     for (;;) {
-        if (j <= last) {
-            if (!((eq_word(t, cx, cz, xs) >> (j - 16 + m)) & 1u)) {
-                pend |= 1u << (j - 20);   // try 0 now, 1 later
-                j++;
-                continue;
-            }
-        } else {
-            leaf(T, t, j, hits, cap, cnt);
+        if (!masks[L]) {
+            if (--L < 0) return;
+            continue;
         }
-        if (!pend) return;
-        const int d = 31 - __clz(pend);   // deepest pending level
-        pend &= ~(1u << d);
-        const int jj = d + 20;
-        t = (t & ((1ull << jj) - 1)) | (1ull << jj);
-        j = jj + 1;
+        const int k = 4 + 4 * L;
+        const uint32_t v = (uint32_t)__ffs((int)masks[L]) - 1u;
+        masks[L] &= masks[L] - 1u;
+        z = (z & ((1u << k) - 1u)) | (v << k);
+        if (L == 6) {
+            check_u(T, t20, h2, h4, ((z - o0) * N.inv) >> 4, hits, cap, cnt);
+            continue;
+        }
+        L++;
+        // Y's nibble k + 4 reads V bits up to k + m - 9 < k + 4 (m <= 4), all set already
+        const uint32_t V = (z - o0) * N.inv;
+        masks[L] = eq_mask(row, kq + N.rho * z, ((s0 ^ (V << 16)) ^ x32) >> m, k + 4, top - (k + 4));
     }
 }
 
@@ -264,9 +284,11 @@ __global__ void __launch_bounds__(kChainThreads) solve_chain_kernel(
     const int2 *__restrict__ offsets, const uint32_t *__restrict__ keymap, const uint32_t *__restrict__ lists,
     const uint32_t *__restrict__ counts, const uint8_t *__restrict__ nib, uint64_t X, SolveHitDev *hits,
     uint32_t hit_cap, unsigned long long *cnt) {
-    __shared__ __align__(16) uint8_t tab[kLiftTable];
-    for (int i = threadIdx.x; i < kLiftTable / 16; i += kChainThreads) ((uint4 *)tab)[i] = ((const uint4 *)nib)[i];
+    __shared__ __align__(16) uint8_t tab[kLiftTable + kEqTable];
+    for (int i = threadIdx.x; i < (kLiftTable + kEqTable) / 16; i += kChainThreads)
+        ((uint4 *)tab)[i] = ((const uint4 *)nib)[i];
     __syncthreads();
+    const uint16_t *eqtab = reinterpret_cast<const uint16_t *>(tab + kLiftTable);
     const int lane = threadIdx.x & 31;
     const uint64_t warps = (uint64_t)gridDim.x * (kChainThreads / 32);
     unsigned long long lifted = 0;
@@ -298,7 +320,14 @@ __global__ void __launch_bounds__(kChainThreads) solve_chain_kernel(
         const uint32_t *list = lists + (size_t)li * kListCap;
         if (lane == 0) lifted += n;
         if (T.eq) {
-            for (uint32_t i = lane; i < n; i += 32) lift_branch(T, list[i], hits, hit_cap, cnt);
+            ChunkTask N;
+            const uint32_t co = ((uint32_t)T.cx * (uint32_t)kA2) >> T.m, ce = ((uint32_t)T.cz * (uint32_t)kA4) >> T.m;
+            N.coef_o_x = 1u;
+            N.inv = inverse_u32(co);
+            N.rho = ce * N.inv;
+            N.row = nullptr;
+            const uint16_t *row = eqtab + ((N.rho & 15u) >> 1) * 256;
+            for (uint32_t i = lane; i < n; i += 32) lift_eq(T, N, row, list[i], hits, hit_cap, cnt);
         } else {
             ChunkTask N;
             const uint32_t cxa = (uint32_t)T.cx * (uint32_t)kA2, cza = (uint32_t)T.cz * (uint32_t)kA4;
@@ -320,7 +349,7 @@ __global__ void __launch_bounds__(kChainThreads) solve_chain_kernel(
 // ---------------------------------------------------------------------------------------------
 struct SolveState {
     uint32_t *hq = nullptr, *hq_off = nullptr;   // region states q0 (mod 2^20) grouped by hut key
-    uint8_t *nib = nullptr;                      // [rho mod 16 / 2][a][y] -> x with x ^ ((a + rho x) mod 16) = y
+    uint8_t *nib = nullptr;   // [rho mod 16 / 2][a][y] -> x with x ^ ((a + rho x) mod 16) = y (rho even), then the odd-rho masks
     SolveSlot *slots = nullptr;
     SolveKey *keys = nullptr;
     uint32_t *keymap = nullptr, *lists = nullptr, *counts = nullptr;
@@ -383,12 +412,18 @@ int solve_state(wg_engine *eng, SolveState **out) {
         SOLVE_CUDA(cudaMemcpy(s->hq, list.data(), sizeof(uint32_t) << 20, cudaMemcpyHostToDevice), "solver tables");
         SOLVE_CUDA(cudaMemcpy(s->hq_off, off.data(), sizeof(uint32_t) * 65, cudaMemcpyHostToDevice), "solver tables");
         // the nibble step's solutions, by search: x ^ ((a + 2r x) mod 16) is a bijection of x
-        std::vector<uint8_t> nib(kLiftTable, 0);
+        std::vector<uint8_t> nib(kLiftTable + kEqTable, 0);
         for (int r = 0; r < 8; r++)
             for (int a = 0; a < 16; a++)
                 for (int x = 0; x < 16; x++) nib[r * 256 + a * 16 + (x ^ ((a + 2 * r * x) & 15))] = (uint8_t)x;
-        SOLVE_CUDA(cudaMalloc(&s->nib, kLiftTable), "solver tables");
-        SOLVE_CUDA(cudaMemcpy(s->nib, nib.data(), kLiftTable, cudaMemcpyHostToDevice), "solver tables");
+        // and the masks of x with x ^ ((a + rho x) mod 16) = y for odd rho = 2r + 1
+        std::vector<uint16_t> eqm(kEqTable / 2, 0);
+        for (int r = 0; r < 8; r++)
+            for (int a = 0; a < 16; a++)
+                for (int x = 0; x < 16; x++) eqm[r * 256 + a * 16 + (x ^ ((a + (2 * r + 1) * x) & 15))] |= (uint16_t)(1u << x);
+        std::memcpy(nib.data() + kLiftTable, eqm.data(), kEqTable);
+        SOLVE_CUDA(cudaMalloc(&s->nib, kLiftTable + kEqTable), "solver tables");
+        SOLVE_CUDA(cudaMemcpy(s->nib, nib.data(), kLiftTable + kEqTable, cudaMemcpyHostToDevice), "solver tables");
     }
     *out = eng->solve;
     return WG_OK;
