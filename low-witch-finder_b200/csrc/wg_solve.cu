@@ -87,6 +87,11 @@ __host__ __device__ __forceinline__ int v2_of(uint32_t v) {
 #endif
 }
 
+// v2(cx) == v2(cz) for cx = 32 rx + ox, cz = 32 rz + oz with 0 <= ox, oz < 24, not both 0.
+__host__ __device__ __forceinline__ bool offsets_eq(int ox, int oz) {
+    return ox != 0 && oz != 0 && v2_of((uint32_t)ox) == v2_of((uint32_t)oz);
+}
+
 // Equation bits of t (low 32): (cx h2) ^ (cz h4) ^ S ^ X.
 __device__ __forceinline__ uint32_t eq_word(uint64_t t, uint32_t cx, uint32_t cz, uint32_t xs) {
     const uint32_t h2 = (uint32_t)((((kA2 * t) + kK2) & kM48) >> 16);
@@ -210,25 +215,42 @@ __device__ __forceinline__ uint32_t eq_mask(const uint16_t *row, uint32_t Aq, ui
     return mk;
 }
 
-__device__ void lift_eq(const ChainTask &T, const ChunkTask &N, const uint16_t *row, uint32_t t20, SolveHitDev *hits,
-                        uint32_t cap, unsigned long long *cnt) {
-    const uint32_t cx = (uint32_t)T.cx, cz = (uint32_t)T.cz, m = (uint32_t)T.m;
-    const uint32_t h2 = (uint32_t)((((kA2 * t20) + kK2) & kM48) >> 16);
-    const uint32_t h4 = (uint32_t)((((kA4 * t20) + kK4) & kM48) >> 16);
-    const uint32_t o0 = (cx * h2) >> m, e0 = (cz * h4) >> m;
-    const uint32_t s0 = t20 ^ (uint32_t)kA, x32 = (uint32_t)T.X;
-    const uint32_t kq = e0 - N.rho * o0;
-    const int top = 32 - (int)m;   // equation bits 0 .. top - 1 exist
-    uint32_t z = o0 & 15u;         // nibble 0: the list's
+// The per-candidate constants of the search: the draws' low words at t20, the odd term o0, and
+// Kq = e0 - rho o0 (rho = (cz A^4) / (cx A^2), odd).
+struct EqCand {
+    uint32_t h2, h4, o0, kq, s0;
+};
+
+__device__ __forceinline__ EqCand eq_cand(const ChainTask &T, const ChunkTask &N, uint32_t t20) {
+    EqCand c;
+    c.h2 = (uint32_t)((((kA2 * t20) + kK2) & kM48) >> 16);
+    c.h4 = (uint32_t)((((kA4 * t20) + kK4) & kM48) >> 16);
+    c.o0 = ((uint32_t)T.cx * c.h2) >> T.m;
+    c.kq = (((uint32_t)T.cz * c.h4) >> T.m) - N.rho * c.o0;
+    c.s0 = t20 ^ (uint32_t)kA;
+    return c;
+}
+
+// Solutions of the nibble at level L (bits 4 + 4L .. 7 + 4L) given z's lower nibbles.  Y's nibble
+// reads V bits up to 4L + m - 9 < 4 + 4L (m <= 4), all set already.
+__device__ __forceinline__ uint32_t eq_level(const ChainTask &T, const ChunkTask &N, const uint16_t *row,
+                                             const EqCand &c, uint32_t z, int L) {
+    const int k = 4 + 4 * L;
+    const uint32_t V = (z - c.o0) * N.inv;
+    const uint32_t Y = ((c.s0 ^ (V << 16)) ^ (uint32_t)T.X) >> T.m;
+    return eq_mask(row, c.kq + N.rho * z, Y, k, 32 - T.m - k);
+}
+
+// Depth-first search below node (z, L0): z holds the nibbles under level L0.
+__device__ void lift_eq_from(const ChainTask &T, const ChunkTask &N, const uint16_t *row, uint32_t t20,
+                             const EqCand &c, uint32_t z, int L0, SolveHitDev *hits, uint32_t cap,
+                             unsigned long long *cnt) {
     uint32_t masks[7];
-    int L = 0;
-    {
-        const uint32_t V = (z - o0) * N.inv;
-        masks[0] = eq_mask(row, kq + N.rho * z, ((s0 ^ (V << 16)) ^ x32) >> m, 4, top - 4);
-    }
+    int L = L0;
+    masks[L] = eq_level(T, N, row, c, z, L);
     for (;;) {
         if (!masks[L]) {
-            if (--L < 0) return;
+            if (--L < L0) return;
             continue;
         }
         const int k = 4 + 4 * L;
@@ -236,13 +258,70 @@ __device__ void lift_eq(const ChainTask &T, const ChunkTask &N, const uint16_t *
         masks[L] &= masks[L] - 1u;
         z = (z & ((1u << k) - 1u)) | (v << k);
         if (L == 6) {
-            check_u(T, t20, h2, h4, ((z - o0) * N.inv) >> 4, hits, cap, cnt);
+            check_u(T, t20, c.h2, c.h4, ((z - c.o0) * N.inv) >> 4, hits, cap, cnt);
             continue;
         }
         L++;
-        // Y's nibble k + 4 reads V bits up to k + m - 9 < k + 4 (m <= 4), all set already
-        const uint32_t V = (z - o0) * N.inv;
-        masks[L] = eq_mask(row, kq + N.rho * z, ((s0 ^ (V << 16)) ^ x32) >> m, k + 4, top - (k + 4));
+        masks[L] = eq_level(T, N, row, c, z, L);
+    }
+}
+
+// One eq task, level by level across the warp: each lane's own search tree has a different size
+// (0 to 16 solutions per nibble), so instead of a search per lane the warp keeps the nodes of a
+// level in a shared queue and every lane expands queue entries; 32 list entries start a round.
+// A node whose children do not fit in the next level's queue is searched depth first by its lane.
+constexpr int kEqQueue = 256;
+constexpr uint32_t kEqNone = 0xFFFFFFFFu;   // queue slot reserved by a node that did not fit
+
+__device__ void eq_task(const ChainTask &T, const ChunkTask &N, const uint16_t *row, const uint32_t *list,
+                        uint32_t n, SolveHitDev *hits, uint32_t cap, unsigned long long *cnt) {
+    __shared__ uint2 queue[kChainThreads / 32][2][kEqQueue];   // (t20, z) per node
+    __shared__ uint32_t qcount[kChainThreads / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x / 32;
+    for (uint32_t base = 0; base < n; base += 32) {
+        uint2 *cur = queue[wid][0], *nxt = queue[wid][1];
+        const uint32_t c0 = min(32u, n - base);
+        if ((uint32_t)lane < c0) {
+            const uint32_t t20 = list[base + lane];
+            cur[lane] = make_uint2(t20, eq_cand(T, N, t20).o0 & 15u);
+        }
+        uint32_t count = c0;
+        for (int L = 0; L < 7 && count; L++) {
+            if (lane == 0) qcount[wid] = 0;
+            __syncwarp();
+            const int k = 4 + 4 * L;
+            for (uint32_t i = (uint32_t)lane; i < count; i += 32) {
+                const uint2 nd = cur[i];
+                if (nd.x == kEqNone) continue;
+                const EqCand c = eq_cand(T, N, nd.x);
+                uint32_t mk = eq_level(T, N, row, c, nd.y, L);
+                if (!mk) continue;
+                if (L == 6) {
+                    for (; mk; mk &= mk - 1u) {
+                        const uint32_t z = nd.y | (((uint32_t)__ffs((int)mk) - 1u) << k);
+                        check_u(T, nd.x, c.h2, c.h4, ((z - c.o0) * N.inv) >> 4, hits, cap, cnt);
+                    }
+                    continue;
+                }
+                const uint32_t pc = (uint32_t)__popc(mk);
+                uint32_t at = atomicAdd(&qcount[wid], pc);
+                if (at + pc <= (uint32_t)kEqQueue) {
+                    for (; mk; mk &= mk - 1u)
+                        nxt[at++] = make_uint2(nd.x, nd.y | (((uint32_t)__ffs((int)mk) - 1u) << k));
+                } else {
+                    for (uint32_t q = at; q < (uint32_t)kEqQueue && q < at + pc; q++) nxt[q] = make_uint2(kEqNone, 0u);
+                    for (; mk; mk &= mk - 1u)
+                        lift_eq_from(T, N, row, nd.x, c, nd.y | (((uint32_t)__ffs((int)mk) - 1u) << k), L + 1, hits,
+                                     cap, cnt);
+                }
+            }
+            __syncwarp();
+            count = min(qcount[wid], (uint32_t)kEqQueue);
+            uint2 *t = cur;
+            cur = nxt;
+            nxt = t;
+            __syncwarp();
+        }
     }
 }
 
@@ -279,16 +358,19 @@ __global__ void __launch_bounds__(256) solve_lists_kernel(const SolveSlot *__res
 }
 
 // One warp per task (slot, region, offset); lanes take the task's list entries.
-__global__ void __launch_bounds__(kChainThreads) solve_chain_kernel(
+template <bool EQ>
+__global__ void __launch_bounds__(kChainThreads, EQ ? 4 : 6) solve_chain_kernel(
     const SolveSlot *__restrict__ slots, uint32_t n_slots, uint64_t n_tasks, const int2 *__restrict__ regions,
     const int2 *__restrict__ offsets, const uint32_t *__restrict__ keymap, const uint32_t *__restrict__ lists,
     const uint32_t *__restrict__ counts, const uint8_t *__restrict__ nib, uint64_t X, SolveHitDev *hits,
     uint32_t hit_cap, unsigned long long *cnt) {
-    __shared__ __align__(16) uint8_t tab[kLiftTable + kEqTable];
-    for (int i = threadIdx.x; i < (kLiftTable + kEqTable) / 16; i += kChainThreads)
-        ((uint4 *)tab)[i] = ((const uint4 *)nib)[i];
+    // the class's table: the nibble lift's (2 KB) or the solution masks (4 KB, after it in `nib`)
+    constexpr int kTab = EQ ? kEqTable : kLiftTable;
+    __shared__ __align__(16) uint8_t tab[kTab];
+    const uint8_t *src = nib + (EQ ? kLiftTable : 0);
+    for (int i = threadIdx.x; i < kTab / 16; i += kChainThreads) ((uint4 *)tab)[i] = ((const uint4 *)src)[i];
     __syncthreads();
-    const uint16_t *eqtab = reinterpret_cast<const uint16_t *>(tab + kLiftTable);
+    const uint16_t *eqtab = reinterpret_cast<const uint16_t *>(tab);
     const int lane = threadIdx.x & 31;
     const uint64_t warps = (uint64_t)gridDim.x * (kChainThreads / 32);
     unsigned long long lifted = 0;
@@ -302,7 +384,10 @@ __global__ void __launch_bounds__(kChainThreads) solve_chain_kernel(
         const SolveSlot &sl = slots[lo];
         const uint64_t local = w - sl.task_begin;
         const uint32_t o = (uint32_t)(local / sl.reg_count), r = (uint32_t)(local % sl.reg_count);
-        const int2 R = regions[sl.reg_begin + r], O = offsets[sl.off_begin + o];
+        const int2 O = offsets[sl.off_begin + o];
+        // the class follows from the offsets (0 < offset < 24, so v2(cx) = v2(ox) unless ox = 0)
+        if (offsets_eq(O.x, O.y) != EQ) continue;
+        const int2 R = regions[sl.reg_begin + r];
         ChainTask T;
         T.ox = O.x;
         T.oz = O.y;
@@ -319,15 +404,14 @@ __global__ void __launch_bounds__(kChainThreads) solve_chain_kernel(
         const uint32_t n = counts[li];
         const uint32_t *list = lists + (size_t)li * kListCap;
         if (lane == 0) lifted += n;
-        if (T.eq) {
+        if constexpr (EQ) {
             ChunkTask N;
             const uint32_t co = ((uint32_t)T.cx * (uint32_t)kA2) >> T.m, ce = ((uint32_t)T.cz * (uint32_t)kA4) >> T.m;
             N.coef_o_x = 1u;
             N.inv = inverse_u32(co);
             N.rho = ce * N.inv;
             N.row = nullptr;
-            const uint16_t *row = eqtab + ((N.rho & 15u) >> 1) * 256;
-            for (uint32_t i = lane; i < n; i += 32) lift_eq(T, N, row, list[i], hits, hit_cap, cnt);
+            eq_task(T, N, eqtab + ((N.rho & 15u) >> 1) * 256, list, n, hits, hit_cap, cnt);
         } else {
             ChunkTask N;
             const uint32_t cxa = (uint32_t)T.cx * (uint32_t)kA2, cza = (uint32_t)T.cz * (uint32_t)kA4;
@@ -589,18 +673,25 @@ int run_solve_batch(wg_engine *eng, SolveState *st, uint64_t X, const std::vecto
     solve_lists_kernel<<<dim3(max_keys, (unsigned)slots.size()), 256, 0, s>>>(st->slots, st->keys, st->hq, st->hq_off, X,
                                                                              st->lists, st->counts, st->cnt);
     if (n_tasks) {
-        // as many blocks as are resident at once: the kernel loops over tasks, so more would only
+        // one kernel per offset class present (the equal-valuation class has its own search); as
+        // many blocks as are resident at once: the kernel loops over tasks, so more would only
         // form a second, mostly idle wave
-        static int per_sm = 0;
-        if (!per_sm) {
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solve_chain_kernel, kChainThreads, 0);
-            if (per_sm < 1) per_sm = 1;
+        bool has_eq = false, has_other = false;
+        for (const int2 &o : offs) (offsets_eq(o.x, o.y) ? has_eq : has_other) = true;
+        static int per_sm[2] = {0, 0};
+        for (int eq = 0; eq < 2; eq++) {
+            if (!(eq ? has_eq : has_other)) continue;
+            if (!per_sm[eq]) {
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &per_sm[eq], eq ? solve_chain_kernel<true> : solve_chain_kernel<false>, kChainThreads, 0);
+                if (per_sm[eq] < 1) per_sm[eq] = 1;
+            }
+            const uint64_t blocks = std::min<uint64_t>((n_tasks + (kChainThreads / 32) - 1) / (kChainThreads / 32),
+                                                       (uint64_t)eng->sm_count * per_sm[eq]);
+            (eq ? solve_chain_kernel<true> : solve_chain_kernel<false>)<<<(unsigned)blocks, kChainThreads, 0, s>>>(
+                st->slots, (uint32_t)slots.size(), n_tasks, st->regions, st->offsets, st->keymap, st->lists,
+                st->counts, st->nib, X, st->hits, kHitCap, st->cnt);
         }
-        const uint64_t blocks = std::min<uint64_t>((n_tasks + (kChainThreads / 32) - 1) / (kChainThreads / 32),
-                                                   (uint64_t)eng->sm_count * per_sm);
-        solve_chain_kernel<<<(unsigned)blocks, kChainThreads, 0, s>>>(
-            st->slots, (uint32_t)slots.size(), n_tasks, st->regions, st->offsets, st->keymap, st->lists, st->counts,
-            st->nib, X, st->hits, kHitCap, st->cnt);
     }
     SOLVE_CUDA(cudaGetLastError(), "solver launch");
     SOLVE_CUDA(cudaEventRecord(eng->ev1, s), "event");
