@@ -219,8 +219,9 @@ typedef struct {
 
 /* The region walk of the Deep Dive solver: for every structure seed s48[0..n) (or, when s48 is
  * NULL, s48_base + i) and every region of [rx0,rx1) x [rz0,rz1), the region's swamp-hut chunk
- * and whether a mineshaft starts there (setLargeFeatureSeed + nextDouble() < 0.004).  Writes up
- * to cap hits to out (host), sorted by (seed_index, rz, rx); *n_out = the number found.  Replaces the
+ * and whether a mineshaft starts there (setLargeFeatureSeed + nextDouble() < 0.004).  Writes the
+ * first cap hits of the (seed_index, rz, rx) order to out (host); *n_out = the number found (may
+ * exceed cap: call again with a bigger buffer for the rest).  Replaces the
  * room walk of hut_lookup_v4 (rcWalkStep / walkStepCarver / rcIsStartS0,
  * engine/gpu/room_core.h:40-175, engine/gpu/hut_lookup_v4_source.cu:47-75): the forward
  * direction; the layout-catalogue direction is wg_deep_solve. */

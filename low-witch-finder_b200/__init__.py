@@ -340,7 +340,7 @@ class Engine:
             if rc != WG_OK:
                 raise self._err(rc, "wg_deep_starts")
             if found.value <= cap:
-                return out[:found.value].copy()
+                return out[:found.value]   # a view: the hits are already in order, no second copy
             cap = int(found.value)
 
     def biome_map(self, seed: int, x0: int, z0: int, w: int, h: int, step: int = 16, ss: int = 1,

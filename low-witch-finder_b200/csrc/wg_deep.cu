@@ -1,8 +1,9 @@
 // Deep Dive region walk (wg_deep_starts): for structure seeds x a region rect, the swamp-hut chunk
-// of every region and whether a mineshaft starts in it.  Integer LCG work only: one thread walks
-// one (seed, rx) column of regions along rz, as the reference's room walker does
-// (engine/gpu/room_core.h:146-175): the region seed advances by 132897987541 per row and the
-// chunk products cx * a, cz * b are formed from the hut offsets.
+// of every region and whether a mineshaft starts in it (the forward direction of the reference's
+// room walker, engine/gpu/room_core.h:146-175).  Integer LCG work only: one thread walks a strip
+// of 64 regions along rx.  The hits come out in (seed, rz, rx) order without a sort: a counting
+// pass, a prefix over the block totals, and a writing pass that walks again and stores each hit
+// at its place.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,35 +28,110 @@ struct DeepHit {
 static_assert(sizeof(DeepHit) == sizeof(wg_deep_start), "deep start layout");
 
 constexpr int kDeepThreads = 256;
-constexpr int kDeepRowsPerThread = 64;   // rz rows one thread walks
+constexpr int kDeepCols = 64;                     // rx columns one thread walks
+constexpr uint64_t kDeepPassTasks = 1ull << 24;   // tasks per pass: 65,536 blocks
 
-__global__ void __launch_bounds__(kDeepThreads) deep_starts_kernel(const int64_t *__restrict__ s48s, uint64_t s48_base,
-                                                                   uint64_t n_seeds, int rx0, int rw, int rz0, int rh,
-                                                                   uint64_t n_tasks, DeepHit *out, uint32_t cap,
-                                                                   unsigned long long *count) {
-    const int strips = (rh + kDeepRowsPerThread - 1) / kDeepRowsPerThread;
-    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n_tasks;
-         t += (uint64_t)gridDim.x * blockDim.x) {
-        // task = (seed, strip, column): neighbouring threads take neighbouring columns of one strip
-        const int col = (int)(t % (uint64_t)rw);
-        const uint64_t rest = t / (uint64_t)rw;
-        const int strip = (int)(rest % (uint64_t)strips);
-        const uint64_t i = rest / (uint64_t)strips;
-        if (i >= n_seeds) continue;
-        const uint64_t s48 = (s48s ? (uint64_t)s48s[i] : s48_base + i) & kDeepMask48;
-        const DeepCtx c = deep_ctx(s48);
-        const int rx = rx0 + col;
-        const int za = rz0 + strip * kDeepRowsPerThread;
-        const int zb = min(rz0 + rh, za + kDeepRowsPerThread);
-        for (int rz = za; rz < zb; rz++) {
-            int cx, cz;
-            hut_chunk(s48, rx, rz, 14357620, cx, cz);
-            const uint64_t carver = deep_carver(c, cx, cz);
-            if (!deep_is_start(carver)) continue;
-            const unsigned long long k = atomicAdd(count, 1ull);
-            if (k < cap) out[k] = DeepHit{i, (int64_t)s48, rx, rz, cx, cz, (int64_t)carver};
-        }
+// Task t = (seed i, row rz, strip of kDeepCols columns), strips fastest, so that walking the
+// tasks in order and each strip along rx visits the regions in the output order (seed, rz, rx).
+struct WalkGeom {
+    const int64_t *s48s;
+    uint64_t s48_base, n_seeds;
+    int rx0, rw, rz0, rh, strips;
+};
+
+template <class F>
+__device__ __forceinline__ void walk_task(const WalkGeom &G, uint64_t t, F &&on_start) {
+    const int strip = (int)(t % (uint64_t)G.strips);
+    const uint64_t rest = t / (uint64_t)G.strips;
+    const int row = (int)(rest % (uint64_t)G.rh);
+    const uint64_t i = rest / (uint64_t)G.rh;
+    if (i >= G.n_seeds) return;
+    const uint64_t s48 = (G.s48s ? (uint64_t)G.s48s[i] : G.s48_base + i) & kDeepMask48;
+    const DeepCtx c = deep_ctx(s48);
+    const int rz = G.rz0 + row;
+    const int xa = G.rx0 + strip * kDeepCols, xb = min(G.rx0 + G.rw, xa + kDeepCols);
+    for (int rx = xa; rx < xb; rx++) {
+        int cx, cz;
+        hut_chunk(s48, rx, rz, 14357620, cx, cz);
+        const uint64_t carver = deep_carver(c, cx, cz);
+        if (deep_is_start(carver)) on_start(i, s48, rx, rz, cx, cz, carver);
     }
+}
+
+// Pass 1: each task's number of starts (at most kDeepCols, one byte) and each block's total.
+__global__ void __launch_bounds__(kDeepThreads) walk_count_kernel(WalkGeom G, uint64_t t0, uint64_t n_tasks,
+                                                                  uint8_t *__restrict__ counts,
+                                                                  uint32_t *__restrict__ block_sums) {
+    const uint64_t k = (uint64_t)blockIdx.x * kDeepThreads + threadIdx.x;
+    uint32_t n = 0;
+    if (k < n_tasks) {
+        walk_task(G, t0 + k, [&](uint64_t, uint64_t, int, int, int, int, uint64_t) { n++; });
+        counts[k] = (uint8_t)n;
+    }
+    const uint32_t w = __reduce_add_sync(0xFFFFFFFFu, n);
+    __shared__ uint32_t warp_sums[kDeepThreads / 32];
+    if ((threadIdx.x & 31) == 0) warp_sums[threadIdx.x / 32] = w;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t tot = 0;
+        for (int q = 0; q < kDeepThreads / 32; q++) tot += warp_sums[q];
+        block_sums[blockIdx.x] = tot;
+    }
+}
+
+// Pass 2 (one block): exclusive prefix of the block totals on top of the starts of earlier passes
+// (*total), which it then advances.
+__global__ void __launch_bounds__(1024) walk_scan_kernel(const uint32_t *__restrict__ block_sums, uint32_t n_blocks,
+                                                         uint64_t *__restrict__ block_base,
+                                                         unsigned long long *__restrict__ total) {
+    __shared__ unsigned long long part[1024];
+    const uint32_t per = (n_blocks + 1023) / 1024, b0 = threadIdx.x * per, b1 = min(n_blocks, b0 + per);
+    unsigned long long s = 0;
+    for (uint32_t b = b0; b < b1; b++) s += block_sums[b];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int d = 1; d < 1024; d <<= 1) {   // inclusive scan of the 1,024 partial sums
+        const unsigned long long v = threadIdx.x >= (unsigned)d ? part[threadIdx.x - d] : 0ull;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned long long base = *total + part[threadIdx.x] - s;
+    for (uint32_t b = b0; b < b1; b++) {
+        block_base[b] = base;
+        base += block_sums[b];
+    }
+    __syncthreads();
+    if (threadIdx.x == 1023) *total += part[1023];
+}
+
+// Pass 3: each task writes its starts at its place in the output order (those past cap are
+// counted but not written).
+__global__ void __launch_bounds__(kDeepThreads) walk_write_kernel(WalkGeom G, uint64_t t0, uint64_t n_tasks,
+                                                                  const uint8_t *__restrict__ counts,
+                                                                  const uint64_t *__restrict__ block_base,
+                                                                  DeepHit *__restrict__ out, uint64_t cap) {
+    const uint64_t k = (uint64_t)blockIdx.x * kDeepThreads + threadIdx.x;
+    const uint32_t n = k < n_tasks ? counts[k] : 0u;
+    // exclusive prefix of n within the block
+    const int lane = threadIdx.x & 31, wid = threadIdx.x / 32;
+    uint32_t incl = n;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= d) incl += v;
+    }
+    __shared__ uint32_t warp_sums[kDeepThreads / 32];
+    if (lane == 31) warp_sums[wid] = incl;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int q = 0; q < wid; q++) before += warp_sums[q];
+    if (!n) return;
+    uint64_t at = block_base[blockIdx.x] + before + incl - n;
+    walk_task(G, t0 + k, [&](uint64_t i, uint64_t s48, int rx, int rz, int cx, int cz, uint64_t carver) {
+        if (at < cap) out[at] = DeepHit{i, (int64_t)s48, rx, rz, cx, cz, (int64_t)carver};
+        at++;
+    });
 }
 
 #define DEEP_CUDA(call, what)                                           \
@@ -66,58 +142,88 @@ __global__ void __launch_bounds__(kDeepThreads) deep_starts_kernel(const int64_t
 
 }  // namespace
 
+struct WalkState {
+    int64_t *s48 = nullptr;
+    DeepHit *out = nullptr;
+    uint8_t *counts = nullptr;
+    uint32_t *block_sums = nullptr;
+    uint64_t *block_base = nullptr;
+    unsigned long long *total = nullptr;
+    uint64_t cap_s48 = 0, cap_out = 0;
+};
+
+void walk_release(wg_engine *eng) {
+    WalkState *w = eng->walk;
+    if (!w) return;
+    cudaFree(w->s48);
+    cudaFree(w->out);
+    cudaFree(w->counts);
+    cudaFree(w->block_sums);
+    cudaFree(w->block_base);
+    cudaFree(w->total);
+    delete w;
+    eng->walk = nullptr;
+}
+
 extern "C" int wg_deep_starts(wg_engine *eng, const int64_t *s48, int64_t s48_base, uint64_t n, int rx0, int rx1,
                               int rz0, int rz1, wg_deep_start *out, uint64_t cap, uint64_t *n_out) {
     if (!eng || rx1 <= rx0 || rz1 <= rz0 || n == 0 || (cap && !out)) return WG_ERR_ARG;
     const int64_t rw = (int64_t)rx1 - rx0, rh = (int64_t)rz1 - rz0;
     if (rw > (1 << 24) || rh > (1 << 24)) return WG_ERR_ARG;
     DEEP_CUDA(cudaSetDevice(eng->device), "cudaSetDevice");
-    const uint64_t strips = (uint64_t)((rh + kDeepRowsPerThread - 1) / kDeepRowsPerThread);
-    const uint64_t n_tasks = n * strips * (uint64_t)rw;
-    // device buffers: the seed list, the hit list (room for cap hits, at least one) and the count
-    const uint32_t dcap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(cap, 1), 1u << 24);
-    int64_t *d_s48 = nullptr;
-    DeepHit *d_out = nullptr;
-    unsigned long long *d_count = nullptr;
-    int rc = WG_OK;
-    cudaError_t e = cudaSuccess;
-    if (s48) e = cudaMalloc(&d_s48, sizeof(int64_t) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&d_out, sizeof(DeepHit) * dcap);
-    if (e == cudaSuccess) e = cudaMalloc(&d_count, sizeof(unsigned long long));
-    if (e == cudaSuccess && s48)
-        e = cudaMemcpyAsync(d_s48, s48, sizeof(int64_t) * n, cudaMemcpyHostToDevice, eng->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), eng->stream);
+    if (!eng->walk) {
+        eng->walk = new (std::nothrow) WalkState();
+        if (!eng->walk) return eng->fail(WG_ERR_NOMEM, "deep starts state");
+        WalkState &w0 = *eng->walk;
+        DEEP_CUDA(cudaMalloc(&w0.counts, kDeepPassTasks), "deep starts buffers");
+        DEEP_CUDA(cudaMalloc(&w0.block_sums, sizeof(uint32_t) * (kDeepPassTasks / kDeepThreads)), "deep starts buffers");
+        DEEP_CUDA(cudaMalloc(&w0.block_base, sizeof(uint64_t) * (kDeepPassTasks / kDeepThreads)), "deep starts buffers");
+        DEEP_CUDA(cudaMalloc(&w0.total, sizeof(unsigned long long)), "deep starts buffers");
+    }
+    WalkState &w = *eng->walk;
+    // the device hit list holds the first cap starts of the output order (at least one slot)
+    const uint64_t dcap = std::min<uint64_t>(std::max<uint64_t>(cap, 1), 1u << 24);
+    if (dcap > w.cap_out) {
+        cudaFree(w.out);
+        w.out = nullptr;
+        w.cap_out = 0;
+        DEEP_CUDA(cudaMalloc(&w.out, sizeof(DeepHit) * dcap), "deep starts hit list");
+        w.cap_out = dcap;
+    }
+    if (s48 && n > w.cap_s48) {
+        cudaFree(w.s48);
+        w.s48 = nullptr;
+        w.cap_s48 = 0;
+        DEEP_CUDA(cudaMalloc(&w.s48, sizeof(int64_t) * n), "deep starts seeds");
+        w.cap_s48 = n;
+    }
+    cudaStream_t st = eng->stream;
+    if (s48) DEEP_CUDA(cudaMemcpyAsync(w.s48, s48, sizeof(int64_t) * n, cudaMemcpyHostToDevice, st), "upload seeds");
+    DEEP_CUDA(cudaMemsetAsync(w.total, 0, sizeof(unsigned long long), st), "memset");
+    WalkGeom G;
+    G.s48s = s48 ? w.s48 : nullptr;
+    G.s48_base = (uint64_t)s48_base;
+    G.n_seeds = n;
+    G.rx0 = rx0;
+    G.rw = (int)rw;
+    G.rz0 = rz0;
+    G.rh = (int)rh;
+    G.strips = (int)((rw + kDeepCols - 1) / kDeepCols);
+    const uint64_t n_tasks = n * (uint64_t)rh * (uint64_t)G.strips;
+    for (uint64_t t0 = 0; t0 < n_tasks; t0 += kDeepPassTasks) {
+        const uint64_t m = std::min<uint64_t>(kDeepPassTasks, n_tasks - t0);
+        const uint32_t blocks = (uint32_t)((m + kDeepThreads - 1) / kDeepThreads);
+        walk_count_kernel<<<blocks, kDeepThreads, 0, st>>>(G, t0, m, w.counts, w.block_sums);
+        walk_scan_kernel<<<1, 1024, 0, st>>>(w.block_sums, blocks, w.block_base, w.total);
+        walk_write_kernel<<<blocks, kDeepThreads, 0, st>>>(G, t0, m, w.counts, w.block_base, w.out, dcap);
+        DEEP_CUDA(cudaGetLastError(), "deep starts launch");
+    }
     unsigned long long found = 0;
-    if (e == cudaSuccess) {
-        const uint64_t blocks = std::min<uint64_t>((n_tasks + kDeepThreads - 1) / kDeepThreads,
-                                                   (uint64_t)eng->sm_count * 64);
-        deep_starts_kernel<<<(unsigned)blocks, kDeepThreads, 0, eng->stream>>>(
-            d_s48, (uint64_t)s48_base, n, rx0, (int)rw, rz0, (int)rh, n_tasks, d_out, dcap, d_count);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(&found, d_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost, eng->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(eng->stream);
-    std::vector<DeepHit> hits;
-    if (e == cudaSuccess && found) {
-        hits.resize(std::min<uint64_t>(found, dcap));
-        e = cudaMemcpy(hits.data(), d_out, sizeof(DeepHit) * hits.size(), cudaMemcpyDeviceToHost);
-    }
-    if (e != cudaSuccess) rc = eng->fail(WG_ERR_CUDA, "deep starts", e);
-    cudaFree(d_s48);
-    cudaFree(d_out);
-    cudaFree(d_count);
-    if (rc) return rc;
+    DEEP_CUDA(cudaMemcpyAsync(&found, w.total, sizeof(found), cudaMemcpyDeviceToHost, st), "read count");
+    DEEP_CUDA(cudaStreamSynchronize(st), "deep starts");
     if (found > dcap && cap > dcap) return eng->fail(WG_ERR_CAPACITY, "deep starts: more than 2^24 hits in one call");
-    std::sort(hits.begin(), hits.end(), [](const DeepHit &x, const DeepHit &y) {
-        if (x.seed_index != y.seed_index) return x.seed_index < y.seed_index;
-        if (x.rz != y.rz) return x.rz < y.rz;
-        return x.rx < y.rx;
-    });
-    // Only the first cap of the sorted order are wanted; when more than cap were found, the
-    // device kept an arbitrary cap of them, so the caller is told the total and retries bigger.
-    const uint64_t nw = std::min<uint64_t>(cap, hits.size());
-    if (nw) std::memcpy(out, hits.data(), sizeof(DeepHit) * nw);
+    const uint64_t nw = std::min<uint64_t>(cap, found);
+    if (nw) DEEP_CUDA(cudaMemcpy(out, w.out, sizeof(DeepHit) * nw, cudaMemcpyDeviceToHost), "copy hits");
     if (n_out) *n_out = found;
     return WG_OK;
 }

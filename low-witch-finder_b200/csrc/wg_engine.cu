@@ -344,6 +344,7 @@ void wg_engine_close(wg_engine *eng) {
     cudaFree(eng->spot_counts);
     p2_release(eng);
     solve_release(eng);
+    walk_release(eng);
     cudaFreeHost(eng->h_counters);
     cudaFreeHost(eng->h_hist);
     if (eng->ev0) cudaEventDestroy(eng->ev0);

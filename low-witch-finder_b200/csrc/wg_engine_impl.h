@@ -49,6 +49,8 @@ struct wg_engine {
     double *p2_vals = nullptr;
     // Deep Dive solver (wg_solve.cu): its device tables and work buffers
     struct SolveState *solve = nullptr;
+    // Deep Dive region walk (wg_deep.cu): its grow-only work buffers
+    struct WalkState *walk = nullptr;
 
     int p2_world_cap = 0, p2_job_cap = 0, p2_hut_cap = 0, p2_result_cap = 0, p2_pt_cap = 0, p2_val_cap = 0;
 
@@ -65,6 +67,8 @@ struct wg_engine {
 void p2_release(wg_engine *eng);
 // Frees the Deep Dive solver state of an engine (called by wg_engine_close).
 void solve_release(wg_engine *eng);
+// Frees the region walk's buffers of an engine (called by wg_engine_close).
+void walk_release(wg_engine *eng);
 
 namespace wg {
 

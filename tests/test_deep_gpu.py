@@ -34,6 +34,21 @@ def test_deep_starts_generator_and_capacity(engine, port):
     assert np.array_equal(np.stack([got["s48"], got["rx"], got["rz"]], 1), want[:, :3])
 
 
+def test_deep_starts_first_cap_in_order(engine, wg):
+    """With room for fewer hits than there are, the call writes the first ones of the
+    (seed_index, rz, rx) order and reports the total (include/witchgpu.h)."""
+    import ctypes as C
+    full = engine.deep_starts(base=777, count=3, rect=(-100, 100, -100, 100))
+    assert len(full) > 300
+    for cap in (1, len(full) // 3, len(full) - 1):
+        out = np.zeros(cap, wg.DEEP_START_DTYPE)
+        found = C.c_uint64()
+        rc = wg.library().wg_deep_starts(engine._h, None, 777, 3, -100, 100, -100, 100, out.ctypes.data, cap,
+                                         C.byref(found))
+        assert rc == 0 and found.value == len(full)
+        assert np.array_equal(out, full[:cap]), cap
+
+
 def test_deep_spots_match_reference(engine):
     d = np.load(os.path.join(GOLDEN, "deep_spots.npz"))
     surv, bad = engine.deep_spots(d["s48"], d["chunk_x"], d["chunk_z"], max_height=int(d["max_height"]))
