@@ -49,6 +49,19 @@ def test_deep_starts_first_cap_in_order(engine, wg):
         assert np.array_equal(out, full[:cap]), cap
 
 
+def test_deep_starts_several_passes(engine):
+    """A walk of more than 2^24 (seed, row, strip) tasks runs in passes whose outputs continue one
+    another: it equals the same seeds walked in two calls."""
+    rect = (-2048, 2048, -2048, 2048)   # 4,096 rows x 64 strips per seed: 65 seeds = 2 passes
+    whole = engine.deep_starts(base=4242, count=65, rect=rect)
+    a = engine.deep_starts(base=4242, count=33, rect=rect)
+    b = engine.deep_starts(base=4242 + 33, count=32, rect=rect)
+    b = b.copy()
+    b["seed_index"] += 33
+    assert len(whole) == len(a) + len(b) > 1_000_000
+    assert np.array_equal(whole, np.concatenate([a, b]))
+
+
 def test_deep_spots_match_reference(engine):
     d = np.load(os.path.join(GOLDEN, "deep_spots.npz"))
     surv, bad = engine.deep_spots(d["s48"], d["chunk_x"], d["chunk_z"], max_height=int(d["max_height"]))
