@@ -1158,15 +1158,18 @@ __device__ void canyon_carve(CarveCtx &c, uint64_t &r0, int ocx, int ocz) {
     }
 }
 
-// applyCarvers for the job's chunk (carver.c:482-523): cells and mask in shared memory.
+// applyCarvers for the job's chunk (carver.c:482-523), one warp per chunk.  The tunnel walks are
+// one serial chain per chunk, so the cells and the mask stay in the job's global memory (L2
+// holds them) and only the canyon width factors take shared memory: the chunks of a call then run
+// all at once instead of two warps per SM.  The job's cells are not read through p2_block_at
+// while J.carved is 0, so they serve as the working copy.
 __global__ void __launch_bounds__(kCarveThreads) p2_carve_kernel(const P2Tables *__restrict__ Tp,
                                                                  const P2World *__restrict__ worlds, P2Chunk *jobs) {
-    extern __shared__ __align__(16) uint8_t smem[];
-    uint8_t *cells = smem;
-    uint32_t *mask = reinterpret_cast<uint32_t *>(smem + kCarveCells);
-    float *width = reinterpret_cast<float *>(smem + kCarveCells + kMaskWords * 4);
+    __shared__ float width[384];
     P2Chunk &J = jobs[blockIdx.x];
     const P2World &W = worlds[J.world];
+    uint8_t *cells = J.cells;
+    uint32_t *mask = J.carve_mask;
     for (int q = threadIdx.x; q < kCarveCells / 4; q += blockDim.x) reinterpret_cast<uint32_t *>(cells)[q] = 0u;
     for (int q = threadIdx.x; q < kMaskWords; q += blockDim.x) mask[q] = 0u;
     __syncwarp();
@@ -1195,8 +1198,7 @@ __global__ void __launch_bounds__(kCarveThreads) p2_carve_kernel(const P2Tables 
             }
         }
     __syncwarp();
-    for (int q = threadIdx.x; q < kCarveCells / 4; q += blockDim.x)
-        reinterpret_cast<uint32_t *>(J.cells)[q] = reinterpret_cast<const uint32_t *>(cells)[q];
+    __threadfence_block();
     if (threadIdx.x == 0) J.carved = 1;
 }
 
@@ -1535,15 +1537,7 @@ void p2_launch_aquifer(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, 
 }
 
 void p2_launch_carve(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s) {
-    static unsigned long long done = 0;
-    const size_t smem = kCarveCells + kMaskWords * 4 + 384 * 4;
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev >= 0 && dev < 64 && !((done >> dev) & 1ull)) {
-        cudaFuncSetAttribute(p2_carve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        done |= 1ull << dev;
-    }
-    p2_carve_kernel<<<n_jobs, kCarveThreads, smem, s>>>(T, worlds, jobs);
+    p2_carve_kernel<<<n_jobs, kCarveThreads, 0, s>>>(T, worlds, jobs);
 }
 
 void p2_launch_biome_map(const P2Tables *T, const P2World *worlds, int tree, int64_t x0, int64_t z0, int w, int h,

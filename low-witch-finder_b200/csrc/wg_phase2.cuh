@@ -143,6 +143,7 @@ struct P2Chunk {
     int32_t aq_level[kAqCells];
     uint8_t aq_type[kAqCells];
     alignas(16) uint8_t cells[kCarveCells];   // CV_* per block, index (lz << 4 | lx) | (y + 64) << 8; copied as words
+    uint32_t carve_mask[kCarveCells / 32];    // the carvers' per-block mask while they run
 };
 static_assert(offsetof(P2Chunk, cells) % 16 == 0, "carve cells are copied as 32-bit words");
 static_assert(offsetof(P2Perlin, perm) % 4 == 0, "tables are written as 32-bit words");
