@@ -267,6 +267,7 @@ int prepare(wg_engine *eng, const std::vector<uint64_t> &seeds, int large, const
     if (!jobs.empty()) {
         p2_launch_grid(eng->p2_tables, eng->p2_worlds, eng->p2_jobs, (int)jobs.size(), eng->stream);
         p2_launch_aquifer(eng->p2_tables, eng->p2_worlds, eng->p2_jobs, (int)jobs.size(), eng->stream);
+        p2_launch_states(eng->p2_tables, eng->p2_worlds, eng->p2_jobs, (int)jobs.size(), eng->stream);
         if (carve) p2_launch_carve(eng->p2_tables, eng->p2_worlds, eng->p2_jobs, (int)jobs.size(), eng->stream);
     }
     P2_CUDA(cudaGetLastError(), "phase-2 launch");

@@ -712,16 +712,32 @@ __device__ __forceinline__ int p2_block_at(const P2Tables &T, const P2World &W, 
 
 __device__ __forceinline__ int carve_index(int lx, int y, int lz) { return ((lz & 15) << 4) | (lx & 15) | ((y + 64) << 8); }
 
-// Surface height (NOT_AIR predicate, y + 1; phase2.c:318-334 and :438-456).
+// Surface height (NOT_AIR predicate, y + 1; phase2.c:318-334 and :438-456) of a column of the job's
+// chunk, from the job's per-block states (p2_states_kernel).
 __device__ int p2_height(const P2Tables &T, const P2World &W, const P2Chunk &J, int x, int z, bool carved) {
+    (void)T;
+    (void)W;
     for (int y = 319; y >= -64; y--) {
-        int st = BS_SOLID;
-        const uint8_t cv = carved ? J.cells[carve_index(x & 15, y, z & 15)] : (uint8_t)CV_UNCHANGED;
-        if (cv != CV_UNCHANGED) st = cv;   // CV_AIR / CV_WATER / CV_LAVA share the BS_* codes
-        else st = p2_block_at(T, W, J, x, y, z);
+        const int ci = carve_index(x & 15, y, z & 15);
+        const uint8_t cv = carved ? J.cells[ci] : (uint8_t)CV_UNCHANGED;
+        const int st = cv != CV_UNCHANGED ? (int)cv : (int)J.natural[ci];   // CV_AIR / _WATER / _LAVA = BS_*
         if (st != BS_AIR) return y + 1;
     }
     return -64;
+}
+
+// Every block of every job's chunk: its pre-carver state and its aquifer substance at density 0,
+// the two things the carvers and the height scans read per block.  One thread per block: these
+// are independent, where the carvers and the column scans are serial chains per chunk / column.
+__global__ void __launch_bounds__(256) p2_states_kernel(const P2Tables *__restrict__ Tp,
+                                                        const P2World *__restrict__ worlds, P2Chunk *jobs) {
+    P2Chunk &J = jobs[blockIdx.y];
+    const P2Tables &T = *Tp;
+    const P2World &W = worlds[J.world];
+    const int q = blockIdx.x * 256 + threadIdx.x;   // carve_index(lx, y, lz)
+    const int x = J.chunk_x * 16 + (q & 15), z = J.chunk_z * 16 + ((q >> 4) & 15), y = (q >> 8) - 64;
+    J.natural[q] = (uint8_t)p2_block_at(T, W, J, x, y, z);
+    J.sub0[q] = y > -56 ? (uint8_t)p2_substance(T, W, J, x, y, z, 0.0) : (uint8_t)BS_LAVA;
 }
 
 // ------------------------------------------------------------------------------------
@@ -969,13 +985,13 @@ __device__ void carve_ellipsoid(CarveCtx &c, int kind, double floor_level, doubl
         int st;
         const uint8_t cv = c.cells[ci];
         if (cv != CV_UNCHANGED) st = cv;
-        else st = p2_block_at(*c.T, *c.W, *c.J, bx, v, bz);
+        else st = c.J->natural[ci];   // p2_block_at(bx, v, bz), precomputed
         if (!(st == BS_SOLID || st == BS_WATER)) continue;
         int cs;
         if (v <= -56) {
             cs = BS_LAVA;
         } else {
-            cs = p2_substance(*c.T, *c.W, *c.J, bx, v, bz, 0.0);
+            cs = c.J->sub0[ci];       // p2_substance(bx, v, bz, 0.0), precomputed
             if (cs == BS_SOLID) continue;
         }
         c.cells[ci] = (uint8_t)cs;
@@ -1534,6 +1550,10 @@ void p2_launch_grid(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int
 
 void p2_launch_aquifer(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s) {
     p2_aquifer_kernel<<<n_jobs, kAqThreads, 0, s>>>(T, worlds, jobs);
+}
+
+void p2_launch_states(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s) {
+    p2_states_kernel<<<dim3(kCarveCells / 256, n_jobs), 256, 0, s>>>(T, worlds, jobs);
 }
 
 void p2_launch_carve(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s) {

@@ -144,6 +144,10 @@ struct P2Chunk {
     uint8_t aq_type[kAqCells];
     alignas(16) uint8_t cells[kCarveCells];   // CV_* per block, index (lz << 4 | lx) | (y + 64) << 8; copied as words
     uint32_t carve_mask[kCarveCells / 32];    // the carvers' per-block mask while they run
+    // per block of the chunk (index as cells): the pre-carver state (lysh_phase2_block_at) and the
+    // aquifer substance at density 0 (the carvers' fill below the lava level is not read)
+    alignas(16) uint8_t natural[kCarveCells];
+    alignas(16) uint8_t sub0[kCarveCells];
 };
 static_assert(offsetof(P2Chunk, cells) % 16 == 0, "carve cells are copied as 32-bit words");
 static_assert(offsetof(P2Perlin, perm) % 4 == 0, "tables are written as 32-bit words");
@@ -187,6 +191,7 @@ void p2_launch_legacy(const P2Tables *T, P2World *worlds, int n_worlds, cudaStre
 void p2_launch_build(const P2Tables *T, P2World *worlds, int n_worlds, cudaStream_t s);
 void p2_launch_grid(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s);
 void p2_launch_aquifer(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s);
+void p2_launch_states(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s);
 void p2_launch_carve(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s);
 void p2_launch_finish(const P2Tables *T, const P2World *worlds, const P2Chunk *jobs, const P2Hut *huts,
                       int n_huts, int tree, P2Result *out, cudaStream_t s);
