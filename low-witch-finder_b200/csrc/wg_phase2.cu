@@ -720,7 +720,7 @@ __device__ int p2_height(const P2Tables &T, const P2World &W, const P2Chunk &J, 
     for (int y = 319; y >= -64; y--) {
         const int ci = carve_index(x & 15, y, z & 15);
         const uint8_t cv = carved ? J.cells[ci] : (uint8_t)CV_UNCHANGED;
-        const int st = cv != CV_UNCHANGED ? (int)cv : (int)J.natural[ci];   // CV_AIR / _WATER / _LAVA = BS_*
+        const int st = cv != CV_UNCHANGED ? (int)cv : (int)(J.states[ci] & 15u);   // CV_AIR / _WATER / _LAVA = BS_*
         if (st != BS_AIR) return y + 1;
     }
     return -64;
@@ -736,8 +736,9 @@ __global__ void __launch_bounds__(256) p2_states_kernel(const P2Tables *__restri
     const P2World &W = worlds[J.world];
     const int q = blockIdx.x * 256 + threadIdx.x;   // carve_index(lx, y, lz)
     const int x = J.chunk_x * 16 + (q & 15), z = J.chunk_z * 16 + ((q >> 4) & 15), y = (q >> 8) - 64;
-    J.natural[q] = (uint8_t)p2_block_at(T, W, J, x, y, z);
-    J.sub0[q] = y > -56 ? (uint8_t)p2_substance(T, W, J, x, y, z, 0.0) : (uint8_t)BS_LAVA;
+    const int nat = p2_block_at(T, W, J, x, y, z);
+    const int sub = y > -56 ? p2_substance(T, W, J, x, y, z, 0.0) : BS_LAVA;
+    J.states[q] = (uint8_t)(nat | (sub << 4));
 }
 
 // ------------------------------------------------------------------------------------
@@ -918,6 +919,8 @@ struct CarveCtx {
     uint8_t *cells;
     uint32_t *mask;
     float *width;                 // canyon width factors (384)
+    double *fx, *fz, *fy;         // carve_ellipsoid's per-row / column / level offsets (shared)
+    uint16_t *cols;               // its columns inside the ellipse (shared, 256)
     int tmin_x, tmin_z;
     double tmid_x, tmid_z;
 };
@@ -960,15 +963,41 @@ __device__ void carve_ellipsoid(CarveCtx &c, int kind, double floor_level, doubl
     if (nxp <= 0 || nzp <= 0 || nyp <= 0) return;
     const int total = nxp * nzp * nyp;
     const int lane = threadIdx.x & 31;
-    for (int q = lane; q < total; q += 32) {
-        const int p = i0 + q / (nzp * nyp);
-        const int s = n0 + (q / nyp) % nzp;
-        const int v = m0 - q % nyp;
+    // the normalised offsets depend on one coordinate each: divide once per row / column / level
+    // (the same expressions, so the same doubles) instead of three times per block
+    for (int q = lane; q < nxp; q += 32) c.fx[q] = ((double)(min_bx + i0 + q) + 0.5 - x) / hr;
+    for (int q = lane; q < nzp; q += 32) c.fz[q] = ((double)(min_bz + n0 + q) + 0.5 - z) / hr;
+    for (int q = lane; q < nyp; q += 32) c.fy[q] = ((double)(m0 - q) - 0.5 - y) / vr;
+    __syncwarp();
+    // the box's columns inside the horizontal ellipse (nx^2 + nz^2 < 1), compacted: the blocks of
+    // the other columns are all skipped by that test
+    int n_in = 0;
+    for (int base = 0; base < nxp * nzp; base += 32) {
+        const int q = base + lane;
+        int pi = 0, si = 0;
+        bool in = false;
+        if (q < nxp * nzp) {
+            pi = q / nzp;
+            si = q - pi * nzp;
+            in = c.fx[pi] * c.fx[pi] + c.fz[si] * c.fz[si] < 1.0;
+        }
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, in);
+        if (in) c.cols[n_in + __popc(m & ((1u << lane) - 1u))] = (uint16_t)((pi << 4) | si);
+        n_in += __popc(m);
+    }
+    __syncwarp();
+    (void)total;
+    const float inv_nyp = 1.0f / (float)nyp;
+    for (int q = lane; q < n_in * nyp; q += 32) {
+        int k = (int)((float)q * inv_nyp);   // q / nyp, corrected below (q < 2^17: one step suffices)
+        if (k * nyp > q) k--;
+        else if ((k + 1) * nyp <= q) k++;
+        const int vi = q - k * nyp, pi = c.cols[k] >> 4, si = c.cols[k] & 15;
+        const int p = i0 + pi, s = n0 + si, v = m0 - vi;
         const int bx = min_bx + p, bz = min_bz + s;
-        const double nx = ((double)bx + 0.5 - x) / hr;
-        const double nz = ((double)bz + 0.5 - z) / hr;
-        if (nx * nx + nz * nz >= 1.0) continue;
-        const double ny = ((double)v - 0.5 - y) / vr;
+        const double nx = c.fx[pi];
+        const double nz = c.fz[si];
+        const double ny = c.fy[vi];
         bool skip;
         if (kind == 0) {
             skip = (ny <= floor_level) || (nx * nx + ny * ny + nz * nz) >= 1.0;
@@ -984,14 +1013,15 @@ __device__ void carve_ellipsoid(CarveCtx &c, int kind, double floor_level, doubl
         // carveBlock
         int st;
         const uint8_t cv = c.cells[ci];
+        const uint32_t pre = c.J->states[ci];   // p2_block_at and p2_substance(.., 0.0), precomputed
         if (cv != CV_UNCHANGED) st = cv;
-        else st = c.J->natural[ci];   // p2_block_at(bx, v, bz), precomputed
+        else st = (int)(pre & 15u);
         if (!(st == BS_SOLID || st == BS_WATER)) continue;
         int cs;
         if (v <= -56) {
             cs = BS_LAVA;
         } else {
-            cs = c.J->sub0[ci];       // p2_substance(bx, v, bz, 0.0), precomputed
+            cs = (int)(pre >> 4);
             if (cs == BS_SOLID) continue;
         }
         c.cells[ci] = (uint8_t)cs;
@@ -1182,6 +1212,8 @@ __device__ void canyon_carve(CarveCtx &c, uint64_t &r0, int ocx, int ocz) {
 __global__ void __launch_bounds__(kCarveThreads) p2_carve_kernel(const P2Tables *__restrict__ Tp,
                                                                  const P2World *__restrict__ worlds, P2Chunk *jobs) {
     __shared__ float width[384];
+    __shared__ double fxs[16], fzs[16], fys[384];
+    __shared__ uint16_t cols[256];
     P2Chunk &J = jobs[blockIdx.x];
     const P2World &W = worlds[J.world];
     uint8_t *cells = J.cells;
@@ -1196,6 +1228,10 @@ __global__ void __launch_bounds__(kCarveThreads) p2_carve_kernel(const P2Tables 
     c.cells = cells;
     c.mask = mask;
     c.width = width;
+    c.fx = fxs;
+    c.fz = fzs;
+    c.fy = fys;
+    c.cols = cols;
     c.tmin_x = J.chunk_x * 16;
     c.tmin_z = J.chunk_z * 16;
     c.tmid_x = (double)(c.tmin_x + 8);

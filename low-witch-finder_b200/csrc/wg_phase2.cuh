@@ -144,10 +144,9 @@ struct P2Chunk {
     uint8_t aq_type[kAqCells];
     alignas(16) uint8_t cells[kCarveCells];   // CV_* per block, index (lz << 4 | lx) | (y + 64) << 8; copied as words
     uint32_t carve_mask[kCarveCells / 32];    // the carvers' per-block mask while they run
-    // per block of the chunk (index as cells): the pre-carver state (lysh_phase2_block_at) and the
-    // aquifer substance at density 0 (the carvers' fill below the lava level is not read)
-    alignas(16) uint8_t natural[kCarveCells];
-    alignas(16) uint8_t sub0[kCarveCells];
+    // per block of the chunk (index as cells): the pre-carver state (lysh_phase2_block_at) in the
+    // low nibble, the aquifer substance at density 0 in the high one (BS_* codes)
+    alignas(16) uint8_t states[kCarveCells];
 };
 static_assert(offsetof(P2Chunk, cells) % 16 == 0, "carve cells are copied as 32-bit words");
 static_assert(offsetof(P2Perlin, perm) % 4 == 0, "tables are written as 32-bit words");
