@@ -1098,25 +1098,45 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
                 S.val[slot][h][e] = slot_sample(src, slot, S.slot_sub[slot], S.slot_lac[slot], px, py, pz);
             }
             __syncthreads();
-            // combine in the reference's order and decide
+            // the six DoublePerlin values per survivor and height, one per thread, each summed in
+            // the reference's order and stored over its own first slot's sample (a task reads and
+            // writes only its own noise's slots)
+            for (uint32_t t = tid; t < m * 12; t += kThreadsB) {
+                const uint32_t e = t / 12, rem = t % 12;
+                const int h = (int)(rem & 1), k = (int)(rem >> 1);
+                const int noise = k == 0 ? N_CAVE_ENTRANCE
+                                  : k == 1 ? N_SPAGHETTI_THICKNESS
+                                  : k == 2 ? N_SPAGHETTI_1
+                                  : k == 3 ? N_SPAGHETTI_2
+                                  : k == 4 ? N_ROUGHNESS_MODULATOR : N_ROUGHNESS;
+                const int base = k == 0 ? kBaseEntrance
+                                 : k == 1 ? kBaseThickness
+                                 : k == 2 ? kBaseSp1
+                                 : k == 3 ? kBaseSp2
+                                 : k == 4 ? kBaseRmod : kBaseRough;
+                const double v = combine(S, noise, base, h, (int)e);
+                S.val[base][h][e] = v;
+            }
+            __syncthreads();
+            // decide in the reference's order
             for (uint32_t e = tid; e < m; e += kThreadsB) {
                 double ent_v[2];
                 for (int h = 0; h < 2; h++) {
                     const int y = h ? 60 : 50;
                     const double te = S.tun[h][e];
-                    double ent = combine(S, N_CAVE_ENTRANCE, kBaseEntrance, h, (int)e);
+                    double ent = S.val[kBaseEntrance][h][e];
                     double t = (10.0 + (double)y) / 40.0;
                     double cl = t < 0.0 ? 0.3 : (t > 1.0 ? 0.0 : lerp(t, 0.3, 0.0));
                     double cc = ent + 0.37 + cl;
-                    double tv = combine(S, N_SPAGHETTI_THICKNESS, kBaseThickness, h, (int)e);
+                    double tv = S.val[kBaseThickness][h][e];
                     double hh = lerp((tv - -1.0) / (1.0 - -1.0), 0.065, 0.088);
-                    double l = combine(S, N_SPAGHETTI_1, kBaseSp1, h, (int)e);
+                    double l = S.val[kBaseSp1][h][e];
                     double mm = fabs(te * l) - hh;
-                    double n = combine(S, N_SPAGHETTI_2, kBaseSp2, h, (int)e);
+                    double n = S.val[kBaseSp2][h][e];
                     double o = fabs(te * n) - hh;
                     double pp = clampd(jmax(mm, o), -1.0, 1.0);
-                    double mod = combine(S, N_ROUGHNESS_MODULATOR, kBaseRmod, h, (int)e);
-                    double rgh = combine(S, N_ROUGHNESS, kBaseRough, h, (int)e);
+                    double mod = S.val[kBaseRmod][h][e];
+                    double rgh = S.val[kBaseRough][h][e];
                     double q = (-0.05 + (-0.05 * mod)) * (-0.4 + fabs(rgh));
                     ent_v[h] = jmin(cc, pp + q);
                 }
