@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -254,10 +255,11 @@ int prepare(wg_engine *eng, const std::vector<uint64_t> &seeds, int large, const
                               wh.size(), cudaMemcpyHostToDevice, eng->stream),
             "upload worlds");
     struct JobHead {
-        int world, chunk_x, chunk_z, skip_above, min_gx, min_gy, min_gz, carved;
+        int world, chunk_x, chunk_z, max_psl, min_gx, min_gy, min_gz, carved;
     };
     std::vector<JobHead> jh(jobs.size());
-    for (size_t i = 0; i < jobs.size(); i++) jh[i] = JobHead{jobs[i].world, jobs[i].cx, jobs[i].cz, 0, 0, 0, 0, 0};
+    for (size_t i = 0; i < jobs.size(); i++)
+        jh[i] = JobHead{jobs[i].world, jobs[i].cx, jobs[i].cz, INT_MIN, 0, 0, 0, 0};
     if (!jobs.empty())
         P2_CUDA(cudaMemcpy2DAsync(eng->p2_jobs, sizeof(P2Chunk), jh.data(), sizeof(JobHead), sizeof(JobHead),
                                   jh.size(), cudaMemcpyHostToDevice, eng->stream),

@@ -648,7 +648,9 @@ __device__ int p2_substance(const P2Tables &T, const P2World &W, const P2Chunk &
     if (density > 0.0) return BS_SOLID;
     int glevel, gtype;
     global_fluid(y, glevel, gtype);
-    if (y > J.skip_above) return level_block_at(glevel, gtype, y);
+    // skipSamplingAboveY from the highest column top around the chunk
+    const int skip_above = (floor_div((J.max_psl + 8) + 12, 12) + 1) * 12 + 11 - 1;
+    if (y > skip_above) return level_block_at(glevel, gtype, y);
     if (level_block_at(glevel, gtype, y) == BS_LAVA) return BS_LAVA;
     const int gx = floor_div(x - 5, 16), gy = floor_div(y + 1, 12), gz = floor_div(z - 5, 16);
     int d[4] = {0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF, 0x7FFFFFFF};
@@ -827,68 +829,66 @@ constexpr int kGridThreads = 256;
 // densities and 3 x 25 x 49 noodle children (phase2.c:73-116).
 __global__ void __launch_bounds__(kGridThreads) p2_grid_kernel(const P2Tables *__restrict__ Tp,
                                                                const P2World *__restrict__ worlds, P2Chunk *jobs) {
-    __shared__ TerrainPoint tp[kGridCols];
-    __shared__ double jag[kGridCols];
+    // CTA (job, gx): the five corner columns c = gx * 5 + k of one cell row, so a job's grid is five
+    // short chains on five SMs instead of one long one
+    __shared__ TerrainPoint tp[5];
+    __shared__ double jag[5];
     const P2Tables &T = *Tp;
     P2Chunk &J = jobs[blockIdx.x];
     const P2World &W = worlds[J.world];
+    const int gx = blockIdx.y;
     const int cx0 = J.chunk_x * 4, cz0 = J.chunk_z * 4;   // first cell of the chunk
-    for (int c = threadIdx.x; c < kGridCols; c += blockDim.x) {
-        const int cell_x = cx0 + c / 5, cell_z = cz0 + c % 5;
+    for (int k = threadIdx.x; k < 5; k += blockDim.x) {
+        const int cell_x = cx0 + gx, cell_z = cz0 + k;
         TerrainInfo ti;
         p2_terrain(T, W, cell_x, cell_z, ti);
-        tp[c] = p2_point_261(T, ti);
-        jag[c] = p2_jagged(T, W, (double)tp[c].peaks, cell_x * 4, cell_z * 4);
+        tp[k] = p2_point_261(T, ti);
+        jag[k] = p2_jagged(T, W, (double)tp[k].peaks, cell_x * 4, cell_z * 4);
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < kGridCols * kGridYs; q += blockDim.x) {
-        const int c = q / kGridYs, i = q % kGridYs;
-        const int bx = (cx0 + c / 5) * 4, bz = (cz0 + c % 5) * 4, y = -64 + i * 8;
+    for (int q = threadIdx.x; q < 5 * kGridYs; q += blockDim.x) {
+        const int k = q / kGridYs, i = q % kGridYs, c = gx * 5 + k;
+        const int bx = (cx0 + gx) * 4, bz = (cz0 + k) * 4, y = -64 + i * 8;
         const double base = p2_blended(T, W, bx, y, bz);
-        J.main[c][i] = p2_noise_column(T, W, bx, y, bz, tp[c], jag[c], base);
+        J.main[c][i] = p2_noise_column(T, W, bx, y, bz, tp[k], jag[k], base);
     }
-    for (int q = threadIdx.x; q < 3 * kGridCols * kGridYs; q += blockDim.x) {
-        const int which = q / (kGridCols * kGridYs), rem = q % (kGridCols * kGridYs);
-        const int c = rem / kGridYs, i = rem % kGridYs;
-        const int bx = (cx0 + c / 5) * 4, bz = (cz0 + c % 5) * 4, y = -64 + i * 8;
+    for (int q = threadIdx.x; q < 3 * 5 * kGridYs; q += blockDim.x) {
+        const int which = q / (5 * kGridYs), rem = q % (5 * kGridYs);
+        const int k = rem / kGridYs, i = rem % kGridYs, c = gx * 5 + k;
+        const int bx = (cx0 + gx) * 4, bz = (cz0 + k) * 4, y = -64 + i * 8;
         J.noodle[which][c][i] = p2_noodle_child(T, W, which + 1, bx, y, bz);
     }
 }
 
 constexpr int kAqThreads = 128;
 
-// One CTA per job: skipSamplingAboveY from the column tops over the grid's x/z span, then
-// every aquifer cell's random anchor and fluid status (aquifer.c:158-196, 379-395, 481-501).
+// The highest column top over the grid's x/z span (skipSamplingAboveY derives from it) and every
+// aquifer cell's random anchor and fluid status (aquifer.c:158-196, 379-395, 481-501).  CTA
+// (job, part) of gridDim.y takes every gridDim.y-th column top (atomicMax into J.max_psl) and
+// aquifer cell, so a job's set-up runs as several short chains side by side.
 __global__ void __launch_bounds__(kAqThreads) p2_aquifer_kernel(const P2Tables *__restrict__ Tp,
                                                                 const P2World *__restrict__ worlds, P2Chunk *jobs) {
-    __shared__ int max_psl;
     const P2Tables &T = *Tp;
     P2Chunk &J = jobs[blockIdx.x];
     const P2World &W = worlds[J.world];
+    const int part = blockIdx.y, parts = gridDim.y;
     const int min_bx = J.chunk_x * 16, min_bz = J.chunk_z * 16;
     const int min_gx = (min_bx - 5) >> 4, max_gx = ((min_bx + 15 - 5) >> 4) + 1;
     const int min_gz = (min_bz - 5) >> 4, max_gz = ((min_bz + 15 - 5) >> 4) + 1;
     const int min_gy = floor_div(-64 + 1, 12) - 1;
-    if (threadIdx.x == 0) {
-        max_psl = -0x7FFFFFFF - 1;
+    if (part == 0 && threadIdx.x == 0) {
         J.min_gx = min_gx;
         J.min_gy = min_gy;
         J.min_gz = min_gz;
     }
-    __syncthreads();
     const int x1 = min_gx * 16, z1 = min_gz * 16, x2 = max_gx * 16 + 9, z2 = max_gz * 16 + 9;
     const int nxs = (x2 - x1) / 4 + 1, nzs = (z2 - z1) / 4 + 1;
-    for (int q = threadIdx.x; q < nxs * nzs; q += blockDim.x) {
+    for (int q = part * (int)blockDim.x + (int)threadIdx.x; q < nxs * nzs; q += parts * (int)blockDim.x) {
         const int x = x1 + (q % nxs) * 4, z = z1 + (q / nxs) * 4;
-        atomicMax(&max_psl, p2_column_top(T, W, x, z));
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const int g = floor_div((max_psl + 8) + 12, 12) + 1;
-        J.skip_above = g * 12 + 11 - 1;
+        atomicMax(&J.max_psl, p2_column_top(T, W, x, z));
     }
     const Xr factory{W.aq_rand_lo, W.aq_rand_hi};
-    for (int idx = threadIdx.x; idx < kAqCells; idx += blockDim.x) {
+    for (int idx = part * (int)blockDim.x + (int)threadIdx.x; idx < kAqCells; idx += parts * (int)blockDim.x) {
         const int dx = idx % kAqX, dz = (idx / kAqX) % kAqZ, dy = idx / (kAqX * kAqZ);
         const int cx = min_gx + dx, cy = min_gy + dy, cz = min_gz + dz;
         Xr rnd = xr_make((uint64_t)mc_hash_code(cx, cy, cz) ^ factory.lo, factory.hi);
@@ -1581,11 +1581,11 @@ void p2_launch_build(const P2Tables *T, P2World *worlds, int n_worlds, cudaStrea
 }
 
 void p2_launch_grid(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s) {
-    p2_grid_kernel<<<n_jobs, kGridThreads, 0, s>>>(T, worlds, jobs);
+    p2_grid_kernel<<<dim3(n_jobs, 5), kGridThreads, 0, s>>>(T, worlds, jobs);
 }
 
 void p2_launch_aquifer(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s) {
-    p2_aquifer_kernel<<<n_jobs, kAqThreads, 0, s>>>(T, worlds, jobs);
+    p2_aquifer_kernel<<<dim3(n_jobs, 4), kAqThreads, 0, s>>>(T, worlds, jobs);
 }
 
 void p2_launch_states(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s) {

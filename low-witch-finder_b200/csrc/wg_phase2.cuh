@@ -134,7 +134,7 @@ enum : int { CV_UNCHANGED = 0, CV_AIR = 1, CV_WATER = 2, CV_LAVA = 3 };
 struct P2Chunk {
     int world;                     // index into the world array
     int chunk_x, chunk_z;
-    int skip_above;                // the aquifer's skipSamplingAboveY
+    int max_psl;                   // highest column top around the chunk (INT_MIN before p2_aquifer_kernel)
     int min_gx, min_gy, min_gz;
     int carved;                    // cells[] holds the carver result
     double main[kGridCols][kGridYs];
