@@ -529,16 +529,27 @@ __device__ bool deep_dark(const P2Tables &T, const P2World &W, int x, int y, int
 __device__ const int kSurfOffsets[13][2] = {{0, 0},   {-2, -1}, {-1, -1}, {0, -1}, {1, -1}, {-3, 0}, {-2, 0},
                                            {-1, 0}, {1, 0},    {-2, 1},  {-1, 1}, {0, 1},  {1, 1}};
 
-// computeFluid (aquifer.c:327-376): level and type.
-__device__ void p2_compute_fluid(const P2Tables &T, const P2World &W, int x, int y, int z, int &out_level,
-                                 int &out_type) {
+// The column top of block column (x, z): from the chunk's table (J non-null) where the column lies
+// in it, else computed.
+__device__ __forceinline__ int p2_top(const P2Tables &T, const P2World &W, const P2Chunk *J, int x, int z) {
+    if (J) {
+        const int qx = (x >> 2) - (4 * J->chunk_x - 16), qz = (z >> 2) - (4 * J->chunk_z - 8);
+        if ((unsigned)qx < (unsigned)kTopX && (unsigned)qz < (unsigned)kTopZ) return J->tops[qz][qx];
+    }
+    return p2_column_top(T, W, x, z);
+}
+
+// computeFluid (aquifer.c:327-376): level and type; the column tops come from the job's table when
+// J is given.
+__device__ void p2_compute_fluid(const P2Tables &T, const P2World &W, const P2Chunk *J, int x, int y, int z,
+                                 int &out_level, int &out_type) {
     int glevel, gtype;
     global_fluid(y, glevel, gtype);
     int min_top = 0x7FFFFFFF;
     bool has_above = false;
     for (int i = 0; i < 13; i++) {
         const int bx = x + kSurfOffsets[i][0] * 16, bz = z + kSurfOffsets[i][1] * 16;
-        const int top = p2_column_top(T, W, bx, bz);
+        const int top = p2_top(T, W, J, bx, bz);
         const int top_adj = top + 8;
         const bool center = (i == 0);
         if (center && y - 12 > top_adj) {
@@ -862,12 +873,11 @@ __global__ void __launch_bounds__(kGridThreads) p2_grid_kernel(const P2Tables *_
 
 constexpr int kAqThreads = 128;
 
-// The highest column top over the grid's x/z span (skipSamplingAboveY derives from it) and every
-// aquifer cell's random anchor and fluid status (aquifer.c:158-196, 379-395, 481-501).  CTA
-// (job, part) of gridDim.y takes every gridDim.y-th column top (atomicMax into J.max_psl) and
-// aquifer cell, so a job's set-up runs as several short chains side by side.
-__global__ void __launch_bounds__(kAqThreads) p2_aquifer_kernel(const P2Tables *__restrict__ Tp,
-                                                                const P2World *__restrict__ worlds, P2Chunk *jobs) {
+// Every column top of the job's table (one thread each) and their maximum over the grid's x/z
+// span, from which skipSamplingAboveY derives (aquifer.c:158-196, column_top.c:94-118).
+// CTA (job, part) of gridDim.y takes every gridDim.y-th entry.
+__global__ void __launch_bounds__(kAqThreads) p2_tops_kernel(const P2Tables *__restrict__ Tp,
+                                                             const P2World *__restrict__ worlds, P2Chunk *jobs) {
     const P2Tables &T = *Tp;
     P2Chunk &J = jobs[blockIdx.x];
     const P2World &W = worlds[J.world];
@@ -875,18 +885,31 @@ __global__ void __launch_bounds__(kAqThreads) p2_aquifer_kernel(const P2Tables *
     const int min_bx = J.chunk_x * 16, min_bz = J.chunk_z * 16;
     const int min_gx = (min_bx - 5) >> 4, max_gx = ((min_bx + 15 - 5) >> 4) + 1;
     const int min_gz = (min_bz - 5) >> 4, max_gz = ((min_bz + 15 - 5) >> 4) + 1;
-    const int min_gy = floor_div(-64 + 1, 12) - 1;
     if (part == 0 && threadIdx.x == 0) {
         J.min_gx = min_gx;
-        J.min_gy = min_gy;
+        J.min_gy = floor_div(-64 + 1, 12) - 1;
         J.min_gz = min_gz;
     }
+    // skipSamplingAboveY's samples: x = x1 + 4 i <= x2, z = z1 + 4 j <= z2
     const int x1 = min_gx * 16, z1 = min_gz * 16, x2 = max_gx * 16 + 9, z2 = max_gz * 16 + 9;
-    const int nxs = (x2 - x1) / 4 + 1, nzs = (z2 - z1) / 4 + 1;
-    for (int q = part * (int)blockDim.x + (int)threadIdx.x; q < nxs * nzs; q += parts * (int)blockDim.x) {
-        const int x = x1 + (q % nxs) * 4, z = z1 + (q / nxs) * 4;
-        atomicMax(&J.max_psl, p2_column_top(T, W, x, z));
+    const int qx0 = 4 * J.chunk_x - 16, qz0 = 4 * J.chunk_z - 8;
+    for (int q = part * (int)blockDim.x + (int)threadIdx.x; q < kTopX * kTopZ; q += parts * (int)blockDim.x) {
+        const int x = (qx0 + q % kTopX) * 4, z = (qz0 + q / kTopX) * 4;
+        const int top = p2_column_top(T, W, x, z);
+        J.tops[q / kTopX][q % kTopX] = (int16_t)top;
+        if (x >= x1 && x <= x2 && z >= z1 && z <= z2) atomicMax(&J.max_psl, top);
     }
+}
+
+// Every aquifer cell's random anchor and fluid status (aquifer.c:379-395, 481-501), computed up
+// front; CTA (job, part) of gridDim.y takes every gridDim.y-th cell.
+__global__ void __launch_bounds__(kAqThreads) p2_aquifer_kernel(const P2Tables *__restrict__ Tp,
+                                                                const P2World *__restrict__ worlds, P2Chunk *jobs) {
+    const P2Tables &T = *Tp;
+    P2Chunk &J = jobs[blockIdx.x];
+    const P2World &W = worlds[J.world];
+    const int part = blockIdx.y, parts = gridDim.y;
+    const int min_gx = J.min_gx, min_gy = J.min_gy, min_gz = J.min_gz;
     const Xr factory{W.aq_rand_lo, W.aq_rand_hi};
     for (int idx = part * (int)blockDim.x + (int)threadIdx.x; idx < kAqCells; idx += parts * (int)blockDim.x) {
         const int dx = idx % kAqX, dz = (idx / kAqX) % kAqZ, dy = idx / (kAqX * kAqZ);
@@ -899,8 +922,8 @@ __global__ void __launch_bounds__(kAqThreads) p2_aquifer_kernel(const P2Tables *
                                (int64_t)(py & 0xFFF);
         J.aq_loc[idx] = packed;
         int level, type;
-        p2_compute_fluid(T, W, (int)(packed >> 38), (int)((packed << 52) >> 52), (int)((packed << 26) >> 38), level,
-                         type);
+        p2_compute_fluid(T, W, &J, (int)(packed >> 38), (int)((packed << 52) >> 52), (int)((packed << 26) >> 38),
+                         level, type);
         J.aq_level[idx] = level;
         J.aq_type[idx] = (uint8_t)type;
     }
@@ -1448,7 +1471,7 @@ __global__ void __launch_bounds__(kFinishThreads) p2_finish_kernel(const P2Table
         const int dx = t / size_z, dz = t % size_z;
         const int x = H.hut_x + dx, z = H.hut_z + dz;
         int level, type;
-        p2_compute_fluid(T, W, x, 62, z, level, type);
+        p2_compute_fluid(T, W, &J, x, 62, z, level, type);
         wet[t] = (type == BS_WATER && 62 < level) ? 1 : 0;
         pre_h[t] = p2_height(T, W, J, x, z, false);
         post_h[t] = p2_height(T, W, J, x, z, true);
@@ -1546,7 +1569,7 @@ __global__ void p2_probe_kernel(const P2Tables *__restrict__ Tp, const P2World *
         }
         case PR_FLUID: {
             int level, type;
-            p2_compute_fluid(T, W, x, y, z, level, type);
+            p2_compute_fluid(T, W, nullptr, x, y, z, level, type);
             v = (double)level * 4.0 + (double)type;
             break;
         }
@@ -1585,7 +1608,8 @@ void p2_launch_grid(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int
 }
 
 void p2_launch_aquifer(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s) {
-    p2_aquifer_kernel<<<dim3(n_jobs, 4), kAqThreads, 0, s>>>(T, worlds, jobs);
+    p2_tops_kernel<<<dim3(n_jobs, 5), kAqThreads, 0, s>>>(T, worlds, jobs);
+    p2_aquifer_kernel<<<dim3(n_jobs, 3), kAqThreads, 0, s>>>(T, worlds, jobs);
 }
 
 void p2_launch_states(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s) {

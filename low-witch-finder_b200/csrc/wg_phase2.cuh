@@ -127,6 +127,10 @@ constexpr int kGridCols = 25;     // 5 x 5 corner columns, index gx * 5 + gz
 constexpr int kGridYs = 49;       // y = -64 + 8 i
 constexpr int kAqX = 3, kAqY = 35, kAqZ = 3, kAqCells = kAqX * kAqY * kAqZ;
 constexpr int kCarveCells = 384 * 16 * 16;
+// Column tops (lysh_preliminary_surface_level, a function of the quart column) around a chunk:
+// quart x from 4 * chunk_x - 16, quart z from 4 * chunk_z - 8.  That covers the aquifer cells'
+// 13 surface samples, the skipSamplingAboveY span and the flood test of a hut in the chunk.
+constexpr int kTopX = 27, kTopZ = 19;
 
 enum : int { BS_SOLID = 0, BS_AIR = 1, BS_WATER = 2, BS_LAVA = 3 };   // lysh_block_state order
 enum : int { CV_UNCHANGED = 0, CV_AIR = 1, CV_WATER = 2, CV_LAVA = 3 };
@@ -134,7 +138,7 @@ enum : int { CV_UNCHANGED = 0, CV_AIR = 1, CV_WATER = 2, CV_LAVA = 3 };
 struct P2Chunk {
     int world;                     // index into the world array
     int chunk_x, chunk_z;
-    int max_psl;                   // highest column top around the chunk (INT_MIN before p2_aquifer_kernel)
+    int max_psl;                   // highest column top around the chunk (INT_MIN before p2_tops_kernel)
     int min_gx, min_gy, min_gz;
     int carved;                    // cells[] holds the carver result
     double main[kGridCols][kGridYs];
@@ -142,6 +146,7 @@ struct P2Chunk {
     int64_t aq_loc[kAqCells];
     int32_t aq_level[kAqCells];
     uint8_t aq_type[kAqCells];
+    int16_t tops[kTopZ][kTopX];    // column tops, quart x - (4 * chunk_x - 16), quart z - (4 * chunk_z - 8)
     alignas(16) uint8_t cells[kCarveCells];   // CV_* per block, index (lz << 4 | lx) | (y + 64) << 8; copied as words
     uint32_t carve_mask[kCarveCells / 32];    // the carvers' per-block mask while they run
     // per block of the chunk (index as cells): the pre-carver state (lysh_phase2_block_at) in the
