@@ -187,7 +187,21 @@ int ensure_tables(wg_engine *eng) {
     int rc = upload(eng, g.nodes, (size_t)g.n_nodes, &h->nodes);
     if (!rc) rc = upload(eng, g.floats, (size_t)g.n_floats, &h->floats);
     if (!rc) rc = upload(eng, g.child, (size_t)g.n_child, &h->child);
-    if (!rc) rc = upload(eng, g.sin_table, (size_t)kSinEntries, &h->sin_table);
+    if (!rc) {   // the sine table as a quarter wave, checked against the full table
+        std::vector<float> quarter(kSinQuarterPad, 0.0f);
+        for (int i = 0; i < kSinQuarter; i++) quarter[i] = g.sin_table[i];
+        h->sin_half_turn = g.sin_table[32768];
+        for (int i = 0; i < kSinEntries; i++) {
+            const int hh = i & 32767, k = hh <= 16384 ? hh : 32768 - hh;
+            float v = (i & 32768) ? -quarter[k] : quarter[k];
+            if (i == 32768) v = h->sin_half_turn;
+            uint32_t a, b;
+            std::memcpy(&a, &v, 4);
+            std::memcpy(&b, &g.sin_table[i], 4);
+            if (a != b) return eng->fail(WG_ERR_ARG, "phase 2: sine table is not a quarter wave");
+        }
+        rc = upload(eng, quarter.data(), quarter.size(), &h->sin_quarter);
+    }
     h->root_offset = g.root_offset;
     h->root_factor = g.root_factor;
     h->root_peak = g.root_peak;

@@ -752,6 +752,7 @@ __global__ void __launch_bounds__(256) p2_states_kernel(const P2Tables *__restri
     const int nat = p2_block_at(T, W, J, x, y, z);
     const int sub = y > -56 ? p2_substance(T, W, J, x, y, z, 0.0) : BS_LAVA;
     J.states[q] = (uint8_t)(nat | (sub << 4));
+    J.cells[q] = (uint8_t)CV_UNCHANGED;   // the carvers' working copy starts untouched
 }
 
 // ------------------------------------------------------------------------------------
@@ -944,20 +945,56 @@ struct CarveCtx {
     float *width;                 // canyon width factors (384)
     double *fx, *fz, *fy;         // carve_ellipsoid's per-row / column / level offsets (shared)
     uint16_t *cols;               // its columns inside the ellipse (shared, 256)
+    const float *sinq;            // Mth.SIN quarter wave (shared)
+    float sin_half_turn;
     int tmin_x, tmin_z;
     double tmid_x, tmid_z;
 };
 
-__device__ __forceinline__ float mc_sin(const P2Tables &T, double a) {
-    return T.sin_table[(int)((long long)(a * 10430.378350470453) & 65535LL)];
+// Mth.SIN[i] from the quarter wave in shared memory: entries 16385..32767 mirror 16383..1, the
+// second half is the first negated, and entry 32768 is its own value.
+__device__ __forceinline__ float sin_entry(const CarveCtx &c, int i) {
+    const int h = i & 32767, k = h <= 16384 ? h : 32768 - h;
+    float v = c.sinq[k];
+    if (i & 32768) v = -v;
+    return i == 32768 ? c.sin_half_turn : v;
 }
-__device__ __forceinline__ float mc_cos(const P2Tables &T, double a) {
-    return T.sin_table[(int)((long long)(a * 10430.378350470453 + 16384.0) & 65535LL)];
+__device__ __forceinline__ float mc_sin(const CarveCtx &c, double a) {
+    return sin_entry(c, (int)((long long)(a * 10430.378350470453) & 65535LL));
+}
+__device__ __forceinline__ float mc_cos(const CarveCtx &c, double a) {
+    return sin_entry(c, (int)((long long)(a * 10430.378350470453 + 16384.0) & 65535LL));
 }
 __device__ __forceinline__ float lcg_float(uint64_t &st) { return (float)lcg_bits(st, 24) * 5.9604645e-8f; }
 __device__ __forceinline__ float uniform_float(uint64_t &st, float lo, float hi) { return lcg_float(st) * (hi - lo) + lo; }
 __device__ __forceinline__ void lcg_set_seed(uint64_t &st, uint64_t s) { st = (s ^ kLcgMul) & kLcgMask; }
 __device__ __forceinline__ int jfloor(double d) { return (int)floor(d); }
+
+// Skip-ahead for java.util.Random: k steps from state s give (A_k s + C_k) mod 2^48, so the
+// fixed run of draws in one carver step comes from independent multiplies instead of a chain.
+struct LcgJump {
+    uint64_t a, c;
+};
+__host__ __device__ constexpr LcgJump lcg_jump(int k) {
+    uint64_t a = 1, c = 0;
+    for (int i = 0; i < k; i++) {
+        a = (a * kLcgMul) & kLcgMask;
+        c = (c * kLcgMul + 0xBULL) & kLcgMask;
+    }
+    return LcgJump{a, c};
+}
+template <int K>
+__device__ __forceinline__ uint64_t lcg_ahead(uint64_t s) {
+    constexpr LcgJump j = lcg_jump(K);
+    return (s * j.a + j.c) & kLcgMask;
+}
+// nextFloat and nextInt(bound), bound a power of two, of the draw that produced state st
+__device__ __forceinline__ float lcg_float_at(uint64_t st) {
+    return (float)(int)(uint32_t)(st >> (48 - 24)) * 5.9604645e-8f;
+}
+__device__ __forceinline__ int lcg_int_pow2_at(uint64_t st, int bound) {
+    return (int)(((int64_t)bound * (int64_t)(int)(uint32_t)(st >> (48 - 31))) >> 31);
+}
 
 // setLargeFeatureSeed (structure.c:26-42)
 __device__ __forceinline__ uint64_t large_feature_state(uint64_t world_seed, int cx, int cz) {
@@ -1017,7 +1054,6 @@ __device__ void carve_ellipsoid(CarveCtx &c, int kind, double floor_level, doubl
         else if ((k + 1) * nyp <= q) k++;
         const int vi = q - k * nyp, pi = c.cols[k] >> 4, si = c.cols[k] & 15;
         const int p = i0 + pi, s = n0 + si, v = m0 - vi;
-        const int bx = min_bx + p, bz = min_bz + s;
         const double nx = c.fx[pi];
         const double nz = c.fz[si];
         const double ny = c.fy[vi];
@@ -1030,15 +1066,13 @@ __device__ void carve_ellipsoid(CarveCtx &c, int kind, double floor_level, doubl
         }
         if (skip) continue;
         const int ci = carve_index(p, v, s);
+        const uint32_t pre = c.J->states[ci];   // p2_block_at and p2_substance(.., 0.0), precomputed
         const uint32_t bit = 1u << (ci & 31);
         const uint32_t old = atomicOr(&c.mask[ci >> 5], bit);
         if (old & bit) continue;
-        // carveBlock
-        int st;
-        const uint8_t cv = c.cells[ci];
-        const uint32_t pre = c.J->states[ci];   // p2_block_at and p2_substance(.., 0.0), precomputed
-        if (cv != CV_UNCHANGED) st = cv;
-        else st = (int)(pre & 15u);
+        // carveBlock.  A block is written only after its mask bit is set, so an unmarked block
+        // still holds its pre-carver state.
+        const int st = (int)(pre & 15u);
         if (!(st == BS_SOLID || st == BS_WATER)) continue;
         int cs;
         if (v <= -56) {
@@ -1069,7 +1103,6 @@ template <bool kBranch>
 __device__ __noinline__ void cave_tunnel(CarveCtx &c, double floor_level, uint64_t seed, double x, double y, double z,
                                          double d4, double d5, float thickness, float yaw, float pitch, int first_step,
                                          int total_steps, double y_scale) {
-    const P2Tables &T = *c.T;
     uint64_t r;
     lcg_set_seed(r, seed);
     const int branch_step = lcg_int(r, total_steps / 2) + total_steps / 4;
@@ -1077,24 +1110,25 @@ __device__ __noinline__ void cave_tunnel(CarveCtx &c, double floor_level, uint64
     float f30 = 0.0f, f31 = 0.0f;
     for (int i = first_step; i < total_steps; i++) {
         const float ang = (float)i * 3.1415927f / (float)total_steps;
-        const double radius = 1.5 + (double)(mc_sin(T, (double)ang) * thickness);
+        const double radius = 1.5 + (double)(mc_sin(c, (double)ang) * thickness);
         const double vert_base = radius * y_scale;
-        const float cos_pitch = mc_cos(T, (double)pitch);
-        x += (double)(mc_cos(T, (double)yaw) * cos_pitch);
-        y += (double)mc_sin(T, (double)pitch);
-        z += (double)(mc_sin(T, (double)yaw) * cos_pitch);
+        const float cos_pitch = mc_cos(c, (double)pitch);
+        x += (double)(mc_cos(c, (double)yaw) * cos_pitch);
+        y += (double)mc_sin(c, (double)pitch);
+        z += (double)(mc_sin(c, (double)yaw) * cos_pitch);
         pitch *= wide ? 0.92f : 0.7f;
         pitch += f31 * 0.1f;
         yaw += f30 * 0.1f;
         f31 *= 0.9f;
         f30 *= 0.75f;
-        {
-            const float a1 = lcg_float(r), b1 = lcg_float(r), c1 = lcg_float(r);
-            f31 += (a1 - b1) * c1 * 2.0f;
-            const float a2 = lcg_float(r), b2 = lcg_float(r), c2 = lcg_float(r);
-            f30 += (a2 - b2) * c2 * 4.0f;
-        }
+        // six nextFloat, then (past the branch point) one nextInt(4): seven draws from r0
+        const uint64_t r0 = r;
+        f31 += (lcg_float_at(lcg_ahead<1>(r0)) - lcg_float_at(lcg_ahead<2>(r0))) * lcg_float_at(lcg_ahead<3>(r0)) *
+               2.0f;
+        f30 += (lcg_float_at(lcg_ahead<4>(r0)) - lcg_float_at(lcg_ahead<5>(r0))) * lcg_float_at(lcg_ahead<6>(r0)) *
+               4.0f;
         if (kBranch && i == branch_step && thickness > 1.0f) {
+            r = lcg_ahead<6>(r0);
             const uint64_t s1 = lcg_long(r);
             const float t1 = lcg_float(r) * 0.5f + 0.5f;
             cave_tunnel<false>(c, floor_level, s1, x, y, z, d4, d5, t1, yaw - 1.5707964f, pitch / 3.0f, i,
@@ -1105,7 +1139,8 @@ __device__ __noinline__ void cave_tunnel(CarveCtx &c, double floor_level, uint64
                                total_steps, 1.0);
             return;
         }
-        if (lcg_int(r, 4) == 0) continue;
+        r = lcg_ahead<7>(r0);
+        if (lcg_int_pow2_at(r, 4) == 0) continue;
         {
             const double dx = x - c.tmid_x, dz = z - c.tmid_z;
             const double dy = (double)(total_steps - i);
@@ -1117,7 +1152,6 @@ __device__ __noinline__ void cave_tunnel(CarveCtx &c, double floor_level, uint64
 }
 
 __device__ void cave_carve(CarveCtx &c, uint64_t &r, int ocx, int ocz, int y_hi) {
-    const P2Tables &T = *c.T;
     const int i10 = lcg_int(r, lcg_int(r, lcg_int(r, 15) + 1) + 1);
     for (int k = 0; k < i10; k++) {
         const int lx = lcg_int(r, 16);
@@ -1132,7 +1166,7 @@ __device__ void cave_carve(CarveCtx &c, uint64_t &r, int ocx, int ocz, int y_hi)
         if (lcg_int(r, 4) == 0) {
             const double room_y_scale = (double)uniform_float(r, 0.1f, 0.9f);
             const float f28 = 1.0f + lcg_float(r) * 6.0f;
-            const float sf = mc_sin(T, 1.5707963705062866);
+            const float sf = mc_sin(c, 1.5707963705062866);
             const double d17 = 1.5 + (double)(sf * f28);
             const double d19 = d17 * room_y_scale;
             carve_ellipsoid(c, 0, floor_level, x + 1.0, (double)y, z, d17, d19);
@@ -1150,7 +1184,6 @@ __device__ void cave_carve(CarveCtx &c, uint64_t &r, int ocx, int ocz, int y_hi)
 }
 
 __device__ void canyon_carve(CarveCtx &c, uint64_t &r0, int ocx, int ocz) {
-    const P2Tables &T = *c.T;
     const int lx = lcg_int(r0, 16);
     double x = (double)(ocx * 16 + lx);
     const int yi = lcg_int(r0, 67 - 10 + 1) + 10;
@@ -1189,34 +1222,35 @@ __device__ void canyon_carve(CarveCtx &c, uint64_t &r0, int ocx, int ocz) {
     double y = (double)yi;
     float yaw_drift = 0.0f, pitch_drift = 0.0f;
     for (int i = 0; i < total_steps; i++) {
+        // two uniform floats, six nextFloat and one nextInt(4): nine draws from r0
+        const uint64_t r0 = r;
         const float ang = (float)i * 3.1415927f / (float)total_steps;
-        double radius = 1.5 + (double)(mc_sin(T, (double)ang) * thickness);
+        double radius = 1.5 + (double)(mc_sin(c, (double)ang) * thickness);
         double vert_radius = radius * y_scale;
-        radius *= (double)uniform_float(r, 0.75f, 1.0f);
+        radius *= (double)(lcg_float_at(lcg_ahead<1>(r0)) * (1.0f - 0.75f) + 0.75f);
         {   // updateVerticalRadius
             const float f1 = (float)total_steps, f2 = (float)i;
             const float f7 = 1.0f - fabsf(0.5f - f2 / f1) * 2.0f;
             const float f8 = 0.0f + 1.0f * f7;
             const double base = (double)f8 * vert_radius;
-            vert_radius = base * (double)uniform_float(r, 0.75f, 1.0f);
+            vert_radius = base * (double)(lcg_float_at(lcg_ahead<2>(r0)) * (1.0f - 0.75f) + 0.75f);
         }
-        const float cos_pitch = mc_cos(T, (double)pitch);
-        const float sin_pitch = mc_sin(T, (double)pitch);
-        x += (double)(mc_cos(T, (double)yaw) * cos_pitch);
+        const float cos_pitch = mc_cos(c, (double)pitch);
+        const float sin_pitch = mc_sin(c, (double)pitch);
+        x += (double)(mc_cos(c, (double)yaw) * cos_pitch);
         y += (double)sin_pitch;
-        z += (double)(mc_sin(T, (double)yaw) * cos_pitch);
+        z += (double)(mc_sin(c, (double)yaw) * cos_pitch);
         pitch *= 0.7f;
         pitch += pitch_drift * 0.05f;
         yaw += yaw_drift * 0.05f;
         pitch_drift *= 0.8f;
         yaw_drift *= 0.5f;
-        {
-            const float a1 = lcg_float(r), b1 = lcg_float(r), c1 = lcg_float(r);
-            pitch_drift += (a1 - b1) * c1 * 2.0f;
-            const float a2 = lcg_float(r), b2 = lcg_float(r), c2 = lcg_float(r);
-            yaw_drift += (a2 - b2) * c2 * 4.0f;
-        }
-        if (lcg_int(r, 4) == 0) continue;
+        pitch_drift += (lcg_float_at(lcg_ahead<3>(r0)) - lcg_float_at(lcg_ahead<4>(r0))) *
+                       lcg_float_at(lcg_ahead<5>(r0)) * 2.0f;
+        yaw_drift += (lcg_float_at(lcg_ahead<6>(r0)) - lcg_float_at(lcg_ahead<7>(r0))) *
+                     lcg_float_at(lcg_ahead<8>(r0)) * 4.0f;
+        r = lcg_ahead<9>(r0);
+        if (lcg_int_pow2_at(r, 4) == 0) continue;
         {
             const double dx = x - c.tmid_x, dz = z - c.tmid_z;
             const double dy = (double)(total_steps - i);
@@ -1237,14 +1271,18 @@ __global__ void __launch_bounds__(kCarveThreads) p2_carve_kernel(const P2Tables 
     __shared__ float width[384];
     __shared__ double fxs[16], fzs[16], fys[384];
     __shared__ uint16_t cols[256];
+    __shared__ uint32_t mask[kMaskWords];   // blocks already carved
+    extern __shared__ float4 sinq4[];       // Mth.SIN quarter wave, kSinQuarterPad floats
     P2Chunk &J = jobs[blockIdx.x];
     const P2World &W = worlds[J.world];
-    uint8_t *cells = J.cells;
-    uint32_t *mask = J.carve_mask;
-    for (int q = threadIdx.x; q < kCarveCells / 4; q += blockDim.x) reinterpret_cast<uint32_t *>(cells)[q] = 0u;
+    uint8_t *cells = J.cells;   // all CV_UNCHANGED (p2_states_kernel)
     for (int q = threadIdx.x; q < kMaskWords; q += blockDim.x) mask[q] = 0u;
+    const float4 *sinq_src = reinterpret_cast<const float4 *>(Tp->sin_quarter);
+    for (int q = threadIdx.x; q < kSinQuarterPad / 4; q += blockDim.x) sinq4[q] = sinq_src[q];
     __syncwarp();
     CarveCtx c;
+    c.sinq = reinterpret_cast<const float *>(sinq4);
+    c.sin_half_turn = Tp->sin_half_turn;
     c.T = Tp;
     c.W = &W;
     c.J = &J;
@@ -1617,7 +1655,10 @@ void p2_launch_states(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, i
 }
 
 void p2_launch_carve(const P2Tables *T, const P2World *worlds, P2Chunk *jobs, int n_jobs, cudaStream_t s) {
-    p2_carve_kernel<<<n_jobs, kCarveThreads, 0, s>>>(T, worlds, jobs);
+    static_assert(kSinQuarterPad % 4 == 0, "the quarter wave is copied as float4");
+    constexpr int smem = kSinQuarterPad * (int)sizeof(float);
+    cudaFuncSetAttribute(p2_carve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    p2_carve_kernel<<<n_jobs, kCarveThreads, smem, s>>>(T, worlds, jobs);
 }
 
 void p2_launch_biome_map(const P2Tables *T, const P2World *worlds, int tree, int64_t x0, int64_t z0, int w, int h,

@@ -104,10 +104,14 @@ struct P2Tables {
     const float *floats;
     const int *child;
     int root_offset, root_factor, root_peak;
-    const float *sin_table;
+    // Mth.SIN as a quarter wave: entries 0..16384 (padded to kSinQuarterPad); the host checks that
+    // they and sin_half_turn (entry 32768) rebuild all 65,536 entries bit for bit
+    const float *sin_quarter;
+    float sin_half_turn;
     BiomeTree trees[kBiomeTrees];
 };
 
+constexpr int kSinQuarter = 16385, kSinQuarterPad = 16388;   // padded to whole 16-byte vectors
 constexpr int kWorldSlotsMax = 192;
 constexpr int kSplineDepth = 8;   // deepest spline nesting the evaluator holds (the game's is 5)
 constexpr int kTreeDepth = 16;    // deepest biome R-tree the search holds
@@ -148,7 +152,6 @@ struct P2Chunk {
     uint8_t aq_type[kAqCells];
     int16_t tops[kTopZ][kTopX];    // column tops, quart x - (4 * chunk_x - 16), quart z - (4 * chunk_z - 8)
     alignas(16) uint8_t cells[kCarveCells];   // CV_* per block, index (lz << 4 | lx) | (y + 64) << 8; copied as words
-    uint32_t carve_mask[kCarveCells / 32];    // the carvers' per-block mask while they run
     // per block of the chunk (index as cells): the pre-carver state (lysh_phase2_block_at) in the
     // low nibble, the aquifer substance at density 0 in the high one (BS_* codes)
     alignas(16) uint8_t states[kCarveCells];
