@@ -338,6 +338,9 @@ def main() -> None:
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-jobs", action="store_true", help="skip the batched-jobs and serving measurements")
+    ap.add_argument("--phase2-only", action="store_true",
+                    help="one phase-1 pass for its survivors, then only the phase-2 measurement (a short "
+                         "command for profiling the phase-2 kernels)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -367,6 +370,16 @@ def main() -> None:
         z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
         z = z ^ (z >> np.uint64(31))
     seeds_np[:] = z.view(np.int64)
+    if args.phase2_only:
+        res = eng.seed_check(seeds=seeds_np, rect=RECT, max_height=MAX_HEIGHT, opts=opts)
+        line = {"phase2": phase2_measure(eng, res.candidates, opts, cpu=False)}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        eng.close()
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     seeds_dev = seeds_host.to(f"cuda:{local}")
     out_cap = 1 << 16
     out_dev = torch.zeros((out_cap, 4), dtype=torch.int64, device=f"cuda:{local}")

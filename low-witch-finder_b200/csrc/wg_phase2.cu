@@ -953,17 +953,23 @@ struct CarveCtx {
 
 // Mth.SIN[i] from the quarter wave in shared memory: entries 16385..32767 mirror 16383..1, the
 // second half is the first negated, and entry 32768 is its own value.
-__device__ __forceinline__ float sin_entry(const CarveCtx &c, int i) {
+// The walks copy the table's address into a SinTab by value, so that it stays in registers
+// while the ellipsoid code stores through other pointers.
+struct SinTab {
+    const float *q;
+    float half_turn;
+};
+__device__ __forceinline__ float sin_entry(const SinTab &t, int i) {
     const int h = i & 32767, k = h <= 16384 ? h : 32768 - h;
-    float v = c.sinq[k];
+    float v = t.q[k];
     if (i & 32768) v = -v;
-    return i == 32768 ? c.sin_half_turn : v;
+    return i == 32768 ? t.half_turn : v;
 }
-__device__ __forceinline__ float mc_sin(const CarveCtx &c, double a) {
-    return sin_entry(c, (int)((long long)(a * 10430.378350470453) & 65535LL));
+__device__ __forceinline__ float mc_sin(const SinTab &t, double a) {
+    return sin_entry(t, (int)((long long)(a * 10430.378350470453) & 65535LL));
 }
-__device__ __forceinline__ float mc_cos(const CarveCtx &c, double a) {
-    return sin_entry(c, (int)((long long)(a * 10430.378350470453 + 16384.0) & 65535LL));
+__device__ __forceinline__ float mc_cos(const SinTab &t, double a) {
+    return sin_entry(t, (int)((long long)(a * 10430.378350470453 + 16384.0) & 65535LL));
 }
 __device__ __forceinline__ float lcg_float(uint64_t &st) { return (float)lcg_bits(st, 24) * 5.9604645e-8f; }
 __device__ __forceinline__ float uniform_float(uint64_t &st, float lo, float hi) { return lcg_float(st) * (hi - lo) + lo; }
@@ -1103,6 +1109,8 @@ template <bool kBranch>
 __device__ __noinline__ void cave_tunnel(CarveCtx &c, double floor_level, uint64_t seed, double x, double y, double z,
                                          double d4, double d5, float thickness, float yaw, float pitch, int first_step,
                                          int total_steps, double y_scale) {
+    const SinTab sn{c.sinq, c.sin_half_turn};
+    const double tmid_x = c.tmid_x, tmid_z = c.tmid_z;
     uint64_t r;
     lcg_set_seed(r, seed);
     const int branch_step = lcg_int(r, total_steps / 2) + total_steps / 4;
@@ -1110,12 +1118,12 @@ __device__ __noinline__ void cave_tunnel(CarveCtx &c, double floor_level, uint64
     float f30 = 0.0f, f31 = 0.0f;
     for (int i = first_step; i < total_steps; i++) {
         const float ang = (float)i * 3.1415927f / (float)total_steps;
-        const double radius = 1.5 + (double)(mc_sin(c, (double)ang) * thickness);
+        const double radius = 1.5 + (double)(mc_sin(sn, (double)ang) * thickness);
         const double vert_base = radius * y_scale;
-        const float cos_pitch = mc_cos(c, (double)pitch);
-        x += (double)(mc_cos(c, (double)yaw) * cos_pitch);
-        y += (double)mc_sin(c, (double)pitch);
-        z += (double)(mc_sin(c, (double)yaw) * cos_pitch);
+        const float cos_pitch = mc_cos(sn, (double)pitch);
+        x += (double)(mc_cos(sn, (double)yaw) * cos_pitch);
+        y += (double)mc_sin(sn, (double)pitch);
+        z += (double)(mc_sin(sn, (double)yaw) * cos_pitch);
         pitch *= wide ? 0.92f : 0.7f;
         pitch += f31 * 0.1f;
         yaw += f30 * 0.1f;
@@ -1142,7 +1150,7 @@ __device__ __noinline__ void cave_tunnel(CarveCtx &c, double floor_level, uint64
         r = lcg_ahead<7>(r0);
         if (lcg_int_pow2_at(r, 4) == 0) continue;
         {
-            const double dx = x - c.tmid_x, dz = z - c.tmid_z;
+            const double dx = x - tmid_x, dz = z - tmid_z;
             const double dy = (double)(total_steps - i);
             const double rr = (double)(thickness + 2.0f + 16.0f);
             if (!(dx * dx + dz * dz - dy * dy <= rr * rr)) return;
@@ -1152,6 +1160,7 @@ __device__ __noinline__ void cave_tunnel(CarveCtx &c, double floor_level, uint64
 }
 
 __device__ void cave_carve(CarveCtx &c, uint64_t &r, int ocx, int ocz, int y_hi) {
+    const SinTab sn{c.sinq, c.sin_half_turn};
     const int i10 = lcg_int(r, lcg_int(r, lcg_int(r, 15) + 1) + 1);
     for (int k = 0; k < i10; k++) {
         const int lx = lcg_int(r, 16);
@@ -1166,7 +1175,7 @@ __device__ void cave_carve(CarveCtx &c, uint64_t &r, int ocx, int ocz, int y_hi)
         if (lcg_int(r, 4) == 0) {
             const double room_y_scale = (double)uniform_float(r, 0.1f, 0.9f);
             const float f28 = 1.0f + lcg_float(r) * 6.0f;
-            const float sf = mc_sin(c, 1.5707963705062866);
+            const float sf = mc_sin(sn, 1.5707963705062866);
             const double d17 = 1.5 + (double)(sf * f28);
             const double d19 = d17 * room_y_scale;
             carve_ellipsoid(c, 0, floor_level, x + 1.0, (double)y, z, d17, d19);
@@ -1184,6 +1193,8 @@ __device__ void cave_carve(CarveCtx &c, uint64_t &r, int ocx, int ocz, int y_hi)
 }
 
 __device__ void canyon_carve(CarveCtx &c, uint64_t &r0, int ocx, int ocz) {
+    const SinTab sn{c.sinq, c.sin_half_turn};
+    const double tmid_x = c.tmid_x, tmid_z = c.tmid_z;
     const int lx = lcg_int(r0, 16);
     double x = (double)(ocx * 16 + lx);
     const int yi = lcg_int(r0, 67 - 10 + 1) + 10;
@@ -1225,7 +1236,7 @@ __device__ void canyon_carve(CarveCtx &c, uint64_t &r0, int ocx, int ocz) {
         // two uniform floats, six nextFloat and one nextInt(4): nine draws from r0
         const uint64_t r0 = r;
         const float ang = (float)i * 3.1415927f / (float)total_steps;
-        double radius = 1.5 + (double)(mc_sin(c, (double)ang) * thickness);
+        double radius = 1.5 + (double)(mc_sin(sn, (double)ang) * thickness);
         double vert_radius = radius * y_scale;
         radius *= (double)(lcg_float_at(lcg_ahead<1>(r0)) * (1.0f - 0.75f) + 0.75f);
         {   // updateVerticalRadius
@@ -1235,11 +1246,11 @@ __device__ void canyon_carve(CarveCtx &c, uint64_t &r0, int ocx, int ocz) {
             const double base = (double)f8 * vert_radius;
             vert_radius = base * (double)(lcg_float_at(lcg_ahead<2>(r0)) * (1.0f - 0.75f) + 0.75f);
         }
-        const float cos_pitch = mc_cos(c, (double)pitch);
-        const float sin_pitch = mc_sin(c, (double)pitch);
-        x += (double)(mc_cos(c, (double)yaw) * cos_pitch);
+        const float cos_pitch = mc_cos(sn, (double)pitch);
+        const float sin_pitch = mc_sin(sn, (double)pitch);
+        x += (double)(mc_cos(sn, (double)yaw) * cos_pitch);
         y += (double)sin_pitch;
-        z += (double)(mc_sin(c, (double)yaw) * cos_pitch);
+        z += (double)(mc_sin(sn, (double)yaw) * cos_pitch);
         pitch *= 0.7f;
         pitch += pitch_drift * 0.05f;
         yaw += yaw_drift * 0.05f;
@@ -1252,7 +1263,7 @@ __device__ void canyon_carve(CarveCtx &c, uint64_t &r0, int ocx, int ocz) {
         r = lcg_ahead<9>(r0);
         if (lcg_int_pow2_at(r, 4) == 0) continue;
         {
-            const double dx = x - c.tmid_x, dz = z - c.tmid_z;
+            const double dx = x - tmid_x, dz = z - tmid_z;
             const double dy = (double)(total_steps - i);
             const double rr = (double)(thickness + 2.0f + 16.0f);
             if (!(dx * dx + dz * dz - dy * dy <= rr * rr)) return;
@@ -1297,19 +1308,32 @@ __global__ void __launch_bounds__(kCarveThreads) p2_carve_kernel(const P2Tables 
     c.tmin_z = J.chunk_z * 16;
     c.tmid_x = (double)(c.tmin_x + 8);
     c.tmid_z = (double)(c.tmin_z + 8);
-    for (int dx = -8; dx <= 8; dx++)
-        for (int dz = -8; dz <= 8; dz++) {
-            const int ox = J.chunk_x + dx, oz = J.chunk_z + dz;
-            for (int ci = 0; ci < 3; ci++) {
-                const float prob = ci == 0 ? 0.15f : (ci == 1 ? 0.07f : 0.01f);
-                uint64_t r = large_feature_state(W.seed + (uint64_t)ci, ox, oz);
-                const float f = lcg_float(r);
-                if (!(f <= prob)) continue;
-                if (ci == 1) cave_carve(c, r, ox, oz, 47);
-                else if (ci == 0) cave_carve(c, r, ox, oz, 180);
-                else canyon_carve(c, r, ox, oz);
-            }
+    // the (dx, dz, carver) triples in order, dx outer: each lane tests one of 32 at a time for
+    // the carver's start probability, and the warp runs the ones that start, in order
+    constexpr int kTriples = 17 * 17 * 3;
+    const int lane = threadIdx.x & 31;
+    for (int base = 0; base < kTriples; base += 32) {
+        const int q = base + lane;
+        bool starts = false;
+        uint64_t rq = 0;
+        if (q < kTriples) {
+            const int ci = q % 3, dx = q / 51 - 8, dz = (q / 3) % 17 - 8;
+            const float prob = ci == 0 ? 0.15f : (ci == 1 ? 0.07f : 0.01f);
+            rq = large_feature_state(W.seed + (uint64_t)ci, J.chunk_x + dx, J.chunk_z + dz);
+            starts = lcg_float(rq) <= prob;
         }
+        unsigned pending = __ballot_sync(0xFFFFFFFFu, starts);
+        while (pending) {
+            const int src = __ffs(pending) - 1;
+            pending &= pending - 1;
+            uint64_t r = __shfl_sync(0xFFFFFFFFu, rq, src);
+            const int t = base + src, ci = t % 3;
+            const int ox = J.chunk_x + t / 51 - 8, oz = J.chunk_z + (t / 3) % 17 - 8;
+            if (ci == 1) cave_carve(c, r, ox, oz, 47);
+            else if (ci == 0) cave_carve(c, r, ox, oz, 180);
+            else canyon_carve(c, r, ox, oz);
+        }
+    }
     __syncwarp();
     __threadfence_block();
     if (threadIdx.x == 0) J.carved = 1;
