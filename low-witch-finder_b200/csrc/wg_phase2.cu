@@ -1273,10 +1273,11 @@ __device__ void canyon_carve(CarveCtx &c, uint64_t &r0, int ocx, int ocz) {
 }
 
 // applyCarvers for the job's chunk (carver.c:482-523), one warp per chunk: a serial chain of tunnel
-// walks and ellipsoids, whose blocks the lanes take in turn.  The cells and the mask stay in the
-// job's global memory (L2 holds them) and shared memory holds only small per-ellipsoid tables, so
-// the chunks of a call all run at once.  The blocks' pre-carver states come from p2_states_kernel;
-// the job's cells are not read as such while J.carved is 0, so they serve as the working copy.
+// walks and ellipsoids, whose blocks the lanes take in turn.  Shared memory holds the carve mask
+// (12 KB), the sine quarter wave (64 KB) and small per-ellipsoid tables — 83 KB, two chunks per
+// SM — while the cells stay in the job's global memory (L2 holds them).  The blocks' pre-carver
+// states come from p2_states_kernel, which also clears the cells; they are not read as such while
+// J.carved is 0, so they serve as the working copy.
 __global__ void __launch_bounds__(kCarveThreads) p2_carve_kernel(const P2Tables *__restrict__ Tp,
                                                                  const P2World *__restrict__ worlds, P2Chunk *jobs) {
     __shared__ float width[384];
