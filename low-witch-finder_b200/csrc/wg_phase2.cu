@@ -726,15 +726,25 @@ __device__ __forceinline__ int p2_block_at(const P2Tables &T, const P2World &W, 
 __device__ __forceinline__ int carve_index(int lx, int y, int lz) { return ((lz & 15) << 4) | (lx & 15) | ((y + 64) << 8); }
 
 // Surface height (NOT_AIR predicate, y + 1; phase2.c:318-334 and :438-456) of a column of the job's
-// chunk, from the job's per-block states (p2_states_kernel).
+// chunk, from the job's per-block states (p2_states_kernel).  The 384 levels are read eight at a
+// time (independent loads) and tested top-down in order.
 __device__ int p2_height(const P2Tables &T, const P2World &W, const P2Chunk &J, int x, int z, bool carved) {
     (void)T;
     (void)W;
-    for (int y = 319; y >= -64; y--) {
-        const int ci = carve_index(x & 15, y, z & 15);
-        const uint8_t cv = carved ? J.cells[ci] : (uint8_t)CV_UNCHANGED;
-        const int st = cv != CV_UNCHANGED ? (int)cv : (int)(J.states[ci] & 15u);   // CV_AIR / _WATER / _LAVA = BS_*
-        if (st != BS_AIR) return y + 1;
+    static_assert((320 + 64) % 8 == 0, "levels in groups of eight");
+    for (int y0 = 319; y0 >= -64; y0 -= 8) {
+        uint8_t cv[8], pre[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int ci = carve_index(x & 15, y0 - k, z & 15);
+            cv[k] = carved ? J.cells[ci] : (uint8_t)CV_UNCHANGED;
+            pre[k] = J.states[ci];
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            const int st = cv[k] != CV_UNCHANGED ? (int)cv[k] : (int)(pre[k] & 15u);   // CV_* = BS_* codes
+            if (st != BS_AIR) return y0 - k + 1;
+        }
     }
     return -64;
 }
