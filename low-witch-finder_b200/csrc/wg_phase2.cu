@@ -1037,7 +1037,6 @@ __device__ void carve_ellipsoid(CarveCtx &c, int kind, double floor_level, doubl
     const int o0 = min(jfloor(z + hr) - min_bz, 15);
     const int nxp = i1 - i0 + 1, nzp = o0 - n0 + 1, nyp = m0 - k0;
     if (nxp <= 0 || nzp <= 0 || nyp <= 0) return;
-    const int total = nxp * nzp * nyp;
     const int lane = threadIdx.x & 31;
     // the normalised offsets depend on one coordinate each: divide once per row / column / level
     // (the same expressions, so the same doubles) instead of three times per block
@@ -1062,7 +1061,6 @@ __device__ void carve_ellipsoid(CarveCtx &c, int kind, double floor_level, doubl
         n_in += __popc(m);
     }
     __syncwarp();
-    (void)total;
     const float inv_nyp = 1.0f / (float)nyp;
     for (int q = lane; q < n_in * nyp; q += 32) {
         int k = (int)((float)q * inv_nyp);   // q / nyp, corrected below (q < 2^17: one step suffices)
