@@ -187,6 +187,29 @@ int ensure_tables(wg_engine *eng) {
     int rc = upload(eng, g.nodes, (size_t)g.n_nodes, &h->nodes);
     if (!rc) rc = upload(eng, g.floats, (size_t)g.n_floats, &h->floats);
     if (!rc) rc = upload(eng, g.child, (size_t)g.n_child, &h->child);
+    if (!rc) {   // legacy octave k starts 259 k Xoroshiro steps in, when no earlier bounded draw rejects
+        const auto step = [](uint64_t &lo, uint64_t &hi) {
+            const uint64_t x = hi ^ lo;
+            lo = ((lo << 49) | (lo >> 15)) ^ x ^ (x << 21);
+            hi = (x << 28) | (x >> 36);
+        };
+        std::vector<uint64_t> jumps((size_t)kLegacyPerlins * 128 * 2, 0);
+        uint64_t clo[128], chi[128];   // column j: the image of basis vector j
+        for (int j = 0; j < 128; j++) {
+            clo[j] = j < 64 ? 1ULL << j : 0;
+            chi[j] = j < 64 ? 0 : 1ULL << (j - 64);
+        }
+        for (int k = 0; k < kLegacyPerlins; k++) {
+            for (int b = 0; b < 128; b++)
+                for (int j = 0; j < 128; j++) {
+                    const uint64_t bit = b < 64 ? (clo[j] >> b) & 1 : (chi[j] >> (b - 64)) & 1;
+                    jumps[((size_t)k * 128 + b) * 2 + (j >> 6)] |= bit << (j & 63);
+                }
+            for (int j = 0; j < 128; j++)
+                for (int n = 0; n < 259; n++) step(clo[j], chi[j]);
+        }
+        rc = upload(eng, jumps.data(), jumps.size(), &h->legacy_jump);
+    }
     if (!rc) {   // the sine table as a quarter wave, checked against the full table
         std::vector<float> quarter(kSinQuarterPad, 0.0f);
         for (int i = 0; i < kSinQuarter; i++) quarter[i] = g.sin_table[i];

@@ -775,19 +775,58 @@ __device__ void walk_perlin(Xr &r) {
     for (int i = 0; i < 256; i++) (void)xr_bounded(r, (uint32_t)(256 - i));
 }
 
-// One thread per world: start states of the 40 legacy octaves (created in sequence from the
+// Whether walk_perlin from r would take a second draw for any of its bounded draws.
+__device__ bool walk_perlin_rejects(Xr r) {
+    (void)xr_next(r);
+    (void)xr_next(r);
+    (void)xr_next(r);
+    for (int i = 0; i < 256; i++) {
+        const uint32_t bound = (uint32_t)(256 - i);
+        const uint64_t v = (uint64_t)(uint32_t)xr_next(r) * bound;
+        if ((uint32_t)v < bound && (uint32_t)v < (0u - bound) % bound) return true;
+    }
+    return false;
+}
+
+// One CTA per world: start states of the 40 legacy octaves (created in sequence from the
 // "minecraft:terrain" random, lower -> upper -> main; interp_noise.c:44-75, noise.c:205-250)
-// and the aquifer's positional random factory (aquifer.c:126-136).
-__global__ void p2_legacy_kernel(const P2Tables *__restrict__ Tp, P2World *worlds, int n_worlds) {
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= n_worlds) return;
+// and the aquifer's positional random factory (aquifer.c:126-136).  An octave's walk takes 259
+// draws unless a bounded draw rejects (odds below 1e-7 per draw), so thread k jumps the stream's
+// state 259 k steps (a GF(2) matrix over the 128-bit state) and checks its own octave's draws;
+// if any octave rejects, thread 0 walks the stream in order instead.
+__global__ void __launch_bounds__(64) p2_legacy_kernel(const P2Tables *__restrict__ Tp, P2World *worlds) {
+    __shared__ int rejected;
     const P2Tables &T = *Tp;
-    P2World &W = worlds[w];
+    P2World &W = worlds[blockIdx.x];
+    const int k = threadIdx.x;
+    if (k == 0) rejected = 0;
+    __syncthreads();
     const Xr fork = seed_fork_of(W.seed);
-    Xr r = xr_make(T.terrain_lo ^ fork.lo, T.terrain_hi ^ fork.hi);
-    for (int k = 0; k < kLegacyPerlins; k++) {
+    const Xr r0 = xr_make(T.terrain_lo ^ fork.lo, T.terrain_hi ^ fork.hi);
+    if (k < kLegacyPerlins) {
+        const ulonglong2 *J = reinterpret_cast<const ulonglong2 *>(T.legacy_jump) + (size_t)k * 128;
+        Xr r{0, 0};
+#pragma unroll 8
+        for (int b = 0; b < 64; b++) {
+            const ulonglong2 m = J[b];
+            r.lo |= (uint64_t)(__popcll((m.x & r0.lo) ^ (m.y & r0.hi)) & 1) << b;
+        }
+#pragma unroll 8
+        for (int b = 0; b < 64; b++) {
+            const ulonglong2 m = J[64 + b];
+            r.hi |= (uint64_t)(__popcll((m.x & r0.lo) ^ (m.y & r0.hi)) & 1) << b;
+        }
         W.legacy_rng[k] = r;
-        walk_perlin(r);
+        if (walk_perlin_rejects(r)) atomicOr(&rejected, 1);
+    }
+    __syncthreads();
+    if (k != 0) return;
+    if (rejected) {
+        Xr r = r0;
+        for (int q = 0; q < kLegacyPerlins; q++) {
+            W.legacy_rng[q] = r;
+            walk_perlin(r);
+        }
     }
     Xr s = xr_from_seed(W.seed);
     Xr base;
@@ -1666,7 +1705,7 @@ __global__ void p2_probe_kernel(const P2Tables *__restrict__ Tp, const P2World *
 // Launchers
 // ------------------------------------------------------------------------------------
 void p2_launch_legacy(const P2Tables *T, P2World *worlds, int n_worlds, cudaStream_t s) {
-    p2_legacy_kernel<<<(n_worlds + 63) / 64, 64, 0, s>>>(T, worlds, n_worlds);
+    if (n_worlds > 0) p2_legacy_kernel<<<n_worlds, 64, 0, s>>>(T, worlds);
 }
 
 void p2_launch_build(const P2Tables *T, P2World *worlds, int n_worlds, cudaStream_t s) {

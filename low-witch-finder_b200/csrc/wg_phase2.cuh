@@ -106,6 +106,9 @@ struct P2Tables {
     int root_offset, root_factor, root_peak;
     // Mth.SIN as a quarter wave: entries 0..16384 (padded to kSinQuarterPad); the host checks that
     // they and sin_half_turn (entry 32768) rebuild all 65,536 entries bit for bit
+    // the legacy octaves' start-state jumps: for octave k, 128 rows of two words whose parity with
+    // the 128-bit Xoroshiro state (lo = bits 0..63) gives bit b of the state 259 k steps later
+    const uint64_t *legacy_jump;
     const float *sin_quarter;
     float sin_half_turn;
     BiomeTree trees[kBiomeTrees];
