@@ -726,22 +726,23 @@ __device__ __forceinline__ int p2_block_at(const P2Tables &T, const P2World &W, 
 __device__ __forceinline__ int carve_index(int lx, int y, int lz) { return ((lz & 15) << 4) | (lx & 15) | ((y + 64) << 8); }
 
 // Surface height (NOT_AIR predicate, y + 1; phase2.c:318-334 and :438-456) of a column of the job's
-// chunk, from the job's per-block states (p2_states_kernel).  The 384 levels are read eight at a
+// chunk, from the job's per-block states (p2_states_kernel).  The 384 levels are read sixteen at a
 // time (independent loads) and tested top-down in order.
 __device__ int p2_height(const P2Tables &T, const P2World &W, const P2Chunk &J, int x, int z, bool carved) {
     (void)T;
     (void)W;
-    static_assert((320 + 64) % 8 == 0, "levels in groups of eight");
-    for (int y0 = 319; y0 >= -64; y0 -= 8) {
-        uint8_t cv[8], pre[8];
+    constexpr int kGroup = 16;
+    static_assert((320 + 64) % kGroup == 0, "levels in whole groups");
+    for (int y0 = 319; y0 >= -64; y0 -= kGroup) {
+        uint8_t cv[kGroup], pre[kGroup];
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
+        for (int k = 0; k < kGroup; k++) {
             const int ci = carve_index(x & 15, y0 - k, z & 15);
             cv[k] = carved ? J.cells[ci] : (uint8_t)CV_UNCHANGED;
             pre[k] = J.states[ci];
         }
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
+        for (int k = 0; k < kGroup; k++) {
             const int st = cv[k] != CV_UNCHANGED ? (int)cv[k] : (int)(pre[k] & 15u);   // CV_* = BS_* codes
             if (st != BS_AIR) return y0 - k + 1;
         }
@@ -1463,26 +1464,43 @@ __device__ int tree_search(const BiomeTree &g, const int64_t np[6]) {
 // (mid_x >> 2, y >> 2, mid_z >> 2), quantised through float, and the nearest leaf of the tree.
 // The offset spline is evaluated at the same quart column (the reference asks for block
 // (qx * 4, qz * 4) >> 2, which is qx, qz again).
-__device__ int p2_biome_params(const P2Tables &T, const P2World &W, int tree, int mid_x, int mid_z, int y,
-                               int64_t np[6]) {
-    const int qx = mid_x >> 2, qy = y >> 2, qz = mid_z >> 2;
+// The y-independent half of the six climate parameters at block column (mid_x, mid_z).
+struct ColumnClimate {
+    double temperature, humidity, c, e, w, offset;
+};
+__device__ ColumnClimate p2_column_climate(const P2Tables &T, const P2World &W, int mid_x, int mid_z) {
     TerrainInfo ti;
-    p2_terrain(T, W, qx, qz, ti);
-    const double temperature = p2_dbl(T, W, Q_TEMPERATURE, ti.sx, 0.0, ti.sz);
-    const double humidity = p2_dbl(T, W, Q_VEGETATION, ti.sx, 0.0, ti.sz);
-    double offset, factor;
-    p2_offset_factor(T, ti, offset, factor);
+    p2_terrain(T, W, mid_x >> 2, mid_z >> 2, ti);
+    ColumnClimate cc;
+    cc.temperature = p2_dbl(T, W, Q_TEMPERATURE, ti.sx, 0.0, ti.sz);
+    cc.humidity = p2_dbl(T, W, Q_VEGETATION, ti.sx, 0.0, ti.sz);
+    double factor;
+    p2_offset_factor(T, ti, cc.offset, factor);
+    cc.c = ti.c;
+    cc.e = ti.e;
+    cc.w = ti.w;
+    return cc;
+}
+
+// The climate point at height y (depth from the column's offset) and the R-tree's biome.
+__device__ int p2_biome_at_y(const P2Tables &T, int tree, const ColumnClimate &cc, int y, int64_t np[6]) {
+    const int qy = y >> 2;
     const double yq = (double)(qy * 4);
-    const double depth = mc_lerp(mc_clamp((yq - -64.0) / (320.0 - -64.0), 0.0, 1.0), 1.5, -1.5) + offset;
-    np[0] = (int64_t)((float)temperature * 10000.0f);
-    np[1] = (int64_t)((float)humidity * 10000.0f);
-    np[2] = (int64_t)((float)ti.c * 10000.0f);
-    np[3] = (int64_t)((float)ti.e * 10000.0f);
+    const double depth = mc_lerp(mc_clamp((yq - -64.0) / (320.0 - -64.0), 0.0, 1.0), 1.5, -1.5) + cc.offset;
+    np[0] = (int64_t)((float)cc.temperature * 10000.0f);
+    np[1] = (int64_t)((float)cc.humidity * 10000.0f);
+    np[2] = (int64_t)((float)cc.c * 10000.0f);
+    np[3] = (int64_t)((float)cc.e * 10000.0f);
     np[4] = (int64_t)((float)depth * 10000.0f);
-    np[5] = (int64_t)((float)ti.w * 10000.0f);
+    np[5] = (int64_t)((float)cc.w * 10000.0f);
     const BiomeTree &g = T.trees[tree];
     const int leaf = tree_search(g, np);
     return leaf >= 0 ? g.biome[leaf] : -1;
+}
+
+__device__ int p2_biome_params(const P2Tables &T, const P2World &W, int tree, int mid_x, int mid_z, int y,
+                               int64_t np[6]) {
+    return p2_biome_at_y(T, tree, p2_column_climate(T, W, mid_x, mid_z), y, np);
 }
 
 __device__ __forceinline__ int64_t floor_div16(int64_t v) { return v >= 0 ? v / 16 : -((-v + 15) / 16); }
@@ -1546,7 +1564,7 @@ __global__ void __launch_bounds__(128) p2_biome_chunks_kernel(const P2Tables *__
     need[k] = settled ? 0 : 1;
 }
 
-constexpr int kFinishThreads = 64;
+constexpr int kFinishThreads = 96;   // 63 footprint columns, the chunk centre, the centre's climate
 
 __global__ void __launch_bounds__(kFinishThreads) p2_finish_kernel(const P2Tables *__restrict__ Tp,
                                                                    const P2World *__restrict__ worlds,
@@ -1555,6 +1573,7 @@ __global__ void __launch_bounds__(kFinishThreads) p2_finish_kernel(const P2Table
                                                                    P2Result *out) {
     __shared__ int pre_h[64], post_h[64], wet[64];
     __shared__ int size_x, size_z;
+    __shared__ ColumnClimate centre;
     const P2Tables &T = *Tp;
     const P2Hut H = huts[blockIdx.x];
     const P2Chunk &J = jobs[H.job];
@@ -1588,6 +1607,8 @@ __global__ void __launch_bounds__(kFinishThreads) p2_finish_kernel(const P2Table
     } else if (t == 63) {
         const int mid_x = (H.hut_x >> 4) * 16 + 8, mid_z = (H.hut_z >> 4) * 16 + 8;
         pre_h[63] = p2_height(T, W, J, mid_x, mid_z, false);
+    } else if (t == 64) {   // the y-independent climate at the chunk centre, beside the column work
+        centre = p2_column_climate(T, W, (H.hut_x >> 4) * 16 + 8, (H.hut_z >> 4) * 16 + 8);
     }
     __syncthreads();
     if (t != 0) return;
@@ -1596,7 +1617,7 @@ __global__ void __launch_bounds__(kFinishThreads) p2_finish_kernel(const P2Table
         const int mid_x = (H.hut_x >> 4) * 16 + 8, mid_z = (H.hut_z >> 4) * 16 + 8;
         const int y = pre_h[63] - 1;
         int64_t np[6];
-        const int winner = p2_biome_params(T, W, tree, mid_x, mid_z, y, np);
+        const int winner = p2_biome_at_y(T, tree, centre, y, np);
         for (int a = 0; a < 6; a++) R.biome_t[a] = np[a];
         R.biome_qx = mid_x >> 2;
         R.biome_qy = y >> 2;
