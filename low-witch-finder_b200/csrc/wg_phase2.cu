@@ -893,32 +893,38 @@ __global__ void __launch_bounds__(kGridThreads) p2_grid_kernel(const P2Tables *_
                                                                const P2World *__restrict__ worlds, P2Chunk *jobs) {
     // CTA (job, gx): the five corner columns c = gx * 5 + k of one cell row, so a job's grid is five
     // short chains on five SMs instead of one long one
+    // short chains on five SMs instead of one long one.  Threads 0..4 evaluate the columns' terrain
+    // points while the others take the samples that do not need them (the blended noise of every
+    // main sample and the three noodle children); the density columns follow the barrier.
     __shared__ TerrainPoint tp[5];
     __shared__ double jag[5];
+    __shared__ double base[5 * kGridYs];
     const P2Tables &T = *Tp;
     P2Chunk &J = jobs[blockIdx.x];
     const P2World &W = worlds[J.world];
     const int gx = blockIdx.y;
     const int cx0 = J.chunk_x * 4, cz0 = J.chunk_z * 4;   // first cell of the chunk
-    for (int k = threadIdx.x; k < 5; k += blockDim.x) {
-        const int cell_x = cx0 + gx, cell_z = cz0 + k;
+    const int t = threadIdx.x;
+    if (t < 5) {
+        const int cell_x = cx0 + gx, cell_z = cz0 + t;
         TerrainInfo ti;
         p2_terrain(T, W, cell_x, cell_z, ti);
-        tp[k] = p2_point_261(T, ti);
-        jag[k] = p2_jagged(T, W, (double)tp[k].peaks, cell_x * 4, cell_z * 4);
+        tp[t] = p2_point_261(T, ti);
+        jag[t] = p2_jagged(T, W, (double)tp[t].peaks, cell_x * 4, cell_z * 4);
+    } else {
+        for (int q = t - 5; q < 4 * 5 * kGridYs; q += (int)blockDim.x - 5) {
+            const int which = q / (5 * kGridYs), rem = q % (5 * kGridYs);   // 0: main, 1..3: noodle
+            const int k = rem / kGridYs, i = rem % kGridYs, c = gx * 5 + k;
+            const int bx = (cx0 + gx) * 4, bz = (cz0 + k) * 4, y = -64 + i * 8;
+            if (which == 0) base[rem] = p2_blended(T, W, bx, y, bz);
+            else J.noodle[which - 1][c][i] = p2_noodle_child(T, W, which, bx, y, bz);
+        }
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < 5 * kGridYs; q += blockDim.x) {
+    for (int q = t; q < 5 * kGridYs; q += blockDim.x) {
         const int k = q / kGridYs, i = q % kGridYs, c = gx * 5 + k;
         const int bx = (cx0 + gx) * 4, bz = (cz0 + k) * 4, y = -64 + i * 8;
-        const double base = p2_blended(T, W, bx, y, bz);
-        J.main[c][i] = p2_noise_column(T, W, bx, y, bz, tp[k], jag[k], base);
-    }
-    for (int q = threadIdx.x; q < 3 * 5 * kGridYs; q += blockDim.x) {
-        const int which = q / (5 * kGridYs), rem = q % (5 * kGridYs);
-        const int k = rem / kGridYs, i = rem % kGridYs, c = gx * 5 + k;
-        const int bx = (cx0 + gx) * 4, bz = (cz0 + k) * 4, y = -64 + i * 8;
-        J.noodle[which][c][i] = p2_noodle_child(T, W, which + 1, bx, y, bz);
+        J.main[c][i] = p2_noise_column(T, W, bx, y, bz, tp[k], jag[k], base[q]);
     }
 }
 
