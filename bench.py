@@ -55,24 +55,42 @@ def measured_peaks() -> dict:
 
 
 # ------------------------------------------------------------------------------------------
-# algorithmic work model of the climate kernel (lane-operations, counted from the source)
+# algorithmic work model of the phase-1 kernels (lane-operations, counted from the source)
 # ------------------------------------------------------------------------------------------
 OPS_PERLIN_BUILD = 7160      # 259 Xoroshiro128++ steps, 256 Lemire draws + byte swaps, RNG derivation
-OPS_Y0_SAMPLE = 244          # 14 table lookups, 62 FP64 ops (x2 issue slots), bit-op gradients
+OPS_Y0_SAMPLE = 244          # FP64 y=0 sample: 14 table lookups, 62 FP64 ops (x2 issue slots), bit-op gradients
+# FP32-core y=0 sample: 14 table lookups (x4), the FP64 coordinate reduction (16 FP64 ops x2 issue
+# slots), 24 gradient-component loads, 51 FP32 ops (3 offsets, 8 gradients x3, 2 fades x5, 7 lerps x2)
+# and the FMA into the running sum
+OPS_Y0_SAMPLE_F32 = 56 + 32 + 24 + 51 + 1
+# 3-D FP64 sample of the cave noises: 14 lookups (x4), 96 FP64 ops (x2), 24 gradient-component loads
+OPS_3D_SAMPLE = 56 + 192 + 24
 OPS_REGION = 40              # java.util.Random placement (2 x nextInt(24)) + coordinates
+# dram__bytes_read.sum + dram__bytes_write.sum per launch, from ncu on `bench.py --profile 1048576`
+# (one launch of each kernel on 2^20 seeds read from a list in HBM; a 2^24-seed step runs 16 such
+# launches, each over its own 2^20 seeds, so the per-launch figure is the full step's per launch)
+TRAFFIC = {"climate_kernel": None, "entrance_kernel": None, "source": "not yet captured"}
 BYTES_PER_SEED_IN = 8        # the int64 seed read from HBM
 BYTES_PER_RECORD = 12        # (unit, offset, count) per seed with climate survivors
 BYTES_PER_SURVIVOR = 4       # region offset per climate survivor
 
 
-def climate_work(st: dict, n_seeds: int, n_regions: int) -> tuple[float, float]:
+def climate_work(st: dict, n_seeds: int, n_regions: int, fp32: bool) -> tuple[float, float]:
     """(lane-ops, algorithmic bytes) of the climate kernel over a request, from its funnel."""
     th = st["tier_hist"]
     rh = st["reject_hist"]
     y0 = sum((t + 2) * th[t] for t in range(7)) + 12 * rh[1] + 18 * (rh[2] + st["climate_survivors"])
-    ops = 18 * n_seeds * OPS_PERLIN_BUILD + y0 * OPS_Y0_SAMPLE + n_seeds * n_regions * OPS_REGION
+    ops = (18 * n_seeds * OPS_PERLIN_BUILD + y0 * (OPS_Y0_SAMPLE_F32 if fp32 else OPS_Y0_SAMPLE)
+           + n_seeds * n_regions * OPS_REGION)
     nbytes = n_seeds * BYTES_PER_SEED_IN + st["climate_survivors"] * BYTES_PER_SURVIVOR
     return float(ops), float(nbytes)
+
+
+def entrance_work(st: dict) -> float:
+    """Lane-ops of the entrance kernel: 18 tables per record (a seed unit with climate survivors),
+    36 3-D samples per survivor (18 slots at y = 50 and 60) plus its 12 octave sums and decision."""
+    n_rec, n_surv = st["records"], st["climate_survivors"]
+    return float(n_rec * 18 * OPS_PERLIN_BUILD + n_surv * (36 * OPS_3D_SAMPLE + 12 * 40 + 120))
 
 
 class ClockSampler:
@@ -312,6 +330,90 @@ def serving_measure(wg, n_req: int = 200) -> dict:
     return out
 
 
+def sorted_hits(wg, out_dev, n: int) -> np.ndarray:
+    """The first n device candidates (wg_candidate rows of out_dev), sorted by (seed_index, rz, rx)."""
+    n = min(int(n), out_dev.shape[0])
+    rows = np.frombuffer(out_dev[:n].cpu().numpy().tobytes(), dtype=wg.CANDIDATE_DTYPE)
+    return np.sort(rows, order=["seed_index", "rz", "rx"])
+
+
+def splitmix_seeds(first: int, n: int) -> np.ndarray:
+    """Seeds first .. first + n - 1 of the config-2 stream, splitmix64(2 + i), as int64."""
+    idx = np.arange(first, first + n, dtype=np.uint64) + np.uint64(GEN_BASE)
+    with np.errstate(over="ignore"):   # splitmix64 over the whole array, mod 2^64
+        z = idx + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return z.view(np.int64)
+
+
+def profile_case(wg, eng, opts, args, local: int) -> None:
+    """--profile N: the headline step (seed list resident in HBM, wg_seed_check_device) on the first
+    N seeds of the stream, --warmup + --steps times, and nothing else: the command ncu captures."""
+    import torch
+    n = int(args.profile)
+    seeds = torch.from_numpy(splitmix_seeds(0, n)).to(f"cuda:{local}")
+    cap = 1 << 16
+    out = torch.zeros((cap, 4), dtype=torch.int64, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream()
+    found, st = 0, {}
+    for _ in range(args.warmup + args.steps):
+        found, st = eng.seed_check_device(seeds.data_ptr(), 0, n, RECT, MAX_HEIGHT, opts, out.data_ptr(), cap,
+                                          stream.cuda_stream)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_case": {"seeds": n, "noise_core": args.noise_core, "found": found,
+                                       "kernel_launches": st["kernel_launches"], "kernel_ms": st["kernel_ms"],
+                                       "records": st["records"], "climate_survivors": st["climate_survivors"],
+                                       "rechecks": st["rechecks"]}}), flush=True)
+
+
+def noise_core_measure(wg, eng, args, step_device, stream, flush, headline: dict) -> dict:
+    """The other noise core on the same device-resident step: seeds/s of both, their ratio, whether
+    the hit sets and funnels agree, how often the FP32 core re-took a gate in FP64, and the measured
+    |FP32 - FP64| of each climate noise (wg_noise_probe, 256 seeds x 4,096 climate points)."""
+    import torch
+    other = "fp64" if args.noise_core == "fp32" else "fp32"
+    eng.set_noise_core(other)
+    for _ in range(args.warmup):
+        step_device()
+    times = []
+    found, st = 0, {}
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        found, st = step_device()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    eng.set_noise_core(args.noise_core)
+    ms_other = sum(times) / len(times)
+    runs = {args.noise_core: headline, other: {"seeds_per_s": N_SEEDS / (ms_other / 1e3), "ms_per_step": ms_other,
+                                               "found": found, "reject_hist": st["reject_hist"],
+                                               "tier_hist": st["tier_hist"], "rechecks": st["rechecks"],
+                                               "kernel_ms": st["kernel_ms"]}}
+    same = (runs["fp32"]["found"] == runs["fp64"]["found"] and runs["fp32"]["reject_hist"] == runs["fp64"]["reject_hist"]
+            and runs["fp32"]["tier_hist"] == runs["fp64"]["tier_hist"])
+    rng = np.random.default_rng(7)
+    xz = (4 * rng.integers(-1_870_000, 1_870_000, size=(4096, 2)) + 2).astype(np.float64)
+    seeds = [wg.splitmix64(GEN_BASE + i) for i in range(256)]
+    err = {}
+    for noise in ("erosion", "temperature", "ridge", "continentalness"):
+        v32, v64 = eng.noise_probe(seeds, noise, xz)
+        err[noise] = float(np.abs(v32 - v64).max())
+    scanned = N_SEEDS * (RECT[1] - RECT[0]) * (RECT[3] - RECT[2])
+    return {"fp32": runs["fp32"], "fp64": runs["fp64"],
+            "fp32_over_fp64": runs["fp64"]["ms_per_step"] / runs["fp32"]["ms_per_step"],
+            "same_hits_and_funnel": bool(same),
+            "recheck_fraction": runs["fp32"]["rechecks"] / scanned,
+            "max_abs_err": err,
+            "max_abs_err_note": ("|FP32 core - FP64| of each y = 0 climate noise over 256 seeds x 4,096 climate points; "
+                                 "the cave densities (entrance, spaghetti, cheese) and phase 2 run in FP64 only, so "
+                                 "their error is 0 by construction"),
+            "bound": "the step's kernels; both cores on the same seeds, CUDA events per step"}
+
+
 def run_reference(args) -> None:
     """--impl reference: the reference's CPU scanner on the host cores, same metric."""
     rank = int(os.environ.get("RANK", "0"))
@@ -345,6 +447,11 @@ def main() -> None:
     ap.add_argument("--phase2-only", action="store_true",
                     help="one phase-1 pass for its survivors, then only the phase-2 measurement (a short "
                          "command for profiling the phase-2 kernels)")
+    ap.add_argument("--noise-core", choices=("fp32", "fp64"), default="fp32",
+                    help="noise core of the headline (the other core is measured beside it)")
+    ap.add_argument("--profile", type=int, default=0, metavar="SEEDS",
+                    help="profiling case only: the headline step on SEEDS device-resident seeds, --warmup "
+                         "untimed steps then --steps steps, no other measurement (a short command for ncu)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -362,18 +469,16 @@ def main() -> None:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
-    eng = wg.Engine(local)
+    eng = wg.Engine(local, noise_core=args.noise_core)
     opts = wg.make_opts(VERSION)
+    if args.profile:
+        profile_case(wg, eng, opts, args, local)
+        eng.close()
+        return
     first = rank * N_SEEDS                       # weak scaling: each rank owns 2^24 seeds of the stream
     seeds_host = torch.empty(N_SEEDS, dtype=torch.int64, pin_memory=True)
     seeds_np = seeds_host.numpy()
-    idx = np.arange(first, first + N_SEEDS, dtype=np.uint64) + np.uint64(GEN_BASE)
-    with np.errstate(over="ignore"):   # splitmix64 over the whole array, mod 2^64
-        z = idx + np.uint64(0x9E3779B97F4A7C15)
-        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
-        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
-        z = z ^ (z >> np.uint64(31))
-    seeds_np[:] = z.view(np.int64)
+    seeds_np[:] = splitmix_seeds(first, N_SEEDS)
     if args.phase2_only:
         res = eng.seed_check(seeds=seeds_np, rect=RECT, max_height=MAX_HEIGHT, opts=opts)
         line = {"phase2": phase2_measure(eng, res.candidates, opts, cpu=False)}
@@ -421,6 +526,7 @@ def main() -> None:
         if world > 1:
             dist.barrier()
     total_ms = sum(times)
+    hits_headline = sorted_hits(wg, out_dev, found)
 
     # ---- end to end through the public host API ----
     e2e_ms = []
@@ -453,20 +559,28 @@ def main() -> None:
         sm_count = torch.cuda.get_device_properties(local).multi_processor_count
         max_mhz = float(peaks.get("sm_max_mhz", 1965.0))
         peak_ops = sm_count * 128 * max_mhz * 1e6
-        ops, nbytes = climate_work(stats, N_SEEDS, n_regions)
+        fp32 = args.noise_core == "fp32"
+        ops, nbytes = climate_work(stats, N_SEEDS, n_regions, fp32)
         launch_ms = kernel_ms[0] / max(1, kernel_launches[0])
         ops_per_launch = ops / max(1, stats["kernel_launches"][0])
         bytes_per_launch = nbytes / max(1, stats["kernel_launches"][0])
         achieved = ops_per_launch / (launch_ms / 1e3)
+        ent_ms = kernel_ms[1] / max(1, kernel_launches[1])
+        ent_ops = entrance_work(stats) / max(1, stats["kernel_launches"][1])
         hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
         cs = clocks.summary()
+        headline = {"seeds_per_s": value, "ms_per_step": total_ms / args.steps, "found": found,
+                    "reject_hist": stats["reject_hist"], "tier_hist": stats["tier_hist"],
+                    "rechecks": stats["rechecks"], "kernel_ms": [k / args.steps for k in kernel_ms]}
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if fp32 else "f64", "data": "synthetic",
             "config": {"workload": "config 2: Seed Check phase 1, 2^24 splitmix64(2 + i) world seeds per GPU x 9x9 "
                                    "swamp-hut regions (1.36e9 (seed, region) checks), floor -50, rules "
-                                   f"{VERSION}, bit-exact FP64", "seeds_per_gpu": N_SEEDS,
+                                   f"{VERSION}, " + ("FP32 noise core with FP64 recheck (verdicts equal the FP64 "
+                                                     "path's)" if fp32 else "bit-exact FP64"),
+                       "noise_core": args.noise_core, "seeds_per_gpu": N_SEEDS,
                        "regions_per_seed": n_regions, "max_height": MAX_HEIGHT, "parallelism": f"seed-shard x{world}",
                        "l2": "256 MiB buffer written between timed steps (outside the events); seed input 134 MB",
                        "inputs": "seed list resident in HBM (value); pinned host seeds via wg_seed_check (e2e)"},
@@ -482,15 +596,30 @@ def main() -> None:
                 "peak_source": f"nominal INT32/FP32 issue rate: {sm_count} SMs x 128 lanes x {max_mhz:.0f} MHz "
                                "(sm_max_mhz of MEASURED_PEAKS.json); the kernel is not HBM- or tensor-bound",
                 "ops_per_launch": ops_per_launch, "launch_ms": launch_ms,
-                # dram__bytes_read.sum + dram__bytes_write.sum of one climate launch of 2^20 seeds x 9x9
-                # (profiles/climate_kernel_2p20_seeds.md): every table and list stays on chip
-                "traffic": 82e3, "traffic_unit": "bytes per launch",
+                "ops_model": ("18 Perlin tables per seed x 7,160 lane-ops, per y=0 sample "
+                              f"{OPS_Y0_SAMPLE_F32 if fp32 else OPS_Y0_SAMPLE} lane-ops x the samples the funnel "
+                              "implies, 40 per (seed, region) placement"),
+                "traffic": TRAFFIC["climate_kernel"], "traffic_unit": "bytes per launch",
+                "traffic_source": TRAFFIC["source"],
+                "algorithmic_bytes": bytes_per_launch,
                 "hbm": {"achieved_gbs": bytes_per_launch / (launch_ms / 1e3) / 1e9, "peak_gbs": hbm_peak,
                         "frac": bytes_per_launch / (launch_ms / 1e3) / 1e9 / hbm_peak,
                         "peak_source": "hbm_gbs of MEASURED_PEAKS.json"},
+                "entrance_kernel": {
+                    "bound": "issue", "unit": "Tlane-op/s", "achieved": ent_ops / (ent_ms / 1e3) / 1e12,
+                    "peak": peak_ops / 1e12, "frac": ent_ops / (ent_ms / 1e3) / peak_ops, "ops_per_launch": ent_ops,
+                    "launch_ms": ent_ms, "traffic": TRAFFIC["entrance_kernel"], "traffic_unit": "bytes per launch",
+                    "ops_model": ("18 Perlin tables per record x 7,160 lane-ops, per climate survivor 36 3-D samples "
+                                  f"x {OPS_3D_SAMPLE} lane-ops + 600 for the octave sums and the decision")},
             },
             "clocks": cs,
         }
+        if world == 1:
+            nc = noise_core_measure(wg, eng, args, step_device, stream, flush, headline)
+            other = "fp64" if fp32 else "fp32"
+            hits_other = sorted_hits(wg, out_dev, nc[other]["found"])
+            nc["same_hits_and_funnel"] = bool(nc["same_hits_and_funnel"] and np.array_equal(hits_other, hits_headline))
+            line["noise_core"] = nc
         line["phase2"] = phase2_measure(eng, res.candidates, opts, cpu=(world == 1 and not args.no_cpu_baseline))
         line["deep_dive"] = deep_measure(eng, opts)
         line["biome_map"] = biome_measure(eng)

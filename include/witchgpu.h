@@ -6,8 +6,7 @@
  * matching the one-ctx-per-thread rule of the reference's lysh API
  * (engine/tools/lysh/src/eval.h:40-47).
  *
- * Each entry point names the reference interface it replaces.  A ctypes / cgo binding of
- * these is shown in INTEGRATION.md.
+ * Each entry point names the reference interface it replaces.
  */
 #ifndef WITCHGPU_H
 #define WITCHGPU_H
@@ -61,6 +60,8 @@ typedef struct {
     double kernel_ms[3];          /* their summed device time (CUDA events around each launch) */
     double gpu_ms;                /* device time of the whole call, CUDA events on its stream */
     double wall_ms;               /* host wall time of the call */
+    int64_t rechecks;             /* FP32 noise core: climate gate decisions re-taken in FP64 */
+    int64_t records;              /* seed units with climate survivors (tables the entrance kernel builds / 18) */
 } wg_scan_stats;
 
 /* Create an engine on CUDA device `device`: context binding, stream, noise tables and work
@@ -73,6 +74,29 @@ void wg_engine_close(wg_engine *e);
 
 /* Message of the engine's last failure ("" if none). */
 const char *wg_engine_error(const wg_engine *e);
+
+/* Noise core of the phase-1 climate gates (erosion tiers, temperature, ridge).
+ *   WG_NOISE_FP32 (the default): samples in FP32 after an FP64 coordinate reduction, gates
+ *     decided from the FP32 sums outside a derived error band and re-taken in FP64 inside it,
+ *     so every verdict equals the FP64 path's; wg_scan_stats.rechecks counts the re-takes.
+ *   WG_NOISE_FP64: every sample in FP64 in the reference's operation order.
+ *   WG_NOISE_FP32_RECHECK_ALL: the FP32 core with every gate re-taken in FP64, a check mode that
+ *     runs the recheck path on every decision (slow; for tests of that path).
+ * The reference has the same choice as a build flag, without the recheck
+ * (PHASE1_FP32_CORE, engine/gpu/low54/device_noise.h:132-160).  WG_ERR_ARG for other values. */
+#define WG_NOISE_FP32 0
+#define WG_NOISE_FP64 1
+#define WG_NOISE_FP32_RECHECK_ALL 2
+int wg_engine_set_noise_core(wg_engine *e, int core);
+
+/* The FP32 core's measured error: out64[b * n_points + i] = the y = 0 DoublePerlin value of climate
+ * noise `noise` in world seeds[b] at noise-space point (xz[2i], 0, xz[2i + 1]) in FP64 (the
+ * reference's lysh_dblnoise_sample_y0, engine/tools/lysh/src/noise.c:320-342), out32[...] = the
+ * same value from the FP32 core's samples.  noise: 0 erosion, 1 temperature, 2 ridge,
+ * 3 continentalness, 4 erosion_large, 5 temperature_large, 6 continentalness_large.  Host
+ * buffers; n_seeds * n_points <= 2^26. */
+int wg_noise_probe(wg_engine *e, const int64_t *seeds, uint64_t n_seeds, int noise, const double *xz,
+                   uint64_t n_points, double *out32, double *out64);
 
 /* lysh's --version / --preset names -> option bits
  * (engine/tools/lysh/src/main.c:104-132).  0 on success, WG_ERR_ARG if unknown.  Each sets only
@@ -125,11 +149,16 @@ int wg_phase1_codes(wg_engine *e, const int64_t *seeds, uint64_t gen_base, uint6
  *
  * Limits: n_seeds <= 65,536 and at most 4,096 regions per seed per call, else WG_ERR_CAPACITY;
  * WG_ERR_CAPACITY also when a call's climate survivors exceed 1,048,576 (or its unit records
- * 131,072, or its deep candidates 65,536).  The work lists live in one 6 MiB file-scope
- * __device__ array that every GPU loading the library holds until the process exits.  The
- * first call on a device uploads the noise tables and looks up that array's address, so make
- * it before any stream capture.  All calls share the array: calls that overlap on the GPU
- * (other streams or host threads) race on it. */
+ * 131,072, or its deep candidates 65,536).  Unlike wg_seed_check_device, a full list is not
+ * re-run in smaller pieces, so the practical size is set by the climate survivors: about 1.7 %
+ * of regions pass the climate gates at the usual rules, so keep n_seeds * regions below about
+ * 2^20 / 0.017 = 6e7 checks per call (about 15,000 seeds on a full 64 x 64 rect, 65,536 seeds up
+ * to ~900 regions).  The work lists live in one 6 MiB file-scope __device__ array that every GPU
+ * loading the library holds until the process exits.  The first call on a device uploads the
+ * noise tables and looks up that array's address, so make it before any stream capture.  Every
+ * call is synchronous: it waits for its stream and reads the list counters back to the host.
+ * All calls share the array: calls that overlap on the GPU (other streams or host threads) race
+ * on it. */
 int wg_seed_check_noalloc(const int64_t *d_seeds, uint64_t gen_base, uint32_t n_seeds,
                           const wg_opts *opts, int max_height, int salt,
                           int rx0, int rx1, int rz0, int rz1,
@@ -227,6 +256,29 @@ typedef struct {
  * direction; the layout-catalogue direction is wg_deep_solve. */
 int wg_deep_starts(wg_engine *e, const int64_t *s48, int64_t s48_base, uint64_t n,
                    int rx0, int rx1, int rz0, int rz1, wg_deep_start *out, uint64_t cap, uint64_t *n_out);
+
+/* A hut on a mineshaft start chunk whose carver state is a catalogued layout. */
+typedef struct {
+    uint64_t seed_index;         /* index of the structure seed in the request */
+    int64_t s48;                 /* structure seed */
+    int32_t rx, rz;              /* hut region */
+    int32_t chunk_x, chunk_z;    /* hut chunk = mineshaft start chunk */
+    int64_t carver;              /* its setLargeFeatureSeed state = the catalogued layout */
+    uint32_t value;              /* that layout's catalogue value (air above the hut floor: hi | lo << 10) */
+    uint32_t pad;
+} wg_sweep_match;
+
+/* The Deep Dive forward sweep with the layout-catalogue probe (hut_lookup_v4 without --solve:
+ * sweepProbeKernel, engine/gpu/hut_lookup_v4_source.cu:77-99, driven per structure seed at
+ * :1504-1530): for every structure seed s48[0..n) (or, when s48 is NULL, s48_base + i) and every
+ * region of [rx0,rx1) x [rz0,rz1), the region's swamp-hut chunk, whether a mineshaft starts there,
+ * and for each start whether its carver state is one of layouts[0..n_layouts) (values[k] is layout
+ * k's catalogue value; values may be NULL).  out receives the first cap matches sorted by
+ * (seed_index, rz, rx); *n_out = all of them (WG_ERR_CAPACITY past 2^20 in one call); starts (may
+ * be NULL) receives each structure seed's number of starts. */
+int wg_deep_sweep(wg_engine *e, const uint64_t *layouts, const uint32_t *values, uint64_t n_layouts,
+                  const int64_t *s48, int64_t s48_base, uint64_t n, int rx0, int rx1, int rz0, int rz1,
+                  wg_sweep_match *out, uint64_t cap, uint64_t *n_out, uint64_t *starts);
 
 /* The Deep Dive terrain stage (hut_lookup_v4 --spots, engine/gpu/hut_lookup_v4_source.cu:1262-1290):
  * for each spot (s48[i], chunk_x[i], chunk_z[i]), the 65,536 world seeds (u << 48) | s48[i],
@@ -341,6 +393,22 @@ typedef struct wg_server wg_server;
  * session API (engine/tools/lysh/src/eval.h:180-205) and hunt.py's worker protocol
  * (hunt.py:1276-1332) are the interfaces it batches. */
 int wg_server_open(int device, uint64_t max_queued_seeds, wg_server **out);
+
+/* Server settings (all-zero = the defaults of wg_server_open). */
+typedef struct {
+    uint64_t max_queued_seeds;   /* host-queued seeds at most (0 = 2^30) */
+    uint64_t arena_seeds;        /* device seed slots (0 = a quarter of the free HBM, at most 2^28);
+                                    a job with more seeds is refused at submit (WG_ERR_CAPACITY) */
+    uint64_t batch_checks;       /* (seed, region) checks per batch (0 = 2^25) */
+    uint64_t fail_job;           /* host-side fault injection for tests: every batch that holds the
+                                    job with this id fails before launch (0 = none) */
+} wg_server_config;
+
+/* wg_server_open with explicit settings.  A failed batch fails no job by itself while the engine
+ * still works: its jobs run again one at a time, and only a job that fails alone ends with the
+ * error (wg_job_status.status); the others' results are those they get alone.  A broken CUDA
+ * context ends every job, queued ones included. */
+int wg_server_open_config(int device, const wg_server_config *cfg, wg_server **out);
 
 /* Queue a job; *job_id identifies it.  Non-blocking. */
 int wg_server_submit(wg_server *s, const wg_job *job, uint64_t *job_id);

@@ -46,29 +46,46 @@ class Stats(C.Structure):
     _fields_ = [("scanned", C.c_int64), ("accepted", C.c_int64), ("climate_survivors", C.c_int64),
                 ("deep_candidates", C.c_int64), ("reject_hist", C.c_int64 * 11), ("tier_hist", C.c_int64 * 7),
                 ("batches", C.c_int64), ("retries", C.c_int64), ("kernel_launches", C.c_int64 * 3),
-                ("kernel_ms", C.c_double * 3), ("gpu_ms", C.c_double), ("wall_ms", C.c_double)]
+                ("kernel_ms", C.c_double * 3), ("gpu_ms", C.c_double), ("wall_ms", C.c_double),
+                ("rechecks", C.c_int64), ("records", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {"scanned": self.scanned, "accepted": self.accepted, "climate_survivors": self.climate_survivors,
                 "deep_candidates": self.deep_candidates, "reject_hist": list(self.reject_hist),
                 "tier_hist": list(self.tier_hist), "batches": self.batches, "retries": self.retries,
                 "kernel_launches": list(self.kernel_launches), "kernel_ms": list(self.kernel_ms),
-                "gpu_ms": self.gpu_ms, "wall_ms": self.wall_ms}
+                "gpu_ms": self.gpu_ms, "wall_ms": self.wall_ms, "rechecks": self.rechecks, "records": self.records}
+
+
+# wg_engine_set_noise_core values
+NOISE_FP32, NOISE_FP64, NOISE_FP32_RECHECK_ALL = 0, 1, 2
+NOISE_CORES = {"fp32": NOISE_FP32, "fp64": NOISE_FP64, "fp32_recheck_all": NOISE_FP32_RECHECK_ALL}
+# wg_noise_probe noise ids (the catalog's NoiseId order)
+PROBE_NOISES = {"erosion": 0, "temperature": 1, "ridge": 2, "continentalness": 3, "erosion_large": 4,
+                "temperature_large": 5, "continentalness_large": 6}
 
 
 CANDIDATE_DTYPE = np.dtype([("seed_index", "<u8"), ("seed", "<i8"), ("rx", "<i4"), ("rz", "<i4"),
                             ("chunk_x", "<i4"), ("chunk_z", "<i4")])
 
 # Every symbol include/witchgpu.h declares.
-EXPORTS = ("wg_engine_open", "wg_engine_close", "wg_engine_error", "wg_parse_version", "wg_parse_preset",
+EXPORTS = ("wg_engine_open", "wg_engine_close", "wg_engine_error", "wg_engine_set_noise_core", "wg_noise_probe",
+           "wg_parse_version", "wg_parse_preset",
            "wg_seed_check", "wg_seed_check_device", "wg_phase1_codes", "wg_seed_check_noalloc",
-           "wg_eval_huts", "wg_grade_scan", "wg_p2_probe", "wg_deep_starts", "wg_deep_spots",
-           "wg_biome_map", "wg_biome_chunks", "wg_deep_solve", "wg_deep_solve_tasks", "wg_seed_check_jobs", "wg_server_open", "wg_server_submit", "wg_server_poll", "wg_server_take",
+           "wg_eval_huts", "wg_grade_scan", "wg_p2_probe", "wg_deep_starts", "wg_deep_sweep", "wg_deep_spots",
+           "wg_biome_map", "wg_biome_chunks", "wg_deep_solve", "wg_deep_solve_tasks", "wg_seed_check_jobs", "wg_server_open", "wg_server_open_config", "wg_server_submit", "wg_server_poll", "wg_server_take",
            "wg_server_stats", "wg_server_close")
 
 # wg_deep_start: a swamp hut whose chunk is a mineshaft start chunk.
 DEEP_START_DTYPE = np.dtype([("seed_index", "<u8"), ("s48", "<i8"), ("rx", "<i4"), ("rz", "<i4"), ("chunk_x", "<i4"), ("chunk_z", "<i4"),
                              ("carver", "<i8")])
+
+# wg_sweep_match: a start chunk whose carver state is a catalogued layout.
+SWEEP_MATCH_DTYPE = np.dtype([("seed_index", "<u8"), ("s48", "<i8"), ("rx", "<i4"), ("rz", "<i4"),
+                              ("chunk_x", "<i4"), ("chunk_z", "<i4"), ("carver", "<i8"), ("value", "<u4"),
+                              ("pad", "<u4")])
+# the +-30M world's hut regions, [rx0, rx1) x [rz0, rz1) (the reference's forward sweep: radius 58,593)
+WORLD_REGIONS = (-58593, 58594, -58593, 58594)
 
 # wg_hut_result (lysh_hut_result's fields, engine/tools/lysh/src/eval.h:63-85).
 HUT_DTYPE = np.dtype([("hut_x", "<i4"), ("hut_z", "<i4"), ("rx", "<i4"), ("rz", "<i4"), ("dir", "<i4"),
@@ -118,6 +135,12 @@ class Job(C.Structure):
                 ("opts", Opts)]
 
 
+class ServerConfig(C.Structure):
+    """wg_server_config: queue and arena limits, batch size, host-side fault injection."""
+    _fields_ = [("max_queued_seeds", C.c_uint64), ("arena_seeds", C.c_uint64), ("batch_checks", C.c_uint64),
+                ("fail_job", C.c_uint64)]
+
+
 class JobStatus(C.Structure):
     _fields_ = [("done", C.c_int32), ("status", C.c_int32), ("found", C.c_uint64), ("queue_ms", C.c_double),
                 ("latency_ms", C.c_double), ("batch_jobs", C.c_uint64)]
@@ -143,6 +166,8 @@ def library() -> C.CDLL:
     lib.wg_engine_close.restype = None
     lib.wg_engine_error.argtypes = [vp]
     lib.wg_engine_error.restype = C.c_char_p
+    lib.wg_engine_set_noise_core.argtypes = [vp, i32]
+    lib.wg_noise_probe.argtypes = [vp, vp, u64, i32, vp, u64, vp, vp]
     lib.wg_parse_version.argtypes = [C.c_char_p, C.POINTER(Opts)]
     lib.wg_parse_preset.argtypes = [C.c_char_p, C.POINTER(Opts)]
     common = [vp, vp, u64, u64, C.POINTER(Opts), i32, i32, i32, i32, i32, i32]
@@ -156,6 +181,7 @@ def library() -> C.CDLL:
                                   C.POINTER(HutGrade)]
     lib.wg_p2_probe.argtypes = [vp, i64, C.POINTER(Opts), i32, vp, u64, vp]
     lib.wg_deep_starts.argtypes = [vp, vp, i64, u64, i32, i32, i32, i32, vp, u64, C.POINTER(u64)]
+    lib.wg_deep_sweep.argtypes = [vp, vp, vp, u64, vp, i64, u64, i32, i32, i32, i32, vp, u64, C.POINTER(u64), vp]
     lib.wg_deep_spots.argtypes = [vp, vp, vp, vp, u64, C.POINTER(Opts), i32, vp, u64, C.POINTER(u64),
                                   C.POINTER(u64)]
     lib.wg_biome_map.argtypes = [vp, i64, C.POINTER(Opts), i64, i64, i32, i32, i32, i32, i32, vp]
@@ -165,6 +191,7 @@ def library() -> C.CDLL:
     lib.wg_deep_solve_tasks.argtypes = [vp, u64, vp, vp, vp, vp, u64, vp, u64, C.POINTER(u64)]
     lib.wg_seed_check_jobs.argtypes = [vp, C.POINTER(Job), u64, vp, u64, C.POINTER(u64), vp, C.POINTER(Stats)]
     lib.wg_server_open.argtypes = [i32, u64, C.POINTER(vp)]
+    lib.wg_server_open_config.argtypes = [i32, C.POINTER(ServerConfig), C.POINTER(vp)]
     lib.wg_server_submit.argtypes = [vp, C.POINTER(Job), C.POINTER(u64)]
     lib.wg_server_poll.argtypes = [vp, u64, i32, C.POINTER(JobStatus)]
     lib.wg_server_take.argtypes = [vp, u64, vp, u64, C.POINTER(u64)]
@@ -203,7 +230,7 @@ class ScanResult:
 class Engine:
     """One engine = one device, one stream, one set of work buffers (not thread-safe)."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, noise_core: str = "fp32"):
         lib = library()
         h = C.c_void_p()
         rc = lib.wg_engine_open(device, C.byref(h))
@@ -212,6 +239,16 @@ class Engine:
                               + (" (no CUDA device)" if rc == WG_ERR_NODEV else ""))
         self._h = h
         self.device = device
+        self.set_noise_core(noise_core)
+
+    def set_noise_core(self, core: str) -> None:
+        """'fp32' (FP32 climate samples, FP64 recheck inside the error band; the default) or 'fp64'."""
+        if core not in NOISE_CORES:
+            raise ValueError(f"unknown noise core {core!r}")
+        rc = library().wg_engine_set_noise_core(self._h, NOISE_CORES[core])
+        if rc != WG_OK:
+            raise self._err(rc, "wg_engine_set_noise_core")
+        self.noise_core = core
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -277,6 +314,19 @@ class Engine:
             raise self._err(rc, "wg_seed_check_device")
         return int(found.value), st.as_dict()
 
+    def noise_probe(self, seeds, noise: str, xz) -> tuple[np.ndarray, np.ndarray]:
+        """(fp32, fp64) y = 0 DoublePerlin values of a climate noise, [n_seeds, n_points] float64:
+        the FP32 core's value beside the reference's FP64 value at noise-space points xz [n, 2]."""
+        s = as_seed_array(seeds)
+        pts = np.ascontiguousarray(xz, dtype=np.float64).reshape(-1, 2)
+        v32 = np.empty((len(s), len(pts)), np.float64)
+        v64 = np.empty((len(s), len(pts)), np.float64)
+        rc = library().wg_noise_probe(self._h, s.ctypes.data, len(s), PROBE_NOISES[noise], pts.ctypes.data,
+                                      len(pts), v32.ctypes.data, v64.ctypes.data)
+        if rc != WG_OK:
+            raise self._err(rc, "wg_noise_probe")
+        return v32, v64
+
     def phase1_codes(self, seeds=None, gen=None, rect=(-4, 5, -4, 5), max_height: int = -50,
                      version: str = DEFAULT_VERSION, preset: str = "NORMAL", salt: int = 0,
                      opts: Opts | None = None) -> tuple[np.ndarray, np.ndarray]:
@@ -341,6 +391,31 @@ class Engine:
                 raise self._err(rc, "wg_deep_starts")
             if found.value <= cap:
                 return out[:found.value]   # a view: the hits are already in order, no second copy
+            cap = int(found.value)
+
+    def deep_sweep(self, layouts, values=None, s48=None, base: int = 0, count: int = 0,
+                   rect=WORLD_REGIONS) -> tuple[np.ndarray, np.ndarray]:
+        """Deep Dive forward sweep with the layout-catalogue probe: (matches SWEEP_MATCH_DTYPE sorted by
+        (seed_index, rz, rx), starts per structure seed uint64)."""
+        keys = np.ascontiguousarray([int(v) & 0xFFFFFFFFFFFF for v in layouts], dtype=np.uint64)
+        vals = None if values is None else np.ascontiguousarray(values, dtype=np.uint32)
+        if s48 is not None:
+            arr = np.ascontiguousarray(np.asarray([int(v) & 0xFFFFFFFFFFFF for v in s48], dtype=np.int64))
+            ptr, n = arr.ctypes.data, len(arr)
+        else:
+            arr, ptr, n = None, None, int(count)
+        cap = 1 << 12
+        starts = np.zeros(n, np.uint64)
+        while True:
+            out = np.zeros(cap, SWEEP_MATCH_DTYPE)
+            found = C.c_uint64()
+            rc = library().wg_deep_sweep(self._h, keys.ctypes.data, None if vals is None else vals.ctypes.data,
+                                         len(keys), ptr, int(base), n, *rect, out.ctypes.data, cap, C.byref(found),
+                                         starts.ctypes.data)
+            if rc != WG_OK:
+                raise self._err(rc, "wg_deep_sweep")
+            if found.value <= cap:
+                return out[:found.value].copy(), starts
             cap = int(found.value)
 
     def biome_map(self, seed: int, x0: int, z0: int, w: int, h: int, step: int = 16, ss: int = 1,
@@ -534,12 +609,14 @@ class Server:
     library's worker thread admits queued jobs as device seed slots free up and runs them in
     shared batches; poll() / take() return a job's status and survivors."""
 
-    def __init__(self, device: int = 0, max_queued_seeds: int = 0):
+    def __init__(self, device: int = 0, max_queued_seeds: int = 0, arena_seeds: int = 0, batch_checks: int = 0,
+                 fail_job: int = 0):
         lib = library()
         h = C.c_void_p()
-        rc = lib.wg_server_open(device, max_queued_seeds, C.byref(h))
+        cfg = ServerConfig(max_queued_seeds, arena_seeds, batch_checks, fail_job)
+        rc = lib.wg_server_open_config(device, C.byref(cfg), C.byref(h))
         if rc != WG_OK:
-            raise EngineError(f"wg_server_open(device={device}) failed with status {rc}")
+            raise EngineError(f"wg_server_open_config(device={device}) failed with status {rc}")
         self._h = h
 
     def submit(self, **job) -> int:

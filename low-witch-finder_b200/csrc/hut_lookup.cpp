@@ -11,6 +11,13 @@
 //            pass the phase-1 gates at the spot region whose hut is the spot chunk, as
 //            "seed,chunkX,chunkZ,layoutX,airHi,airLo" rows appended to O (header when empty);
 //            exit 1 when a spot is not a mineshaft start chunk (:1262-1290)
+//   forward  --catalog C --first-index F --count N [--max-height -54] [--out O] [--quiet]
+//            (the reference's default mode, :1504-1533): structure seed
+//            s48 = (index * 0x9E3779B97F4A7D + 0x2545F4914F6CDD) mod 2^48 for each index of the range
+//            (:27-29, :1505); every hut region of the +-30M world (radius 58,593) swept for huts on
+//            mineshaft start chunks whose carver state is a catalogued layout (wg_deep_sweep); each
+//            match's 65,536 world seeds through the terrain stage as in --spots; the reference's
+//            per-seed line on stderr and its summary line on stdout
 //
 // The tuning flags of the reference (--fused-*, --task-batch, --ero-*, --batch, --u-*) are
 // accepted and change nothing: the solver and the gates here are exact.  The terrain gates are
@@ -29,6 +36,12 @@
 #include "../../include/witchgpu.h"
 
 namespace {
+
+// The terrain stage of one call's spots: survivors appended to `out` as the reference's rows.
+// Returns the survivor count, or -1 on failure; *not_start counts spots that are not start chunks.
+long long terrain_rows(wg_engine *eng, const std::vector<int64_t> &s48, const std::vector<int32_t> &cx,
+                       const std::vector<int32_t> &cz, const std::vector<uint64_t> &layout,
+                       const std::vector<uint32_t> &value, int max_h, FILE *out, uint64_t *not_start);
 
 bool read_catalog(const char *path, std::map<uint64_t, std::pair<unsigned, unsigned>> &cat) {
     FILE *f = std::fopen(path, "r");
@@ -72,6 +85,39 @@ int fail(const char *msg) {
     return 2;
 }
 
+long long terrain_rows(wg_engine *eng, const std::vector<int64_t> &s48, const std::vector<int32_t> &cx,
+                       const std::vector<int32_t> &cz, const std::vector<uint64_t> &layout,
+                       const std::vector<uint32_t> &value, int max_h, FILE *out, uint64_t *not_start) {
+    wg_opts o{};   // wg_parse_version sets the version bits only; NORMAL preset
+    wg_parse_version("1.19.x~26.1", &o);
+    long long total = 0;
+    *not_start = 0;
+    for (size_t i0 = 0; i0 < s48.size(); i0 += 4096) {
+        const size_t n = std::min<size_t>(4096, s48.size() - i0);
+        std::vector<wg_candidate> c(1 << 16);
+        uint64_t got = 0, bad = 0;
+        int rc;
+        for (;;) {
+            rc = wg_deep_spots(eng, s48.data() + i0, cx.data() + i0, cz.data() + i0, n, &o, max_h, c.data(), c.size(),
+                               &got, &bad);
+            if (rc || got <= c.size()) break;
+            c.resize(got);
+        }
+        if (rc) {
+            std::fprintf(stderr, "terrain stage failed: %s\n", wg_engine_error(eng));
+            return -1;
+        }
+        *not_start += bad;
+        for (uint64_t k = 0; k < got; k++) {
+            const size_t spot = i0 + (size_t)(c[k].seed_index >> 16);
+            std::fprintf(out, "%lld,%d,%d,%llu,%u,%u\n", (long long)c[k].seed, cx[spot], cz[spot],
+                         (unsigned long long)layout[spot], value[spot] & 0x3FF, (value[spot] >> 10) & 0x3FF);
+            total++;
+        }
+    }
+    return total;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -79,7 +125,7 @@ int main(int argc, char **argv) {
     const char *out_path = "hut_lookup_out.csv";
     long long first = 0, count = 1;
     int regx = -1, regz = -1, max_h = -54;
-    bool solve5 = false, quiet = false;
+    bool solve5 = false, quiet = false, solve_flag = false;
     for (int i = 1; i < argc; i++) {
         const char *a = argv[i];
         auto val = [&]() -> const char * { return i + 1 < argc ? argv[++i] : nullptr; };
@@ -100,8 +146,8 @@ int main(int argc, char **argv) {
         } else if (!std::strcmp(a, "--far")) regx = regz = 2;
         else if (!std::strcmp(a, "--solve5")) solve5 = true;
         else if (!std::strcmp(a, "--quiet")) quiet = true;
-        else if (!std::strcmp(a, "--solve-only") || !std::strcmp(a, "--solve") || !std::strcmp(a, "--ero-split") ||
-                 !std::strcmp(a, "--timing") || !std::strcmp(a, "--no-async"))
+        else if (!std::strcmp(a, "--solve-only") || !std::strcmp(a, "--solve")) solve_flag = true;
+        else if (!std::strcmp(a, "--ero-split") || !std::strcmp(a, "--timing") || !std::strcmp(a, "--no-async"))
             ;
         else if (!std::strncmp(a, "--fused-", 8) || !std::strncmp(a, "--ero-", 6) || !std::strcmp(a, "--task-batch") ||
                  !std::strcmp(a, "--batch") || !std::strcmp(a, "--u-lo") || !std::strcmp(a, "--u-hi") ||
@@ -139,40 +185,81 @@ int main(int argc, char **argv) {
         if (!out) { std::fprintf(stderr, "cannot write %s\n", out_path); wg_engine_close(eng); return 1; }
         std::fseek(out, 0, SEEK_END);
         if (std::ftell(out) == 0) std::fprintf(out, "seed,chunkX,chunkZ,layoutX,airHi,airLo\n");
-        wg_opts o{};   // wg_parse_version sets the version bits only; NORMAL preset
-        wg_parse_version("1.19.x~26.1", &o);
-        uint64_t total = 0, bad_all = 0;
+        std::vector<uint64_t> layout(s48.size());
+        std::vector<uint32_t> zero(s48.size(), 0);
+        for (size_t i = 0; i < s48.size(); i++) layout[i] = carver_state((uint64_t)s48[i], cx[i], cz[i]);
+        uint64_t bad_all = 0;
         const auto t0 = std::chrono::steady_clock::now();
-        for (size_t i0 = 0; i0 < s48.size(); i0 += 4096) {
-            const size_t n = std::min<size_t>(4096, s48.size() - i0);
-            std::vector<wg_candidate> c(1 << 16);
-            uint64_t got = 0, bad = 0;
-            for (;;) {
-                rc = wg_deep_spots(eng, s48.data() + i0, cx.data() + i0, cz.data() + i0, n, &o, max_h, c.data(),
-                                   c.size(), &got, &bad);
-                if (rc || got <= c.size()) break;
-                c.resize(got);
-            }
-            if (rc) { std::fprintf(stderr, "terrain stage failed: %s\n", wg_engine_error(eng)); break; }
-            bad_all += bad;
-            for (uint64_t k = 0; k < got; k++) {
-                const size_t spot = i0 + (size_t)(c[k].seed_index >> 16);
-                std::fprintf(out, "%lld,%d,%d,%llu,0,0\n", (long long)c[k].seed, cx[spot], cz[spot],
-                             (unsigned long long)carver_state((uint64_t)s48[spot], cx[spot], cz[spot]));
-                total++;
-            }
-        }
+        const long long total = terrain_rows(eng, s48, cx, cz, layout, zero, max_h, out, &bad_all);
         std::fclose(out);
         if (bad_all) std::fprintf(stderr, "*** %llu spots are not mineshaft start chunks\n", (unsigned long long)bad_all);
         const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         std::printf("spots: %zu spots (%llu not a start), %llu terrain survivors -> %s; terrain %.3f s (%.1f ms per spot)\n",
-                    s48.size(), (unsigned long long)bad_all, (unsigned long long)total, out_path, secs,
+                    s48.size(), (unsigned long long)bad_all, (unsigned long long)std::max(0LL, total), out_path, secs,
                     s48.empty() ? 0.0 : 1e3 * secs / (double)s48.size());
         wg_engine_close(eng);
-        return rc ? 1 : (bad_all ? 1 : 0);
+        return total < 0 ? 1 : (bad_all ? 1 : 0);
     }
 
-    if (!solve5) { wg_engine_close(eng); return fail("only --solve5 and --spots are supported"); }
+    if (!solve5 && !solve_flag) {
+        // forward mode: sweep the world per structure seed, probe the catalogue, terrain-check the matches
+        if (first < 0 || count < 1) { wg_engine_close(eng); return fail("--first-index >= 0 and --count >= 1"); }
+        std::vector<uint64_t> keys;
+        std::vector<uint32_t> vals;
+        for (const auto &kv : cat) {
+            keys.push_back(kv.first);
+            vals.push_back(kv.second.first | (kv.second.second << 10));
+        }
+        if (keys.empty()) { wg_engine_close(eng); return fail("empty catalogue"); }
+        if (!quiet) std::printf("catalogue: %zu layouts\n", keys.size());
+        FILE *out = std::fopen(out_path, "a");
+        if (!out) { std::fprintf(stderr, "cannot write %s\n", out_path); wg_engine_close(eng); return 1; }
+        std::fseek(out, 0, SEEK_END);
+        if (std::ftell(out) == 0) std::fprintf(out, "seed,chunkX,chunkZ,layoutX,airHi,airLo\n");
+        const auto t0 = std::chrono::steady_clock::now();
+        auto wall = [&]() { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); };
+        unsigned long long tot_matches = 0, tot_surv = 0;
+        int status = 0;
+        std::vector<wg_sweep_match> m(1 << 12);
+        for (long long si = 0; si < count && !status; si++) {
+            const int64_t s48 = (int64_t)(((uint64_t)(first + si) * 0x9E3779B97F4A7DULL + 0x2545F4914F6CDDULL) &
+                                          0xFFFFFFFFFFFFull);
+            uint64_t got = 0, starts = 0;
+            for (;;) {
+                rc = wg_deep_sweep(eng, keys.data(), vals.data(), keys.size(), &s48, 0, 1, -58593, 58594, -58593, 58594,
+                                   m.data(), m.size(), &got, &starts);
+                if (rc || got <= m.size()) break;
+                m.resize(got);
+            }
+            if (rc) { std::fprintf(stderr, "sweep failed: %s\n", wg_engine_error(eng)); status = 1; break; }
+            std::vector<int64_t> ss(got, s48);
+            std::vector<int32_t> mx(got), mz(got);
+            std::vector<uint64_t> lay(got);
+            std::vector<uint32_t> val(got);
+            for (uint64_t k = 0; k < got; k++) {
+                mx[k] = m[k].chunk_x;
+                mz[k] = m[k].chunk_z;
+                lay[k] = (uint64_t)m[k].carver;
+                val[k] = m[k].value;
+            }
+            uint64_t bad = 0;
+            const long long surv = got ? terrain_rows(eng, ss, mx, mz, lay, val, max_h, out, &bad) : 0;
+            if (surv < 0) { status = 1; break; }
+            std::fflush(out);
+            tot_matches += got;
+            tot_surv += (unsigned long long)surv;
+            if (!quiet)
+                std::fprintf(stderr, "S48 %lld (index %lld): %llu hut starts, %llu catalogue matches, %llu terrain survivors | %.1f s\n",
+                             (long long)s48, first + si, (unsigned long long)starts, (unsigned long long)got,
+                             (unsigned long long)surv, wall());
+        }
+        std::fclose(out);
+        std::printf("done:%lld structure seeds, %llu matches, %llu survivors -> %s (%.1f s, %.2f s per structure seed)\n",
+                    count, tot_matches, tot_surv, out_path, wall(), wall() / (double)count);
+        wg_engine_close(eng);
+        return status;
+    }
+    if (!solve5) { wg_engine_close(eng); return fail("--solve / --solve-only need --solve5 here"); }
     std::vector<wg_solve_bundle> bundles;
     if (plan_path) {
         FILE *pf = std::fopen(plan_path, "r");

@@ -3,15 +3,26 @@
 // :1328-1339 CSV, :1365-1387 worker loop), on top of libwitchgpu.so.
 //
 // Differences a caller can observe:
-//   * The candidate set is exactly lysh's phase-1 survivor set (lysh_phase1_check_ex),
-//     not the reference GPU scanner's superset; there is no lossy density prefilter, so
-//     --no-density-prefilter / --climate-gate / --no-climate-gate / --block are accepted
-//     and change nothing.
+//   * The rows written are the exact hit set: lysh's phase-1 survivors (lysh_phase1_check_ex)
+//     confirmed by lysh's phase 2 (lysh_eval_hut: biome gate, flood test, post-carver footprint
+//     heights) at --phase2-max-y (default: --max-height as given, before the clamp below, as
+//     lysh scan's default), on the GPU through wg_eval_huts.  The 6th CSV column (the reference's
+//     gpuEst) holds the hut's floor y, avg_y.  hunt.py reads the first three columns and
+//     re-confirms each row with `lysh hut` at its ceiling (<= -50, hunt.py:1347-1349), which
+//     accepts a subset of these rows, so its results are those of the phase-1 superset with one
+//     `lysh hut` per hit instead of one per candidate.  --phase1-candidates writes the phase-1
+//     superset instead, with "nan" in the 6th column.  There is no lossy density prefilter, so
+//     --no-density-prefilter / --climate-gate / --no-climate-gate / --block are accepted and
+//     change nothing.
 //   * --max-height is clamped like lysh's phase1CheckHeight (-50 / -54 -> -50,
 //     engine/tools/lysh/src/main.c:135-137).
 //   * --version / --preset take lysh's names (default 1.19.x~26.1, the hunt driver's);
 //     --v26-2 selects the 26.2 ridge rule as before.
-//   * The 6th CSV column (gpuEst) is "nan": the reference's prefilter estimate does not exist.
+//   * --self-test re-checks sampled regions of the request's first 16 seeds (the reference's
+//     sampling, up to 20,000 regions per seed at a fixed stride, phase1_scan.cu:1289-1326) through
+//     the engine's plain FP64 noise core and compares each verdict with the scan's phase-1
+//     survivor list (the FP32 core's); prints the reference's summary line and fails the request
+//     (rc 1) on any mismatch.
 //   * --quad-bases sweeps (base, high 16 bits) as the reference does (:64-86, :700-724):
 //     index i of the request is the seed bases[g >> 16] | (g & 0xffff) << 48 with
 //     g = offset * 65536 + i; the seeds are expanded on the host in slices.  Combining it
@@ -54,7 +65,19 @@ struct Params {
     long long max_hut_dist = -1;        // --max-hut-dist; < 0 = no position gate
     int gate_x = 0, gate_z = 0;
     bool require_all = false;
+    bool phase1_only = false;           // --phase1-candidates: write the phase-1 survivors unconfirmed
+    bool have_p2_max_y = false;         // --phase2-max-y given
+    int p2_max_y = -40;                 // phase-2 ceiling (default: --max-height before the clamp)
+    bool self_test = false;
 };
+
+uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ULL;
+    uint64_t z = x;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
 
 // Seeds of a --quad-bases request: request index i -> bases[g >> 16] | (g & 0xffff) << 48,
 // g = offset * 65536 + i (phase1_scan.cu:79-86).
@@ -159,8 +182,13 @@ bool parse(const std::vector<std::string> &t, Params &p) {
             }
         } else if (a == "--out") p.out_path = next(a.c_str());
         else if (a == "--block") (void)next(a.c_str());
-        else if (a == "--self-test" || a == "--no-density-prefilter" || a == "--climate-gate" ||
-                 a == "--no-climate-gate" || a == "--worker") {
+        else if (a == "--self-test") p.self_test = true;
+        else if (a == "--phase1-candidates") p.phase1_only = true;
+        else if (a == "--phase2-max-y") {
+            p.p2_max_y = std::atoi(next(a.c_str()).c_str());
+            p.have_p2_max_y = true;
+        } else if (a == "--no-density-prefilter" || a == "--climate-gate" || a == "--no-climate-gate" ||
+                   a == "--worker") {
         } else if (a == "--quad-bases") p.quad_path = next(a.c_str());
         else if (a == "--quad-base-offset") p.quad_offset = std::atoll(next(a.c_str()).c_str());
         else if (a == "--quad-base-limit") p.quad_limit = std::atoll(next(a.c_str()).c_str());
@@ -197,6 +225,7 @@ bool parse(const std::vector<std::string> &t, Params &p) {
         std::fprintf(stderr, "empty region range\n");
         return false;
     }
+    if (!p.have_p2_max_y) p.p2_max_y = p.max_height;
     if (p.max_height < -50) p.max_height = -50;
     return true;
 }
@@ -272,10 +301,102 @@ bool all_regions_filter(wg_engine *eng, const Params &p, std::vector<wg_candidat
     return true;
 }
 
+// The world seed of request index i.
+int64_t request_seed(const Params &p, uint64_t i) {
+    if (!p.quad_bases.empty()) return quad_seed(p, i);
+    if (p.gen) return (int64_t)splitmix64(p.gen_base + i);
+    return p.seeds[i];
+}
+
+// --self-test: sampled regions of the first 16 seeds re-checked through the FP64 noise core, one
+// one-region job each, against the scan's phase-1 survivors `cands` (phase1_scan.cu:1289-1326).
+// Returns the number of mismatches, or -1 if the check itself failed.
+long long self_test(wg_engine *eng, const Params &p, uint64_t n_seeds, const std::vector<wg_candidate> &cands) {
+    const uint64_t rw = (uint64_t)(p.max_rx - p.min_rx), rh = (uint64_t)(p.max_rz - p.min_rz);
+    const uint64_t total = rw * rh, step = total > 20000 ? total / 20000 : 1;
+    const uint64_t ns = std::min<uint64_t>(n_seeds, 16);
+    std::vector<int64_t> seeds(ns);
+    std::vector<wg_job> jobs;
+    for (uint64_t s = 0; s < ns; s++) {
+        seeds[s] = request_seed(p, s);
+        for (uint64_t idx = 0; idx < total; idx += step) {
+            wg_job j{};
+            j.seeds = &seeds[s];
+            j.n_seeds = 1;
+            j.rx0 = p.min_rx + (int)(idx % rw);
+            j.rz0 = p.min_rz + (int)(idx / rw);
+            j.rx1 = j.rx0 + 1;
+            j.rz1 = j.rz0 + 1;
+            j.max_height = p.max_height;
+            j.opts = p.opts;
+            jobs.push_back(j);
+        }
+    }
+    std::vector<uint64_t> job_found(jobs.size(), 0);
+    std::vector<wg_candidate> got(jobs.size() + 1);
+    uint64_t n_got = 0;
+    wg_engine_set_noise_core(eng, WG_NOISE_FP64);
+    const int rc = wg_seed_check_jobs(eng, jobs.data(), jobs.size(), got.data(), got.size(), &n_got,
+                                      job_found.data(), nullptr);
+    wg_engine_set_noise_core(eng, WG_NOISE_FP32);
+    if (rc) {
+        std::fprintf(stderr, "self-test scan failed (%d): %s\n", rc, wg_engine_error(eng));
+        return -1;
+    }
+    std::vector<std::pair<int64_t, std::pair<int, int>>> hits;   // (seed index, (rx, rz)) of the scan
+    for (const wg_candidate &c : cands)
+        if (c.seed_index < ns) hits.push_back({(int64_t)c.seed_index, {c.rx, c.rz}});
+    std::sort(hits.begin(), hits.end());
+    long long mismatches = 0;
+    for (size_t k = 0; k < jobs.size(); k++) {
+        const int64_t s = (int64_t)(k / ((total + step - 1) / step));
+        const bool dev = std::binary_search(hits.begin(), hits.end(), std::make_pair(s, std::make_pair(jobs[k].rx0, jobs[k].rz0)));
+        const bool fp64 = job_found[k] != 0;
+        if (dev != fp64) {
+            if (mismatches < 5)
+                std::printf("  MISMATCH seed=%" PRId64 " region(%d,%d): scan=%d fp64=%d\n", seeds[s], jobs[k].rx0,
+                            jobs[k].rz0, (int)dev, (int)fp64);
+            mismatches++;
+        }
+    }
+    std::printf("self-test: checked %zu sampled regions across %" PRIu64 " seed(s), %lld mismatches -> %s\n",
+                jobs.size(), ns, mismatches, mismatches == 0 ? "PASS" : "FAIL");
+    return mismatches;
+}
+
+// Phase 2 for the phase-1 survivors: keeps the huts lysh_eval_hut accepts at the ceiling, with
+// their floor y.
+bool confirm(wg_engine *eng, const Params &p, std::vector<wg_candidate> &cands, std::vector<int> &floor_y) {
+    floor_y.clear();
+    if (cands.empty()) return true;
+    std::vector<int64_t> seeds(cands.size());
+    std::vector<int32_t> hx(cands.size()), hz(cands.size());
+    for (size_t i = 0; i < cands.size(); i++) {
+        seeds[i] = cands[i].seed;
+        hx[i] = cands[i].chunk_x * 16;
+        hz[i] = cands[i].chunk_z * 16;
+    }
+    std::vector<wg_hut_result> res(cands.size());
+    const int rc = wg_eval_huts(eng, seeds.data(), hx.data(), hz.data(), cands.size(), &p.opts, p.p2_max_y, res.data());
+    if (rc) {
+        std::fprintf(stderr, "phase 2 failed (%d): %s\n", rc, wg_engine_error(eng));
+        return false;
+    }
+    std::vector<wg_candidate> kept;
+    for (size_t i = 0; i < cands.size(); i++)
+        if (res[i].ok) {
+            kept.push_back(cands[i]);
+            floor_y.push_back(res[i].avg_y);
+        }
+    cands.swap(kept);
+    return true;
+}
+
 int run_scan(wg_engine *eng, const Params &p) {
     const bool quad = !p.quad_bases.empty();
     const uint64_t n = quad ? (uint64_t)p.quad_limit * 65536ull : p.gen ? (uint64_t)p.gen_count : p.seeds.size();
     std::vector<wg_candidate> out;
+    std::vector<int> floor_y;
     int64_t scanned = 0;
     auto t0 = std::chrono::steady_clock::now();
     if (quad) {
@@ -291,14 +412,21 @@ int run_scan(wg_engine *eng, const Params &p) {
     } else if (!check_seeds(eng, p, p.gen ? nullptr : p.seeds.data(), p.gen_base, n, 0, out, scanned)) {
         return 1;
     }
+    long long mismatches = 0;
+    if (p.self_test && (mismatches = self_test(eng, p, n, out)) < 0) return 1;
     if (p.max_hut_dist >= 0)
         out.erase(std::remove_if(out.begin(), out.end(), [&](const wg_candidate &c) { return !within_gate(p, c); }),
                   out.end());
     if (p.require_all && !out.empty() && !all_regions_filter(eng, p, out)) return 1;
+    const uint64_t phase1 = out.size();
+    if (!p.phase1_only && !confirm(eng, p, out, floor_y)) return 1;
     const uint64_t found = out.size();
     double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     std::printf("kernel: %.3f s  candidates=%" PRIu64 "  (%.2f M region-seed-checks/s across %" PRIu64 " seed(s))\n",
                 secs, found, secs > 0 ? (double)scanned / secs / 1e6 : 0.0, n);
+    if (!p.phase1_only)
+        std::printf("phase 2: %" PRIu64 " phase-1 survivors, %" PRIu64 " huts with floor <= %d\n", phase1, found,
+                    p.p2_max_y);
     if (!p.out_path.empty()) {
         FILE *f = std::fopen(p.out_path.c_str(), "w");
         if (!f) {
@@ -306,11 +434,18 @@ int run_scan(wg_engine *eng, const Params &p) {
             return 1;
         }
         std::fprintf(f, "seed,chunkX,chunkZ,blockX,blockZ,gpuEst\n");
-        for (const wg_candidate &c : out)
-            std::fprintf(f, "%" PRId64 ",%d,%d,%d,%d,nan\n", c.seed, c.chunk_x, c.chunk_z, c.chunk_x * 16,
-                         c.chunk_z * 16);
+        for (size_t i = 0; i < out.size(); i++) {
+            const wg_candidate &c = out[i];
+            std::fprintf(f, "%" PRId64 ",%d,%d,%d,%d,", c.seed, c.chunk_x, c.chunk_z, c.chunk_x * 16, c.chunk_z * 16);
+            if (p.phase1_only) std::fprintf(f, "nan\n");
+            else std::fprintf(f, "%d\n", floor_y[i]);
+        }
         std::fclose(f);
         std::printf("wrote %zu candidates to %s\n", out.size(), p.out_path.c_str());
+    }
+    if (mismatches) {
+        std::fprintf(stderr, "self-test FAILED\n");
+        return 1;
     }
     return 0;
 }
@@ -335,7 +470,10 @@ void usage() {
         "  --max-height <n>     phase-1 maxHeight, default -40 (-50/-54 -> -50)\n"
         "  --version <v>        lysh version name (default 1.19.x~26.1); --v26-2 = 26.2 ridge rule\n"
         "  --preset <p>         NORMAL | LARGE_BIOMES | SINGLE_BIOME\n"
-        "  --out <file>         CSV seed,chunkX,chunkZ,blockX,blockZ,gpuEst\n"
+        "  --out <file>         CSV seed,chunkX,chunkZ,blockX,blockZ,gpuEst (gpuEst = the hut's floor y)\n"
+        "  --phase2-max-y <y>   phase-2 ceiling: keep huts with floor <= y (default --max-height)\n"
+        "  --phase1-candidates  write every phase-1 survivor (unconfirmed, gpuEst nan)\n"
+        "  --self-test          re-check sampled regions through the FP64 noise core; rc 1 on a mismatch\n"
         "  --quad-bases <file>  sweep every base x its 65,536 high-16-bit variants\n"
         "  --quad-base-offset <n> / --quad-base-limit <n>  slice of the base list (limit <= 32767)\n"
         "  --max-hut-dist <d>   keep huts within d blocks of --gate-center-x/--gate-center-z\n"

@@ -317,6 +317,94 @@ __device__ __forceinline__ double perlin_3d(const T &P, double ox, double oy, do
     return perlin_core(P, i, j, k, g, hm, hm - 1, l, fade(g), fade(h), fade(l));
 }
 
+// ------------------------------------------------------------------------------------
+// FP32 noise core (the climate samples of the FP32-plus-FP64-recheck path)
+// ------------------------------------------------------------------------------------
+// The coordinate reduction stays in FP64 exactly as above (d = x + ox, its floor and the
+// fraction d - floor(d), which is exact), since a float cannot hold the fraction of a
+// coordinate of magnitude ~1e5.  Everything after it works on values in [-2, 2] and runs in
+// FP32 with the operation sequence below, whose error against the exact real-valued sample
+// (the same lattice cell and hashes, exact fractions g, l and y origin hy) is bounded here.
+// u = 2^-24 is the unit roundoff; "half-ulp" bounds a round-to-nearest result.
+//
+//  G = rn(g), L = rn(l), H = rn(hy) from exact doubles in [0, 1):      |err| <= u/2
+//  G1 = G - 1 (exact for G >= 1/2, else rounds in (-1, -1/2]):          |err| <= u
+//  FY = rn(fade(hy)) (fade taken in FP64):                             |err| <= u/2 + 2^-52
+//  FX = fade_f32(G) evaluated as 1/2 + s (15/8 + s^2 (6 s^2 - 5)), s = G - 1/2:
+//      s exact (Sterbenz) or within u/4; s^2 within u/8 (value <= 1/4); 6 s^2 - 5 in
+//      [-5, -3.5] within u*4 * 1.19; the 15/8 step in [0.625, 1.875] within 2.81 u; the last
+//      FMA within 1.41 u + u/2 of rounding; with fade' <= 1.875 carrying the u/2 input error
+//      and the u/4 of s:  |FX - fade(g)| <= 3.32 u <= 4 u
+//  corner dot (two +-1 components; the zero one adds nothing): one rounded add of two
+//      coordinates, each within u, value <= 2:                          |err| <= 3 u
+//  lerp(t, a, b) as (a - t a) + t b (two FMAs, each value <= 2 -> u of rounding each):
+//      |err| <= max(err a, err b) + |t err| * |b - a| + 2 u, with |b - a| <= 4
+//      x lerps: 3 u + 4 * 4 u + 2 u = 21 u;  y lerps: 21 u + 4 * u/2 + 2 u = 25 u;
+//      z lerp: 25 u + 4 * 4 u + 2 u = 43 u   (T slightly above 1 after rounding: x 1.0001)
+// So |FP32 sample - exact| <= 44 u = 2.62e-6 (kPerlinF32ErrUlps), and |sample| <= 2.  The
+// FP64 sample of the reference order is within ~1e-14 of the exact value; the gates add that
+// and the sums' own roundings (build_climate_steps).  No FMA contraction is left to the
+// compiler: every FP32 operation below is an explicit intrinsic.
+__device__ __forceinline__ float fade_f32(float t) {
+    const float s = __fsub_rn(t, 0.5f);
+    const float s2 = __fmul_rn(s, s);
+    const float p = __fmaf_rn(6.0f, s2, -5.0f);
+    const float q = __fmaf_rn(s2, p, 1.875f);
+    return __fmaf_rn(s, q, 0.5f);
+}
+__device__ __forceinline__ float lerp_f32(float t, float a, float b) {
+    return __fmaf_rn(t, b, __fmaf_rn(-t, a, a));
+}
+
+// Table reader of the FP32 core: bytes as ColTable, gradient components as floats
+// (gtf[component * 16 + hash] in {-1, 0, 1}).
+template <int STRIDE>
+struct ColTableF {
+    const uint8_t *t;
+    const float *gtf;
+    __device__ __forceinline__ int operator()(int k) const { return t[k * STRIDE]; }
+    __device__ __forceinline__ float grad(int hash, float x, float y, float z) const {
+        const int h = hash & 15;
+        return __fmaf_rn(gtf[h], x, __fmaf_rn(gtf[16 + h], y, __fmul_rn(gtf[32 + h], z)));
+    }
+};
+
+__device__ __forceinline__ void fill_grad_table_f32(float *gtf, int tid) {
+    if (tid < kGradWords) {
+        const int c = tid / 16;
+        const uint32_t codes = c == 0 ? kGradCodeX : (c == 1 ? kGradCodeY : kGradCodeZ);
+        const uint32_t code = (codes >> (2 * (tid % 16))) & 3u;
+        gtf[tid] = code == 0 ? 0.0f : (code == 1 ? 1.0f : -1.0f);
+    }
+}
+
+// One Perlin sampler at y = 0 in the FP32 core; hyf / fyf are rn(hy) and rn(fade(hy)) of the
+// table's y origin fraction, jy its floor.  x, z are the FP64 sampling coordinates.
+template <class T>
+__device__ __forceinline__ float perlin_y0_f32(const T &P, double ox, double oz, int jy, float hyf, float fyf,
+                                               double x, double z) {
+    const double d = x + ox, f = z + oz;
+    const double fd = floor(d), ff = floor(f);
+    const int i = (int)fd, k = (int)ff;
+    const float g = __double2float_rn(d - fd), l = __double2float_rn(f - ff);
+    const float g1 = __fsub_rn(g, 1.0f), l1 = __fsub_rn(l, 1.0f), hy1 = __fsub_rn(hyf, 1.0f);
+    const int a = P(i & 255), b = P((i + 1) & 255);
+    const int c = P((a + jy) & 255), dd = P((a + jy + 1) & 255);
+    const int e = P((b + jy) & 255), ee = P((b + jy + 1) & 255);
+    const float v000 = P.grad(P((c + k) & 255), g, hyf, l);
+    const float v100 = P.grad(P((e + k) & 255), g1, hyf, l);
+    const float v010 = P.grad(P((dd + k) & 255), g, hy1, l);
+    const float v110 = P.grad(P((ee + k) & 255), g1, hy1, l);
+    const float v001 = P.grad(P((c + k + 1) & 255), g, hyf, l1);
+    const float v101 = P.grad(P((e + k + 1) & 255), g1, hyf, l1);
+    const float v011 = P.grad(P((dd + k + 1) & 255), g, hy1, l1);
+    const float v111 = P.grad(P((ee + k + 1) & 255), g1, hy1, l1);
+    const float fx = fade_f32(g), fz = fade_f32(l);
+    const float x00 = lerp_f32(fx, v000, v100), x10 = lerp_f32(fx, v010, v110);
+    const float x01 = lerp_f32(fx, v001, v101), x11 = lerp_f32(fx, v011, v111);
+    return lerp_f32(fz, lerp_f32(fyf, x00, x10), lerp_f32(fyf, x01, x11));
+}
+
 constexpr double kDblScale = 1.0181268882175227;
 
 // Java Math.min / Math.max with the signed-zero rules (mcmath.h).

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -60,6 +61,55 @@ void wg::build_climate_steps(const NoiseSpec *specs, int erosion, int temperatur
             }
         base += 2 * n.npresent;
     }
+    // FP32 core: each running FP32 sum (erosion over steps 0..7; temperature 8..11; ridge 12..17,
+    // each from zero) is s_k = fma(cf_k, v_k, s_{k-1}) with |v_k - exact sample| <= eps (the
+    // Perlin bound) and |exact sample| <= 2.  Per step the error grows by
+    //   |c_k| (eps + 2.01 u)          (the sample's error and cf_k = rn(c_k), c_k = c1 * c2)
+    // + 2.01 u sum_{i<=k} |c_i|       (the FMA's rounding of a partial sum of that magnitude),
+    // u = 2^-24.  The band half-width is twice that bound plus 1e-10, which covers the FP64
+    // path's own distance from the exact value (~1e-13) and the rounding of sum * amp against
+    // the threshold.
+    const double u = 1.0 / 16777216.0, eps = kPerlinF32ErrUlps * u, vmax = 2.01;
+    double err = 0.0, mag = 0.0;
+    for (int i = 0; i < kClimateSteps; i++) {
+        ClimateStep &s = st[i];
+        if (i == 0 || i == 8 || i == 12) err = mag = 0.0;   // a new running sum starts
+        const double c = s.c1 * s.c2;
+        mag += std::fabs(c);
+        err += std::fabs(c) * (eps + vmax * u) + vmax * u * mag;
+        s.cf = (float)c;
+        s.err = (float)(2.0 * err + 1e-10);
+        if (s.act == ACT_TIER || s.act == ACT_TIER_LAST) {
+            const double center = s.thr / s.amp, half = 2.0 * err + 1e-10;
+            s.lo = std::nextafter((float)(center - half), -INFINITY);
+            s.hi = std::nextafter((float)(center + half), INFINITY);
+        }
+    }
+}
+
+F32Bands wg::build_f32_bands(const ClimateStep *st) {
+    F32Bands b;
+    const double t_amp = st[11].amp, r_amp = st[17].amp, t_half = st[11].err, r_half = st[17].err;
+    const double t_thr[2] = {-0.45, 0.2}, r_thr[4] = {-0.91, -0.42, 0.42, 0.91};
+    for (int i = 0; i < 2; i++) {
+        b.t_lo[i] = std::nextafter((float)(t_thr[i] / t_amp - t_half), -INFINITY);
+        b.t_hi[i] = std::nextafter((float)(t_thr[i] / t_amp + t_half), INFINITY);
+    }
+    for (int i = 0; i < 4; i++) {
+        b.r_lo[i] = std::nextafter((float)(r_thr[i] / r_amp - r_half), -INFINITY);
+        b.r_hi[i] = std::nextafter((float)(r_thr[i] / r_amp + r_half), INFINITY);
+    }
+    return b;
+}
+
+void wg::upload_phase1_tables() {
+    NoiseSpec specs[N_NOISE_COUNT];
+    build_noise_specs(specs);
+    ClimateStep normal[kClimateSteps], large[kClimateSteps];
+    build_climate_steps(specs, N_EROSION, N_TEMPERATURE, normal);
+    build_climate_steps(specs, N_EROSION_LARGE, N_TEMPERATURE_LARGE, large);
+    const F32Bands bands[2] = {build_f32_bands(normal), build_f32_bands(large)};
+    upload_tables(specs, normal, large, bands);
 }
 
 #define WG_CUDA(call, what)                                        \
@@ -122,6 +172,8 @@ int run_batch(wg_engine *eng, const BatchArgs &proto, uint64_t unit0, uint32_t n
     for (int i = 0; i < P1_KINDS; i++) st.reject_hist[i] += (int64_t)eng->h_hist[i];
     for (int i = 0; i < kTiers; i++) st.tier_hist[i] += (int64_t)eng->h_hist[P1_KINDS + i];
     st.climate_survivors += eng->h_counters[CNT_SURVIVORS];
+    st.rechecks += eng->h_counters[CNT_RECHECK];
+    st.records += eng->h_counters[CNT_RECORDS];
     st.deep_candidates += eng->h_counters[CNT_DEEP];
     uint32_t nf = eng->h_counters[CNT_FINAL];
     if (nf) {
@@ -149,6 +201,7 @@ BatchArgs base_args(wg_engine *eng, const wg_opts &opts, int salt) {
     a.pre_26_2 = opts.pre_26_2;
     a.single_biome = opts.single_biome;
     a.large_biomes = opts.large_biomes;
+    a.fp32_core = eng->fp32_core;
     a.rec_unit = eng->rec_unit;
     a.rec_off = eng->rec_off;
     a.rec_cnt = eng->rec_cnt;
@@ -299,12 +352,7 @@ int wg_engine_open(int device, wg_engine **out) {
         WG_CUDA(cudaEventCreate(&eng->ev0), "event");
         WG_CUDA(cudaEventCreate(&eng->ev1), "event");
         for (int k = 0; k < 4; k++) WG_CUDA(cudaEventCreate(&eng->kev[k]), "event");
-        NoiseSpec specs[N_NOISE_COUNT];
-        build_noise_specs(specs);
-        ClimateStep normal[kClimateSteps], large[kClimateSteps];
-        build_climate_steps(specs, N_EROSION, N_TEMPERATURE, normal);
-        build_climate_steps(specs, N_EROSION_LARGE, N_TEMPERATURE_LARGE, large);
-        upload_tables(specs, normal, large);
+        upload_phase1_tables();
         WG_CUDA(cudaGetLastError(), "upload tables");
         WG_CUDA(cudaMalloc(&eng->rec_unit, sizeof(uint32_t) * kCapRec), "alloc");
         WG_CUDA(cudaMalloc(&eng->rec_off, sizeof(uint32_t) * kCapRec), "alloc");
@@ -356,6 +404,45 @@ void wg_engine_close(wg_engine *eng) {
 }
 
 const char *wg_engine_error(const wg_engine *eng) { return eng ? eng->err.c_str() : "no engine"; }
+
+int wg_noise_probe(wg_engine *eng, const int64_t *seeds, uint64_t n_seeds, int noise, const double *xz,
+                   uint64_t n_points, double *out32, double *out64) {
+    if (!eng || !seeds || !xz || !out32 || !out64 || n_seeds == 0 || n_points == 0 || noise < 0 ||
+        noise > N_CONTINENTALNESS_LARGE || n_seeds > (1u << 20) || n_points > (1u << 20) ||
+        n_seeds * n_points > (1ull << 26))
+        return eng ? eng->fail(WG_ERR_ARG, "noise probe: bad noise id or sizes") : WG_ERR_ARG;
+    WG_CUDA(cudaSetDevice(eng->device), "cudaSetDevice");
+    int64_t *d_seeds = nullptr;
+    double *d_xz = nullptr, *d_out = nullptr;
+    const size_t n_out = (size_t)(n_seeds * n_points);
+    int rc = [&]() -> int {
+        WG_CUDA(cudaMalloc(&d_seeds, sizeof(int64_t) * n_seeds), "alloc");
+        WG_CUDA(cudaMalloc(&d_xz, sizeof(double) * 2 * n_points), "alloc");
+        WG_CUDA(cudaMalloc(&d_out, sizeof(double) * 2 * n_out), "alloc");
+        WG_CUDA(cudaMemcpyAsync(d_seeds, seeds, sizeof(int64_t) * n_seeds, cudaMemcpyHostToDevice, eng->stream),
+                "copy");
+        WG_CUDA(cudaMemcpyAsync(d_xz, xz, sizeof(double) * 2 * n_points, cudaMemcpyHostToDevice, eng->stream), "copy");
+        launch_noise_probe(d_seeds, (uint32_t)n_seeds, noise, d_xz, (uint32_t)n_points, d_out, d_out + n_out,
+                           eng->stream);
+        WG_CUDA(cudaGetLastError(), "noise probe launch");
+        WG_CUDA(cudaMemcpyAsync(out32, d_out, sizeof(double) * n_out, cudaMemcpyDeviceToHost, eng->stream), "copy");
+        WG_CUDA(cudaMemcpyAsync(out64, d_out + n_out, sizeof(double) * n_out, cudaMemcpyDeviceToHost, eng->stream),
+                "copy");
+        WG_CUDA(cudaStreamSynchronize(eng->stream), "noise probe");
+        return WG_OK;
+    }();
+    cudaFree(d_seeds);
+    cudaFree(d_xz);
+    cudaFree(d_out);
+    return rc;
+}
+
+int wg_engine_set_noise_core(wg_engine *eng, int core) {
+    if (!eng || (core != WG_NOISE_FP32 && core != WG_NOISE_FP64 && core != WG_NOISE_FP32_RECHECK_ALL))
+        return WG_ERR_ARG;
+    eng->fp32_core = core == WG_NOISE_FP64 ? 0 : (core == WG_NOISE_FP32 ? 1 : 2);
+    return WG_OK;
+}
 
 int wg_seed_check(wg_engine *eng, const int64_t *seeds, uint64_t gen_base, uint64_t n_seeds, const wg_opts *opts,
                   int max_height, int salt, int rx0, int rx1, int rz0, int rz1, wg_candidate *out, uint64_t cap,

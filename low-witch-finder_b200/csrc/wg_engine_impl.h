@@ -21,6 +21,7 @@ struct P2Result;
 struct wg_engine {
     int device = 0;
     int sm_count = 148;
+    int fp32_core = 1;   // 1 FP32 core with FP64 rechecks, 0 FP64, 2 FP32 core re-taking every gate in FP64
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string err;

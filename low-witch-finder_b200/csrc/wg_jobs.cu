@@ -163,10 +163,13 @@ bool Scheduler::admit(SchedJob *j, int *rc) {
 
 int Scheduler::step(std::vector<SchedJob *> &finished, std::vector<SchedJob *> &members) {
     members.clear();
+    last_suspect_ = nullptr;
     if (order_.empty()) return WG_OK;
+    SchedJob *alone = suspects_.empty() ? nullptr : *suspects_.begin();   // a suspect runs by itself
+    last_suspect_ = alone;
     int rc = flush_uploads();   // the staged seeds of newly admitted jobs
     if (rc) return rc;
-    const SchedJob &lead = **order_.begin();
+    const SchedJob &lead = alone ? *alone : **order_.begin();
     uint64_t budget = step_work_;
     if (lead.opts.single_biome)   // every region survives the climate stage
         budget = std::min<uint64_t>(budget, kCapSurv / 2);
@@ -177,7 +180,7 @@ int Scheduler::step(std::vector<SchedJob *> &finished, std::vector<SchedJob *> &
     int misses = 0;   // consecutive jobs whose windows no longer fit the budget
     for (SchedJob *j : order_) {
         if (units >= kMaxUnits || budget == 0 || misses >= 64) break;
-        if (!same_rules(*j, lead)) continue;
+        if (!same_rules(*j, lead) || (alone && j != alone)) continue;
         uint64_t k = std::min<uint64_t>(j->units - j->dispatched, kMaxUnits - units);
         uint64_t kb = budget / j->win;
         if (kb == 0) {
@@ -225,6 +228,10 @@ int Scheduler::step(std::vector<SchedJob *> &finished, std::vector<SchedJob *> &
                                     eng_->stream);
     if (e != cudaSuccess) return eng_->fail(WG_ERR_CUDA, "upload job table", e);
 
+    if (fail_job)
+        for (const SchedJob *j : members)
+            if (j->id == fail_job) return eng_->fail(WG_ERR_CUDA, "injected batch failure");
+
     BatchArgs a = base_args(eng_, lead.opts, lead.salt);
     a.seeds = d_arena_;
     a.jobs = d_table_;
@@ -235,6 +242,8 @@ int Scheduler::step(std::vector<SchedJob *> &finished, std::vector<SchedJob *> &
     rc = run_batch(eng_, a, 0, (uint32_t)units, sink, stats);
     stage_used_ = 0;   // the batch's closing sync also ended the staged copies
     if (rc) return rc;
+    if (alone) suspects_.erase(alone);   // it passed by itself: an ordinary job again
+    last_suspect_ = nullptr;
 
     // survivors back to their jobs: seed_index is an arena slot until here
     std::vector<std::pair<uint64_t, size_t>> by_off(members.size());
@@ -274,8 +283,33 @@ void Scheduler::fail_all(int rc, std::vector<SchedJob *> &finished) {
         finished.push_back(j);
     }
     order_.clear();
+    suspects_.clear();
+    last_suspect_ = nullptr;
     runs_.clear();
     stage_used_ = 0;
+}
+
+void Scheduler::isolate(const std::vector<SchedJob *> &members) {
+    for (SchedJob *j : members) suspects_.insert(j);
+}
+
+void Scheduler::fail_suspect(int rc, std::vector<SchedJob *> &finished) {
+    SchedJob *j = last_suspect_;
+    last_suspect_ = nullptr;
+    if (!j) return;
+    cudaStreamSynchronize(eng_->stream);   // no staged copy may still read the staging buffer
+    order_.erase(j);
+    suspects_.erase(j);
+    j->status = rc;
+    release(j->arena_off, j->seeds.size());
+    finished.push_back(j);
+}
+
+// Whether an engine can run more batches after a failure: a non-sticky error is cleared here; a
+// broken context fails the synchronisation.
+bool engine_usable(wg_engine *eng) {
+    cudaGetLastError();
+    return cudaStreamSynchronize(eng->stream) == cudaSuccess && cudaGetLastError() == cudaSuccess;
 }
 
 }  // namespace wg
@@ -370,8 +404,8 @@ void server_loop(wg_server *s) {
             s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty() || !sched.idle(); });
             if (s->stop) return;
         }
-        // admit in arrival order while the seed arena has room (only this thread pops the queue)
-        int rc = WG_OK;
+        // admit in arrival order while the seed arena has room (only this thread pops the queue);
+        // a job whose admission fails (its seed upload) ends alone with that status
         for (;;) {
             SchedJob *j = nullptr;
             {
@@ -379,14 +413,36 @@ void server_loop(wg_server *s) {
                 if (s->queue.empty()) break;
                 j = s->queue.front();
             }
-            if (!sched.admit(j, &rc)) break;
+            int arc = WG_OK;
+            const bool in = sched.admit(j, &arc);
+            if (!in && arc == WG_OK) break;   // no room yet
             std::lock_guard<std::mutex> lk(s->mu);
             s->queue.pop_front();
             s->queued_seeds -= j->seeds.size();
+            if (!in) {
+                j->status = arc;
+                j->t_start = j->t_done = Clock::now();
+                j->started = j->done = true;
+                std::vector<int64_t>().swap(j->seeds);
+                s->cv_done.notify_all();
+            }
         }
         const auto t_step = Clock::now();
-        if (rc == WG_OK) rc = sched.step(finished, members);
-        if (rc) sched.fail_all(rc, finished);
+        int rc = sched.step(finished, members);
+        bool broken = false;
+        if (rc) {
+            // Failure isolation: while the engine still works, a failed batch fails no job by
+            // itself; its jobs run again one at a time, and only a job that fails alone ends
+            // with the error.  A broken context ends every job, queued ones included.
+            if (!engine_usable(s->eng)) {
+                sched.fail_all(rc, finished);
+                broken = true;
+            } else if (sched.last_was_suspect()) {
+                sched.fail_suspect(rc, finished);
+            } else {
+                sched.isolate(members);
+            }
+        }
         const auto t_end = Clock::now();
         std::lock_guard<std::mutex> lk(s->mu);
         for (SchedJob *j : members) {
@@ -405,7 +461,7 @@ void server_loop(wg_server *s) {
             j->done = true;
             std::vector<int64_t>().swap(j->seeds);
         }
-        if (rc) {   // a failed batch also fails the jobs still queued behind it
+        if (broken) {   // a broken engine also fails the jobs still queued behind it
             for (SchedJob *j : s->queue) {
                 j->status = rc;
                 j->t_start = j->t_done = t_end;
@@ -424,9 +480,11 @@ void server_loop(wg_server *s) {
 
 extern "C" {
 
-int wg_server_open(int device, uint64_t max_queued_seeds, wg_server **out) {
+int wg_server_open_config(int device, const wg_server_config *cfg, wg_server **out) {
     if (!out) return WG_ERR_ARG;
     *out = nullptr;
+    wg_server_config c{};
+    if (cfg) c = *cfg;
     auto s = std::make_unique<wg_server>();
     s->device = device;
     int rc = wg_engine_open(device, &s->eng);
@@ -434,10 +492,12 @@ int wg_server_open(int device, uint64_t max_queued_seeds, wg_server **out) {
     // seeds resident on the device: a quarter of the free HBM, at most 2^28 (2 GiB)
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 1ull << 30;
-    const uint64_t arena = std::max<uint64_t>(1ull << 20, std::min<uint64_t>(free_b / 4 / sizeof(int64_t), 1ull << 28));
-    s->max_queued = max_queued_seeds ? max_queued_seeds : (1ull << 30);
+    const uint64_t arena = c.arena_seeds ? c.arena_seeds
+                                         : std::max<uint64_t>(1ull << 20, std::min<uint64_t>(free_b / 4 / sizeof(int64_t), 1ull << 28));
+    s->max_queued = c.max_queued_seeds ? c.max_queued_seeds : (1ull << 30);
     // small batches keep a short job's wait behind the batch in flight short
-    s->sched = std::make_unique<Scheduler>(s->eng, arena, kWorkPerBatch / 4);
+    s->sched = std::make_unique<Scheduler>(s->eng, arena, c.batch_checks ? c.batch_checks : kWorkPerBatch / 4);
+    s->sched->fail_job = c.fail_job;
     rc = s->sched->init();
     if (rc) {
         s->sched.reset();
@@ -447,6 +507,12 @@ int wg_server_open(int device, uint64_t max_queued_seeds, wg_server **out) {
     s->worker = std::thread(server_loop, s.get());
     *out = s.release();
     return WG_OK;
+}
+
+int wg_server_open(int device, uint64_t max_queued_seeds, wg_server **out) {
+    wg_server_config c{};
+    c.max_queued_seeds = max_queued_seeds;
+    return wg_server_open_config(device, &c, out);
 }
 
 int wg_server_submit(wg_server *s, const wg_job *job, uint64_t *job_id) {

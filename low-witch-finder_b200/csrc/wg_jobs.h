@@ -56,8 +56,20 @@ class Scheduler {
     int step(std::vector<SchedJob *> &finished, std::vector<SchedJob *> &members);
     // Ends every admitted job with status rc (after a failed step) and frees their seed slots.
     void fail_all(int rc, std::vector<SchedJob *> &finished);
+    // After a failed step whose engine is still usable: the step's members become suspects, and
+    // the following steps run one suspect at a time; a suspect whose own step fails ends with
+    // that status (its seed slots freed), the others go on as before.  Units of the failed step
+    // were not marked dispatched, so they run again.
+    void isolate(const std::vector<SchedJob *> &members);
+    // Whether the last failed step ran a single suspect (its failure is that job's own).
+    bool last_was_suspect() const { return last_suspect_ != nullptr; }
+    // Ends the suspect of the last failed step with status rc.
+    void fail_suspect(int rc, std::vector<SchedJob *> &finished);
     bool idle() const { return order_.empty(); }
     uint64_t arena_seeds() const { return arena_cap_; }
+    // Host-side fault injection (tests): every step holding the job with this id fails with
+    // WG_ERR_CUDA before its kernels are launched (0 = none).
+    uint64_t fail_job = 0;
     wg_scan_stats stats{};
 
    private:
@@ -80,6 +92,8 @@ class Scheduler {
     std::set<SchedJob *, ByWork> order_;   // the admitted jobs (keys change only while out of the set)
     std::vector<Candidate> found_;
     std::vector<JobGeom> table_;
+    std::set<SchedJob *> suspects_;       // members of a failed step, run alone until they pass
+    SchedJob *last_suspect_ = nullptr;    // the suspect the last step ran alone
     // Seeds of small jobs are gathered in a pinned staging buffer and copied to the arena in
     // runs of consecutive slots before the next batch.
     int64_t *h_stage_ = nullptr;

@@ -60,12 +60,7 @@ int g_sm_count[kMaxDevices] = {};
 int setup_device(int dev) {
     std::lock_guard<std::mutex> lock(g_setup_mu);
     if (g_scratch_ptr[dev]) return WG_OK;
-    NoiseSpec specs[N_NOISE_COUNT];
-    build_noise_specs(specs);
-    ClimateStep normal[kClimateSteps], large[kClimateSteps];
-    build_climate_steps(specs, N_EROSION, N_TEMPERATURE, normal);
-    build_climate_steps(specs, N_EROSION_LARGE, N_TEMPERATURE_LARGE, large);
-    upload_tables(specs, normal, large);
+    upload_phase1_tables();
     if (cudaGetLastError() != cudaSuccess) return WG_ERR_CUDA;
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return WG_ERR_CUDA;
@@ -112,6 +107,7 @@ extern "C" int wg_seed_check_noalloc(const int64_t *d_seeds, uint64_t gen_base, 
         a.single_biome = opts->single_biome;
         a.large_biomes = opts->large_biomes;
     }
+    a.fp32_core = 1;   // the engine's default noise core
     a.counters = reinterpret_cast<uint32_t *>(base + kOffCounters);
     a.hist = reinterpret_cast<unsigned long long *>(base + kOffHist);
     a.rec_unit = reinterpret_cast<uint32_t *>(base + kOffRecUnit);

@@ -2,6 +2,8 @@
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "wg_device.cuh"
 #include "wg_phase1.cuh"
 
@@ -13,6 +15,7 @@ __constant__ NoiseSpec c_noise[N_NOISE_COUNT];
 __constant__ ClimateStep c_steps[2][kClimateSteps];     // [large_biomes][step]
 __constant__ int8_t c_slot_a[2][kSlotsA][3];             // climate slots: noise, sub, octave
 __constant__ int8_t c_slot_c[2][kSlotsC][3];             // cave slots (the entrance kernel uses the first 18)
+__constant__ F32Bands c_bands[2];                        // [large_biomes] FP32 core: temperature / ridge bands
 
 // Slot bases of each noise inside the cave slot set (sub 0 octaves, then sub 1 octaves).
 constexpr int kBaseEntrance = 0, kBaseRarity = 6, kBaseThickness = 8, kBaseSp1 = 10, kBaseSp2 = 12;
@@ -34,8 +37,10 @@ static void fill_slots(int8_t (*dst)[3], const NoiseSpec *specs, const int *nois
     (void)expect;
 }
 
-void upload_tables(const NoiseSpec *specs, const ClimateStep *steps_normal, const ClimateStep *steps_large) {
+void upload_tables(const NoiseSpec *specs, const ClimateStep *steps_normal, const ClimateStep *steps_large,
+                   const F32Bands *bands) {
     cudaMemcpyToSymbol(c_noise, specs, sizeof(NoiseSpec) * N_NOISE_COUNT);
+    cudaMemcpyToSymbol(c_bands, bands, sizeof(F32Bands) * 2);
     ClimateStep st[2][kClimateSteps];
     for (int i = 0; i < kClimateSteps; i++) {
         st[0][i] = steps_normal[i];
@@ -223,16 +228,35 @@ struct ClimateSteps {
     double sc[kClimateSteps], lac[kClimateSteps], c1[kClimateSteps], c2[kClimateSteps];
     double thr[kClimateSteps], amp[kClimateSteps];
     int slot[kClimateSteps], act[kClimateSteps], tier[kClimateSteps];
+    float cf[kClimateSteps], lo[kClimateSteps], hi[kClimateSteps];   // FP32 core (ClimateStep)
 };
 
+// Per-table y origin: the FP64 path keeps hy and fade(hy) as doubles; the FP32 core keeps hy as a
+// double (for its FP64 rechecks, which recompute fade(hy) in the reference's order) and
+// rn(hy), rn(fade(hy)) as floats.
+template <bool F32>
+struct TableY {
+    double hy[kSlotsA * kUnits], fy[kSlotsA * kUnits];
+    __device__ __forceinline__ double fy64(int o) const { return fy[o]; }
+};
+template <>
+struct TableY<true> {
+    double hy[kSlotsA * kUnits];
+    float hyf[kSlotsA * kUnits], fyf[kSlotsA * kUnits];
+    __device__ __forceinline__ double fy64(int o) const { return fade(hy[o]); }
+};
+
+template <bool F32>
 struct ClimateSmem {
+    using Real = typename std::conditional<F32, float, double>::type;
     uint8_t perm[kSlotsA * kPitch];           // slot s, row k, unit u at s * kPitch + k * kUnits + u
-    double ox[kSlotsA * kUnits], oz[kSlotsA * kUnits], hy[kSlotsA * kUnits], fy[kSlotsA * kUnits];
+    double ox[kSlotsA * kUnits], oz[kSlotsA * kUnits];
+    TableY<F32> ty;
     int jy[kSlotsA * kUnits];
     int2 pos[kChunk * kUnits];                 // hut chunk (cx, cz) of window offset c0 + j, unit u
     union {
-        double tsum[kTierList];                // erosion partial sum of each tier-0 survivor
-        double val[kClimateList * 6];          // parallel temperature / ridge samples (after the tiers)
+        Real tsum[kTierList];                  // erosion partial sum of each tier-0 survivor
+        Real val[kClimateList * 6];            // parallel temperature / ridge samples (after the tiers)
     };
     uint32_t tlist[kTierList];                 // tier-0 survivors of the chunk: unit << 16 | (j - c0)
     uint32_t clist[kClimateList];              // erosion survivors of the chunk
@@ -249,10 +273,11 @@ struct ClimateSmem {
     uint32_t rwu[kUnits];                      // rect width of the unit's job
     unsigned int hist[P1_KINDS + kTiers];
     uint32_t grad[kGradWords];
+    float gradf[kGradWords];
     ClimateSteps steps;
 };
 
-size_t climate_smem_bytes() { return sizeof(ClimateSmem); }
+size_t climate_smem_bytes(bool fp32_core) { return fp32_core ? sizeof(ClimateSmem<true>) : sizeof(ClimateSmem<false>); }
 
 // A record holding one survivor, for a unit whose shared list is full.
 __device__ void emit_single(const BatchArgs &a, uint32_t u, uint32_t off_in_win) {
@@ -269,14 +294,15 @@ __device__ void emit_single(const BatchArgs &a, uint32_t u, uint32_t off_in_win)
     }
 }
 
-__device__ __forceinline__ void keep_survivor(ClimateSmem &S, const BatchArgs &a, int iu, uint32_t j) {
+template <class Sm>
+__device__ __forceinline__ void keep_survivor(Sm &S, const BatchArgs &a, int iu, uint32_t j) {
     uint32_t q = atomicAdd(&S.cnt[iu], 1u);
     if (q < kRecordCap) S.surv[iu * kRecordCap + q] = j;
     else emit_single(a, blockIdx.x * kUnits + (uint32_t)iu, j);
 }
 
-__device__ __forceinline__ void climate_reject(ClimateSmem &S, const BatchArgs &a, int iu, uint32_t j, int code,
-                                               int tier) {
+template <class Sm>
+__device__ __forceinline__ void climate_reject(Sm &S, const BatchArgs &a, int iu, uint32_t j, int code, int tier) {
     atomicAdd(&S.hist[code], 1u);
     if (tier >= 0) atomicAdd(&S.hist[P1_KINDS + tier], 1u);
     note_code(a, S.g[iu], S.rbase[iu] + j, code, tier);
@@ -297,24 +323,66 @@ struct TierCounts {
     }
 };
 
-__device__ __forceinline__ void erosion_reject(const ClimateSmem &S, const BatchArgs &a, TierCounts &tc, int iu,
-                                               uint32_t j, int tier) {
+template <class Sm>
+__device__ __forceinline__ void erosion_reject(const Sm &S, const BatchArgs &a, TierCounts &tc, int iu, uint32_t j,
+                                               int tier) {
     tc.add(tier);
     note_code(a, S.g[iu], S.rbase[iu] + j, P1_EROSION, tier);
 }
 
-// One y = 0 Perlin sample of climate step k for unit iu at climate point (xc, zc).
-__device__ __forceinline__ double climate_sample(const ClimateSmem &S, int iu, int k, double xc, double zc) {
+// One y = 0 Perlin sample of climate step k for unit iu at climate point (xc, zc), in FP64 with
+// the reference's operations (the FP64 path, and the FP32 core's rechecks).
+template <class Sm>
+__device__ __forceinline__ double climate_sample(const Sm &S, int iu, int k, double xc, double zc) {
     const ClimateSteps &st = S.steps;
     const int slot = st.slot[k];
     const int o = slot * kUnits + iu;
     const double sc = st.sc[k], lac = st.lac[k];
     ColTable<kUnits> T{S.perm + slot * kPitch + iu, S.grad};
-    return perlin_y0(T, S.ox[o], S.oz[o], S.jy[o], S.hy[o], S.fy[o], keep_precision((xc * sc) * lac),
+    return perlin_y0(T, S.ox[o], S.oz[o], S.jy[o], S.ty.hy[o], S.ty.fy64(o), keep_precision((xc * sc) * lac),
                      keep_precision((zc * sc) * lac));
 }
 
-__device__ __forceinline__ void climate_point(const ClimateSmem &S, int iu, uint32_t jl, double &xc, double &zc) {
+// The same sample in the FP32 core (coordinates reduced in FP64, the rest in FP32).
+__device__ __forceinline__ float climate_sample_f32(const ClimateSmem<true> &S, int iu, int k, double xc, double zc) {
+    const ClimateSteps &st = S.steps;
+    const int slot = st.slot[k];
+    const int o = slot * kUnits + iu;
+    const double sc = st.sc[k], lac = st.lac[k];
+    ColTableF<kUnits> T{S.perm + slot * kPitch + iu, S.gradf};
+    return perlin_y0_f32(T, S.ox[o], S.oz[o], S.jy[o], S.ty.hyf[o], S.ty.fyf[o], keep_precision((xc * sc) * lac),
+                         keep_precision((zc * sc) * lac));
+}
+
+// FP64 octave sum of climate steps [k0, k1] in the reference's order (sum += (c1 * v) * c2):
+// the exact partial sum an FP32 recheck decides on.
+template <class Sm>
+__device__ __noinline__ double climate_sum64(const Sm &S, int iu, int k0, int k1, double xc, double zc) {
+    const ClimateSteps &st = S.steps;
+    double sum = 0.0;
+    for (int k = k0; k <= k1; k++) sum += (st.c1[k] * climate_sample(S, iu, k, xc, zc)) * st.c2[k];
+    return sum;
+}
+
+// FP64 DoublePerlin value of a temperature / ridge noise whose steps are k0 .. k0 + n - 1 (sub A,
+// then sub B; ACT_END_SUB_A closes sub A), as the state machine combines it.
+template <class Sm>
+__device__ __noinline__ double climate_value64(const Sm &S, int iu, int k0, int n, double xc, double zc) {
+    const ClimateSteps &st = S.steps;
+    double sum = 0.0, sum_a = 0.0;
+    for (int p = 0; p < n; p++) {
+        const int k = k0 + p;
+        sum += (st.c1[k] * climate_sample(S, iu, k, xc, zc)) * st.c2[k];
+        if (st.act[k] == ACT_END_SUB_A) {
+            sum_a = sum;
+            sum = 0.0;
+        }
+    }
+    return (sum_a + sum) * st.amp[k0 + n - 1];
+}
+
+template <class Sm>
+__device__ __forceinline__ void climate_point(const Sm &S, int iu, uint32_t jl, double &xc, double &zc) {
     const int2 c = S.pos[jl * kUnits + iu];
     xc = (c.x * 16 + 8) / 4.0;
     zc = (c.y * 16 + 8) / 4.0;
@@ -323,8 +391,10 @@ __device__ __forceinline__ void climate_point(const ClimateSmem &S, int iu, uint
 // The erosion tiers from step k0 for one region (e = unit << 16 | offset in the chunk), one Perlin
 // sample per loop trip, run by one thread: the path for a tier-0 survivor that finds the tier list
 // full.  A region that passes the last tier is handed to the climate list; if that list is full
-// too, this thread also runs its temperature and ridge steps.
-__device__ void climate_rest(ClimateSmem &S, const BatchArgs &a, TierCounts &tc, uint32_t e, uint32_t c0, int k0, double sum,
+// too, this thread also runs its temperature and ridge steps.  Always FP64 (the FP32 core enters
+// it with k0 = 0 and recomputes the partial sum exactly).
+template <class Sm>
+__device__ void climate_rest(Sm &S, const BatchArgs &a, TierCounts &tc, uint32_t e, uint32_t c0, int k0, double sum,
                              double xc, double zc) {
     const ClimateSteps &st = S.steps;
     const int iu = (int)(e >> 16);
@@ -386,14 +456,26 @@ __device__ void climate_rest(ClimateSmem &S, const BatchArgs &a, TierCounts &tc,
 // region, a uniform loop that rejects ~57 %; (2) the remaining erosion tiers for the survivors,
 // taken from a shared list by any thread; (3) temperature and (4) ridge for the ~5 % that pass
 // erosion, one sample per thread, summed per region in the reference's order.
+//
+// F32 (the FP32 noise core): every sample of the four phases is taken in FP32 (perlin_y0_f32)
+// and the partial sums are carried in FP32.  A gate decides from the FP32 value when it lies
+// outside the step's error band ([lo, hi) around the threshold in sum space, from the derived
+// bound); inside the band the thread recomputes that region's samples in FP64 in the reference's
+// order and decides exactly as the FP64 path does.  So every decision, and with it the reject
+// codes, tier histogram and survivor set, equals the FP64 path's.
+template <bool F32>
 __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
+    using Real = typename ClimateSmem<F32>::Real;
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    ClimateSmem &S = *reinterpret_cast<ClimateSmem *>(smem_raw);
+    ClimateSmem<F32> &S = *reinterpret_cast<ClimateSmem<F32> *>(smem_raw);
     const int tid = threadIdx.x;
     const int my_slot = tid / kUnits, uu = tid % kUnits;
     const int large = a.large_biomes ? 1 : 0;
+    uint32_t rechecks = 0;
+    const bool all_rechecks = F32 && a.fp32_core == 2;   // every FP32 gate re-taken in FP64 (a check mode)
     if (tid < P1_KINDS + kTiers) S.hist[tid] = 0;
     fill_grad_table(S.grad, tid);
+    if (F32) fill_grad_table_f32(S.gradf, tid);
     if (tid < kClimateSteps) {
         const ClimateStep &c = c_steps[large][tid];
         S.steps.sc[tid] = c.sc;
@@ -405,6 +487,9 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
         S.steps.slot[tid] = c.slot;
         S.steps.act[tid] = c.act;
         S.steps.tier[tid] = c.tier;
+        S.steps.cf[tid] = c.cf;
+        S.steps.lo[tid] = c.lo;
+        S.steps.hi[tid] = c.hi;
     }
 
     const uint32_t u = blockIdx.x * kUnits + (uint32_t)uu;
@@ -442,8 +527,13 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
             double hy = oy - jy;
             S.ox[o] = ox;
             S.oz[o] = oz;
-            S.hy[o] = hy;
-            S.fy[o] = fade(hy);
+            S.ty.hy[o] = hy;
+            if constexpr (F32) {
+                S.ty.hyf[o] = __double2float_rn(hy);
+                S.ty.fyf[o] = __double2float_rn(fade(hy));
+            } else {
+                S.ty.fy[o] = fade(hy);
+            }
             S.jy[o] = jy;
         }
     }
@@ -491,10 +581,25 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                 }
                 double xc, zc;
                 climate_point(S, iu, jl, xc, zc);
-                double sum = 0.0;
-                sum += (st.c1[0] * climate_sample(S, iu, 0, xc, zc)) * st.c2[0];
-                sum += (st.c1[1] * climate_sample(S, iu, 1, xc, zc)) * st.c2[1];
-                const bool pass = !(sum * st.amp[1] < st.thr[1]);
+                Real sum;
+                bool pass;
+                if constexpr (F32) {
+                    sum = __fmul_rn(st.cf[0], climate_sample_f32(S, iu, 0, xc, zc));
+                    sum = __fmaf_rn(st.cf[1], climate_sample_f32(S, iu, 1, xc, zc), sum);
+                    if (!all_rechecks && sum < st.lo[1]) {
+                        pass = false;
+                    } else if (!all_rechecks && sum >= st.hi[1]) {
+                        pass = true;
+                    } else {   // inside the error band: decide in FP64
+                        rechecks++;
+                        pass = !(climate_sum64(S, iu, 0, 1, xc, zc) * st.amp[1] < st.thr[1]);
+                    }
+                } else {
+                    sum = 0.0;
+                    sum += (st.c1[0] * climate_sample(S, iu, 0, xc, zc)) * st.c2[0];
+                    sum += (st.c1[1] * climate_sample(S, iu, 1, xc, zc)) * st.c2[1];
+                    pass = !(sum * st.amp[1] < st.thr[1]);
+                }
                 // warp-aggregated append of the survivors to the tier list
                 cg::coalesced_group grp = cg::coalesced_threads();
                 const unsigned m = grp.ballot(pass);
@@ -508,9 +613,11 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                     if (t < kTierList) {
                         S.tlist[t] = ((uint32_t)iu << 16) | jl;
                         S.tsum[t] = sum;
+                    } else if (F32) {
+                        // list full: this thread walks the region through the rest itself, in FP64
+                        climate_rest(S, a, tc, ((uint32_t)iu << 16) | jl, c0, 0, 0.0, xc, zc);
                     } else {
-                        // list full: this thread walks the region through the rest itself
-                        climate_rest(S, a, tc, ((uint32_t)iu << 16) | jl, c0, 2, sum, xc, zc);
+                        climate_rest(S, a, tc, ((uint32_t)iu << 16) | jl, c0, 2, (double)sum, xc, zc);
                     }
                 }
             }
@@ -531,23 +638,38 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                 const uint32_t n_t = S.tcount[(k - 1) & 1];
                 if (tid == 0) S.tcount[k & 1] = 0;
                 const double c1 = st.c1[k], c2 = st.c2[k], amp = st.amp[k], thr = st.thr[k];
+                const float cf = st.cf[k], lo = st.lo[k], hi = st.hi[k];
                 const int tier = st.tier[k];
                 const bool last = st.act[k] == ACT_TIER_LAST;
                 uint32_t ke[kPer];
-                double ks[kPer];
+                Real ks[kPer];
 #pragma unroll
                 for (int r = 0; r < kPer; r++) {
                     const uint32_t q = (uint32_t)tid + (uint32_t)(r * kThreadsA);
                     ke[r] = 0xFFFFFFFFu;
-                    ks[r] = 0.0;
+                    ks[r] = 0;
                     if (q < n_t) {
                         const uint32_t e = S.tlist[q];
                         const int iu = (int)(e >> 16);
                         double xc, zc;
                         climate_point(S, iu, e & 0xFFFFu, xc, zc);
-                        double sum = S.tsum[q];
-                        sum += (c1 * climate_sample(S, iu, k, xc, zc)) * c2;
-                        if (sum * amp < thr) {
+                        Real sum = S.tsum[q];
+                        bool reject;
+                        if constexpr (F32) {
+                            sum = __fmaf_rn(cf, climate_sample_f32(S, iu, k, xc, zc), sum);
+                            if (!all_rechecks && sum < lo) {
+                                reject = true;
+                            } else if (!all_rechecks && sum >= hi) {
+                                reject = false;
+                            } else {   // inside the error band: the exact partial sum of steps 0..k
+                                rechecks++;
+                                reject = climate_sum64(S, iu, 0, k, xc, zc) * amp < thr;
+                            }
+                        } else {
+                            sum += (c1 * climate_sample(S, iu, k, xc, zc)) * c2;
+                            reject = sum * amp < thr;
+                        }
+                        if (reject) {
                             erosion_reject(S, a, tc, iu, c0 + (e & 0xFFFFu), tier);
                         } else {
                             ke[r] = e;
@@ -594,22 +716,40 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
             const int iu = (int)(e >> 16);
             double xc, zc;
             climate_point(S, iu, e & 0xFFFFu, xc, zc);
-            S.val[t] = climate_sample(S, iu, kT0 + (int)(t % 4), xc, zc);
+            if constexpr (F32) S.val[t] = climate_sample_f32(S, iu, kT0 + (int)(t % 4), xc, zc);
+            else S.val[t] = climate_sample(S, iu, kT0 + (int)(t % 4), xc, zc);
         }
         __syncthreads();
         for (uint32_t i = tid; i < n_cl; i += kThreadsA) {
             const uint32_t e = S.clist[i];
-            double sum = 0.0, sum_a = 0.0;
-            for (int p = 0; p < 4; p++) {   // the state machine's accumulation, steps kT0..kT0+3
-                const int k = kT0 + p;
-                sum += (st.c1[k] * S.val[i * 4 + p]) * st.c2[k];
-                if (st.act[k] == ACT_END_SUB_A) {
-                    sum_a = sum;
-                    sum = 0.0;
+            bool bad;
+            if constexpr (F32) {
+                float sum = 0.0f;
+                for (int p = 0; p < 4; p++) sum = __fmaf_rn(st.cf[kT0 + p], S.val[i * 4 + p], sum);
+                const F32Bands &B = c_bands[large];
+                if (all_rechecks || (sum >= B.t_lo[0] && sum < B.t_hi[0]) || (sum >= B.t_lo[1] && sum < B.t_hi[1])) {
+                    rechecks++;
+                    double xc, zc;
+                    climate_point(S, (int)(e >> 16), e & 0xFFFFu, xc, zc);
+                    const double t = climate_value64(S, (int)(e >> 16), kT0, 4, xc, zc);
+                    bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
+                } else {
+                    const bool low = sum < B.t_lo[0], high = sum >= B.t_hi[1];   // t < -0.45, t > 0.2
+                    bad = a.mc_1_18_2 ? low : (low || high);
                 }
+            } else {
+                double sum = 0.0, sum_a = 0.0;
+                for (int p = 0; p < 4; p++) {   // the state machine's accumulation, steps kT0..kT0+3
+                    const int k = kT0 + p;
+                    sum += (st.c1[k] * S.val[i * 4 + p]) * st.c2[k];
+                    if (st.act[k] == ACT_END_SUB_A) {
+                        sum_a = sum;
+                        sum = 0.0;
+                    }
+                }
+                const double t = (sum_a + sum) * st.amp[kT0 + 3];
+                bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
             }
-            const double t = (sum_a + sum) * st.amp[kT0 + 3];
-            const bool bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
             if (bad) climate_reject(S, a, (int)(e >> 16), c0 + (e & 0xFFFFu), P1_TEMPERATURE, -1);
             else S.rlist[atomicAdd(&S.n_rlist, 1u)] = e;
         }
@@ -622,29 +762,54 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
             const int iu = (int)(e >> 16);
             double xc, zc;
             climate_point(S, iu, e & 0xFFFFu, xc, zc);
-            S.val[t] = climate_sample(S, iu, kR0 + (int)(t % 6), xc, zc);
+            if constexpr (F32) S.val[t] = climate_sample_f32(S, iu, kR0 + (int)(t % 6), xc, zc);
+            else S.val[t] = climate_sample(S, iu, kR0 + (int)(t % 6), xc, zc);
         }
         __syncthreads();
         for (uint32_t i = tid; i < n_rl; i += kThreadsA) {
             const uint32_t e = S.rlist[i];
             const int iu = (int)(e >> 16);
             const uint32_t j = c0 + (e & 0xFFFFu);
-            double sum = 0.0, sum_a = 0.0;
-            for (int p = 0; p < 6; p++) {
-                const int k = kR0 + p;
-                sum += (st.c1[k] * S.val[i * 6 + p]) * st.c2[k];
-                if (st.act[k] == ACT_END_SUB_A) {
-                    sum_a = sum;
-                    sum = 0.0;
+            bool bad;
+            if constexpr (F32) {
+                float sum = 0.0f;
+                for (int p = 0; p < 6; p++) sum = __fmaf_rn(st.cf[kR0 + p], S.val[i * 6 + p], sum);
+                const F32Bands &B = c_bands[large];
+                bool inside = all_rechecks;
+                for (int q = 0; q < 4; q++) inside |= sum >= B.r_lo[q] && sum < B.r_hi[q];
+                if (inside) {
+                    rechecks++;
+                    double xc, zc;
+                    climate_point(S, iu, e & 0xFFFFu, xc, zc);
+                    const double rg = climate_value64(S, iu, kR0, 6, xc, zc);
+                    bad = (rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91);
+                } else {
+                    // above[q]: the ridge value lies above threshold q (-0.91, -0.42, 0.42, 0.91)
+                    const bool a0 = sum >= B.r_hi[0], a1 = sum >= B.r_hi[1], a2 = sum >= B.r_hi[2],
+                               a3 = sum >= B.r_hi[3];
+                    bad = (a2 && !a3) || (!a1 && a0) || (!a.pre_26_2 && !a0);
                 }
+            } else {
+                double sum = 0.0, sum_a = 0.0;
+                for (int p = 0; p < 6; p++) {
+                    const int k = kR0 + p;
+                    sum += (st.c1[k] * S.val[i * 6 + p]) * st.c2[k];
+                    if (st.act[k] == ACT_END_SUB_A) {
+                        sum_a = sum;
+                        sum = 0.0;
+                    }
+                }
+                const double rg = (sum_a + sum) * st.amp[kR0 + 5];
+                bad = (rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91);
             }
-            const double rg = (sum_a + sum) * st.amp[kR0 + 5];
-            if ((rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91))
-                climate_reject(S, a, iu, j, P1_RIDGE, -1);
-            else
-                keep_survivor(S, a, iu, j);
+            if (bad) climate_reject(S, a, iu, j, P1_RIDGE, -1);
+            else keep_survivor(S, a, iu, j);
         }
         __syncthreads();
+    }
+    if constexpr (F32) {
+        const uint32_t n = __reduce_add_sync(0xFFFFFFFFu, rechecks);
+        if ((tid & 31) == 0 && n) atomicAdd(&a.counters[CNT_RECHECK], n);
     }
 
     // ---- erosion rejections counted in registers: one warp sum per tier ----
@@ -690,10 +855,81 @@ static void allow_dynamic_smem(K kernel, size_t bytes, unsigned long long &done_
 }
 
 void launch_climate(const BatchArgs &a, cudaStream_t s) {
-    static unsigned long long done = 0;
-    allow_dynamic_smem(climate_kernel, sizeof(ClimateSmem), done);
+    static unsigned long long done64 = 0, done32 = 0;
     int grid = (int)((a.n_units + kUnits - 1) / kUnits);
-    climate_kernel<<<grid, kThreadsA, sizeof(ClimateSmem), s>>>(a);
+    if (a.fp32_core) {
+        allow_dynamic_smem(climate_kernel<true>, sizeof(ClimateSmem<true>), done32);
+        climate_kernel<true><<<grid, kThreadsA, sizeof(ClimateSmem<true>), s>>>(a);
+    } else {
+        allow_dynamic_smem(climate_kernel<false>, sizeof(ClimateSmem<false>), done64);
+        climate_kernel<false><<<grid, kThreadsA, sizeof(ClimateSmem<false>), s>>>(a);
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Noise probe: one y = 0 DoublePerlin noise of one world seed per CTA, sampled at a list of
+// points both in FP64 (the reference's order, noise.c:320-342) and in the FP32 core (the
+// samples of perlin_y0_f32 summed as the climate kernel sums them, times the amplitude): the
+// measured error of the FP32 core.
+// ------------------------------------------------------------------------------------
+constexpr int kProbeThreads = 256;
+constexpr int kProbeStride = 20;   // bytes per table row: one column per table (<= 18 tables)
+
+__global__ void __launch_bounds__(kProbeThreads) noise_probe_kernel(const int64_t *seeds, int noise, const double *xz,
+                                                                     uint32_t n_points, double *out32, double *out64) {
+    __shared__ __align__(16) uint8_t perm[256 * kProbeStride];
+    __shared__ double ox[2 * kMaxOct], oz[2 * kMaxOct], hy[2 * kMaxOct], fy[2 * kMaxOct];
+    __shared__ float hyf[2 * kMaxOct], fyf[2 * kMaxOct];
+    __shared__ int jy[2 * kMaxOct];
+    __shared__ uint32_t grad[kGradWords];
+    __shared__ float gradf[kGradWords];
+    const int t = threadIdx.x;
+    const NoiseSpec &ns = c_noise[noise];
+    const int np = ns.npresent;
+    const uint64_t seed = (uint64_t)seeds[blockIdx.x];
+    fill_grad_table(grad, t);
+    fill_grad_table_f32(gradf, t);
+    perm_blocks_init<kProbeStride, 256 * kProbeStride>(perm, 1, t, kProbeThreads);
+    __syncthreads();
+    if (t < 2 * np) {
+        Xr r = octave_rng(ns, seed_fork_of(seed), t / np, t % np);
+        double x0, y0, z0;
+        perlin_shuffle<kProbeStride>(perm + t, r, x0, y0, z0);
+        const int j = (int)floor(y0);
+        const double h = y0 - j;
+        ox[t] = x0;
+        oz[t] = z0;
+        jy[t] = j;
+        hy[t] = h;
+        fy[t] = fade(h);
+        hyf[t] = __double2float_rn(h);
+        fyf[t] = __double2float_rn(fade(h));
+    }
+    __syncthreads();
+    for (uint32_t i = t; i < n_points; i += kProbeThreads) {
+        const double x = xz[2 * i], z = xz[2 * i + 1];
+        double a = 0.0, b = 0.0;
+        float s = 0.0f;
+        for (int q = 0; q < 2 * np; q++) {
+            const int p = q % np;
+            const double sc = q < np ? 1.0 : kDblScale, l = ns.lac[p];
+            const double px = keep_precision((x * sc) * l), pz = keep_precision((z * sc) * l);
+            const ColTable<kProbeStride> T{perm + q, grad};
+            const ColTableF<kProbeStride> TF{perm + q, gradf};
+            const double v = perlin_y0(T, ox[q], oz[q], jy[q], hy[q], fy[q], px, pz);
+            if (q < np) a += (ns.amp[p] * v) * ns.per[p];
+            else b += (ns.amp[p] * v) * ns.per[p];
+            s = __fmaf_rn((float)(ns.amp[p] * ns.per[p]), perlin_y0_f32(TF, ox[q], oz[q], jy[q], hyf[q], fyf[q], px, pz), s);
+        }
+        const size_t o = (size_t)blockIdx.x * n_points + i;
+        out64[o] = (a + b) * ns.amplitude;
+        out32[o] = (double)s * ns.amplitude;
+    }
+}
+
+void launch_noise_probe(const int64_t *d_seeds, uint32_t n_seeds, int noise, const double *d_xz, uint32_t n_points,
+                        double *d_out32, double *d_out64, cudaStream_t s) {
+    noise_probe_kernel<<<n_seeds, kProbeThreads, 0, s>>>(d_seeds, noise, d_xz, n_points, d_out32, d_out64);
 }
 
 // ------------------------------------------------------------------------------------

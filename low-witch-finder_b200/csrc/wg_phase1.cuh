@@ -59,6 +59,7 @@ enum : int {
     CNT_DEEP,          // candidates that passed Entrance(50) and Entrance(60)
     CNT_FINAL,         // phase-1 survivors
     CNT_OVERFLOW,      // bit 0 records/survivors, bit 1 deep list, bit 2 final list
+    CNT_RECHECK,       // FP32 noise core: gate decisions re-taken in FP64 (value inside the error band)
     CNT_WORDS = 8
 };
 
@@ -104,6 +105,8 @@ struct BatchArgs {
     int salt;
     int max_height;
     int mc_1_18_2, pre_26_2, single_biome, large_biomes;
+    int fp32_core;                // 1: climate samples in FP32, FP64 recheck inside the error band;
+                                  // 2: the same, every gate re-taken in FP64; 0: FP64
 
     uint32_t *rec_unit;           // [cap_rec] batch-local unit of each record
     uint32_t *rec_off;            // [cap_rec] first entry in surv_region
@@ -129,16 +132,38 @@ struct BatchArgs {
     uint32_t n_jobs = 0;
 };
 
-// One evaluation step of the climate state machine (a single y=0 Perlin sample).
+// One evaluation step of the climate state machine (a single y=0 Perlin sample).  The last
+// four fields serve the FP32 noise core: cf = (float)(c1 * c2), and for a tier step the band
+// [lo, hi) of partial sums (in sum space, i.e. before the amplitude) inside which an FP32
+// partial sum cannot decide the tier; err is the bound on |FP32 partial sum - FP64 partial sum|
+// after this step.
 struct ClimateStep {
     double sc, lac, c1, c2, thr, amp;
     int slot, act, tier, pad;
+    float cf, lo, hi, err;
 };
+
+// Undecidable bands of the FP32 core for the temperature and ridge gates, in sum space
+// (the DoublePerlin's octave sum before the amplitude): t_*[0] around -0.45, t_*[1] around 0.2;
+// r_*[0..3] around -0.91, -0.42, 0.42, 0.91.  A total in [lo, hi) is re-taken in FP64.
+struct F32Bands {
+    float t_lo[2], t_hi[2];
+    float r_lo[4], r_hi[4];
+};
+
+// Bound on |FP32 Perlin sample - exact sample| of perlin_y0_f32 (wg_device.cuh), in units of
+// 2^-24; derived operation by operation in the comment above perlin_y0_f32.
+constexpr double kPerlinF32ErrUlps = 44.0;
 enum : int { ACT_NONE = 0, ACT_TIER, ACT_TIER_LAST, ACT_END_SUB_A, ACT_TEMPERATURE, ACT_RIDGE };
 constexpr int kClimateSteps = kSlotsA;
 
-// Host: the 18-step climate sequence for one preset (wg_engine.cu).
+// Host: the 18-step climate sequence for one preset, with the FP32 core's error bands
+// (wg_engine.cu); the temperature / ridge bands of the same preset.
 void build_climate_steps(const NoiseSpec *specs, int erosion, int temperature, ClimateStep *steps);
+F32Bands build_f32_bands(const ClimateStep *steps);
+// Host: builds the noise parameters, climate steps and FP32 bands of both presets and uploads
+// them to the current device's constant memory (upload_tables).
+void upload_phase1_tables();
 
 // An item of the breadth-first climate stage for one-region units: the unit, its partial sums.
 struct SpotItem {
@@ -147,16 +172,21 @@ struct SpotItem {
 };
 
 // Launchers (wg_phase1.cu).
-void upload_tables(const NoiseSpec *specs, const ClimateStep *steps_normal, const ClimateStep *steps_large);
+void upload_tables(const NoiseSpec *specs, const ClimateStep *steps_normal, const ClimateStep *steps_large,
+                   const F32Bands *bands);
 void launch_climate(const BatchArgs &a, cudaStream_t s);
 void launch_entrance(const BatchArgs &a, int grid, cudaStream_t s);
 void launch_ladder(const BatchArgs &a, int grid, cudaStream_t s);
-size_t climate_smem_bytes();
+size_t climate_smem_bytes(bool fp32_core);
 // The climate stage of a batch whose units have one region each (spots mode), breadth first over
 // two item lists of `cap` entries (counts: 2 words, device); climate survivors become records.
 void launch_spot_climate(const BatchArgs &a, SpotItem *list0, SpotItem *list1, uint32_t *counts, uint32_t cap,
                          int sm_count, cudaStream_t s);
 size_t spot_smem_bytes();
 size_t entrance_smem_bytes();
+// The FP32 core's error probe: noise `noise` (NoiseId) of seed d_seeds[b] at y = 0 and the n_points
+// (x, z) of d_xz, FP32 core -> d_out32[b * n_points + i], FP64 -> d_out64[...].
+void launch_noise_probe(const int64_t *d_seeds, uint32_t n_seeds, int noise, const double *d_xz, uint32_t n_points,
+                        double *d_out32, double *d_out64, cudaStream_t s);
 
 }  // namespace wg

@@ -892,7 +892,6 @@ constexpr int kGridThreads = 256;
 __global__ void __launch_bounds__(kGridThreads) p2_grid_kernel(const P2Tables *__restrict__ Tp,
                                                                const P2World *__restrict__ worlds, P2Chunk *jobs) {
     // CTA (job, gx): the five corner columns c = gx * 5 + k of one cell row, so a job's grid is five
-    // short chains on five SMs instead of one long one
     // short chains on five SMs instead of one long one.  Threads 0..4 evaluate the columns' terrain
     // points while the others take the samples that do not need them (the blended noise of every
     // main sample and the three noodle children); the density columns follow the barrier.

@@ -18,7 +18,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(HERE, "_build", "libwitch_oracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "liblysh_ref.so")
 REF_BIN = os.path.join(HERE, "_ref", "lysh")
-REF_SRC = "/root/reference/engine/tools/lysh/src"
+
+
+def reference_root() -> str:
+    """Where the reference's sources lie: $WG_REFERENCE_ROOT, else a `reference` directory beside
+    this repository's root."""
+    return os.environ.get("WG_REFERENCE_ROOT") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+
+
+REF_SRC = os.path.join(reference_root(), "engine", "tools", "lysh", "src")
 
 
 def build(ref: bool | None = None) -> None:
@@ -27,7 +35,7 @@ def build(ref: bool | None = None) -> None:
     if ref is None:
         ref = os.path.isdir(REF_SRC)
     if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8", f"REF={reference_root()}"], check=True)
 
 
 class WoOpts(C.Structure):
@@ -184,7 +192,7 @@ class RoomRef:
 
     def __init__(self, path: str = ROOM_LIB):
         if not os.path.exists(path):
-            raise FileNotFoundError(f"{path} is missing (make -C oracle ref needs the reference sources)")
+            raise FileNotFoundError(f"{path} is missing (make -C oracle ref REF=<reference root> needs the reference sources)")
         lib = C.CDLL(path)
         lib.roomh_is_start.argtypes = [C.c_int64, C.c_int, C.c_int]
         lib.roomh_walk.restype = C.c_longlong
@@ -208,7 +216,7 @@ class Ref:
 
     def __init__(self, path: str = REF_LIB):
         if not os.path.exists(path):
-            raise FileNotFoundError(f"{path} is missing (make -C oracle ref needs the reference sources)")
+            raise FileNotFoundError(f"{path} is missing (make -C oracle ref REF=<reference root> needs the reference sources)")
         lib = C.CDLL(path)
         lib.refh_parse_version.argtypes = [C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.refh_hut_in_region.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]

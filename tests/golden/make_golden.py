@@ -1,6 +1,6 @@
 """Generates the golden fixtures in this folder from the reference's own lysh.
 
-Run from the repository root after `make -C oracle ref` (which compiles lysh from the
+Run from the repository root after `make -C oracle ref REF=<reference root>` (which compiles lysh from the
 reference sources into oracle/_ref/):
 
     python tests/golden/make_golden.py

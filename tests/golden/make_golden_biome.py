@@ -1,6 +1,6 @@
 """Writes the biome-map golden fixtures from the reference's own biome_map tool.
 
-Run from the repository root after `make -C oracle ref` (which builds oracle/_ref/biome_map from
+Run from the repository root after `make -C oracle ref REF=<reference root>` (which builds oracle/_ref/biome_map from
 engine/tools/mineshaft/biome_map.c and the lysh sources):
 
     python tests/golden/make_golden_biome.py

@@ -1,6 +1,6 @@
 """Generates the Deep Dive golden fixtures in this folder from the reference's own code.
 
-Run from the repository root after `make -C oracle ref`:
+Run from the repository root after `make -C oracle ref REF=<reference root>`:
 
     python tests/golden/make_golden_deep.py
 

@@ -1,6 +1,6 @@
 """Generates the phase-2 golden fixtures in this folder from the reference's own lysh.
 
-Run from the repository root after `make -C oracle ref` (lysh compiled from the reference
+Run from the repository root after `make -C oracle ref REF=<reference root>` (lysh compiled from the reference
 sources into oracle/_ref/):
 
     python tests/golden/make_golden_p2.py

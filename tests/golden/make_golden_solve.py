@@ -1,6 +1,6 @@
 """Writes the Deep Dive solver's golden hits from the reference's own GPU engine.
 
-Needs a GPU and the reference solver built here first (`make -C oracle refsolver`, which compiles
+Needs a GPU and the reference solver built here first (`make -C oracle refsolver REF=<reference root>`, which compiles
 engine/gpu/hut_lookup_v4_source.cu into oracle/_ref/hut_lookup_v4).  On the GPU machine:
 
     python tests/golden/make_golden_solve.py --out deep_solve.npz

@@ -31,7 +31,7 @@ def test_header_and_exports(wg):
 def test_struct_layouts(wg):
     assert C.sizeof(wg.Opts) == 20
     assert wg.CANDIDATE_DTYPE.itemsize == 32
-    assert C.sizeof(wg.Stats) == 8 * (4 + 11 + 7 + 2 + 3) + 8 * 3 + 16
+    assert C.sizeof(wg.Stats) == 8 * (4 + 11 + 7 + 2 + 3) + 8 * 3 + 16 + 16
 
 
 def test_job_struct_layouts_match_the_header(wg, tmp_path):

@@ -1,6 +1,11 @@
 """GPU: the phase1_scan worker protocol as hunt.py drives it (GpuScanWorker, hunt.py:1276-1332):
 ===WORKER_READY===, one request per stdin line, CSV out, ===SCAN_DONE rc=0===, a bad line
-answered with ===SCAN_ERROR...=== without stopping the worker, clean exit on EOF."""
+answered with ===SCAN_ERROR...=== without stopping the worker, clean exit on EOF.
+
+By default the worker writes the exact hit set (phase-1 survivors that lysh_eval_hut accepts at
+the phase-2 ceiling), with the hut's floor y in the 6th column; --phase1-candidates writes the
+phase-1 survivors instead.  hunt.py reads only the first three columns and re-confirms every row
+with `lysh hut` at a ceiling <= -50, so both outputs give it the same results."""
 from __future__ import annotations
 
 import csv
@@ -13,11 +18,23 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def read_csv(path):
+def read_csv(path, floor=False):
     with open(path) as f:
         rows = list(csv.reader(f))
     assert rows[0] == ["seed", "chunkX", "chunkZ", "blockX", "blockZ", "gpuEst"]
+    if floor:
+        return [(int(r[0]), int(r[1]), int(r[2]), int(r[3]), int(r[4]), int(r[5])) for r in rows[1:]]
     return [(int(r[0]), int(r[1]), int(r[2]), int(r[3]), int(r[4])) for r in rows[1:]]
+
+
+def exact_rows(engine, cands, max_y):
+    """The worker's default output for phase-1 survivors `cands`: the huts lysh_eval_hut accepts."""
+    if len(cands) == 0:
+        return []
+    res = engine.eval_huts(cands["seed"], cands["chunk_x"].astype(np.int64) * 16,
+                           cands["chunk_z"].astype(np.int64) * 16, max_y=max_y)
+    return [(int(c["seed"]), int(c["chunk_x"]), int(c["chunk_z"]), int(c["chunk_x"]) * 16, int(c["chunk_z"]) * 16,
+             int(r["avg_y"])) for c, r in zip(cands, res) if r["ok"]]
 
 
 def test_worker_protocol(wg, engine, tmp_path):
@@ -39,17 +56,21 @@ def test_worker_protocol(wg, engine, tmp_path):
         # hunt.py's request for a 40,000-block area (ScanRun.rect: r = 40000 // 512 + 1)
         assert ask(f"--seed {seed} --min-region-x -79 --max-region-x 79 --min-region-z -79 "
                    f"--max-region-z 79 --max-height -50 --out cands.csv") == "===SCAN_DONE rc=0==="
-        rows = read_csv(tmp_path / "cands.csv")
-        assert rows == [(seed, -987, -1073, -15792, -17168)]
+        # hunt.py SCAN_REFERENCE: /tp -15792 -54 -17168, the floor in the 6th column
+        assert read_csv(tmp_path / "cands.csv", floor=True) == [(seed, -987, -1073, -15792, -17168, -54)]
         assert ask("--seed 1 --bogus-flag") == "===SCAN_ERROR: bad request line==="
-        # a UTF-8 BOM is stripped, negative seeds wrap like strtoull, seed lists work
+        # a UTF-8 BOM is stripped, negative seeds wrap like strtoull, seed lists work; the phase-2
+        # ceiling is --max-height as given (-54) while phase 1 runs at the clamped -50
         (tmp_path / "seeds.txt").write_text(f"{seed}, -5\n 17\n")
         assert ask("\ufeff--seed-list seeds.txt --min-region-x -79 --max-region-x 79 --min-region-z -79 "
                    "--max-region-z 79 --max-height -54 --out b.csv") == "===SCAN_DONE rc=0==="
-        got = read_csv(tmp_path / "b.csv")
         want = engine.seed_check(seeds=[seed, -5, 17], rect=(-79, 79, -79, 79), max_height=-50).candidates
-        assert got == [(int(c["seed"]), int(c["chunk_x"]), int(c["chunk_z"]), int(c["chunk_x"]) * 16,
-                        int(c["chunk_z"]) * 16) for c in want]
+        assert read_csv(tmp_path / "b.csv", floor=True) == exact_rows(engine, want, -54)
+        assert ask("\ufeff--seed-list seeds.txt --min-region-x -79 --max-region-x 79 --min-region-z -79 "
+                   "--max-region-z 79 --max-height -54 --phase1-candidates --out p.csv") == "===SCAN_DONE rc=0==="
+        assert read_csv(tmp_path / "p.csv") == [(int(c["seed"]), int(c["chunk_x"]), int(c["chunk_z"]),
+                                                 int(c["chunk_x"]) * 16, int(c["chunk_z"]) * 16) for c in want]
+        assert len(want) > 1
         assert ask("--seed-gen 2 65536 --min-region-x -4 --max-region-x 5 --min-region-z -4 --max-region-z 5 "
                    "--max-height -50 --out g.csv") == "===SCAN_DONE rc=0==="
         assert read_csv(tmp_path / "g.csv") == []
@@ -60,15 +81,50 @@ def test_worker_protocol(wg, engine, tmp_path):
 
 
 def test_single_shot_cli(wg, engine, tmp_path):
-    r = subprocess.run([wg.WORKER_PATH, "--seed-gen", "2", "4194304", "--min-region-x", "-4", "--max-region-x", "5",
-                        "--min-region-z", "-4", "--max-region-z", "5", "--max-height", "-50", "--out", "c.csv"],
-                       cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    args = [wg.WORKER_PATH, "--seed-gen", "2", "4194304", "--min-region-x", "-4", "--max-region-x", "5",
+            "--min-region-z", "-4", "--max-region-z", "5", "--max-height", "-50"]
+    r = subprocess.run(args + ["--phase1-candidates", "--out", "c.csv"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=300)
     assert r.returncode == 0, r.stderr
     assert "candidates=52" in r.stdout
     rows = read_csv(tmp_path / "c.csv")
     g = np.load(os.path.join(os.path.dirname(__file__), "golden", "c2_4m_survivors.npz"))["survivors"]
     assert rows == [(int(c["seed"]), int(c["chunk_x"]), int(c["chunk_z"]), int(c["chunk_x"]) * 16,
                      int(c["chunk_z"]) * 16) for c in g]
+    # the default output: those 52 through phase 2 at the ceiling -50
+    r = subprocess.run(args + ["--out", "h.csv"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "phase 2: 52 phase-1 survivors" in r.stdout
+    assert read_csv(tmp_path / "h.csv", floor=True) == exact_rows(engine, g, -50)
+
+
+def test_exact_hits_at_a_relaxed_ceiling(wg, engine, tmp_path):
+    """Phase 1 at max_height 100 with --phase2-max-y 100: many phase-1 survivors, of which phase 2
+    keeps the biome-ok, dry huts with floor <= 100; the rows and floors equal wg_eval_huts'."""
+    rect = ["--min-region-x", "-8", "--max-region-x", "8", "--min-region-z", "-8", "--max-region-z", "8"]
+    rows = _scan(wg, tmp_path, "--seed-gen", "5", "20000", *rect, "--max-height", "100", "--phase2-max-y", "100",
+                 phase1=False)
+    cands = engine.seed_check(gen=(5, 20000), rect=(-8, 8, -8, 8), max_height=100).candidates
+    want = exact_rows(engine, cands, 100)
+    assert rows == want
+    assert 0 < len(want) < len(cands)
+
+
+def test_self_test_passes(wg, tmp_path):
+    """--self-test re-checks the sampled regions through the FP64 noise core: every region of the
+    SCAN_REFERENCE seed's 40,000-block rect (24,964 regions, stride 1) and a 20,000-region sample of
+    each of 16 seeds of a larger rect."""
+    r = subprocess.run([wg.WORKER_PATH, "--seed", "1473884015873122059", "--min-region-x", "-79", "--max-region-x",
+                        "79", "--min-region-z", "-79", "--max-region-z", "79", "--max-height", "-50", "--self-test",
+                        "--out", "s.csv"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "self-test: checked 24964 sampled regions across 1 seed(s), 0 mismatches -> PASS" in r.stdout
+    r = subprocess.run([wg.WORKER_PATH, "--seed-gen", "3", "64", "--min-region-x", "-200", "--max-region-x", "200",
+                        "--min-region-z", "-200", "--max-region-z", "200", "--max-height", "100", "--self-test",
+                        "--phase1-candidates", "--out", "t.csv"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "self-test: checked 320000 sampled regions across 16 seed(s), 0 mismatches -> PASS" in r.stdout
 
 
 def _rows(cands):
@@ -76,11 +132,12 @@ def _rows(cands):
             for c in cands]
 
 
-def _scan(wg, tmp_path, *args, out="q.csv"):
-    r = subprocess.run([wg.WORKER_PATH, *args, "--out", out], cwd=tmp_path, capture_output=True, text=True,
+def _scan(wg, tmp_path, *args, out="q.csv", phase1=True):
+    extra = ["--phase1-candidates"] if phase1 else []
+    r = subprocess.run([wg.WORKER_PATH, *args, *extra, "--out", out], cwd=tmp_path, capture_output=True, text=True,
                        timeout=600)
     assert r.returncode == 0, r.stderr
-    return read_csv(tmp_path / out)
+    return read_csv(tmp_path / out, floor=not phase1)
 
 
 def test_quad_bases_and_position_gate(wg, port, bind_mod, tmp_path):
