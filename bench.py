@@ -262,6 +262,9 @@ def jobs_measure(wg, eng, n_jobs: int = 65536) -> dict:
     survivors out (wall clock; device time from the call's own CUDA events), after a warm-up on
     the first 64 jobs."""
     jobs = wg.uneven_jobs(n_jobs=n_jobs)
+    t0 = time.perf_counter()
+    tuning = eng.tune()
+    tune_s = time.perf_counter() - t0
     eng.seed_check_jobs(jobs[:64])
     t0 = time.perf_counter()
     got, st = eng.seed_check_jobs(jobs)
@@ -269,9 +272,13 @@ def jobs_measure(wg, eng, n_jobs: int = 65536) -> dict:
     seeds = sum(len(j["seeds"]) for j in jobs)
     return {"jobs": n_jobs, "seeds": seeds, "checks": st["scanned"], "survivors": st["accepted"],
             "seeds_per_s": seeds / secs, "checks_per_s": st["scanned"] / secs, "ms": 1e3 * secs,
-            "gpu_ms": st["gpu_ms"], "kernel_ms": st["kernel_ms"], "batches": st["batches"],
+            "gpu_ms": st["gpu_ms"], "slices": st["batches"], "retries": st["retries"],
             "gpu_launches": sum(st["kernel_launches"]),
-            "timing": "wall clock around wg_seed_check_jobs (host seed lists in, survivors out)"}
+            "mode": "device work queue: all seeds resident, one graph launch per rule set whose device-side "
+                    "while-loop takes slices of units off the queue",
+            "tuning": tuning, "tuning_s": tune_s,
+            "timing": "wall clock around wg_seed_check_jobs (host seed lists in, survivors out), after "
+                      "wg_engine_tune on this GPU"}
 
 
 def serving_measure(wg, n_req: int = 200) -> dict:

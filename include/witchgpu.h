@@ -374,6 +374,36 @@ typedef struct {
     uint64_t batch_jobs;         /* jobs flattened into that batch (the job included) */
 } wg_job_status;
 
+/* How wg_seed_check_jobs runs: 1 (the default) = every job's seeds resident at once and the whole
+ * job list as one CUDA graph launch, whose device-side loop takes slices of units off a queue,
+ * runs the phase-1 kernels on each and appends the survivors, with no host synchronisation
+ * between slices (it falls back to 0 when the seeds exceed 2^27); 0 = the host batch loop.  The
+ * reference has no batched-job path. */
+int wg_engine_set_job_queue(wg_engine *e, int device_queue);
+
+/* Autotuned job settings: for each job class (regions per seed up to max_regions[k]) the regions
+ * per work unit, and the (seed, region) checks per queue slice, each the fastest of the candidates
+ * timed on the device on probe jobs of that class (seed counts log-uniform 1..4,096).  The
+ * reference tunes its scanner per GPU with a measured sweep (hunt.py:927-1019). */
+typedef struct {
+    uint32_t max_regions[4];          /* class k: rects of up to this many regions (class 3: any) */
+    uint32_t window[4];               /* regions per unit chosen for the class */
+    uint32_t window_candidates[4][4]; /* the windows timed (0 = none) */
+    double window_ms[4][4];           /* their device time on the class's probe jobs */
+    uint64_t budget;                  /* (seed, region) checks per queue slice chosen */
+    uint64_t budget_candidates[3];
+    double budget_ms[3];              /* device time of all classes' probe jobs at each budget */
+} wg_tune_report;
+
+/* Times the candidates on this engine's GPU (a few seconds) and keeps the fastest settings for the
+ * engine's later wg_seed_check_jobs calls; report (may be NULL) receives the measurements. */
+int wg_engine_tune(wg_engine *e, wg_tune_report *report);
+
+/* Sets the job settings directly (e.g. from a saved tuning): window[4] regions per unit per class
+ * (NULL or 0 = the default rule: a whole seed up to 4,096 regions, else 2,048), budget checks per
+ * slice (0 = 2^27). */
+int wg_engine_set_tuning(wg_engine *e, const uint32_t *window, uint64_t budget);
+
 /* Many Seed Check jobs at once (uneven seed counts, rects and floors), flattened into shared
  * device batches: every batch covers slices of several jobs through the kernels' job table.
  * Survivors are written job by job (job order, then seed_index, rz, rx; seed_index is the seed's

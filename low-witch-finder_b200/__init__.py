@@ -73,7 +73,8 @@ EXPORTS = ("wg_engine_open", "wg_engine_close", "wg_engine_error", "wg_engine_se
            "wg_parse_version", "wg_parse_preset",
            "wg_seed_check", "wg_seed_check_device", "wg_phase1_codes", "wg_seed_check_noalloc",
            "wg_eval_huts", "wg_grade_scan", "wg_p2_probe", "wg_deep_starts", "wg_deep_sweep", "wg_deep_spots",
-           "wg_biome_map", "wg_biome_chunks", "wg_deep_solve", "wg_deep_solve_tasks", "wg_seed_check_jobs", "wg_server_open", "wg_server_open_config", "wg_server_submit", "wg_server_poll", "wg_server_take",
+           "wg_biome_map", "wg_biome_chunks", "wg_deep_solve", "wg_deep_solve_tasks", "wg_seed_check_jobs", "wg_engine_set_job_queue", "wg_engine_tune", "wg_engine_set_tuning",
+           "wg_server_open", "wg_server_open_config", "wg_server_submit", "wg_server_poll", "wg_server_take",
            "wg_server_stats", "wg_server_close")
 
 # wg_deep_start: a swamp hut whose chunk is a mineshaft start chunk.
@@ -135,6 +136,24 @@ class Job(C.Structure):
                 ("opts", Opts)]
 
 
+class TuneReport(C.Structure):
+    """wg_tune_report: per job class the regions-per-unit candidates and their device times."""
+    _fields_ = [("max_regions", C.c_uint32 * 4), ("window", C.c_uint32 * 4),
+                ("window_candidates", (C.c_uint32 * 4) * 4), ("window_ms", (C.c_double * 4) * 4),
+                ("budget", C.c_uint64), ("budget_candidates", C.c_uint64 * 3), ("budget_ms", C.c_double * 3)]
+
+    def as_dict(self) -> dict:
+        classes = []
+        for c in range(4):
+            cands = [(int(self.window_candidates[c][q]), float(self.window_ms[c][q])) for q in range(4)
+                     if self.window_candidates[c][q]]
+            classes.append({"max_regions": int(self.max_regions[c]), "window": int(self.window[c]),
+                            "candidates": [{"window": w, "ms": ms} for w, ms in cands]})
+        return {"classes": classes, "budget": int(self.budget),
+                "budget_candidates": [{"checks": int(self.budget_candidates[q]), "ms": float(self.budget_ms[q])}
+                                      for q in range(3)]}
+
+
 class ServerConfig(C.Structure):
     """wg_server_config: queue and arena limits, batch size, host-side fault injection."""
     _fields_ = [("max_queued_seeds", C.c_uint64), ("arena_seeds", C.c_uint64), ("batch_checks", C.c_uint64),
@@ -192,6 +211,9 @@ def library() -> C.CDLL:
     lib.wg_seed_check_jobs.argtypes = [vp, C.POINTER(Job), u64, vp, u64, C.POINTER(u64), vp, C.POINTER(Stats)]
     lib.wg_server_open.argtypes = [i32, u64, C.POINTER(vp)]
     lib.wg_server_open_config.argtypes = [i32, C.POINTER(ServerConfig), C.POINTER(vp)]
+    lib.wg_engine_set_job_queue.argtypes = [vp, i32]
+    lib.wg_engine_tune.argtypes = [vp, C.POINTER(TuneReport)]
+    lib.wg_engine_set_tuning.argtypes = [vp, vp, u64]
     lib.wg_server_submit.argtypes = [vp, C.POINTER(Job), C.POINTER(u64)]
     lib.wg_server_poll.argtypes = [vp, u64, i32, C.POINTER(JobStatus)]
     lib.wg_server_take.argtypes = [vp, u64, vp, u64, C.POINTER(u64)]
@@ -506,6 +528,28 @@ class Engine:
         del keep
         bounds = np.concatenate([[0], np.cumsum(per[:len(jobs)].astype(np.int64))])
         return [out[bounds[i]:bounds[i + 1]].copy() for i in range(len(jobs))], st.as_dict()
+
+    def set_job_queue(self, device_queue: bool) -> None:
+        """seed_check_jobs through the device work queue (True, the default) or the host batch loop."""
+        rc = library().wg_engine_set_job_queue(self._h, 1 if device_queue else 0)
+        if rc != WG_OK:
+            raise self._err(rc, "wg_engine_set_job_queue")
+
+    def tune(self) -> dict:
+        """wg_engine_tune: times the job settings' candidates on this GPU and keeps the fastest."""
+        r = TuneReport()
+        rc = library().wg_engine_tune(self._h, C.byref(r))
+        if rc != WG_OK:
+            raise self._err(rc, "wg_engine_tune")
+        return r.as_dict()
+
+    def set_tuning(self, windows=None, budget: int = 0) -> None:
+        """wg_engine_set_tuning: regions per unit per job class (None = the default rule) and checks
+        per queue slice (0 = the default)."""
+        w = None if windows is None else (C.c_uint32 * 4)(*[int(v) for v in windows])
+        rc = library().wg_engine_set_tuning(self._h, None if w is None else C.cast(w, C.c_void_p), int(budget))
+        if rc != WG_OK:
+            raise self._err(rc, "wg_engine_set_tuning")
 
     def deep_spots(self, s48, chunk_x, chunk_z, max_height: int = -54, version: str = DEFAULT_VERSION,
                    preset: str = "NORMAL", opts: Opts | None = None) -> tuple[np.ndarray, int]:

@@ -345,41 +345,86 @@ __device__ __forceinline__ double perlin_3d(const T &P, double ox, double oy, do
 // FP64 sample of the reference order is within ~1e-14 of the exact value; the gates add that
 // and the sums' own roundings (build_climate_steps).  No FMA contraction is left to the
 // compiler: every FP32 operation below is an explicit intrinsic.
-__device__ __forceinline__ float fade_f32(float t) {
-    const float s = __fsub_rn(t, 0.5f);
-    const float s2 = __fmul_rn(s, s);
-    const float p = __fmaf_rn(6.0f, s2, -5.0f);
-    const float q = __fmaf_rn(s2, p, 1.875f);
-    return __fmaf_rn(s, q, 0.5f);
+// Two FP32 lanes per instruction (PTX f32x2, sm_100): each lane is the scalar operation with its
+// own round-to-nearest, so a packed step and two scalar steps give the same bits.
+struct F2 {
+    unsigned long long v;
+};
+__device__ __forceinline__ F2 f2(float a, float b) {
+    F2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2_split(F2 r, float &a, float &b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r.v)); }
+__device__ __forceinline__ F2 f2_fma(F2 a, F2 b, F2 c) {
+    F2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return d;
+}
+__device__ __forceinline__ F2 f2_mul(F2 a, F2 b) {
+    F2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+__device__ __forceinline__ F2 f2_add(F2 a, F2 b) {
+    F2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+    return d;
+}
+// fade_f32 on both lanes: 1/2 + s (15/8 + s^2 (6 s^2 - 5)), s = t - 1/2
+__device__ __forceinline__ F2 fade_f32x2(F2 t) {
+    const F2 s = f2_add(t, f2(-0.5f, -0.5f));
+    const F2 s2 = f2_mul(s, s);
+    const F2 p = f2_fma(f2(6.0f, 6.0f), s2, f2(-5.0f, -5.0f));
+    const F2 q = f2_fma(s2, p, f2(1.875f, 1.875f));
+    return f2_fma(s, q, f2(0.5f, 0.5f));
+}
+// lerp(t, a, b) = (a - t a) + t b on both lanes
+__device__ __forceinline__ F2 lerp_f32x2(F2 t, F2 a, F2 b) {
+    float t0, t1;
+    f2_split(t, t0, t1);
+    return f2_fma(t, b, f2_fma(f2(-t0, -t1), a, a));
 }
 __device__ __forceinline__ float lerp_f32(float t, float a, float b) {
     return __fmaf_rn(t, b, __fmaf_rn(-t, a, a));
 }
 
-// Table reader of the FP32 core: bytes as ColTable, gradient components as floats
-// (gtf[component * 16 + hash] in {-1, 0, 1}).
+// Table reader of the FP32 core.  Byte k of the table is at t[k * STRIDE] as in ColTable, and the
+// table has a row 256 holding a copy of row 0 (written after the shuffle, in the slot block's
+// padding), so that the pair P[k], P[(k + 1) & 255] is two loads from one address.  Gradient
+// components come as one 16-byte (x, y, z, 0) vector per hash (gt4[hash]).
 template <int STRIDE>
 struct ColTableF {
     const uint8_t *t;
-    const float *gtf;
-    __device__ __forceinline__ int operator()(int k) const { return t[k * STRIDE]; }
+    const float4 *gt4;
+    __device__ __forceinline__ void pair(int k, int &lo, int &hi) const {
+        const uint8_t *r = t + (k & 255) * STRIDE;
+        lo = r[0];
+        hi = r[STRIDE];
+    }
     __device__ __forceinline__ float grad(int hash, float x, float y, float z) const {
-        const int h = hash & 15;
-        return __fmaf_rn(gtf[h], x, __fmaf_rn(gtf[16 + h], y, __fmul_rn(gtf[32 + h], z)));
+        const float4 g = gt4[hash & 15];
+        return __fmaf_rn(g.x, x, __fmaf_rn(g.y, y, __fmul_rn(g.z, z)));
     }
 };
 
-__device__ __forceinline__ void fill_grad_table_f32(float *gtf, int tid) {
-    if (tid < kGradWords) {
-        const int c = tid / 16;
-        const uint32_t codes = c == 0 ? kGradCodeX : (c == 1 ? kGradCodeY : kGradCodeZ);
-        const uint32_t code = (codes >> (2 * (tid % 16))) & 3u;
-        gtf[tid] = code == 0 ? 0.0f : (code == 1 ? 1.0f : -1.0f);
+// The (x, y, z, 0) gradient vectors of the game's 16 hashes as floats.
+__device__ __forceinline__ void fill_grad_table_f32(float4 *gt4, int tid) {
+    if (tid < 16) {
+        float c[3];
+        const uint32_t codes[3] = {kGradCodeX, kGradCodeY, kGradCodeZ};
+        for (int q = 0; q < 3; q++) {
+            const uint32_t code = (codes[q] >> (2 * tid)) & 3u;
+            c[q] = code == 0 ? 0.0f : (code == 1 ? 1.0f : -1.0f);
+        }
+        gt4[tid] = make_float4(c[0], c[1], c[2], 0.0f);
     }
 }
 
 // One Perlin sampler at y = 0 in the FP32 core; hyf / fyf are rn(hy) and rn(fade(hy)) of the
-// table's y origin fraction, jy its floor.  x, z are the FP64 sampling coordinates.
+// table's y origin fraction, jy its floor.  x, z are the FP64 sampling coordinates.  The corner
+// values are paired along z, (v.0, v.1), so the x and y lerps and both fades run two lanes per
+// instruction; every lane performs the operations the bound above counts.
 template <class T>
 __device__ __forceinline__ float perlin_y0_f32(const T &P, double ox, double oz, int jy, float hyf, float fyf,
                                                double x, double z) {
@@ -387,22 +432,30 @@ __device__ __forceinline__ float perlin_y0_f32(const T &P, double ox, double oz,
     const double fd = floor(d), ff = floor(f);
     const int i = (int)fd, k = (int)ff;
     const float g = __double2float_rn(d - fd), l = __double2float_rn(f - ff);
-    const float g1 = __fsub_rn(g, 1.0f), l1 = __fsub_rn(l, 1.0f), hy1 = __fsub_rn(hyf, 1.0f);
-    const int a = P(i & 255), b = P((i + 1) & 255);
-    const int c = P((a + jy) & 255), dd = P((a + jy + 1) & 255);
-    const int e = P((b + jy) & 255), ee = P((b + jy + 1) & 255);
-    const float v000 = P.grad(P((c + k) & 255), g, hyf, l);
-    const float v100 = P.grad(P((e + k) & 255), g1, hyf, l);
-    const float v010 = P.grad(P((dd + k) & 255), g, hy1, l);
-    const float v110 = P.grad(P((ee + k) & 255), g1, hy1, l);
-    const float v001 = P.grad(P((c + k + 1) & 255), g, hyf, l1);
-    const float v101 = P.grad(P((e + k + 1) & 255), g1, hyf, l1);
-    const float v011 = P.grad(P((dd + k + 1) & 255), g, hy1, l1);
-    const float v111 = P.grad(P((ee + k + 1) & 255), g1, hy1, l1);
-    const float fx = fade_f32(g), fz = fade_f32(l);
-    const float x00 = lerp_f32(fx, v000, v100), x10 = lerp_f32(fx, v010, v110);
-    const float x01 = lerp_f32(fx, v001, v101), x11 = lerp_f32(fx, v011, v111);
-    return lerp_f32(fz, lerp_f32(fyf, x00, x10), lerp_f32(fyf, x01, x11));
+    const F2 gl = f2(g, l);
+    float g1, l1;
+    f2_split(f2_add(gl, f2(-1.0f, -1.0f)), g1, l1);   // g - 1, l - 1
+    const float hy1 = __fsub_rn(hyf, 1.0f);
+    int a, b, c, dd, e, ee;
+    P.pair(i, a, b);
+    P.pair(a + jy, c, dd);
+    P.pair(b + jy, e, ee);
+    int h000, h001, h100, h101, h010, h011, h110, h111;
+    P.pair(c + k, h000, h001);
+    P.pair(e + k, h100, h101);
+    P.pair(dd + k, h010, h011);
+    P.pair(ee + k, h110, h111);
+    const F2 v00 = f2(P.grad(h000, g, hyf, l), P.grad(h001, g, hyf, l1));     // (v000, v001)
+    const F2 v10 = f2(P.grad(h100, g1, hyf, l), P.grad(h101, g1, hyf, l1));   // (v100, v101)
+    const F2 v01 = f2(P.grad(h010, g, hy1, l), P.grad(h011, g, hy1, l1));     // (v010, v011)
+    const F2 v11 = f2(P.grad(h110, g1, hy1, l), P.grad(h111, g1, hy1, l1));   // (v110, v111)
+    float fx, fz;
+    f2_split(fade_f32x2(gl), fx, fz);
+    const F2 x0 = lerp_f32x2(f2(fx, fx), v00, v10);    // (x00, x01)
+    const F2 x1 = lerp_f32x2(f2(fx, fx), v01, v11);    // (x10, x11)
+    float y0, y1;
+    f2_split(lerp_f32x2(f2(fyf, fyf), x0, x1), y0, y1);
+    return lerp_f32(fz, y0, y1);
 }
 
 constexpr double kDblScale = 1.0181268882175227;

@@ -15,6 +15,7 @@
 #include "wg_deep.cuh"
 #include "wg_engine_impl.h"
 #include "wg_phase1.cuh"
+#include "wg_queue.h"
 
 using namespace wg;
 
@@ -393,6 +394,7 @@ void wg_engine_close(wg_engine *eng) {
     p2_release(eng);
     solve_release(eng);
     walk_release(eng);
+    queue_release(eng);
     cudaFreeHost(eng->h_counters);
     cudaFreeHost(eng->h_hist);
     if (eng->ev0) cudaEventDestroy(eng->ev0);

@@ -16,12 +16,18 @@ struct P2World;
 struct P2Chunk;
 struct P2Hut;
 struct P2Result;
+struct QueueRes;
 }  // namespace wg
 
 struct wg_engine {
     int device = 0;
     int sm_count = 148;
     int fp32_core = 1;   // 1 FP32 core with FP64 rechecks, 0 FP64, 2 FP32 core re-taking every gate in FP64
+    int job_queue = 1;   // wg_seed_check_jobs through the device work queue (1) or the host batch loop (0)
+    // autotuned job settings (wg_engine_tune): regions per unit per job class (0 = window_for's
+    // rule) and (seed, region) checks per queue slice (0 = kWorkPerBatch)
+    uint32_t tuned_win[4] = {0, 0, 0, 0};
+    uint64_t tuned_budget = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::string err;
@@ -52,6 +58,8 @@ struct wg_engine {
     struct SolveState *solve = nullptr;
     // Deep Dive region walk (wg_deep.cu): its grow-only work buffers
     struct WalkState *walk = nullptr;
+    // device work queue of batched jobs (wg_queue.cu): its state and output buffer
+    wg::QueueRes *queue = nullptr;
 
     int p2_world_cap = 0, p2_job_cap = 0, p2_hut_cap = 0, p2_result_cap = 0, p2_pt_cap = 0, p2_val_cap = 0;
 
@@ -92,6 +100,20 @@ inline bool spot_path(bool jobs, uint64_t win, bool codes, bool single_biome) {
 
 // Regions per unit window: a whole seed when its rect is small, else 2048-region windows.
 uint32_t window_for(uint64_t n_regions);
+
+// Job classes of the autotuner by regions per seed: <= 16, <= 256, <= 4096, more.
+constexpr uint64_t kJobClassMax[4] = {16, 256, 4096, ~0ull};
+inline int job_class(uint64_t n_regions) {
+    int c = 0;
+    while (c < 3 && n_regions > kJobClassMax[c]) c++;
+    return c;
+}
+// A job's window: the engine's tuned value for its class, else window_for's rule.
+inline uint32_t job_window(const wg_engine *eng, uint64_t n_regions) {
+    const uint32_t w = eng ? eng->tuned_win[job_class(n_regions)] : 0u;
+    if (!w) return window_for(n_regions);
+    return (uint32_t)(n_regions < w ? n_regions : w);
+}
 
 // One phase-1 request over one rect (wg_engine.cu).
 struct Request {

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -19,6 +20,7 @@
 #include "../../include/witchgpu.h"
 #include "wg_device.cuh"
 #include "wg_jobs.h"
+#include "wg_queue.h"
 
 namespace wg {
 
@@ -40,7 +42,7 @@ bool candidate_order(const Candidate &x, const Candidate &y) {
 
 }  // namespace
 
-int sched_job_init(SchedJob &j, const wg_job &spec) {
+int sched_job_init(SchedJob &j, const wg_job &spec, const wg_engine *eng) {
     if (spec.n_seeds == 0 || spec.rx1 <= spec.rx0 || spec.rz1 <= spec.rz0) return WG_ERR_ARG;
     const uint64_t rw = (uint64_t)((int64_t)spec.rx1 - spec.rx0), rh = (uint64_t)((int64_t)spec.rz1 - spec.rz0);
     if (rw > kMaxRectSide || rh > kMaxRectSide) return WG_ERR_ARG;
@@ -51,7 +53,7 @@ int sched_job_init(SchedJob &j, const wg_job &spec) {
     j.rz0 = spec.rz0;
     j.rw = (int)rw;
     j.n_regions = rw * rh;
-    j.win = window_for(j.n_regions);
+    j.win = job_window(eng, j.n_regions);
     j.n_win = (j.n_regions + j.win - 1) / j.win;
     if (spec.n_seeds > ~0ull / j.n_win) return WG_ERR_ARG;
     j.units = spec.n_seeds * j.n_win;
@@ -316,6 +318,99 @@ bool engine_usable(wg_engine *eng) {
 
 using namespace wg;
 
+namespace {
+
+// The jobs through the device work queue: every job's seeds resident at once, one job table per
+// rule set, one graph launch per table (wg_queue.cu).  Returns WG_ERR_CAPACITY when the jobs do not
+// fit (the caller then takes the host batch loop).
+int jobs_on_device_queue(wg_engine *eng, std::vector<SchedJob> &js, uint64_t total_seeds, wg_scan_stats &st) {
+    constexpr uint64_t kQueueSeeds = 1ull << 27;
+    if (total_seeds > kQueueSeeds) return WG_ERR_CAPACITY;
+    int64_t *d_seeds = nullptr;
+    JobGeom *d_table = nullptr;
+    std::vector<int64_t> all;
+    std::vector<uint64_t> off(js.size());
+    all.reserve(total_seeds);
+    for (size_t i = 0; i < js.size(); i++) {
+        off[i] = all.size();
+        all.insert(all.end(), js[i].seeds.begin(), js[i].seeds.end());
+    }
+    std::vector<char> done(js.size(), 0);
+    int rc = [&]() -> int {
+        cudaError_t e = cudaMalloc(&d_seeds, sizeof(int64_t) * std::max<size_t>(all.size(), 1));
+        if (e == cudaSuccess) e = cudaMalloc(&d_table, sizeof(JobGeom) * js.size());
+        if (e != cudaSuccess) return eng->fail(WG_ERR_NOMEM, "job queue buffers", e);
+        e = cudaMemcpyAsync(d_seeds, all.data(), sizeof(int64_t) * all.size(), cudaMemcpyHostToDevice, eng->stream);
+        if (e != cudaSuccess) return eng->fail(WG_ERR_CUDA, "upload job seeds", e);
+        for (size_t lead = 0; lead < js.size(); lead++) {
+            if (done[lead]) continue;
+            // one table: the lead's rule set
+            std::vector<JobGeom> table;
+            std::vector<size_t> member;
+            uint64_t units = 0;
+            uint32_t min_win = ~0u;
+            for (size_t i = lead; i < js.size(); i++) {
+                if (done[i] || !same_rules(js[i], js[lead])) continue;
+                JobGeom g;
+                std::memset(&g, 0, sizeof g);
+                g.unit0 = units;
+                g.seed0 = off[i];
+                g.n_win = js[i].n_win;
+                g.n_regions = js[i].n_regions;
+                g.win = js[i].win;
+                g.rx0 = js[i].rx0;
+                g.rz0 = js[i].rz0;
+                g.rw = js[i].rw;
+                g.max_height = js[i].max_height;
+                table.push_back(g);
+                member.push_back(i);
+                units += js[i].units;
+                min_win = std::min(min_win, js[i].win);
+                done[i] = 1;
+            }
+            e = cudaMemcpyAsync(d_table, table.data(), sizeof(JobGeom) * table.size(), cudaMemcpyHostToDevice,
+                                eng->stream);
+            if (e != cudaSuccess) return eng->fail(WG_ERR_CUDA, "upload job table", e);
+            const uint64_t budget = eng->tuned_budget ? eng->tuned_budget : kWorkPerBatch;
+            const uint64_t by_budget = (budget + min_win - 1) / min_win;
+            const uint32_t max_units = (uint32_t)std::min<uint64_t>({(uint64_t)kMaxUnits, units, std::max<uint64_t>(by_budget, 1)});
+            BatchArgs a = base_args(eng, js[lead].opts, js[lead].salt);
+            a.seeds = d_seeds;
+            a.jobs = d_table;
+            a.n_jobs = (uint32_t)table.size();
+            std::vector<Candidate> found;
+            const uint64_t slice = js[lead].opts.single_biome ? std::min<uint64_t>(budget, kCapSurv / 2) : budget;
+            int r = run_queue(eng, a, units, max_units, slice, found, st);
+            if (r) return r;
+            // survivors back to their jobs: seed_index is a slot of the concatenated seed list
+            std::vector<std::pair<uint64_t, size_t>> by_off(member.size());
+            for (size_t k = 0; k < member.size(); k++) by_off[k] = {off[member[k]], member[k]};
+            std::sort(by_off.begin(), by_off.end());
+            for (Candidate c : found) {
+                auto it = std::upper_bound(by_off.begin(), by_off.end(), std::make_pair(c.seed_index, ~(size_t)0));
+                if (it == by_off.begin()) continue;
+                --it;
+                SchedJob &j = js[it->second];
+                c.seed_index -= it->first;
+                if (c.seed_index >= j.seeds.size()) continue;
+                j.found.push_back(c);
+            }
+        }
+        return WG_OK;
+    }();
+    cudaFree(d_seeds);
+    cudaFree(d_table);
+    if (rc) return rc;
+    for (SchedJob &j : js) {
+        std::sort(j.found.begin(), j.found.end(), candidate_order);
+        st.scanned += (int64_t)(j.seeds.size() * j.n_regions);
+        st.accepted += (int64_t)j.found.size();
+    }
+    return WG_OK;
+}
+
+}  // namespace
+
 extern "C" int wg_seed_check_jobs(wg_engine *eng, const wg_job *jobs, uint64_t n_jobs, wg_candidate *out,
                                   uint64_t cap, uint64_t *n_out, uint64_t *job_found, wg_scan_stats *stats) {
     if (!eng || (n_jobs && !jobs) || (cap && !out)) return WG_ERR_ARG;
@@ -325,11 +420,42 @@ extern "C" int wg_seed_check_jobs(wg_engine *eng, const wg_job *jobs, uint64_t n
     std::vector<SchedJob> js(n_jobs);
     uint64_t total = 0, largest = 0;
     for (uint64_t i = 0; i < n_jobs; i++) {
-        const int rc = sched_job_init(js[i], jobs[i]);
+        const int rc = sched_job_init(js[i], jobs[i], eng);
         if (rc) return eng->fail(rc, rc == WG_ERR_NOMEM ? "job seeds" : "job: empty or oversized");
         js[i].id = i;
         total += js[i].seeds.size();
         largest = std::max<uint64_t>(largest, js[i].seeds.size());
+    }
+    if (eng->job_queue && n_jobs) {
+        wg_scan_stats qst{};
+        e = cudaEventRecord(eng->ev0, eng->stream);
+        if (e != cudaSuccess) return eng->fail(WG_ERR_CUDA, "event", e);
+        int rc = jobs_on_device_queue(eng, js, total, qst);
+        if (rc == WG_OK) {
+            e = cudaEventRecord(eng->ev1, eng->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(eng->ev1);
+            if (e != cudaSuccess) return eng->fail(WG_ERR_CUDA, "event", e);
+            uint64_t w = 0, all = 0;
+            for (uint64_t i = 0; i < n_jobs; i++) {
+                if (job_found) job_found[i] = js[i].found.size();
+                for (const Candidate &c : js[i].found) {
+                    if (w < cap) std::memcpy(&out[w++], &c, sizeof c);
+                    all++;
+                }
+            }
+            if (n_out) *n_out = all;
+            if (stats) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, eng->ev0, eng->ev1);
+                qst.gpu_ms = ms;
+                qst.wall_ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+                *stats = qst;
+            }
+            return WG_OK;
+        }
+        if (rc != WG_ERR_CAPACITY) return rc;
+        // too large for one resident queue: the host batch loop below
+        for (SchedJob &j : js) j.found.clear();
     }
     // seeds resident on the device at once: all of them, up to 2^27 (1 GiB), and the largest job
     Scheduler sched(eng, std::min<uint64_t>(std::max<uint64_t>(total, 1), std::max<uint64_t>(largest, 1ull << 27)),
@@ -519,7 +645,7 @@ int wg_server_submit(wg_server *s, const wg_job *job, uint64_t *job_id) {
     if (!s || !job) return WG_ERR_ARG;
     const auto t = Clock::now();
     auto j = std::make_unique<SchedJob>();
-    int rc = sched_job_init(*j, *job);
+    int rc = sched_job_init(*j, *job, s->eng);
     if (rc) return rc;
     if (j->seeds.size() > s->sched->arena_seeds()) return WG_ERR_CAPACITY;
     j->t_submit = t;
@@ -589,4 +715,142 @@ void wg_server_close(wg_server *s) {
     delete s;
 }
 
+int wg_engine_set_job_queue(wg_engine *eng, int device_queue) {
+    if (!eng || (device_queue != 0 && device_queue != 1)) return WG_ERR_ARG;
+    eng->job_queue = device_queue;
+    return WG_OK;
+}
+
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Autotuner of the batched-job settings: per job class (regions per seed), the regions per unit
+// (more regions per unit build fewer Perlin tables per region, fewer give more independent units),
+// then the (seed, region) checks per queue slice, each by timing the candidates on the device on
+// probe jobs of that class (seed counts log-uniform 1..4,096 as in the uneven-jobs workload, from a
+// splitmix64 stream).  The reference tunes its scanner per GPU the same way (a measured sweep of
+// launch settings, kept per card).
+// ---------------------------------------------------------------------------------------------
+namespace {
+
+constexpr int kTuneSides[4] = {3, 13, 41, 129};   // probe rect side of each class (9 .. 16,641 regions)
+constexpr int kTuneJobs = 256;
+
+std::vector<wg_job> probe_jobs(int cls, uint64_t stream) {
+    std::vector<wg_job> jobs;
+    uint64_t k = 0;
+    const int side = kTuneSides[cls], r0 = -(side / 2);
+    for (int i = 0; i < kTuneJobs; i++) {
+        const double u = (double)(splitmix64(stream + k++) >> 11) * 0x1.0p-53;
+        const uint64_t n = std::max<uint64_t>(1, (uint64_t)std::floor(std::pow(4096.0, u)));
+        wg_job j{};
+        j.gen_base = splitmix64(stream + k++);
+        j.n_seeds = n;
+        j.rx0 = r0;
+        j.rx1 = r0 + side;
+        j.rz0 = r0;
+        j.rz1 = r0 + side;
+        j.max_height = -50;
+        wg_parse_version("1.19.x~26.1", &j.opts);
+        jobs.push_back(j);
+    }
+    return jobs;
+}
+
+// Device time of one device-queue run of the jobs under the engine's current settings.
+int time_jobs(wg_engine *eng, const std::vector<wg_job> &spec, double &ms) {
+    std::vector<SchedJob> js(spec.size());
+    uint64_t total = 0;
+    for (size_t i = 0; i < spec.size(); i++) {
+        const int rc = sched_job_init(js[i], spec[i], eng);
+        if (rc) return eng->fail(rc, "tune: probe job");
+        js[i].id = i;
+        total += js[i].seeds.size();
+    }
+    wg_scan_stats st{};
+    cudaError_t e = cudaEventRecord(eng->ev0, eng->stream);
+    if (e != cudaSuccess) return eng->fail(WG_ERR_CUDA, "event", e);
+    const int rc = jobs_on_device_queue(eng, js, total, st);
+    if (rc) return rc;
+    e = cudaEventRecord(eng->ev1, eng->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(eng->ev1);
+    if (e != cudaSuccess) return eng->fail(WG_ERR_CUDA, "event", e);
+    float f = 0.f;
+    cudaEventElapsedTime(&f, eng->ev0, eng->ev1);
+    ms = f;
+    return WG_OK;
+}
+
+}  // namespace
+
+extern "C" int wg_engine_tune(wg_engine *eng, wg_tune_report *rep) {
+    if (!eng) return WG_ERR_ARG;
+    cudaError_t e = cudaSetDevice(eng->device);
+    if (e != cudaSuccess) return eng->fail(WG_ERR_CUDA, "cudaSetDevice", e);
+    wg_tune_report r;
+    std::memset(&r, 0, sizeof r);
+    const uint32_t saved_win[4] = {eng->tuned_win[0], eng->tuned_win[1], eng->tuned_win[2], eng->tuned_win[3]};
+    const uint64_t saved_budget = eng->tuned_budget;
+    std::vector<wg_job> all;
+    int rc = WG_OK;
+    eng->tuned_budget = 0;
+    for (int c = 0; c < 4 && rc == WG_OK; c++) {
+        const uint64_t R = (uint64_t)kTuneSides[c] * kTuneSides[c];
+        r.max_regions[c] = (uint32_t)std::min<uint64_t>(kJobClassMax[c], 0xFFFFFFFFull);
+        // candidates: the whole seed per unit, and splits of it (large rects: 1,024 .. 16,384)
+        uint32_t cand[4] = {0, 0, 0, 0};
+        if (c < 3) {
+            cand[0] = (uint32_t)R;
+            cand[1] = (uint32_t)((R + 1) / 2);
+        } else {
+            cand[0] = 2048;
+            cand[1] = 4096;
+            cand[2] = 8192;
+            cand[3] = 16384;
+        }
+        const std::vector<wg_job> jobs = probe_jobs(c, 0x7E57000000000000ull + (uint64_t)c * 0x10000ull);
+        all.insert(all.end(), jobs.begin(), jobs.end());
+        double best = 0.0;
+        for (int q = 0; q < 4 && cand[q] && rc == WG_OK; q++) {
+            eng->tuned_win[c] = cand[q];
+            double ms = 0.0;
+            rc = time_jobs(eng, jobs, ms);                 // warm-up of this setting
+            if (rc == WG_OK) rc = time_jobs(eng, jobs, ms);
+            r.window_candidates[c][q] = cand[q];
+            r.window_ms[c][q] = ms;
+            if (rc == WG_OK && (q == 0 || ms < best)) {
+                best = ms;
+                r.window[c] = cand[q];
+            }
+        }
+        eng->tuned_win[c] = r.window[c];
+    }
+    const uint64_t budgets[3] = {1ull << 25, 1ull << 26, 1ull << 27};
+    double best = 0.0;
+    for (int q = 0; q < 3 && rc == WG_OK; q++) {
+        eng->tuned_budget = budgets[q];
+        double ms = 0.0;
+        rc = time_jobs(eng, all, ms);
+        r.budget_candidates[q] = budgets[q];
+        r.budget_ms[q] = ms;
+        if (rc == WG_OK && (q == 0 || ms < best)) {
+            best = ms;
+            r.budget = budgets[q];
+        }
+    }
+    if (rc) {   // keep the settings the engine had
+        for (int c = 0; c < 4; c++) eng->tuned_win[c] = saved_win[c];
+        eng->tuned_budget = saved_budget;
+        return rc;
+    }
+    eng->tuned_budget = r.budget;
+    if (rep) *rep = r;
+    return WG_OK;
+}
+
+extern "C" int wg_engine_set_tuning(wg_engine *eng, const uint32_t *window, uint64_t budget) {
+    if (!eng) return WG_ERR_ARG;
+    for (int c = 0; c < 4; c++) eng->tuned_win[c] = window ? window[c] : 0u;
+    eng->tuned_budget = budget;
+    return WG_OK;
+}

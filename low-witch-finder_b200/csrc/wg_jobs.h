@@ -35,9 +35,10 @@ struct SchedJob {
     uint64_t remaining_work() const { return (units - dispatched) * (uint64_t)win; }
 };
 
-// Fills a SchedJob's geometry and host seeds from a public job description; WG_ERR_ARG if the
-// job is empty or its rect is out of range.
-int sched_job_init(SchedJob &j, const wg_job &spec);
+// Fills a SchedJob's geometry and host seeds from a public job description (the window from the
+// engine's tuned settings when eng is given); WG_ERR_ARG if the job is empty or its rect is out
+// of range.
+int sched_job_init(SchedJob &j, const wg_job &spec, const wg_engine *eng);
 
 // Runs the admitted jobs of one engine batch by batch.  Not thread-safe: one thread drives it.
 class Scheduler {

@@ -273,7 +273,7 @@ struct ClimateSmem {
     uint32_t rwu[kUnits];                      // rect width of the unit's job
     unsigned int hist[P1_KINDS + kTiers];
     uint32_t grad[kGradWords];
-    float gradf[kGradWords];
+    float4 gt4[16];                            // FP32 core: gradient vector per hash
     ClimateSteps steps;
 };
 
@@ -349,7 +349,7 @@ __device__ __forceinline__ float climate_sample_f32(const ClimateSmem<true> &S, 
     const int slot = st.slot[k];
     const int o = slot * kUnits + iu;
     const double sc = st.sc[k], lac = st.lac[k];
-    ColTableF<kUnits> T{S.perm + slot * kPitch + iu, S.gradf};
+    ColTableF<kUnits> T{S.perm + slot * kPitch + iu, S.gt4};
     return perlin_y0_f32(T, S.ox[o], S.oz[o], S.jy[o], S.ty.hyf[o], S.ty.fyf[o], keep_precision((xc * sc) * lac),
                          keep_precision((zc * sc) * lac));
 }
@@ -468,6 +468,8 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
     using Real = typename ClimateSmem<F32>::Real;
     extern __shared__ __align__(16) uint8_t smem_raw[];
     ClimateSmem<F32> &S = *reinterpret_cast<ClimateSmem<F32> *>(smem_raw);
+    batch_range(a);
+    if (blockIdx.x * kUnits >= a.n_units) return;   // past this batch (a launch sized for a larger one)
     const int tid = threadIdx.x;
     const int my_slot = tid / kUnits, uu = tid % kUnits;
     const int large = a.large_biomes ? 1 : 0;
@@ -475,7 +477,7 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
     const bool all_rechecks = F32 && a.fp32_core == 2;   // every FP32 gate re-taken in FP64 (a check mode)
     if (tid < P1_KINDS + kTiers) S.hist[tid] = 0;
     fill_grad_table(S.grad, tid);
-    if (F32) fill_grad_table_f32(S.gradf, tid);
+    if (F32) fill_grad_table_f32(S.gt4, tid);
     if (tid < kClimateSteps) {
         const ClimateStep &c = c_steps[large][tid];
         S.steps.sc[tid] = c.sc;
@@ -521,7 +523,9 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                       p = c_slot_a[large][my_slot][2];
             Xr r = octave_rng(c_noise[noise], seed_fork_of(seed), sub, p);
             double ox, oy, oz;
-            perlin_shuffle<kUnits>(S.perm + my_slot * kPitch + uu, r, ox, oy, oz);
+            uint8_t *col = S.perm + my_slot * kPitch + uu;
+            perlin_shuffle<kUnits>(col, r, ox, oy, oz);
+            col[256 * kUnits] = col[0];   // row 256 = row 0, in the slot's padding (ColTableF)
             const int o = my_slot * kUnits + uu;
             int jy = (int)floor(oy);
             double hy = oy - jy;
@@ -854,14 +858,15 @@ static void allow_dynamic_smem(K kernel, size_t bytes, unsigned long long &done_
     if (dev >= 0 && dev < 64) done_mask |= 1ull << dev;
 }
 
+static unsigned long long g_smem_done64 = 0, g_smem_done32 = 0, g_smem_done_ent = 0;
+
 void launch_climate(const BatchArgs &a, cudaStream_t s) {
-    static unsigned long long done64 = 0, done32 = 0;
     int grid = (int)((a.n_units + kUnits - 1) / kUnits);
     if (a.fp32_core) {
-        allow_dynamic_smem(climate_kernel<true>, sizeof(ClimateSmem<true>), done32);
+        allow_dynamic_smem(climate_kernel<true>, sizeof(ClimateSmem<true>), g_smem_done32);
         climate_kernel<true><<<grid, kThreadsA, sizeof(ClimateSmem<true>), s>>>(a);
     } else {
-        allow_dynamic_smem(climate_kernel<false>, sizeof(ClimateSmem<false>), done64);
+        allow_dynamic_smem(climate_kernel<false>, sizeof(ClimateSmem<false>), g_smem_done64);
         climate_kernel<false><<<grid, kThreadsA, sizeof(ClimateSmem<false>), s>>>(a);
     }
 }
@@ -877,24 +882,25 @@ constexpr int kProbeStride = 20;   // bytes per table row: one column per table 
 
 __global__ void __launch_bounds__(kProbeThreads) noise_probe_kernel(const int64_t *seeds, int noise, const double *xz,
                                                                      uint32_t n_points, double *out32, double *out64) {
-    __shared__ __align__(16) uint8_t perm[256 * kProbeStride];
+    __shared__ __align__(16) uint8_t perm[257 * kProbeStride];   // row 256 = row 0 (ColTableF)
     __shared__ double ox[2 * kMaxOct], oz[2 * kMaxOct], hy[2 * kMaxOct], fy[2 * kMaxOct];
     __shared__ float hyf[2 * kMaxOct], fyf[2 * kMaxOct];
     __shared__ int jy[2 * kMaxOct];
     __shared__ uint32_t grad[kGradWords];
-    __shared__ float gradf[kGradWords];
+    __shared__ float4 gt4[16];
     const int t = threadIdx.x;
     const NoiseSpec &ns = c_noise[noise];
     const int np = ns.npresent;
     const uint64_t seed = (uint64_t)seeds[blockIdx.x];
     fill_grad_table(grad, t);
-    fill_grad_table_f32(gradf, t);
-    perm_blocks_init<kProbeStride, 256 * kProbeStride>(perm, 1, t, kProbeThreads);
+    fill_grad_table_f32(gt4, t);
+    perm_blocks_init<kProbeStride, 257 * kProbeStride>(perm, 1, t, kProbeThreads);
     __syncthreads();
     if (t < 2 * np) {
         Xr r = octave_rng(ns, seed_fork_of(seed), t / np, t % np);
         double x0, y0, z0;
         perlin_shuffle<kProbeStride>(perm + t, r, x0, y0, z0);
+        perm[256 * kProbeStride + t] = perm[t];
         const int j = (int)floor(y0);
         const double h = y0 - j;
         ox[t] = x0;
@@ -915,7 +921,7 @@ __global__ void __launch_bounds__(kProbeThreads) noise_probe_kernel(const int64_
             const double sc = q < np ? 1.0 : kDblScale, l = ns.lac[p];
             const double px = keep_precision((x * sc) * l), pz = keep_precision((z * sc) * l);
             const ColTable<kProbeStride> T{perm + q, grad};
-            const ColTableF<kProbeStride> TF{perm + q, gradf};
+            const ColTableF<kProbeStride> TF{perm + q, gt4};
             const double v = perlin_y0(T, ox[q], oz[q], jy[q], hy[q], fy[q], px, pz);
             if (q < np) a += (ns.amp[p] * v) * ns.per[p];
             else b += (ns.amp[p] * v) * ns.per[p];
@@ -1235,6 +1241,7 @@ __device__ __forceinline__ int free_slot(int i) { return i < kBaseSp1 ? i : i + 
 __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     EntranceSmem &S = *reinterpret_cast<EntranceSmem *>(smem_raw);
+    batch_range(a);
     const int tid = threadIdx.x;
     const int my_slot = tid / kUnits, rr = tid % kUnits;
     if (tid < P1_KINDS) S.hist[tid] = 0;
@@ -1403,8 +1410,7 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
 }
 
 void launch_entrance(const BatchArgs &a, int grid, cudaStream_t s) {
-    static unsigned long long done = 0;
-    allow_dynamic_smem(entrance_kernel, sizeof(EntranceSmem), done);
+    allow_dynamic_smem(entrance_kernel, sizeof(EntranceSmem), g_smem_done_ent);
     entrance_kernel<<<grid, kThreadsB, sizeof(EntranceSmem), s>>>(a);
 }
 
@@ -1441,6 +1447,7 @@ __device__ __forceinline__ double combine_vals(int noise, const double *v, int s
 
 __global__ void __launch_bounds__(kThreadsC) ladder_kernel(BatchArgs a) {
     __shared__ __align__(16) LadderSmem S;
+    batch_range(a);
     const int t = threadIdx.x;
     const int large = a.large_biomes ? 1 : 0;
     const int cont_noise = large ? N_CONTINENTALNESS_LARGE : N_CONTINENTALNESS;
@@ -1636,19 +1643,30 @@ __global__ void __launch_bounds__(kThreadsC) ladder_kernel(BatchArgs a) {
 
 // grid <= 0: as many blocks as are resident at once (the kernel loops over candidates, so blocks
 // beyond the resident count would only form a second, mostly idle wave)
+static int g_ladder_per_sm = 0, g_ladder_sms = 0;
+
+static void ladder_geometry() {
+    if (g_ladder_per_sm) return;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_ladder_sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_ladder_per_sm, ladder_kernel, kThreadsC, 0);
+    if (g_ladder_per_sm < 1) g_ladder_per_sm = 1;
+}
+
 void launch_ladder(const BatchArgs &a, int grid, cudaStream_t s) {
     if (grid <= 0) {
-        static int per_sm = 0, sms = 0;
-        if (!per_sm) {
-            int dev = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ladder_kernel, kThreadsC, 0);
-            if (per_sm < 1) per_sm = 1;
-        }
-        grid = sms * per_sm;
+        ladder_geometry();
+        grid = g_ladder_sms * g_ladder_per_sm;
     }
     ladder_kernel<<<grid, kThreadsC, 0, s>>>(a);
+}
+
+void prepare_phase1_launches() {
+    allow_dynamic_smem(climate_kernel<true>, sizeof(ClimateSmem<true>), g_smem_done32);
+    allow_dynamic_smem(climate_kernel<false>, sizeof(ClimateSmem<false>), g_smem_done64);
+    allow_dynamic_smem(entrance_kernel, sizeof(EntranceSmem), g_smem_done_ent);
+    ladder_geometry();
 }
 
 }  // namespace wg

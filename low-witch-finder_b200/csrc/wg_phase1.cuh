@@ -130,7 +130,21 @@ struct BatchArgs {
     // max_height per job; seeds from `seeds`); unit0 .. unit0 + n_units are global units of it.
     const JobGeom *jobs = nullptr;
     uint32_t n_jobs = 0;
+
+    // Optional device work queue (wg_queue.cu): when set, the batch's unit0 and n_units are read
+    // from dyn[0], dyn[1] at kernel start instead of the fields above (a graph replays the same
+    // launches while a device kernel moves the batch along the queue); n_units above is then the
+    // largest batch the launch geometry covers.
+    const uint64_t *dyn = nullptr;
 };
+
+// The batch range of a launch: dyn when set, else the launch's own fields.
+__device__ __forceinline__ void batch_range(BatchArgs &a) {
+    if (a.dyn) {
+        a.unit0 = a.dyn[0];
+        a.n_units = (uint32_t)a.dyn[1];
+    }
+}
 
 // One evaluation step of the climate state machine (a single y=0 Perlin sample).  The last
 // four fields serve the FP32 noise core: cf = (float)(c1 * c2), and for a tier step the band
@@ -177,6 +191,9 @@ void upload_tables(const NoiseSpec *specs, const ClimateStep *steps_normal, cons
 void launch_climate(const BatchArgs &a, cudaStream_t s);
 void launch_entrance(const BatchArgs &a, int grid, cudaStream_t s);
 void launch_ladder(const BatchArgs &a, int grid, cudaStream_t s);
+// Sets the kernels' shared-memory limits and the ladder's resident-block count on the current
+// device, so that the launch functions make no further runtime calls (a stream capture may follow).
+void prepare_phase1_launches();
 size_t climate_smem_bytes(bool fp32_core);
 // The climate stage of a batch whose units have one region each (spots mode), breadth first over
 // two item lists of `cap` entries (counts: 2 words, device); climate survivors become records.

@@ -85,6 +85,53 @@ def test_uneven_jobs_sample(engine, wg):
     assert st["accepted"] == sum(len(g) for g in got)
 
 
+def test_device_queue_equals_host_loop(engine, wg):
+    """The device work queue (one graph launch, slices taken off the queue on the device) and the
+    host batch loop give every job the same survivors and the same funnel."""
+    jobs = mixed_jobs(wg) + wg.uneven_jobs(n_jobs=64, base=5)
+    engine.set_job_queue(True)
+    got_q, st_q = engine.seed_check_jobs(jobs)
+    engine.set_job_queue(False)
+    try:
+        got_h, st_h = engine.seed_check_jobs(jobs)
+    finally:
+        engine.set_job_queue(True)
+    for i in range(len(jobs)):
+        assert np.array_equal(got_q[i], got_h[i]), i
+    for k in ("reject_hist", "tier_hist", "scanned", "accepted", "climate_survivors", "deep_candidates"):
+        assert st_q[k] == st_h[k], k
+    assert st_q["batches"] >= 1
+
+
+def test_device_queue_overflow_retries(engine, wg, port, bind_mod):
+    """SINGLE_BIOME jobs pass every region through the climate stage: the queue's slices overflow
+    the work lists and are re-run smaller on the device; results still equal the oracle's."""
+    jobs = [{"gen": (9 + k, 400), "rect": (-20, 20, -20, 20), "max_height": -50, "preset": "SINGLE_BIOME"}
+            for k in range(3)]
+    got, st = engine.seed_check_jobs(jobs)
+    r = bind_mod.rules("1.19.x~26.1", "SINGLE_BIOME")
+    for i, job in enumerate(jobs):
+        want, _ = port.scan_seeds(r, -50, job["rect"], gen=job["gen"])
+        assert np.array_equal(got[i], want), i
+
+
+def test_tuner_picks_measured_settings(wg):
+    """wg_engine_tune times each class's candidates on the device and keeps the fastest; a tuned
+    engine's jobs equal the untuned engine's."""
+    with wg.Engine(0) as eng:
+        jobs = wg.uneven_jobs(n_jobs=96, base=11)
+        before, _ = eng.seed_check_jobs(jobs)
+        rep = eng.tune()
+        assert len(rep["classes"]) == 4
+        for c in rep["classes"]:
+            ms = {x["window"]: x["ms"] for x in c["candidates"]}
+            assert c["window"] in ms and ms[c["window"]] == min(ms.values()) and all(v > 0 for v in ms.values())
+        assert rep["budget"] in [x["checks"] for x in rep["budget_candidates"]]
+        after, _ = eng.seed_check_jobs(jobs)
+        for i in range(len(jobs)):
+            assert np.array_equal(before[i], after[i]), i
+
+
 def test_jobs_errors(engine, wg):
     with pytest.raises(wg.EngineError):
         engine.seed_check_jobs([{"gen": (1, 10), "rect": (0, 0, 0, 1)}])
