@@ -220,6 +220,18 @@ def deep_measure(eng, opts) -> dict:
     t0 = time.perf_counter()
     surv, bad = eng.deep_spots(spots["s48"], spots["chunk_x"], spots["chunk_z"], max_height=-54, opts=opts)
     spot_s = time.perf_counter() - t0
+    # config 4, a stated slice: structure seeds (hi16 << 32) | lo32, hi16 = the top 16 bits of
+    # splitmix64(4), lo32 = 0, 1, 2, 3; each swept over the whole +-30M world with the catalogued
+    # layouts of the -58 / -59 hunts (data/hunt/58, data/hunt/59) probed at every start
+    wg = load_package()
+    hi16 = wg.splitmix64(4) >> 48
+    c4_seeds = [(hi16 << 32) | lo for lo in range(4)]
+    layouts = [231564844655014, 156186219368766, 270840896143627]
+    eng.deep_sweep(layouts, s48=c4_seeds[:1], rect=(-64, 64, -64, 64))
+    t0 = time.perf_counter()
+    c4_matches, c4_starts = eng.deep_sweep(layouts, s48=c4_seeds, rect=wg.WORLD_REGIONS)
+    c4_s = time.perf_counter() - t0
+    world_regions = (wg.WORLD_REGIONS[1] - wg.WORLD_REGIONS[0]) * (wg.WORLD_REGIONS[3] - wg.WORLD_REGIONS[2])
     # the solver on the -58 plan line (layout 231564844655014, regime 22, class odd: data/hunt/58)
     plan = [(231564844655014, (2, 2), "odd")]
     eng.deep_solve(plan, 0, 2)
@@ -236,6 +248,17 @@ def deep_measure(eng, opts) -> dict:
             "terrain": {"spots": int(len(spots)), "world_seeds": int(len(spots)) << 16,
                         "world_seeds_per_s": (len(spots) << 16) / spot_s, "ms": 1e3 * spot_s,
                         "survivors": int(len(surv)), "max_height": -54},
+            "c4": {"slice": "structure seeds (hi16 << 32) | lo32, hi16 = splitmix64(4) >> 48, lo32 = 0..3, each "
+                            "over every hut region of the +-30M world (117,187^2), catalogue = the 3 layouts of "
+                            "data/hunt/58 and /59",
+                   "structure_seeds": len(c4_seeds), "regions": len(c4_seeds) * world_regions,
+                   "starts": int(c4_starts.sum()), "matches": int(len(c4_matches)),
+                   "structure_seeds_per_s": len(c4_seeds) / c4_s, "regions_per_s": len(c4_seeds) * world_regions / c4_s,
+                   "world_seeds_per_s_equivalent": (len(c4_seeds) << 16) / c4_s, "ms": 1e3 * c4_s,
+                   "note": ("world seeds/s = structure seeds/s x 65,536 (each structure seed stands for its 65,536 "
+                            "upper-16-bit world seeds); the terrain stage that expands a match runs at the "
+                            "`terrain` rate; the reference's own figure is about 94 M world seeds/s for that "
+                            "stage (hunt.py:463-464)")},
             "timing": "wall clock around wg_deep_solve / wg_deep_starts / wg_deep_spots (host buffers in and "
                       "out); device time of the solver from its CUDA events"}
 
