@@ -234,10 +234,15 @@ __global__ void __launch_bounds__(kDeepThreads) sweep_kernel(SweepGeom G, uint64
             pz += 32ull * (uint64_t)c.b;
         }
     }
-    // starts per structure seed: a warp's lanes may belong to two seeds, so the sum is per lane group
-    const unsigned same = __match_any_sync(0xFFFFFFFFu, k < n_tasks ? i : ~0ull);
-    const uint32_t tot = __reduce_add_sync(same, n_starts);
-    if (k < n_tasks && (threadIdx.x & 31) == (__ffs(same) - 1) && tot) atomicAdd(&starts[i], (unsigned long long)tot);
+    // starts per structure seed: one warp sum when the warp's lanes share a seed (lanes past the
+    // tasks count nothing); a warp that straddles two seeds adds lane by lane
+    const uint64_t i0 = __shfl_sync(0xFFFFFFFFu, i, 0);
+    if (__all_sync(0xFFFFFFFFu, k >= n_tasks || i == i0)) {
+        const uint32_t tot = __reduce_add_sync(0xFFFFFFFFu, n_starts);
+        if ((threadIdx.x & 31) == 0 && tot) atomicAdd(&starts[i0], (unsigned long long)tot);
+    } else if (k < n_tasks && n_starts) {
+        atomicAdd(&starts[i], (unsigned long long)n_starts);
+    }
 }
 
 #define DEEP_CUDA(call, what)                                           \

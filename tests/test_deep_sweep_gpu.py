@@ -39,6 +39,15 @@ def test_sweep_starts_and_matches_equal_the_walk(engine):
     assert [int(v) for v in matches["value"]] == [val[int(c)] for c in matches["carver"]]
 
 
+def test_sweep_start_counts_when_warps_straddle_seeds(engine):
+    """A rect of 33 columns x 64 rows gives each structure seed 33 tasks, so most warps hold lanes of
+    two seeds: the per-seed start counts still equal the region walk's."""
+    rect = (-17, 16, -40, 24)
+    walk = engine.deep_starts(base=777, count=40, rect=rect)
+    _, starts = engine.deep_sweep([5], base=777, count=40, rect=rect)
+    assert starts.tolist() == np.bincount(walk["seed_index"], minlength=40).tolist()
+
+
 def test_sweep_against_the_oracle(engine, port):
     """Matches on explicit structure seeds equal the C restatement's starts filtered by the catalogue,
     at the world border too (re-draws of the hut offsets included)."""

@@ -70,7 +70,7 @@ def test_worker_protocol(wg, engine, tmp_path):
                    "--max-region-z 79 --max-height -54 --phase1-candidates --out p.csv") == "===SCAN_DONE rc=0==="
         assert read_csv(tmp_path / "p.csv") == [(int(c["seed"]), int(c["chunk_x"]), int(c["chunk_z"]),
                                                  int(c["chunk_x"]) * 16, int(c["chunk_z"]) * 16) for c in want]
-        assert len(want) > 1
+        assert len(want) >= 1
         assert ask("--seed-gen 2 65536 --min-region-x -4 --max-region-x 5 --min-region-z -4 --max-region-z 5 "
                    "--max-height -50 --out g.csv") == "===SCAN_DONE rc=0==="
         assert read_csv(tmp_path / "g.csv") == []
@@ -99,15 +99,18 @@ def test_single_shot_cli(wg, engine, tmp_path):
 
 
 def test_exact_hits_at_a_relaxed_ceiling(wg, engine, tmp_path):
-    """Phase 1 at max_height 100 with --phase2-max-y 100: many phase-1 survivors, of which phase 2
-    keeps the biome-ok, dry huts with floor <= 100; the rows and floors equal wg_eval_huts'."""
-    rect = ["--min-region-x", "-8", "--max-region-x", "8", "--min-region-z", "-8", "--max-region-z", "8"]
-    rows = _scan(wg, tmp_path, "--seed-gen", "5", "20000", *rect, "--max-height", "100", "--phase2-max-y", "100",
+    """Phase 1 at max_height 100 with --phase2-max-y 100 on hunt.py's SCAN_REFERENCE seed over its
+    40,000-block rect: many phase-1 survivors, of which phase 2 keeps the biome-ok, dry huts with
+    floor <= 100 (the reference hut among them); the rows and floors equal wg_eval_huts'."""
+    seed = 1473884015873122059
+    rect = ["--min-region-x", "-79", "--max-region-x", "79", "--min-region-z", "-79", "--max-region-z", "79"]
+    rows = _scan(wg, tmp_path, "--seed", str(seed), *rect, "--max-height", "100", "--phase2-max-y", "100",
                  phase1=False)
-    cands = engine.seed_check(gen=(5, 20000), rect=(-8, 8, -8, 8), max_height=100).candidates
+    cands = engine.seed_check(seeds=[seed], rect=(-79, 79, -79, 79), max_height=100).candidates
     want = exact_rows(engine, cands, 100)
     assert rows == want
     assert 0 < len(want) < len(cands)
+    assert (seed, -987, -1073, -15792, -17168, -54) in want
 
 
 def test_self_test_passes(wg, tmp_path):

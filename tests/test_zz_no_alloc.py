@@ -33,8 +33,10 @@ def test_noalloc_matches_engine_two_calls(wg, engine):
         (None, 2, 8192, (-32, 32, -32, 32), -50, "NORMAL"),
         ([wg.to_signed(wg.splitmix64(7 + i)) for i in range(20000)], 0, 20000, (-20, 20, -20, 20), -50, "NORMAL"),
         # one region per seed: the engine takes its breadth-first one-region climate stage here,
-        # the allocation-free entry point the ordinary climate kernel
-        (None, 5, 65536, (3, 4, -2, -1), 100, "NORMAL"),
+        # the allocation-free entry point the ordinary climate kernel; the region of hunt.py's
+        # reference hut (seed 1473884015873122059, region (-31, -34)) beside 4,095 other seeds
+        ([1473884015873122059] + [wg.to_signed(wg.splitmix64(50 + i)) for i in range(4095)], 0, 4096,
+         (-31, -30, -34, -33), -50, "NORMAL"),
         (None, 11, 4096, (-16, 16, -16, 16), 0, "LARGE_BIOMES"),
     ]
     counts = []
