@@ -103,12 +103,24 @@ F32Bands wg::build_f32_bands(const ClimateStep *st) {
     return b;
 }
 
+namespace {
+double g_climate_lac_max = 1.0;   // the largest lacunarity of a climate step (both presets)
+}
+
+bool wg::coords_small(int64_t lo, int64_t hi) {
+    const double r = (double)std::max<int64_t>(std::llabs(lo), std::llabs(hi));
+    return (4.0 * (32.0 * r + 23.0) + 2.0) * 1.02 * g_climate_lac_max < 0.99e7;
+}
+
 void wg::upload_phase1_tables() {
     NoiseSpec specs[N_NOISE_COUNT];
     build_noise_specs(specs);
     ClimateStep normal[kClimateSteps], large[kClimateSteps];
     build_climate_steps(specs, N_EROSION, N_TEMPERATURE, normal);
     build_climate_steps(specs, N_EROSION_LARGE, N_TEMPERATURE_LARGE, large);
+    double lac = 0.0;
+    for (int k = 0; k < kClimateSteps; k++) lac = std::max(lac, std::max(normal[k].lac, large[k].lac));
+    g_climate_lac_max = lac;
     const F32Bands bands[2] = {build_f32_bands(normal), build_f32_bands(large)};
     upload_tables(specs, normal, large, bands);
 }
@@ -242,6 +254,8 @@ int run_request(wg_engine *eng, const Request &rq, Sink &sink, wg_scan_stats &st
     a.spot_s48 = rq.d_spot_s48;
     a.spot_rx = rq.d_spot_rx;
     a.spot_rz = rq.d_spot_rz;
+    // spots shift the rect by their own regions: only plain requests are proved small
+    a.small_coords = !rq.d_spot_s48 && coords_small(std::min(rq.rx0, rq.rz0), std::max(rq.rx1, rq.rz1) - 1ll) ? 1 : 0;
 
     uint64_t per_batch = std::min<uint64_t>(kMaxUnits, std::max<uint64_t>(32, kWorkPerBatch / win));
     if (rq.opts.single_biome)  // every region survives the climate stage

@@ -40,6 +40,12 @@ bool candidate_order(const Candidate &x, const Candidate &y) {
     return x.rx < y.rx;
 }
 
+// Whether a job's climate coordinates are proved inside maintainPrecision's identity range.
+bool job_small(const SchedJob &j) {
+    const int64_t rh = (int64_t)(j.n_regions / (uint64_t)j.rw);
+    return coords_small(std::min<int64_t>(j.rx0, j.rz0), std::max<int64_t>(j.rx0 + j.rw, j.rz0 + rh) - 1);
+}
+
 }  // namespace
 
 int sched_job_init(SchedJob &j, const wg_job &spec, const wg_engine *eng) {
@@ -238,6 +244,8 @@ int Scheduler::step(std::vector<SchedJob *> &finished, std::vector<SchedJob *> &
     a.seeds = d_arena_;
     a.jobs = d_table_;
     a.n_jobs = (uint32_t)table.size();
+    a.small_coords = 1;
+    for (const SchedJob *j : members) a.small_coords &= job_small(*j) ? 1 : 0;
     found_.clear();
     Sink sink;
     sink.host = &found_;
@@ -378,6 +386,8 @@ int jobs_on_device_queue(wg_engine *eng, std::vector<SchedJob> &js, uint64_t tot
             a.seeds = d_seeds;
             a.jobs = d_table;
             a.n_jobs = (uint32_t)table.size();
+            a.small_coords = 1;
+            for (size_t k : member) a.small_coords &= job_small(js[k]) ? 1 : 0;
             std::vector<Candidate> found;
             const uint64_t slice = js[lead].opts.single_biome ? std::min<uint64_t>(budget, kCapSurv / 2) : budget;
             int r = run_queue(eng, a, units, max_units, slice, found, st);

@@ -108,6 +108,7 @@ extern "C" int wg_seed_check_noalloc(const int64_t *d_seeds, uint64_t gen_base, 
         a.large_biomes = opts->large_biomes;
     }
     a.fp32_core = 1;   // the engine's default noise core
+    a.small_coords = coords_small(std::min(rx0, rz0), std::max(rx1, rz1) - 1ll) ? 1 : 0;
     a.counters = reinterpret_cast<uint32_t *>(base + kOffCounters);
     a.hist = reinterpret_cast<unsigned long long *>(base + kOffHist);
     a.rec_unit = reinterpret_cast<uint32_t *>(base + kOffRecUnit);

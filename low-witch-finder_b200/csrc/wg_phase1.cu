@@ -343,15 +343,19 @@ __device__ __forceinline__ double climate_sample(const Sm &S, int iu, int k, dou
                      keep_precision((zc * sc) * lac));
 }
 
-// The same sample in the FP32 core (coordinates reduced in FP64, the rest in FP32).
+// The same sample in the FP32 core (coordinates reduced in FP64, the rest in FP32).  SMALL: the
+// host has shown every coordinate of the batch to lie inside maintainPrecision's identity range
+// (BatchArgs::small_coords), so the check is left out and the sample is one branch-free block.
+template <bool SMALL>
 __device__ __forceinline__ float climate_sample_f32(const ClimateSmem<true> &S, int iu, int k, double xc, double zc) {
     const ClimateSteps &st = S.steps;
     const int slot = st.slot[k];
     const int o = slot * kUnits + iu;
     const double sc = st.sc[k], lac = st.lac[k];
     ColTableF<kUnits> T{S.perm + slot * kPitch + iu, S.gt4};
-    return perlin_y0_f32(T, S.ox[o], S.oz[o], S.jy[o], S.ty.hyf[o], S.ty.fyf[o], keep_precision((xc * sc) * lac),
-                         keep_precision((zc * sc) * lac));
+    const double x = (xc * sc) * lac, z = (zc * sc) * lac;
+    return perlin_y0_f32(T, S.ox[o], S.oz[o], S.jy[o], S.ty.hyf[o], S.ty.fyf[o], SMALL ? x : keep_precision(x),
+                         SMALL ? z : keep_precision(z));
 }
 
 // FP64 octave sum of climate steps [k0, k1] in the reference's order (sum += (c1 * v) * c2):
@@ -463,7 +467,7 @@ __device__ void climate_rest(Sm &S, const BatchArgs &a, TierCounts &tc, uint32_t
 // bound); inside the band the thread recomputes that region's samples in FP64 in the reference's
 // order and decides exactly as the FP64 path does.  So every decision, and with it the reject
 // codes, tier histogram and survivor set, equals the FP64 path's.
-template <bool F32>
+template <bool F32, bool SMALL>
 __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
     using Real = typename ClimateSmem<F32>::Real;
     extern __shared__ __align__(16) uint8_t smem_raw[];
@@ -575,36 +579,9 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
         // ---- tier 0 for every region: samples 0A and 0B with loop-invariant parameters ----
         {
             const int nq = kUnits * kChunk;
-            for (int q = tid; q < nq; q += kThreadsA) {
-                const int iu = q % kUnits;
-                const uint32_t jl = (uint32_t)(q / kUnits), j = c0 + jl;
-                if (j >= S.end[iu]) continue;
-                if (a.single_biome) {  // phase1.c:96: the climate gates are skipped
-                    keep_survivor(S, a, iu, j);
-                    continue;
-                }
-                double xc, zc;
-                climate_point(S, iu, jl, xc, zc);
-                Real sum;
-                bool pass;
-                if constexpr (F32) {
-                    sum = __fmul_rn(st.cf[0], climate_sample_f32(S, iu, 0, xc, zc));
-                    sum = __fmaf_rn(st.cf[1], climate_sample_f32(S, iu, 1, xc, zc), sum);
-                    if (!all_rechecks && sum < st.lo[1]) {
-                        pass = false;
-                    } else if (!all_rechecks && sum >= st.hi[1]) {
-                        pass = true;
-                    } else {   // inside the error band: decide in FP64
-                        rechecks++;
-                        pass = !(climate_sum64(S, iu, 0, 1, xc, zc) * st.amp[1] < st.thr[1]);
-                    }
-                } else {
-                    sum = 0.0;
-                    sum += (st.c1[0] * climate_sample(S, iu, 0, xc, zc)) * st.c2[0];
-                    sum += (st.c1[1] * climate_sample(S, iu, 1, xc, zc)) * st.c2[1];
-                    pass = !(sum * st.amp[1] < st.thr[1]);
-                }
-                // warp-aggregated append of the survivors to the tier list
+            // the decision's bookkeeping: warp-aggregated append of a survivor to the tier list
+            auto tier0_decide = [&](int iu, uint32_t jl, Real sum, bool pass, double xc, double zc) {
+                const uint32_t j = c0 + jl;
                 cg::coalesced_group grp = cg::coalesced_threads();
                 const unsigned m = grp.ballot(pass);
                 uint32_t base = 0;
@@ -623,6 +600,73 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                     } else {
                         climate_rest(S, a, tc, ((uint32_t)iu << 16) | jl, c0, 2, (double)sum, xc, zc);
                     }
+                }
+            };
+            if (a.single_biome) {   // phase1.c:96: the climate gates are skipped
+                for (int q = tid; q < nq; q += kThreadsA) {
+                    const int iu = q % kUnits;
+                    const uint32_t j = c0 + (uint32_t)(q / kUnits);
+                    if (j < S.end[iu]) keep_survivor(S, a, iu, j);
+                }
+            } else if constexpr (F32) {
+                // two regions per loop trip: their four samples are independent chains of dependent
+                // table loads, computed before any decision so that they overlap
+#pragma unroll 1
+                for (int q0 = tid; q0 < nq; q0 += 2 * kThreadsA) {
+                    int iu[2];
+                    uint32_t jl[2];
+                    bool ok[2];
+                    double xc[2], zc[2];
+                    float v0[2], v1[2];
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int q = q0 + h * kThreadsA;
+                        ok[h] = q < nq;
+                        const int qq = ok[h] ? q : 0;
+                        iu[h] = qq % kUnits;
+                        jl[h] = (uint32_t)(qq / kUnits);
+                        ok[h] = ok[h] && c0 + jl[h] < S.end[iu[h]];
+                        climate_point(S, iu[h], jl[h], xc[h], zc[h]);
+                        if (!ok[h]) xc[h] = zc[h] = 2.0;   // a harmless point for an unused lane
+                    }
+                    if (__any_sync(0xFFFFFFFFu, ok[1])) {
+#pragma unroll
+                        for (int h = 0; h < 2; h++) {
+                            v0[h] = climate_sample_f32<SMALL>(S, iu[h], 0, xc[h], zc[h]);
+                            v1[h] = climate_sample_f32<SMALL>(S, iu[h], 1, xc[h], zc[h]);
+                        }
+                    } else {   // no lane of the warp has a second region
+                        v0[0] = climate_sample_f32<SMALL>(S, iu[0], 0, xc[0], zc[0]);
+                        v1[0] = climate_sample_f32<SMALL>(S, iu[0], 1, xc[0], zc[0]);
+                        v0[1] = v1[1] = 0.0f;
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        if (!ok[h]) continue;
+                        const float sum = __fmaf_rn(st.cf[1], v1[h], __fmul_rn(st.cf[0], v0[h]));
+                        bool pass;
+                        if (!all_rechecks && sum < st.lo[1]) {
+                            pass = false;
+                        } else if (!all_rechecks && sum >= st.hi[1]) {
+                            pass = true;
+                        } else {   // inside the error band: decide in FP64
+                            rechecks++;
+                            pass = !(climate_sum64(S, iu[h], 0, 1, xc[h], zc[h]) * st.amp[1] < st.thr[1]);
+                        }
+                        tier0_decide(iu[h], jl[h], sum, pass, xc[h], zc[h]);
+                    }
+                }
+            } else {
+                for (int q = tid; q < nq; q += kThreadsA) {
+                    const int iu = q % kUnits;
+                    const uint32_t jl = (uint32_t)(q / kUnits), j = c0 + jl;
+                    if (j >= S.end[iu]) continue;
+                    double xc, zc;
+                    climate_point(S, iu, jl, xc, zc);
+                    double sum = 0.0;
+                    sum += (st.c1[0] * climate_sample(S, iu, 0, xc, zc)) * st.c2[0];
+                    sum += (st.c1[1] * climate_sample(S, iu, 1, xc, zc)) * st.c2[1];
+                    tier0_decide(iu, jl, sum, !(sum * st.amp[1] < st.thr[1]), xc, zc);
                 }
             }
         }
@@ -647,37 +691,72 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                 const bool last = st.act[k] == ACT_TIER_LAST;
                 uint32_t ke[kPer];
                 Real ks[kPer];
+                if constexpr (F32) {
+                    // every item's sample first (independent chains of table loads), then the checks
+                    uint32_t e[kPer];
+                    double xc[kPer], zc[kPer];
+                    float v[kPer];
 #pragma unroll
-                for (int r = 0; r < kPer; r++) {
-                    const uint32_t q = (uint32_t)tid + (uint32_t)(r * kThreadsA);
-                    ke[r] = 0xFFFFFFFFu;
-                    ks[r] = 0;
-                    if (q < n_t) {
-                        const uint32_t e = S.tlist[q];
-                        const int iu = (int)(e >> 16);
-                        double xc, zc;
-                        climate_point(S, iu, e & 0xFFFFu, xc, zc);
-                        Real sum = S.tsum[q];
+                    for (int r = 0; r < kPer; r++) {
+                        const uint32_t q = (uint32_t)tid + (uint32_t)(r * kThreadsA);
+                        e[r] = q < n_t ? S.tlist[q] : 0u;
+                        climate_point(S, (int)(e[r] >> 16), e[r] & 0xFFFFu, xc[r], zc[r]);
+                        if (q >= n_t) xc[r] = zc[r] = 2.0;   // a harmless point for an unused slot
+                    }
+                    // two chains at a time: three would not fit the registers
+                    if (__any_sync(0xFFFFFFFFu, (uint32_t)tid + kThreadsA < n_t)) {
+                        v[0] = climate_sample_f32<SMALL>(S, (int)(e[0] >> 16), k, xc[0], zc[0]);
+                        v[1] = climate_sample_f32<SMALL>(S, (int)(e[1] >> 16), k, xc[1], zc[1]);
+                    } else {   // no lane of the warp has a second item
+                        v[0] = climate_sample_f32<SMALL>(S, (int)(e[0] >> 16), k, xc[0], zc[0]);
+                        v[1] = 0.0f;
+                    }
+                    static_assert(kPer == 3, "the sample calls below assume three items per thread");
+                    if ((uint32_t)tid + 2u * kThreadsA < n_t) v[2] = climate_sample_f32<SMALL>(S, (int)(e[2] >> 16), k, xc[2], zc[2]);
+                    else v[2] = 0.0f;
+#pragma unroll
+                    for (int r = 0; r < kPer; r++) {
+                        const uint32_t q = (uint32_t)tid + (uint32_t)(r * kThreadsA);
+                        ke[r] = 0xFFFFFFFFu;
+                        ks[r] = 0;
+                        if (q >= n_t) continue;
+                        const int iu = (int)(e[r] >> 16);
+                        const float sum = __fmaf_rn(cf, v[r], S.tsum[q]);
                         bool reject;
-                        if constexpr (F32) {
-                            sum = __fmaf_rn(cf, climate_sample_f32(S, iu, k, xc, zc), sum);
-                            if (!all_rechecks && sum < lo) {
-                                reject = true;
-                            } else if (!all_rechecks && sum >= hi) {
-                                reject = false;
-                            } else {   // inside the error band: the exact partial sum of steps 0..k
-                                rechecks++;
-                                reject = climate_sum64(S, iu, 0, k, xc, zc) * amp < thr;
-                            }
-                        } else {
-                            sum += (c1 * climate_sample(S, iu, k, xc, zc)) * c2;
-                            reject = sum * amp < thr;
+                        if (!all_rechecks && sum < lo) {
+                            reject = true;
+                        } else if (!all_rechecks && sum >= hi) {
+                            reject = false;
+                        } else {   // inside the error band: the exact partial sum of steps 0..k
+                            rechecks++;
+                            reject = climate_sum64(S, iu, 0, k, xc[r], zc[r]) * amp < thr;
                         }
                         if (reject) {
-                            erosion_reject(S, a, tc, iu, c0 + (e & 0xFFFFu), tier);
+                            erosion_reject(S, a, tc, iu, c0 + (e[r] & 0xFFFFu), tier);
                         } else {
-                            ke[r] = e;
+                            ke[r] = e[r];
                             ks[r] = sum;
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < kPer; r++) {
+                        const uint32_t q = (uint32_t)tid + (uint32_t)(r * kThreadsA);
+                        ke[r] = 0xFFFFFFFFu;
+                        ks[r] = 0;
+                        if (q < n_t) {
+                            const uint32_t e = S.tlist[q];
+                            const int iu = (int)(e >> 16);
+                            double xc, zc;
+                            climate_point(S, iu, e & 0xFFFFu, xc, zc);
+                            double sum = S.tsum[q];
+                            sum += (c1 * climate_sample(S, iu, k, xc, zc)) * c2;
+                            if (sum * amp < thr) {
+                                erosion_reject(S, a, tc, iu, c0 + (e & 0xFFFFu), tier);
+                            } else {
+                                ke[r] = e;
+                                ks[r] = sum;
+                            }
                         }
                     }
                 }
@@ -720,7 +799,7 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
             const int iu = (int)(e >> 16);
             double xc, zc;
             climate_point(S, iu, e & 0xFFFFu, xc, zc);
-            if constexpr (F32) S.val[t] = climate_sample_f32(S, iu, kT0 + (int)(t % 4), xc, zc);
+            if constexpr (F32) S.val[t] = climate_sample_f32<SMALL>(S, iu, kT0 + (int)(t % 4), xc, zc);
             else S.val[t] = climate_sample(S, iu, kT0 + (int)(t % 4), xc, zc);
         }
         __syncthreads();
@@ -766,7 +845,7 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
             const int iu = (int)(e >> 16);
             double xc, zc;
             climate_point(S, iu, e & 0xFFFFu, xc, zc);
-            if constexpr (F32) S.val[t] = climate_sample_f32(S, iu, kR0 + (int)(t % 6), xc, zc);
+            if constexpr (F32) S.val[t] = climate_sample_f32<SMALL>(S, iu, kR0 + (int)(t % 6), xc, zc);
             else S.val[t] = climate_sample(S, iu, kR0 + (int)(t % 6), xc, zc);
         }
         __syncthreads();
@@ -858,16 +937,19 @@ static void allow_dynamic_smem(K kernel, size_t bytes, unsigned long long &done_
     if (dev >= 0 && dev < 64) done_mask |= 1ull << dev;
 }
 
-static unsigned long long g_smem_done64 = 0, g_smem_done32 = 0, g_smem_done_ent = 0;
+static unsigned long long g_smem_done64 = 0, g_smem_done32 = 0, g_smem_done32s = 0, g_smem_done_ent = 0;
 
 void launch_climate(const BatchArgs &a, cudaStream_t s) {
     int grid = (int)((a.n_units + kUnits - 1) / kUnits);
-    if (a.fp32_core) {
-        allow_dynamic_smem(climate_kernel<true>, sizeof(ClimateSmem<true>), g_smem_done32);
-        climate_kernel<true><<<grid, kThreadsA, sizeof(ClimateSmem<true>), s>>>(a);
+    if (a.fp32_core && a.small_coords) {
+        allow_dynamic_smem(climate_kernel<true, true>, sizeof(ClimateSmem<true>), g_smem_done32s);
+        climate_kernel<true, true><<<grid, kThreadsA, sizeof(ClimateSmem<true>), s>>>(a);
+    } else if (a.fp32_core) {
+        allow_dynamic_smem(climate_kernel<true, false>, sizeof(ClimateSmem<true>), g_smem_done32);
+        climate_kernel<true, false><<<grid, kThreadsA, sizeof(ClimateSmem<true>), s>>>(a);
     } else {
-        allow_dynamic_smem(climate_kernel<false>, sizeof(ClimateSmem<false>), g_smem_done64);
-        climate_kernel<false><<<grid, kThreadsA, sizeof(ClimateSmem<false>), s>>>(a);
+        allow_dynamic_smem(climate_kernel<false, false>, sizeof(ClimateSmem<false>), g_smem_done64);
+        climate_kernel<false, false><<<grid, kThreadsA, sizeof(ClimateSmem<false>), s>>>(a);
     }
 }
 
@@ -1663,8 +1745,9 @@ void launch_ladder(const BatchArgs &a, int grid, cudaStream_t s) {
 }
 
 void prepare_phase1_launches() {
-    allow_dynamic_smem(climate_kernel<true>, sizeof(ClimateSmem<true>), g_smem_done32);
-    allow_dynamic_smem(climate_kernel<false>, sizeof(ClimateSmem<false>), g_smem_done64);
+    allow_dynamic_smem(climate_kernel<true, true>, sizeof(ClimateSmem<true>), g_smem_done32s);
+    allow_dynamic_smem(climate_kernel<true, false>, sizeof(ClimateSmem<true>), g_smem_done32);
+    allow_dynamic_smem(climate_kernel<false, false>, sizeof(ClimateSmem<false>), g_smem_done64);
     allow_dynamic_smem(entrance_kernel, sizeof(EntranceSmem), g_smem_done_ent);
     ladder_geometry();
 }

@@ -107,6 +107,8 @@ struct BatchArgs {
     int mc_1_18_2, pre_26_2, single_biome, large_biomes;
     int fp32_core;                // 1: climate samples in FP32, FP64 recheck inside the error band;
                                   // 2: the same, every gate re-taken in FP64; 0: FP64
+    int small_coords;             // every climate coordinate of the batch lies inside
+                                  // maintainPrecision's identity range (coords_small)
 
     uint32_t *rec_unit;           // [cap_rec] batch-local unit of each record
     uint32_t *rec_off;            // [cap_rec] first entry in surv_region
@@ -178,6 +180,10 @@ F32Bands build_f32_bands(const ClimateStep *steps);
 // Host: builds the noise parameters, climate steps and FP32 bands of both presets and uploads
 // them to the current device's constant memory (upload_tables).
 void upload_phase1_tables();
+// Host: whether every climate sampling coordinate of regions with rx, rz in [lo, hi] (inclusive)
+// stays inside maintainPrecision's identity range (|v| < 1e7): a climate point is 4 * chunk + 2 with
+// |chunk| <= 32 |r| + 23, scaled by at most 1.0181268882175227 and the largest climate lacunarity.
+bool coords_small(int64_t lo, int64_t hi);
 
 // An item of the breadth-first climate stage for one-region units: the unit, its partial sums.
 struct SpotItem {
