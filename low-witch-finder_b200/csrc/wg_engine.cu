@@ -155,7 +155,7 @@ int run_batch(wg_engine *eng, const BatchArgs &proto, uint64_t unit0, uint32_t n
         launch_climate(a, eng->stream);
     }
     WG_CUDA(cudaEventRecord(eng->kev[1], eng->stream), "event");
-    launch_entrance(a, eng->sm_count * 2, eng->stream);
+    launch_entrance(a, 0, eng->stream);
     WG_CUDA(cudaEventRecord(eng->kev[2], eng->stream), "event");
     launch_ladder(a, 0, eng->stream);
     WG_CUDA(cudaEventRecord(eng->kev[3], eng->stream), "event");

@@ -273,7 +273,7 @@ struct ClimateSmem {
     uint32_t rwu[kUnits];                      // rect width of the unit's job
     unsigned int hist[P1_KINDS + kTiers];
     uint32_t grad[kGradWords];
-    float4 gt4[16];                            // FP32 core: gradient vector per hash
+    GradF gf;                                  // FP32 core: the gradient vectors as floats
     ClimateSteps steps;
 };
 
@@ -352,7 +352,7 @@ __device__ __forceinline__ float climate_sample_f32(const ClimateSmem<true> &S, 
     const int slot = st.slot[k];
     const int o = slot * kUnits + iu;
     const double sc = st.sc[k], lac = st.lac[k];
-    ColTableF<kUnits> T{S.perm + slot * kPitch + iu, S.gt4};
+    ColTableF<kUnits> T{S.perm + slot * kPitch + iu, &S.gf};
     const double x = (xc * sc) * lac, z = (zc * sc) * lac;
     return perlin_y0_f32(T, S.ox[o], S.oz[o], S.jy[o], S.ty.hyf[o], S.ty.fyf[o], SMALL ? x : keep_precision(x),
                          SMALL ? z : keep_precision(z));
@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
     const bool all_rechecks = F32 && a.fp32_core == 2;   // every FP32 gate re-taken in FP64 (a check mode)
     if (tid < P1_KINDS + kTiers) S.hist[tid] = 0;
     fill_grad_table(S.grad, tid);
-    if (F32) fill_grad_table_f32(S.gt4, tid);
+    if (F32) fill_grad_table_f32(&S.gf, tid);
     if (tid < kClimateSteps) {
         const ClimateStep &c = c_steps[large][tid];
         S.steps.sc[tid] = c.sc;
@@ -609,52 +609,24 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                     if (j < S.end[iu]) keep_survivor(S, a, iu, j);
                 }
             } else if constexpr (F32) {
-                // two regions per loop trip: their four samples are independent chains of dependent
-                // table loads, computed before any decision so that they overlap
-#pragma unroll 1
-                for (int q0 = tid; q0 < nq; q0 += 2 * kThreadsA) {
-                    int iu[2];
-                    uint32_t jl[2];
-                    bool ok[2];
-                    double xc[2], zc[2];
-                    float v0[2], v1[2];
-#pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        const int q = q0 + h * kThreadsA;
-                        ok[h] = q < nq;
-                        const int qq = ok[h] ? q : 0;
-                        iu[h] = qq % kUnits;
-                        jl[h] = (uint32_t)(qq / kUnits);
-                        ok[h] = ok[h] && c0 + jl[h] < S.end[iu[h]];
-                        climate_point(S, iu[h], jl[h], xc[h], zc[h]);
-                        if (!ok[h]) xc[h] = zc[h] = 2.0;   // a harmless point for an unused lane
+                for (int q = tid; q < nq; q += kThreadsA) {
+                    const int iu = q % kUnits;
+                    const uint32_t jl = (uint32_t)(q / kUnits);
+                    if (c0 + jl >= S.end[iu]) continue;
+                    double xc, zc;
+                    climate_point(S, iu, jl, xc, zc);
+                    float sum = __fmul_rn(st.cf[0], climate_sample_f32<SMALL>(S, iu, 0, xc, zc));
+                    sum = __fmaf_rn(st.cf[1], climate_sample_f32<SMALL>(S, iu, 1, xc, zc), sum);
+                    bool pass;
+                    if (!all_rechecks && sum < st.lo[1]) {
+                        pass = false;
+                    } else if (!all_rechecks && sum >= st.hi[1]) {
+                        pass = true;
+                    } else {   // inside the error band: decide in FP64
+                        rechecks++;
+                        pass = !(climate_sum64(S, iu, 0, 1, xc, zc) * st.amp[1] < st.thr[1]);
                     }
-                    if (__any_sync(0xFFFFFFFFu, ok[1])) {
-#pragma unroll
-                        for (int h = 0; h < 2; h++) {
-                            v0[h] = climate_sample_f32<SMALL>(S, iu[h], 0, xc[h], zc[h]);
-                            v1[h] = climate_sample_f32<SMALL>(S, iu[h], 1, xc[h], zc[h]);
-                        }
-                    } else {   // no lane of the warp has a second region
-                        v0[0] = climate_sample_f32<SMALL>(S, iu[0], 0, xc[0], zc[0]);
-                        v1[0] = climate_sample_f32<SMALL>(S, iu[0], 1, xc[0], zc[0]);
-                        v0[1] = v1[1] = 0.0f;
-                    }
-#pragma unroll
-                    for (int h = 0; h < 2; h++) {
-                        if (!ok[h]) continue;
-                        const float sum = __fmaf_rn(st.cf[1], v1[h], __fmul_rn(st.cf[0], v0[h]));
-                        bool pass;
-                        if (!all_rechecks && sum < st.lo[1]) {
-                            pass = false;
-                        } else if (!all_rechecks && sum >= st.hi[1]) {
-                            pass = true;
-                        } else {   // inside the error band: decide in FP64
-                            rechecks++;
-                            pass = !(climate_sum64(S, iu[h], 0, 1, xc[h], zc[h]) * st.amp[1] < st.thr[1]);
-                        }
-                        tier0_decide(iu[h], jl[h], sum, pass, xc[h], zc[h]);
-                    }
+                    tier0_decide(iu, jl, sum, pass, xc, zc);
                 }
             } else {
                 for (int q = tid; q < nq; q += kThreadsA) {
@@ -692,36 +664,17 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                 uint32_t ke[kPer];
                 Real ks[kPer];
                 if constexpr (F32) {
-                    // every item's sample first (independent chains of table loads), then the checks
-                    uint32_t e[kPer];
-                    double xc[kPer], zc[kPer];
-                    float v[kPer];
-#pragma unroll
-                    for (int r = 0; r < kPer; r++) {
-                        const uint32_t q = (uint32_t)tid + (uint32_t)(r * kThreadsA);
-                        e[r] = q < n_t ? S.tlist[q] : 0u;
-                        climate_point(S, (int)(e[r] >> 16), e[r] & 0xFFFFu, xc[r], zc[r]);
-                        if (q >= n_t) xc[r] = zc[r] = 2.0;   // a harmless point for an unused slot
-                    }
-                    // two chains at a time: three would not fit the registers
-                    if (__any_sync(0xFFFFFFFFu, (uint32_t)tid + kThreadsA < n_t)) {
-                        v[0] = climate_sample_f32<SMALL>(S, (int)(e[0] >> 16), k, xc[0], zc[0]);
-                        v[1] = climate_sample_f32<SMALL>(S, (int)(e[1] >> 16), k, xc[1], zc[1]);
-                    } else {   // no lane of the warp has a second item
-                        v[0] = climate_sample_f32<SMALL>(S, (int)(e[0] >> 16), k, xc[0], zc[0]);
-                        v[1] = 0.0f;
-                    }
-                    static_assert(kPer == 3, "the sample calls below assume three items per thread");
-                    if ((uint32_t)tid + 2u * kThreadsA < n_t) v[2] = climate_sample_f32<SMALL>(S, (int)(e[2] >> 16), k, xc[2], zc[2]);
-                    else v[2] = 0.0f;
 #pragma unroll
                     for (int r = 0; r < kPer; r++) {
                         const uint32_t q = (uint32_t)tid + (uint32_t)(r * kThreadsA);
                         ke[r] = 0xFFFFFFFFu;
                         ks[r] = 0;
                         if (q >= n_t) continue;
-                        const int iu = (int)(e[r] >> 16);
-                        const float sum = __fmaf_rn(cf, v[r], S.tsum[q]);
+                        const uint32_t e = S.tlist[q];
+                        const int iu = (int)(e >> 16);
+                        double xc, zc;
+                        climate_point(S, iu, e & 0xFFFFu, xc, zc);
+                        const float sum = __fmaf_rn(cf, climate_sample_f32<SMALL>(S, iu, k, xc, zc), S.tsum[q]);
                         bool reject;
                         if (!all_rechecks && sum < lo) {
                             reject = true;
@@ -729,12 +682,12 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                             reject = false;
                         } else {   // inside the error band: the exact partial sum of steps 0..k
                             rechecks++;
-                            reject = climate_sum64(S, iu, 0, k, xc[r], zc[r]) * amp < thr;
+                            reject = climate_sum64(S, iu, 0, k, xc, zc) * amp < thr;
                         }
                         if (reject) {
-                            erosion_reject(S, a, tc, iu, c0 + (e[r] & 0xFFFFu), tier);
+                            erosion_reject(S, a, tc, iu, c0 + (e & 0xFFFFu), tier);
                         } else {
-                            ke[r] = e[r];
+                            ke[r] = e;
                             ks[r] = sum;
                         }
                     }
@@ -969,13 +922,13 @@ __global__ void __launch_bounds__(kProbeThreads) noise_probe_kernel(const int64_
     __shared__ float hyf[2 * kMaxOct], fyf[2 * kMaxOct];
     __shared__ int jy[2 * kMaxOct];
     __shared__ uint32_t grad[kGradWords];
-    __shared__ float4 gt4[16];
+    __shared__ GradF gf;
     const int t = threadIdx.x;
     const NoiseSpec &ns = c_noise[noise];
     const int np = ns.npresent;
     const uint64_t seed = (uint64_t)seeds[blockIdx.x];
     fill_grad_table(grad, t);
-    fill_grad_table_f32(gt4, t);
+    fill_grad_table_f32(&gf, t);
     perm_blocks_init<kProbeStride, 257 * kProbeStride>(perm, 1, t, kProbeThreads);
     __syncthreads();
     if (t < 2 * np) {
@@ -1003,7 +956,7 @@ __global__ void __launch_bounds__(kProbeThreads) noise_probe_kernel(const int64_
             const double sc = q < np ? 1.0 : kDblScale, l = ns.lac[p];
             const double px = keep_precision((x * sc) * l), pz = keep_precision((z * sc) * l);
             const ColTable<kProbeStride> T{perm + q, grad};
-            const ColTableF<kProbeStride> TF{perm + q, gt4};
+            const ColTableF<kProbeStride> TF{perm + q, &gf};
             const double v = perlin_y0(T, ox[q], oz[q], jy[q], hy[q], fy[q], px, pz);
             if (q < np) a += (ns.amp[p] * v) * ns.per[p];
             else b += (ns.amp[p] * v) * ns.per[p];
@@ -1491,7 +1444,17 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
     if (tid < P1_KINDS && S.hist[tid]) atomicAdd(&a.hist[tid], (unsigned long long)S.hist[tid]);
 }
 
+// grid <= 0: one CTA per tile the batch can produce (records <= units, and <= the list's capacity;
+// a CTA past the batch's tiles returns at once).  Separate CTAs start their table builds at
+// different times, so the two on an SM are seldom in the same phase: one's build fills the issue
+// slots the other's latency-bound sampling leaves free, which persistent CTAs started together
+// did not do.  The kernel still loops over tiles with a grid stride, so any grid is correct.
 void launch_entrance(const BatchArgs &a, int grid, cudaStream_t s) {
+    if (grid <= 0) {
+        const uint64_t recs = a.n_units < a.cap_rec ? a.n_units : a.cap_rec;
+        grid = (int)((recs + kUnits - 1) / kUnits);
+        if (grid < 1) grid = 1;
+    }
     allow_dynamic_smem(entrance_kernel, sizeof(EntranceSmem), g_smem_done_ent);
     entrance_kernel<<<grid, kThreadsB, sizeof(EntranceSmem), s>>>(a);
 }

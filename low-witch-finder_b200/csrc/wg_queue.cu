@@ -186,7 +186,7 @@ int run_queue(wg_engine *eng, const BatchArgs &proto, uint64_t total_units, uint
                    "capture");
         queue_plan_kernel<<<1, 32, 0, s>>>(R.q, proto.jobs, a.counters, a.hist);
         launch_climate(a, s);
-        launch_entrance(a, eng->sm_count * 2, s);
+        launch_entrance(a, 0, s);
         launch_ladder(a, 0, s);
         queue_commit_kernel<<<1, 256, 0, s>>>(R.q, a.counters, a.hist, a.out, R.out, R.cap, cond);
         cudaGraph_t captured = nullptr;

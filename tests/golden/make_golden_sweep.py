@@ -18,6 +18,17 @@ origin (from the C restatement oracle/witch_oracle.c, wo_deep_starts) plus three
 The fixture keeps the structure seeds, the catalogue, and the reference's start and match counts
 per structure seed (its terrain survivors too, for the record: its terrain gates are its own staged
 tests, not lysh's phase 1).
+
+Second step, on any machine with g++ (no GPU):
+
+    python tests/golden/make_golden_sweep.py --cpu <reference root>
+
+adds the same per-seed start counts from the reference's room walk header compiled on the CPU
+(sweep_world_counts.cpp), once with plain -O2 and once with -O2 -fwrapv, and the starts whose
+region re-draws nextInt(24) under each build.  The header's re-draw test (room_core.h:94, :100) is
+signed 32-bit arithmetic that overflows exactly when a re-draw is due: the optimised builds drop
+the loop (the -O2 counts equal the GPU engine's), while with defined wrapping the loop runs as
+java.util.Random.nextInt and lysh's lysh_lcg_next_int_bound (rng.c:213-226) do.
 """
 from __future__ import annotations
 
@@ -43,10 +54,49 @@ def forward_s48(index: int) -> int:
     return (index * 0x9E3779B97F4A7D + 0x2545F4914F6CDD) & MASK48
 
 
+def cpu_counts(ref_root: str, s48s: list[int], wrap: bool) -> tuple[list[int], list[tuple[int, ...]]]:
+    """Whole-world start counts of the reference's room walk (sweep_world_counts.cpp compiled against
+    its engine/gpu/room_core.h), with plain -O2 or with -O2 -fwrapv; and the starts whose region
+    re-draws nextInt(24), as (s48, rx, rz, chunk x, chunk z)."""
+    src = os.path.join(os.path.dirname(os.path.abspath(__file__)), "sweep_world_counts.cpp")
+    with tempfile.TemporaryDirectory() as tmp:
+        exe = os.path.join(tmp, "counts")
+        flags = ["-O2", "-fopenmp"] + (["-fwrapv"] if wrap else [])
+        subprocess.run(["g++", *flags, "-I", os.path.join(ref_root, "engine", "gpu"), src, "-o", exe], check=True)
+        r = subprocess.run([exe, *map(str, s48s)], capture_output=True, text=True, check=True, timeout=3600)
+    starts, redraw = [], []
+    for line in r.stdout.splitlines():
+        p = line.split()
+        if p[0] == "seed":
+            starts.append(int(p[3]))
+        elif p[0] == "redraw_start":
+            redraw.append(tuple(int(x) for x in p[1:]))
+    return starts, sorted(redraw)
+
+
+def add_cpu_counts(path: str, ref_root: str) -> None:
+    """Adds the CPU counts of both builds to an existing fixture."""
+    g = dict(np.load(path))
+    s48s = [int(s) for s in g["s48"]]
+    for wrap, tag in ((False, "o2"), (True, "wrapv")):
+        starts, redraw = cpu_counts(ref_root, s48s, wrap)
+        g[f"cpu_starts_{tag}"] = np.array(starts, np.uint64)
+        g[f"redraw_starts_{tag}"] = np.array(redraw, np.int64).reshape(-1, 5)
+        print(f"{tag}: starts {starts}, re-draw starts {redraw}")
+    np.savez(path, **g)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden", "deep_sweep.npz"))
+    ap.add_argument("--cpu", metavar="REF_ROOT",
+                    help="instead of running the reference's GPU engine, add to the fixture at --out the "
+                         "whole-world counts of the reference's room walk built on the CPU with -O2 and with "
+                         "-O2 -fwrapv (REF_ROOT: the reference's root)")
     args = ap.parse_args()
+    if args.cpu:
+        add_cpu_counts(args.out, args.cpu)
+        return
     import bind
     port = bind.Port()
     s48s = [forward_s48(FIRST + i) for i in range(COUNT)]

@@ -42,6 +42,35 @@ def test_spot_fixture_known_answers():
     assert d["start"][-1] == 0 and d["counts"][-1] == 0
 
 
+def test_sweep_fixture_redraw_accounting():
+    """The whole-world sweep fixture: the reference's room walk built on the CPU with -O2 counts
+    what its GPU engine counted; built with -fwrapv (nextInt(24) re-draws as java.util.Random does)
+    the counts differ only by the starts of regions that re-draw, which the fixture lists per build."""
+    g = np.load(os.path.join(GOLDEN, "deep_sweep.npz"))
+    assert g["cpu_starts_o2"].tolist() == g["ref_starts"].tolist()
+    for i, s in enumerate(g["s48"]):
+        n_o2 = int((g["redraw_starts_o2"][:, 0] == s).sum())
+        n_java = int((g["redraw_starts_wrapv"][:, 0] == s).sum())
+        assert int(g["cpu_starts_wrapv"][i]) - int(g["cpu_starts_o2"][i]) == n_java - n_o2
+    assert len(g["redraw_starts_o2"]) + len(g["redraw_starts_wrapv"]) > 0
+
+
+def test_oracle_redraw_regions_follow_java(port):
+    """At each region of the sweep fixture whose hut re-draws, the oracle (whose nextInt re-draws
+    like java.util.Random and lysh's rng.c:213-226) has a start exactly where the -fwrapv build has
+    one; the chunks the -O2 build reports there are starts of the carver test but not the hut's."""
+    g = np.load(os.path.join(GOLDEN, "deep_sweep.npz"))
+    java = {(int(r[0]), int(r[1]), int(r[2])): [int(v) for v in r] for r in g["redraw_starts_wrapv"]}
+    for key, row in java.items():
+        got = port.deep_starts([key[0]], (key[1], key[1] + 1, key[2], key[2] + 1))
+        assert got[:, :5].tolist() == [row]
+    for s48, rx, rz, cx, cz in (tuple(int(v) for v in r) for r in g["redraw_starts_o2"]):
+        assert port.mineshaft_start(s48, cx, cz)[0]
+        got = port.deep_starts([s48], (rx, rx + 1, rz, rz + 1))
+        assert (cx, cz) not in [(int(r[3]), int(r[4])) for r in got]
+        assert len(got) == (1 if (s48, rx, rz) in java else 0)
+
+
 def test_room_reference_pinned(bind_mod):
     if not os.path.exists(bind_mod.ROOM_LIB):
         pytest.skip("oracle/_ref not built (needs the reference sources)")

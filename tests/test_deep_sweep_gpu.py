@@ -64,9 +64,20 @@ def test_sweep_against_the_oracle(engine, port):
 
 def test_sweep_whole_world_counts_equal_reference(engine, wg):
     """Every region of the +-30M world for three structure seeds of the reference's forward
-    enumeration: starts and catalogue matches per seed equal the reference engine's."""
+    enumeration: starts per seed equal the reference's room walk with nextInt(24) re-drawing as
+    java.util.Random does (its header built with -fwrapv); catalogue matches equal its GPU engine's.
+    The reference's optimised builds drop the re-draw (a signed-overflow test), which moves one
+    start of seed 1001 and two of seed 1002: the fixture lists them, and each listed region is
+    checked alone."""
     g = np.load(os.path.join(GOLDEN, "deep_sweep.npz"))
     matches, starts = engine.deep_sweep([int(x) for x in g["layouts"]], g["values"], s48=[int(s) for s in g["s48"]],
                                         rect=wg.WORLD_REGIONS)
-    assert starts.tolist() == g["ref_starts"].tolist()
+    assert starts.tolist() == g["cpu_starts_wrapv"].tolist()
     assert np.bincount(matches["seed_index"], minlength=len(g["s48"])).tolist() == g["ref_matches"].tolist()
+    java = {(int(r[0]), int(r[1]), int(r[2])): (int(r[3]), int(r[4])) for r in g["redraw_starts_wrapv"]}
+    for s48, rx, rz, cx, cz in g["redraw_starts_o2"]:
+        _, n = engine.deep_sweep([5], s48=[int(s48)], rect=(int(rx), int(rx) + 1, int(rz), int(rz) + 1))
+        assert n.tolist() == [1 if (int(s48), int(rx), int(rz)) in java else 0]
+    for (s48, rx, rz), (cx, cz) in java.items():
+        walk = engine.deep_starts(s48=[s48], rect=(rx, rx + 1, rz, rz + 1))
+        assert [(int(w["chunk_x"]), int(w["chunk_z"])) for w in walk] == [(cx, cz)]

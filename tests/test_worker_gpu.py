@@ -98,19 +98,21 @@ def test_single_shot_cli(wg, engine, tmp_path):
     assert read_csv(tmp_path / "h.csv", floor=True) == exact_rows(engine, g, -50)
 
 
-def test_exact_hits_at_a_relaxed_ceiling(wg, engine, tmp_path):
-    """Phase 1 at max_height 100 with --phase2-max-y 100 on hunt.py's SCAN_REFERENCE seed over its
-    40,000-block rect: many phase-1 survivors, of which phase 2 keeps the biome-ok, dry huts with
-    floor <= 100 (the reference hut among them); the rows and floors equal wg_eval_huts'."""
+def test_exact_hits_follow_the_phase2_ceiling(wg, engine, tmp_path):
+    """--phase2-max-y sets phase 2's ceiling apart from phase 1's (-50 here): on hunt.py's
+    SCAN_REFERENCE seed over its 40,000-block rect the reference hut (floor -54) is kept at a
+    ceiling of -54 or 100 and dropped at -55; at each ceiling the rows and floors equal
+    wg_eval_huts' over the phase-1 survivors."""
     seed = 1473884015873122059
+    ref = (seed, -987, -1073, -15792, -17168, -54)
     rect = ["--min-region-x", "-79", "--max-region-x", "79", "--min-region-z", "-79", "--max-region-z", "79"]
-    rows = _scan(wg, tmp_path, "--seed", str(seed), *rect, "--max-height", "100", "--phase2-max-y", "100",
-                 phase1=False)
-    cands = engine.seed_check(seeds=[seed], rect=(-79, 79, -79, 79), max_height=100).candidates
-    want = exact_rows(engine, cands, 100)
-    assert rows == want
-    assert 0 < len(want) < len(cands)
-    assert (seed, -987, -1073, -15792, -17168, -54) in want
+    cands = engine.seed_check(seeds=[seed], rect=(-79, 79, -79, 79), max_height=-50).candidates
+    for ceiling, kept in ((-54, True), (-55, False), (100, True)):
+        rows = _scan(wg, tmp_path, "--seed", str(seed), *rect, "--max-height", "-50", "--phase2-max-y",
+                     str(ceiling), phase1=False)
+        want = exact_rows(engine, cands, ceiling)
+        assert rows == want
+        assert (ref in want) == kept
 
 
 def test_self_test_passes(wg, tmp_path):
