@@ -69,7 +69,10 @@ OPS_REGION = 40              # java.util.Random placement (2 x nextInt(24)) + co
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, from ncu on `bench.py --profile 1048576`
 # (one launch of each kernel on 2^20 seeds read from a list in HBM; a 2^24-seed step runs 16 such
 # launches, each over its own 2^20 seeds, so the per-launch figure is the full step's per launch)
-TRAFFIC = {"climate_kernel": None, "entrance_kernel": None, "source": "not yet captured"}
+TRAFFIC = {"climate_kernel": 8557312 + 0, "entrance_kernel": 20939520 + 0,
+           "source": "ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none "
+                     "-k regex:'climate_kernel|entrance_kernel|ladder_kernel' -s 3 -c 3 python bench.py --profile "
+                     "1048576 --warmup 1 --steps 1 (the timed step's launches; read + write bytes)"}
 BYTES_PER_SEED_IN = 8        # the int64 seed read from HBM
 BYTES_PER_RECORD = 12        # (unit, offset, count) per seed with climate survivors
 BYTES_PER_SURVIVOR = 4       # region offset per climate survivor
