@@ -33,12 +33,23 @@ def test_oracle_walk_matches_reference_fixture(port):
 
 
 def test_spot_fixture_known_answers():
+    """The terrain-stage fixture: hunt.py's four TERRAIN_REFERENCE spots pass exactly their known
+    seed's variant; every data/finds.tsv hut with coordinates (50, depths -55 to -59) is a start
+    chunk whose known world seed is among lysh's phase-1 survivors at -54; the extra chunk is no
+    start."""
     d = np.load(os.path.join(GOLDEN, "deep_spots.npz"))
     seeds = [s for s, _, _ in KNOWN[1:]]
     passed = d["passed"]
     off = np.concatenate([[0], np.cumsum(d["counts"])])
     for i, seed in enumerate(seeds):
         assert passed[off[i]:off[i + 1]].tolist() == [(seed & ((1 << 64) - 1)) >> 48]
+        assert int(d["seed"][i]) == seed
+    finds = [i for i in range(len(d["s48"])) if int(d["depth"][i]) != 0]
+    assert len(finds) == 50 and set(int(d["depth"][i]) for i in finds) == {-55, -57, -58, -59}
+    for i in finds:
+        seed = int(d["seed"][i]) & ((1 << 64) - 1)
+        assert d["start"][i] == 1 and int(d["s48"][i]) == seed & M48
+        assert (seed >> 48) in passed[off[i]:off[i + 1]].tolist(), i
     assert d["start"][-1] == 0 and d["counts"][-1] == 0
 
 

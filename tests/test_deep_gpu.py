@@ -73,3 +73,8 @@ def test_deep_spots_match_reference(engine):
         i, u = int(row["seed_index"]) >> 16, int(row["seed_index"]) & 0xFFFF
         assert (int(row["seed"]) & ((1 << 64) - 1)) == (u << 48) | int(d["s48"][i])
         assert (row["chunk_x"], row["chunk_z"]) == (d["chunk_x"][i], d["chunk_z"][i])
+    # every known find (hunt.py's TERRAIN_REFERENCE and the 50 located data/finds.tsv huts) survives
+    got = set(int(s) for s in surv["seed"])
+    for i, seed in enumerate(d["seed"]):
+        if int(seed):
+            assert int(seed) in got, (i, int(seed))
