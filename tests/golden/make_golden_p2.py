@@ -12,8 +12,9 @@ lysh_grade_scan and the phase-2 probes), i.e. from the reference implementation:
                  value there (blended noise, raw and interpolated density, column tops, terrain
                  info, computeFluid, block states, surface heights before / after carvers)
   p2_huts.npz    lysh_eval_hut on forced hut positions: the 81 region huts of the first config-1
-                 seeds (hunt.py's version), a few seeds under other versions / presets, and the
-                 185 phase-1 survivors of config 2
+                 seeds (hunt.py's version), a few seeds under other versions / presets, the
+                 185 phase-1 survivors of config 2, the SCAN_REFERENCE hut and the 50 located
+                 data/finds.tsv huts (the reference's data file, read at generation time)
   p2_grade.json  lysh_grade_scan of the SCAN_REFERENCE seed over its 40,000-block rect
 """
 from __future__ import annotations
@@ -117,6 +118,11 @@ def huts(ref: bind.Ref) -> None:
         add(2, s, o, hxz)
     # set 3: the SCAN_REFERENCE hut
     add(3, SCAN_REFERENCE, o, [(-987 * 16, -1073 * 16)])
+    # set 4: every located data/finds.tsv hut (real deep huts: biome-OK and dry; their plain-terrain
+    # floor, before the mineshaft room the finisher adds, decides the verdict at the ceiling)
+    from make_golden_deep import read_finds
+    for _depth, seed, x, z in read_finds():
+        add(4, seed & 0xFFFFFFFFFFFFFFFF, o, [((x // 16) * 16, (z // 16) * 16)])
     cols = ["set", "seed", "hut_x", "hut_z", "mc_1_18_2", "single_biome", "pre_26_2", "large_biomes",
             "biome_tree"] + list(bind.EVAL_FIELDS)
     out = {c: np.array([int(r[i]) for r in rows], dtype=np.int64) for i, c in enumerate(cols)}

@@ -41,6 +41,17 @@ def test_hut_fixtures_pinned(ref, bind_mod):
             assert e[f] == int(h[f][i]), (i, f)
 
 
+def test_hut_fixture_accept_side():
+    """The accept path (biome-OK, not flooded, floor under the ceiling) is covered by real finds:
+    the 50 located data/finds.tsv huts (set 4) are all accepted by lysh at -50, 62 forced huts in
+    all are biome-OK and dry."""
+    h = np.load(os.path.join(GOLDEN, "p2_huts.npz"))
+    s4 = h["set"] == 4
+    assert s4.sum() == 50 and (h["ok"][s4] == 1).all() and (h["biome_ok"][s4] == 1).all()
+    assert (h["flooded"][s4] == 0).all() and (h["avg_y"][s4] <= -50).all()
+    assert ((h["biome_ok"] == 1) & (h["flooded"] == 0)).sum() >= 62
+
+
 def test_grade_fixture_pinned(ref):
     g = json.load(open(os.path.join(GOLDEN, "p2_grade.json")))
     hits, st = ref.grade_scan(g["seed"], _rules(g["opts"]), g["max_height"], tuple(g["rect"]), g["max_y"],
