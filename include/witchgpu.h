@@ -291,6 +291,55 @@ int wg_deep_spots(wg_engine *e, const int64_t *s48, const int32_t *chunk_x, cons
                   const wg_opts *opts, int max_height, wg_candidate *out, uint64_t cap, uint64_t *n_out,
                   uint64_t *not_start);
 
+/* ---------------- the mineshaft finisher (hunt.py finish_row) ---------------- */
+
+/* One piece of a mineshaft tree, as `mstree` prints it (engine/tools/mstree/mstree.cpp:17-33):
+ * kind 'R' room, 'C' corridor, 'X' / 'Y' one- / two-storey crossing, 'S' stairs; the inclusive
+ * block box; facing 0 N, 1 S, 2 W, 3 E (-1 for the room); the parent's index (-1 for the room);
+ * rails on a corridor. */
+typedef struct {
+    int32_t kind, x0, y0, z0, x1, y1, z1, facing, parent, rails;
+} wg_ms_piece;
+
+/* The mineshaft tree of world seed ws at chunk (chunk_x, chunk_z) (mstree <ws> <cx> <cz>): the
+ * start test, MineShaftPieces generation and the move below sea level.  Writes up to cap pieces
+ * (at most 512 exist), *n_out = their number, *room_floor = the room's floor y.  Returns
+ * WG_ERR_ARG when the chunk is not a mineshaft start (mstree's exit 3), WG_ERR_CAPACITY when the
+ * tree exceeds the generator's 512 pieces, 16 open pieces or byte-range boxes (the reference
+ * reports those trees as failed too). */
+int wg_mineshaft_tree(wg_engine *e, int64_t ws, int32_t chunk_x, int32_t chunk_z, wg_ms_piece *out, uint32_t cap,
+                      uint32_t *n_out, int32_t *room_floor);
+
+/* The finisher's measurements of one Deep Dive survivor (world seed, hut chunk): everything
+ * hunt.py's finish_row (hunt.py:277-333) reads from lysh hut, mstree, biome_at, msroom and
+ * skyscan.  Heights and floors are block y; the footprint is the 7 x 9 blocks at the chunk origin
+ * (finish_row runs msroom with MC_SHAPE=79 and skyscan with 7 x 9). */
+typedef struct {
+    int32_t hut_x, hut_z;          /* 16 * chunk */
+    int32_t verdict_ok;            /* lysh hut --max-y 100 --phase2-max-y 100: ACCEPT */
+    int32_t avg_y;                 /* its floor */
+    int32_t tree_status;           /* 0 tree built, 1 not a mineshaft start, 2 tree too large */
+    int32_t pieces, room_floor;    /* mstree: pieces, the room's floor (its first line's y) */
+    int32_t biome[2];              /* biome_at --ms --y room_floor: 1.21.5 tree, 26.2 tree (BIOME_26) */
+    int32_t nat;                   /* msroom EXACT: the footprint floor without the mineshaft */
+    int32_t top[2], refused[2];    /* msroom EXACT: top0 / top1 floors and refused pieces */
+    int32_t no_guard[2];           /* msroom EXACT: ng0 / ng1 floors (liquid guard off) */
+    int64_t sum_nat, sum_top[2], sum_no_guard[2];   /* the footprint height sums behind them */
+    /* skyscan --list over the footprint: height sum (mean = sum / 63), min, max, columns at or
+     * below -54, lava and solid blocks from y -59 up to each surface, the corner heights, columns
+     * above -53 */
+    int64_t scan_sum;
+    int32_t scan_min, scan_max, le54, lava, solid, nw, ne, sw, se, above53;
+} wg_finish_row;
+
+/* The finisher over n survivors (ws[i], chunk_x[i], chunk_z[i]) on the GPU: lysh's hut verdict,
+ * the mineshaft tree, the deep-dark biomes at the room floor, the carved floors and the footprint
+ * scan, written to out[i].  Rows whose chunk is no start or whose tree failed carry tree_status
+ * and no floors.  hunt.py turns a row into its result line only when verdict_ok, tree_status 0,
+ * not both biomes deep dark (183) and top[1] <= its min_r. */
+int wg_finish_rows(wg_engine *e, const int64_t *ws, const int32_t *chunk_x, const int32_t *chunk_z, uint64_t n,
+                   wg_finish_row *out);
+
 /* ---------------- biome map ---------------- */
 
 /* biome_map's raster (engine/tools/mineshaft/biome_map.c): w x h bytes (z outer, x inner; w, h

@@ -75,7 +75,7 @@ EXPORTS = ("wg_engine_open", "wg_engine_close", "wg_engine_error", "wg_engine_se
            "wg_eval_huts", "wg_grade_scan", "wg_p2_probe", "wg_deep_starts", "wg_deep_sweep", "wg_deep_spots",
            "wg_biome_map", "wg_biome_chunks", "wg_deep_solve", "wg_deep_solve_tasks", "wg_seed_check_jobs", "wg_engine_set_job_queue", "wg_engine_tune", "wg_engine_set_tuning",
            "wg_server_open", "wg_server_open_config", "wg_server_submit", "wg_server_poll", "wg_server_take",
-           "wg_server_stats", "wg_server_close")
+           "wg_server_stats", "wg_server_close", "wg_mineshaft_tree", "wg_finish_rows")
 
 # wg_deep_start: a swamp hut whose chunk is a mineshaft start chunk.
 DEEP_START_DTYPE = np.dtype([("seed_index", "<u8"), ("s48", "<i8"), ("rx", "<i4"), ("rz", "<i4"), ("chunk_x", "<i4"), ("chunk_z", "<i4"),
@@ -85,6 +85,25 @@ DEEP_START_DTYPE = np.dtype([("seed_index", "<u8"), ("s48", "<i8"), ("rx", "<i4"
 SWEEP_MATCH_DTYPE = np.dtype([("seed_index", "<u8"), ("s48", "<i8"), ("rx", "<i4"), ("rz", "<i4"),
                               ("chunk_x", "<i4"), ("chunk_z", "<i4"), ("carver", "<i8"), ("value", "<u4"),
                               ("pad", "<u4")])
+def _signed64(v: int) -> int:
+    """A 64-bit seed given signed or unsigned, as the signed value the C ABI takes."""
+    v = int(v) & 0xFFFFFFFFFFFFFFFF
+    return v - (1 << 64) if v >= 1 << 63 else v
+
+
+# wg_ms_piece: one piece of a mineshaft tree as mstree prints it (kind is the letter's code).
+MS_PIECE_DTYPE = np.dtype([("kind", "<i4"), ("x0", "<i4"), ("y0", "<i4"), ("z0", "<i4"), ("x1", "<i4"), ("y1", "<i4"),
+                           ("z1", "<i4"), ("facing", "<i4"), ("parent", "<i4"), ("rails", "<i4")])
+# wg_finish_row: the mineshaft finisher's measurements of one Deep Dive survivor.
+FINISH_DTYPE = np.dtype([("hut_x", "<i4"), ("hut_z", "<i4"), ("verdict_ok", "<i4"), ("avg_y", "<i4"),
+                         ("tree_status", "<i4"), ("pieces", "<i4"), ("room_floor", "<i4"), ("biome", "<i4", (2,)),
+                         ("nat", "<i4"), ("top", "<i4", (2,)), ("refused", "<i4", (2,)), ("no_guard", "<i4", (2,)),
+                         ("sum_nat", "<i8"), ("sum_top", "<i8", (2,)), ("sum_no_guard", "<i8", (2,)),
+                         ("scan_sum", "<i8"), ("scan_min", "<i4"), ("scan_max", "<i4"), ("le54", "<i4"),
+                         ("lava", "<i4"), ("solid", "<i4"), ("nw", "<i4"), ("ne", "<i4"), ("sw", "<i4"), ("se", "<i4"),
+                         ("above53", "<i4")])
+DEEP_DARK = 183
+
 # the +-30M world's hut regions, [rx0, rx1) x [rz0, rz1) (the reference's forward sweep: radius 58,593)
 WORLD_REGIONS = (-58593, 58594, -58593, 58594)
 
@@ -204,6 +223,8 @@ def library() -> C.CDLL:
     lib.wg_deep_spots.argtypes = [vp, vp, vp, vp, u64, C.POINTER(Opts), i32, vp, u64, C.POINTER(u64),
                                   C.POINTER(u64)]
     lib.wg_biome_map.argtypes = [vp, i64, C.POINTER(Opts), i64, i64, i32, i32, i32, i32, i32, vp]
+    lib.wg_mineshaft_tree.argtypes = [vp, i64, i32, i32, vp, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(i32)]
+    lib.wg_finish_rows.argtypes = [vp, vp, vp, vp, u64, vp]
     lib.wg_biome_chunks.argtypes = [vp, i64, C.POINTER(Opts), vp, vp, u64, vp]
     lib.wg_deep_solve.argtypes = [vp, C.POINTER(SolveBundle), u64, u64, u64, vp, u64, C.POINTER(u64),
                                   C.POINTER(SolveStats)]
@@ -439,6 +460,29 @@ class Engine:
             if found.value <= cap:
                 return out[:found.value].copy(), starts
             cap = int(found.value)
+
+    def mineshaft_tree(self, ws: int, chunk_x: int, chunk_z: int) -> tuple[np.ndarray, int]:
+        """wg_mineshaft_tree: (pieces MS_PIECE_DTYPE in mstree's order, the room's floor y)."""
+        out = np.zeros(512, MS_PIECE_DTYPE)
+        n, floor = C.c_uint32(), C.c_int()
+        rc = library().wg_mineshaft_tree(self._h, _signed64(ws), chunk_x, chunk_z, out.ctypes.data, len(out),
+                                         C.byref(n), C.byref(floor))
+        if rc != WG_OK:
+            raise self._err(rc, "wg_mineshaft_tree")
+        return out[:n.value].copy(), int(floor.value)
+
+    def finish_rows(self, ws, chunk_x, chunk_z) -> np.ndarray:
+        """wg_finish_rows: FINISH_DTYPE per survivor (world seed, hut chunk)."""
+        s = np.ascontiguousarray(np.asarray([_signed64(v) for v in ws], dtype=np.int64))
+        cx = np.ascontiguousarray(chunk_x, dtype=np.int32)
+        cz = np.ascontiguousarray(chunk_z, dtype=np.int32)
+        if not (len(s) == len(cx) == len(cz)):
+            raise ValueError("ws, chunk_x, chunk_z differ in length")
+        out = np.zeros(len(s), FINISH_DTYPE)
+        rc = library().wg_finish_rows(self._h, s.ctypes.data, cx.ctypes.data, cz.ctypes.data, len(s), out.ctypes.data)
+        if rc != WG_OK:
+            raise self._err(rc, "wg_finish_rows")
+        return out
 
     def biome_map(self, seed: int, x0: int, z0: int, w: int, h: int, step: int = 16, ss: int = 1,
                   version: str = "26.3", y: int = 63) -> np.ndarray:

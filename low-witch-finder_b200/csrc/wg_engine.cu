@@ -409,6 +409,7 @@ void wg_engine_close(wg_engine *eng) {
     solve_release(eng);
     walk_release(eng);
     queue_release(eng);
+    finish_release(eng);
     cudaFreeHost(eng->h_counters);
     cudaFreeHost(eng->h_hist);
     if (eng->ev0) cudaEventDestroy(eng->ev0);

@@ -60,6 +60,8 @@ struct wg_engine {
     struct WalkState *walk = nullptr;
     // device work queue of batched jobs (wg_queue.cu): its state and output buffer
     wg::QueueRes *queue = nullptr;
+    // mineshaft finisher (wg_finish.cu): its grow-only buffers
+    struct FinishState *finish = nullptr;
 
     int p2_world_cap = 0, p2_job_cap = 0, p2_hut_cap = 0, p2_result_cap = 0, p2_pt_cap = 0, p2_val_cap = 0;
 
@@ -78,8 +80,17 @@ void p2_release(wg_engine *eng);
 void solve_release(wg_engine *eng);
 // Frees the region walk's buffers of an engine (called by wg_engine_close).
 void walk_release(wg_engine *eng);
+// Frees the finisher's buffers of an engine (called by wg_engine_close).
+void finish_release(wg_engine *eng);
 
 namespace wg {
+
+// Phase-2 state of up to 512 chunks (wg_p2engine.cu): the seed-independent tables, the worlds of
+// `seeds` (large biomes or not) and, per chunk i (world index world[i], chunk cx[i], cz[i]), its
+// grid, aquifer, block states and carver result in eng->p2_worlds / eng->p2_jobs, chunk i at
+// index i.  Asynchronous on eng->stream.
+int p2_prepare_chunks(wg_engine *eng, const std::vector<uint64_t> &seeds, int large, const std::vector<int> &world,
+                      const std::vector<int> &cx, const std::vector<int> &cz);
 
 // Per-batch work budget: (seed, region) checks per batch and units per batch, and the sizes of
 // the engine's phase-1 work lists.

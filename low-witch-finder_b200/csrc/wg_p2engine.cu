@@ -386,6 +386,17 @@ int eval_huts(wg_engine *eng, const int64_t *seeds, const int32_t *hx, const int
 
 }  // namespace
 
+int wg::p2_prepare_chunks(wg_engine *eng, const std::vector<uint64_t> &seeds, int large, const std::vector<int> &world,
+                          const std::vector<int> &cx, const std::vector<int> &cz) {
+    if (world.size() > (size_t)kJobsPerBatch || cx.size() != world.size() || cz.size() != world.size())
+        return eng->fail(WG_ERR_ARG, "phase-2 chunks: more than 512 chunks per call");
+    int rc = ensure_tables(eng);
+    if (rc) return rc;
+    std::vector<JobKey> jobs(world.size());
+    for (size_t i = 0; i < world.size(); i++) jobs[i] = JobKey{world[i], cx[i], cz[i]};
+    return prepare(eng, seeds, large, jobs, true);
+}
+
 void p2_release(wg_engine *eng) {
     for (void *p : eng->p2_game) cudaFree(p);
     eng->p2_game.clear();

@@ -1569,6 +1569,19 @@ __global__ void __launch_bounds__(128) p2_biome_chunks_kernel(const P2Tables *__
     need[k] = settled ? 0 : 1;
 }
 
+// The biome winner of the R-tree `tree` at column (x, z) with first occupied height y, in world
+// pts[4k] (biome_at: lysh_swamp_hut_biome_ok with a constant height callback, biome.c:94-156).
+// pts holds (world, x, z, y) per point; x and z are the column's middle blocks.
+__global__ void __launch_bounds__(128) p2_biome_points_kernel(const P2Tables *__restrict__ Tp,
+                                                              const P2World *__restrict__ worlds, int tree,
+                                                              const int32_t *__restrict__ pts, int n,
+                                                              int32_t *__restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    int64_t np[6];
+    out[k] = p2_biome_params(*Tp, worlds[pts[4 * k]], tree, pts[4 * k + 1], pts[4 * k + 2], pts[4 * k + 3], np);
+}
+
 constexpr int kFinishThreads = 96;   // 63 footprint columns, the chunk centre, the centre's climate
 
 __global__ void __launch_bounds__(kFinishThreads) p2_finish_kernel(const P2Tables *__restrict__ Tp,
@@ -1768,6 +1781,11 @@ void p2_launch_biome_map(const P2Tables *T, const P2World *worlds, int tree, int
 void p2_launch_biome_chunks(const P2Tables *T, const P2World *worlds, int tree, const int32_t *cx, const int32_t *cz,
                             int n, uint8_t *out, uint8_t *need, cudaStream_t s) {
     p2_biome_chunks_kernel<<<(n + 127) / 128, 128, 0, s>>>(T, worlds, tree, cx, cz, n, out, need);
+}
+
+void p2_launch_biome_points(const P2Tables *T, const P2World *worlds, int tree, const int32_t *pts, int n,
+                            int32_t *out, cudaStream_t s) {
+    if (n > 0) p2_biome_points_kernel<<<(n + 127) / 128, 128, 0, s>>>(T, worlds, tree, pts, n, out);
 }
 
 void p2_launch_finish(const P2Tables *T, const P2World *worlds, const P2Chunk *jobs, const P2Hut *huts, int n_huts,

@@ -214,5 +214,8 @@ void p2_launch_biome_map(const P2Tables *T, const P2World *worlds, int tree, int
                          int step, int ss, int y, uint8_t *out, cudaStream_t s);
 void p2_launch_biome_chunks(const P2Tables *T, const P2World *worlds, int tree, const int32_t *cx, const int32_t *cz,
                             int n, uint8_t *out, uint8_t *need, cudaStream_t s);
+// Biome winner per point (world, x, z, y) of pts (4 ints per point): the finisher's biome_at.
+void p2_launch_biome_points(const P2Tables *T, const P2World *worlds, int tree, const int32_t *pts, int n,
+                            int32_t *out, cudaStream_t s);
 
 }  // namespace wg

@@ -117,3 +117,19 @@ def test_solver_struct_layouts_match_the_header(wg, tmp_path):
     got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     assert got == [C.sizeof(wg.SolveBundle), wg.SolveBundle.tier.offset, wg.SOLVE_HIT_DTYPE.itemsize,
                    wg.SOLVE_HIT_DTYPE.fields["layout"][1], C.sizeof(wg.SolveStats)]
+
+
+def test_finisher_struct_layouts_match_the_header(wg, tmp_path):
+    fields = ["verdict_ok", "room_floor", "biome", "nat", "top", "refused", "no_guard", "sum_nat", "sum_top",
+              "sum_no_guard", "scan_sum", "scan_min", "above53"]
+    src = tmp_path / "finish_layout.c"
+    src.write_text(
+        '#include <stddef.h>\n#include <stdio.h>\n#include "witchgpu.h"\n'
+        'int main(void) { printf("%zu %zu %zu", sizeof(wg_ms_piece), offsetof(wg_ms_piece, rails), sizeof(wg_finish_row));'
+        + "".join(f' printf(" %zu", offsetof(wg_finish_row, {f}));' for f in fields) + ' return 0; }\n')
+    exe = tmp_path / "finish_layout"
+    subprocess.run(["gcc", "-I", os.path.dirname(wg.HEADER_PATH), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    want = [wg.MS_PIECE_DTYPE.itemsize, wg.MS_PIECE_DTYPE.fields["rails"][1], wg.FINISH_DTYPE.itemsize]
+    want += [wg.FINISH_DTYPE.fields[f][1] for f in fields]
+    assert got == want

@@ -90,3 +90,22 @@ def test_room_reference_pinned(bind_mod):
     got = room.walk(d["s48"][:3], tuple(int(v) for v in d["rects"][0]))
     want = d["rows0"][np.isin(d["rows0"][:, 0], d["s48"][:3])]
     assert np.array_equal(got, want)
+
+
+def test_finisher_fixture_known_answers():
+    """The finisher fixture (the reference's own tools): hunt.py's REFERENCE is accepted with the
+    mineshaft floor at -58, and every located data/finds.tsv hut's listed depth lies between the
+    carved floors msroom gives for the two top-layer cases (top1 <= depth <= top0); for 47 of the
+    50 it is top1, the value hunt.py prints."""
+    fx = np.load(os.path.join(GOLDEN, "finish_rows.npz"))
+    assert (fx["verdict_ok"][0], fx["start"][0], fx["top1"][0]) == (1, 1, -58)
+    d = np.load(os.path.join(GOLDEN, "deep_spots.npz"))
+    finds = {(int(d["seed"][i]), int(d["chunk_x"][i]), int(d["chunk_z"][i])): int(d["depth"][i])
+             for i in range(len(d["s48"])) if int(d["depth"][i]) != 0}
+    seen = {}
+    for i in range(len(fx["ws"])):
+        key = (int(fx["ws"][i]), int(fx["cx"][i]), int(fx["cz"][i]))
+        if key in finds:
+            assert fx["start"][i] == 1 and int(fx["top1"][i]) <= finds[key] <= int(fx["top0"][i]), key
+            seen[key] = int(fx["top1"][i]) == finds[key]
+    assert len(seen) == 50 and sum(seen.values()) == 47
