@@ -19,6 +19,13 @@
 //            match's 65,536 world seeds through the terrain stage as in --spots; the reference's
 //            per-seed line on stderr and its summary line on stdout
 //
+//   finish   --finish ROWS [--min-r R]
+//            the mineshaft finisher over terrain-stage rows "seed,chunkX,chunkZ[,layoutX,airHi,airLo]"
+//            (a header line is skipped): per row what hunt.py's finish_row computes through lysh,
+//            mstree, biome_at, msroom and skyscan (hunt.py:277-333), here one wg_finish_rows call for
+//            all rows; the result line of each accepted row on stdout, in finish_row's format, and a
+//            summary on stderr
+//
 // The tuning flags of the reference (--fused-*, --task-batch, --ero-*, --batch, --u-*) are
 // accepted and change nothing: the solver and the gates here are exact.  The terrain gates are
 // lysh's phase 1 (lysh_phase1_check_ex) at --max-height with the hunt driver's version
@@ -120,8 +127,90 @@ long long terrain_rows(wg_engine *eng, const std::vector<int64_t> &s48, const st
 
 }  // namespace
 
+namespace {
+
+// One terrain-stage row for the finisher.
+struct FinishIn {
+    int64_t ws;
+    int32_t cx, cz;
+    std::string layout, hi, lo;
+};
+
+// --finish: the result line of every accepted row, exactly as finish_row prints it:
+// "%4d  terrain %4s  refused %2s  if-none-refused %4s  NW %4s  max %4s  lava %4s  air %s/%s  biome %s
+//  layout %s  seed %s  /tp %d %d %d" (hunt.py:329-331), where the floor is msroom's top1, "refused"
+// its first (top0) count, "if-none-refused" ng1, NW / max / lava skyscan's, biome the 1.21.5-tree
+// biome at the room floor.  A row is rejected when lysh does not accept the hut at 100, the chunk is
+// no mineshaft start, the room floor is deep dark in both biome sets, or the floor is above min_r.
+int run_finish(wg_engine *eng, const char *path, int min_r) {
+    FILE *f = std::fopen(path, "r");
+    if (!f) {
+        std::fprintf(stderr, "cannot read %s\n", path);
+        return 1;
+    }
+    std::vector<FinishIn> rows;
+    char ln[512];
+    while (std::fgets(ln, sizeof ln, f)) {
+        if (!(ln[0] == '-' || (ln[0] >= '0' && ln[0] <= '9'))) continue;   // header or blank
+        std::vector<std::string> t;
+        std::string cur;
+        for (const char *p = ln; *p && *p != '\n' && *p != '\r'; p++) {
+            if (*p == ',' || *p == ' ' || *p == '\t') {
+                if (!cur.empty()) t.push_back(cur);
+                cur.clear();
+            } else {
+                cur += *p;
+            }
+        }
+        if (!cur.empty()) t.push_back(cur);
+        if (t.size() < 3) continue;
+        FinishIn r;
+        r.ws = std::strtoll(t[0].c_str(), nullptr, 10);
+        r.cx = (int32_t)std::atoi(t[1].c_str());
+        r.cz = (int32_t)std::atoi(t[2].c_str());
+        r.layout = t.size() > 3 ? t[3] : "0";
+        r.hi = t.size() > 4 ? t[4] : "0";
+        r.lo = t.size() > 5 ? t[5] : "0";
+        rows.push_back(r);
+    }
+    std::fclose(f);
+    std::vector<int64_t> ws(rows.size());
+    std::vector<int32_t> cx(rows.size()), cz(rows.size());
+    for (size_t i = 0; i < rows.size(); i++) {
+        ws[i] = rows[i].ws;
+        cx[i] = rows[i].cx;
+        cz[i] = rows[i].cz;
+    }
+    std::vector<wg_finish_row> out(rows.size());
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = wg_finish_rows(eng, ws.data(), cx.data(), cz.data(), rows.size(), out.data());
+    if (rc) {
+        std::fprintf(stderr, "wg_finish_rows: %s\n", wg_engine_error(eng));
+        return 1;
+    }
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    size_t kept = 0;
+    for (size_t i = 0; i < rows.size(); i++) {
+        const wg_finish_row &r = out[i];
+        if (!r.verdict_ok || r.tree_status != 0) continue;
+        if (r.biome[0] == 183 && r.biome[1] == 183) continue;   // deep dark in both sets: no mineshaft
+        if (r.top[1] > min_r) continue;
+        kept++;
+        std::printf("%4d  terrain %4d  refused %2d  if-none-refused %4d  NW %4d  max %4d  lava %4d  air %s/%s  "
+                    "biome %d  layout %s  seed %" PRId64 "  /tp %d %d %d\n",
+                    r.top[1], r.nat, r.refused[0], r.no_guard[1], r.nw, r.scan_max, r.lava, rows[i].hi.c_str(),
+                    rows[i].lo.c_str(), r.biome[0], rows[i].layout.c_str(), rows[i].ws, r.hut_x, r.top[1], r.hut_z);
+    }
+    std::fprintf(stderr, "finish: %zu rows, %zu accepted, %.3f s\n", rows.size(), kept, secs);
+    return 0;
+}
+
+}  // namespace
+
 int main(int argc, char **argv) {
     const char *cat_path = nullptr, *plan_path = nullptr, *spots_path = nullptr, *hits_path = nullptr;
+    const char *finish_path = nullptr;
+    int min_r = 999;
     const char *out_path = "hut_lookup_out.csv";
     long long first = 0, count = 1;
     int regx = -1, regz = -1, max_h = -54;
@@ -132,6 +221,8 @@ int main(int argc, char **argv) {
         if (!std::strcmp(a, "--catalog")) cat_path = val();
         else if (!std::strcmp(a, "--plan")) plan_path = val();
         else if (!std::strcmp(a, "--spots")) spots_path = val();
+        else if (!std::strcmp(a, "--finish")) finish_path = val();
+        else if (!std::strcmp(a, "--min-r")) { const char *v = val(); if (v) min_r = std::atoi(v); }
         else if (!std::strcmp(a, "--dump-hits")) hits_path = val();
         else if (!std::strcmp(a, "--out")) out_path = val();
         else if (!std::strcmp(a, "--first-index")) { const char *v = val(); if (v) first = std::atoll(v); }
@@ -157,6 +248,16 @@ int main(int argc, char **argv) {
             std::fprintf(stderr, "unknown arg %s\n", a);
             return 2;
         }
+    }
+    if (finish_path) {
+        wg_engine *feng = nullptr;
+        if (wg_engine_open(0, &feng)) {
+            std::fprintf(stderr, "no GPU engine\n");
+            return 1;
+        }
+        const int frc = run_finish(feng, finish_path, min_r);
+        wg_engine_close(feng);
+        return frc;
     }
     if (!cat_path) return fail("usage: hut_lookup --catalog cat.txt (--solve-only --solve5 --plan P | --spots S) ...");
     std::map<uint64_t, std::pair<unsigned, unsigned>> cat;

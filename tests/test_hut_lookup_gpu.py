@@ -61,3 +61,33 @@ def test_terrain_command(wg, engine, golden, tmp_path):
         r = subprocess.run([wg.HUT_LOOKUP_PATH, "--catalog", "cat.txt", "--spots", "bad.txt", "--out", "b.csv"],
                            capture_output=True, text=True, cwd=tmp_path, timeout=600)
         assert r.returncode == 1 and "not" in r.stderr
+
+
+def test_finish_command(wg, tmp_path):
+    """hut_lookup --finish over the finisher fixture's rows prints, for every row hunt.py's
+    finish_row accepts, the same line finish_row builds from the reference tools' outputs
+    (hunt.py:277-333), and nothing for the others; hunt.py's selftest condition holds for REFERENCE."""
+    import os
+    fx = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "finish_rows.npz"))
+    layout, hi, lo = ["0"] * len(fx["ws"]), ["0"] * len(fx["ws"]), ["0"] * len(fx["ws"])
+    layout[0], hi[0], lo[0] = "254754461452089", "329", "323"   # hunt.py:83
+    with open(tmp_path / "rows.csv", "w") as f:
+        f.write("seed,chunkX,chunkZ,layoutX,airHi,airLo\n")
+        for i in range(len(fx["ws"])):
+            f.write(f"{int(fx['ws'][i])},{int(fx['cx'][i])},{int(fx['cz'][i])},{layout[i]},{hi[i]},{lo[i]}\n")
+    r = subprocess.run([wg.HUT_LOOKUP_PATH, "--finish", "rows.csv"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    want = []
+    for i in range(len(fx["ws"])):
+        if not (fx["verdict_ok"][i] and fx["start"][i]) or (fx["biome0"][i] == 183 and fx["biome1"][i] == 183):
+            continue
+        r1 = int(fx["top1"][i])
+        want.append("%4d  terrain %4s  refused %2s  if-none-refused %4s  NW %4s  max %4s  lava %4s  air %s/%s  "
+                    "biome %s  layout %s  seed %s  /tp %d %d %d"
+                    % (r1, fx["nat"][i], fx["refused"][i][0], fx["ng1"][i], fx["nw"][i], fx["scan_max"][i],
+                       fx["lava"][i], hi[i], lo[i], fx["biome0"][i], layout[i], int(fx["ws"][i]),
+                       16 * int(fx["cx"][i]), r1, 16 * int(fx["cz"][i])))
+    assert r.stdout.splitlines() == want
+    assert len(want) > 50
+    assert int(want[0].split()[0]) <= -58 and "/tp -29646048 -58 -22084400" in want[0]
