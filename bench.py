@@ -241,6 +241,18 @@ def deep_measure(eng, opts) -> dict:
     t0 = time.perf_counter()
     shits, sst = eng.deep_solve(plan, 4096, 64)
     solve_s = time.perf_counter() - t0
+    # the mineshaft finisher over 1,024 start chunks of the walk under fixed upper seed bits
+    rng = np.random.default_rng(9)
+    fin = hits[:1024]
+    fin_ws = [((int(u) << 48) | (int(s) & 0xFFFFFFFFFFFF)) for u, s in zip(rng.integers(0, 1 << 16, len(fin)), fin["s48"])]
+    eng.finish_rows(fin_ws[:2], fin["chunk_x"][:2], fin["chunk_z"][:2])
+    t0 = time.perf_counter()
+    frows = eng.finish_rows(fin_ws, fin["chunk_x"], fin["chunk_z"])
+    fin_s = time.perf_counter() - t0
+    finisher = {"rows": len(fin_ws), "rows_per_s": len(fin_ws) / fin_s, "ms": 1e3 * fin_s,
+                "accepted_by_lysh": int(frows["verdict_ok"].sum()), "trees": int((frows["tree_status"] == 0).sum()),
+                "pieces": int(frows["pieces"].sum()),
+                "cpu_baseline": finisher_cpu_baseline(fin_ws[:16], fin["chunk_x"][:16], fin["chunk_z"][:16])}
     return {"solver": {"plan": "231564844655014 22 odd", "groups": sst["groups"], "regions": sst["regions"],
                        "tasks": sst["tasks"], "candidates": sst["candidates"], "hits": sst["hits"],
                        "tasks_per_s": sst["tasks"] / solve_s, "groups_per_s": sst["groups"] / solve_s,
@@ -262,8 +274,52 @@ def deep_measure(eng, opts) -> dict:
                             "upper-16-bit world seeds); the terrain stage that expands a match runs at the "
                             "`terrain` rate; the reference's own figure is about 94 M world seeds/s for that "
                             "stage (hunt.py:463-464)")},
-            "timing": "wall clock around wg_deep_solve / wg_deep_starts / wg_deep_spots (host buffers in and "
-                      "out); device time of the solver from its CUDA events"}
+            "finisher": finisher,
+            "timing": "wall clock around wg_deep_solve / wg_deep_starts / wg_deep_spots / wg_finish_rows (host "
+                      "buffers in and out); device time of the solver from its CUDA events"}
+
+
+def finisher_cpu_baseline(ws, cx, cz) -> dict | None:
+    """hunt.py's finish_row as the reference runs it (one process per tool: lysh hut, mstree, biome_at
+    x 2, msroom, skyscan) on the first survivors, with the reference's tools built from its sources
+    into oracle/_ref; None when they are not there."""
+    ref = os.path.join(ROOT, "oracle", "_ref")
+    tools = ("lysh", "mstree", "biome_at", "msroom", "skyscan")
+    if not all(os.path.exists(os.path.join(ref, t)) for t in tools):
+        return None
+    import subprocess
+    import tempfile
+
+    def run(args, stdin=None, env=None):
+        return subprocess.run(args, input=stdin, capture_output=True, text=True, env=dict(os.environ, **(env or {})),
+                              timeout=120).stdout
+
+    t0 = time.perf_counter()
+    for w, x, z in zip(ws, cx, cz):
+        w = w - (1 << 64) if w >= 1 << 63 else w
+        hx, hz = 16 * int(x), 16 * int(z)
+        run([os.path.join(ref, "lysh"), "hut", "--seed", str(w), "--x", str(hx), "--z", str(hz), "--max-y", "100",
+             "--phase2-max-y", "100", "--version", "1.19.x~26.1"])
+        tree = run([os.path.join(ref, "mstree"), str(w), str(int(x)), str(int(z))])
+        if not tree.strip():
+            continue
+        fl = tree.split()[2]
+        for env in (None, {"BIOME_26": "1"}):
+            run([os.path.join(ref, "biome_at"), "--seed", str(w), "--cx", str(int(x)), "--cz", str(int(z)), "--ms",
+                 "--y", fl], env=env)
+        run([os.path.join(ref, "msroom"), "--seed", str(w), "--x", str(hx), "--z", str(hz)], stdin=tree,
+            env={"MC_SHAPE": "79", "MC_TRIALS": "0"})
+        with tempfile.NamedTemporaryFile("w", suffix=".csv", delete=False) as f:
+            f.write("X,u,wx,wz,fw,fd,dx,dz,bound\n%d,%d,%d,%d,7,9,%d,%d,0\n"
+                    % (w & 0xFFFFFFFFFFFF, (w >> 48) & 0xFFFF, hx, hz, int(x), int(z)))
+        try:
+            run([os.path.join(ref, "skyscan"), "--list", f.name])
+        finally:
+            os.remove(f.name)
+    secs = time.perf_counter() - t0
+    return {"value": len(ws) / secs, "unit": "rows/s", "cores": 1, "kind": "reference",
+            "sample": f"the first {len(ws)} rows through the reference's finisher tools, one process per tool "
+                      "as hunt.py's finish_row spawns them"}
 
 
 def biome_measure(eng) -> dict:
