@@ -246,6 +246,9 @@ struct TableY<true> {
     __device__ __forceinline__ double fy64(int o) const { return fade(hy[o]); }
 };
 
+constexpr int kClimateWarps = kThreadsA / 32;
+constexpr int kWarpList = 112;   // tier-0 survivors a warp carries (a warp has <= 192 regions a chunk, ~43 % pass)
+
 template <bool F32>
 struct ClimateSmem {
     using Real = typename std::conditional<F32, float, double>::type;
@@ -254,18 +257,14 @@ struct ClimateSmem {
     TableY<F32> ty;
     int jy[kSlotsA * kUnits];
     int2 pos[kChunk * kUnits];                 // hut chunk (cx, cz) of window offset c0 + j, unit u
-    union {
-        Real tsum[kTierList];                  // erosion partial sum of each tier-0 survivor
-        Real val[kClimateList * 6];            // parallel temperature / ridge samples (after the tiers)
-    };
-    uint32_t tlist[kTierList];                 // tier-0 survivors of the chunk: unit << 16 | (j - c0)
-    uint32_t clist[kClimateList];              // erosion survivors of the chunk
-    uint32_t rlist[kClimateList];              // ... that also passed temperature
-    uint32_t n_tlist, t_next, n_clist, n_rlist;
-    uint32_t tcount[2];                        // list lengths of the breadth-first tier steps (ping-pong)
+    // each warp's survivors of the chunk (unit << 16 | (j - c0)) and their erosion partial sums:
+    // the tier-0 survivors of the warp's own regions, compacted in place after every later step
+    uint32_t wl[kClimateWarps][kWarpList];
+    Real wsum[kClimateWarps][kWarpList];
+    uint32_t wn[kClimateWarps];
     uint32_t surv[kUnits * kRecordCap];
     uint32_t cnt[kUnits];
-    uint32_t end[kUnits];                      // end of the current chunk, per unit
+    uint32_t len[kUnits];                      // regions in the unit's window (0: past the batch)
     uint64_t g[kUnits], rbase[kUnits], seed[kUnits];   // seed index, first region, world seed
     uint32_t col0[kUnits];                     // column of the unit's first region in its rect row
     int row0[kUnits];                          // rz of the unit's first region
@@ -392,11 +391,10 @@ __device__ __forceinline__ void climate_point(const Sm &S, int iu, uint32_t jl, 
     zc = (c.y * 16 + 8) / 4.0;
 }
 
-// The erosion tiers from step k0 for one region (e = unit << 16 | offset in the chunk), one Perlin
-// sample per loop trip, run by one thread: the path for a tier-0 survivor that finds the tier list
-// full.  A region that passes the last tier is handed to the climate list; if that list is full
-// too, this thread also runs its temperature and ridge steps.  Always FP64 (the FP32 core enters
-// it with k0 = 0 and recomputes the partial sum exactly).
+// The climate steps from step k0 for one region (e = unit << 16 | offset in the chunk), one Perlin
+// sample per loop trip, run by one thread: the path for a tier-0 survivor that finds its warp's
+// list full.  Always FP64 (the FP32 core enters it with k0 = 0 and recomputes the partial sum
+// exactly).
 template <class Sm>
 __device__ void climate_rest(Sm &S, const BatchArgs &a, TierCounts &tc, uint32_t e, uint32_t c0, int k0, double sum,
                              double xc, double zc) {
@@ -418,14 +416,8 @@ __device__ void climate_rest(Sm &S, const BatchArgs &a, TierCounts &tc, uint32_t
                 if (sum * st.amp[k] < st.thr[k]) {
                     erosion_reject(S, a, tc, iu, j, st.tier[k]);
                     return;
-                } else {
-                    const uint32_t q = atomicAdd(&S.n_clist, 1u);
-                    if (q < kClimateList) {
-                        S.clist[q] = e;
-                        return;
-                    }
-                    sum = 0.0;   // list full: finish it here
                 }
+                sum = 0.0;   // temperature and ridge follow here
                 break;
             case ACT_END_SUB_A:
                 sum_a = sum;
@@ -508,6 +500,7 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
     const uint32_t len = valid ? up.len : 0;
     if (tid < kUnits) {
         S.cnt[tid] = 0;
+        S.len[tid] = len;
         S.g[tid] = g;
         S.rbase[tid] = up.rbase;
         S.seed[tid] = seed;
@@ -553,14 +546,21 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
     const uint32_t cta_len = max_len;
     const ClimateSteps &st = S.steps;
 
+    // The regions of a chunk are evaluated warp by warp: a warp stages the hut chunks of its own
+    // regions (q = tid + r * kThreadsA), takes tier 0 for them, and carries its tier-0 survivors
+    // through the remaining erosion tiers, temperature and ridge in its own list, synchronising
+    // with __syncwarp only: no step of one warp waits for another warp.
+    const int warp = tid >> 5, lane = tid & 31;
+    uint32_t *const wl = S.wl[warp];
+    Real *const wsum = S.wsum[warp];
+    const unsigned lanes_below = (1u << lane) - 1u;
+    constexpr int kT0 = 8, kR0 = 12;   // first temperature / ridge step
     for (uint32_t c0 = 0; c0 < cta_len; c0 += kChunk) {
-        // ---- stage the hut chunks of this chunk of regions, all units at once ----
-        if (tid < kUnits) S.end[tid] = (valid && c0 < len) ? min(len, c0 + (uint32_t)kChunk) : c0;
-        __syncthreads();
+        // ---- stage the hut chunks of this warp's regions (j < len: c0 + q / kUnits < c0 + kChunk) ----
         for (int q = tid; q < kChunk * kUnits; q += kThreadsA) {
             const int qu = q % kUnits;
             const uint32_t j = c0 + (uint32_t)(q / kUnits);
-            if (j >= S.end[qu]) continue;
+            if (j >= S.len[qu]) continue;
             const uint32_t t = S.col0[qu] + j;   // region offset from the unit's first row start
             const uint32_t rw = S.rwu[qu];
             const int rz = S.row0[qu] + (int)(t / rw), rx = S.rx0u[qu] + (int)(t % rw);
@@ -568,32 +568,27 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
             hut_chunk(S.seed[qu], rx, rz, a.salt, cx, cz);
             S.pos[q] = make_int2(cx, cz);
         }
-        if (tid == 0) {
-            S.n_tlist = 0;
-            S.t_next = 0;
-            S.n_clist = 0;
-            S.n_rlist = 0;
-        }
-        __syncthreads();
+        if (lane == 0) S.wn[warp] = 0;
+        __syncwarp();
 
         // ---- tier 0 for every region: samples 0A and 0B with loop-invariant parameters ----
         {
             const int nq = kUnits * kChunk;
-            // the decision's bookkeeping: warp-aggregated append of a survivor to the tier list
+            // the decision's bookkeeping: warp-aggregated append of a survivor to the warp's list
             auto tier0_decide = [&](int iu, uint32_t jl, Real sum, bool pass, double xc, double zc) {
                 const uint32_t j = c0 + jl;
                 cg::coalesced_group grp = cg::coalesced_threads();
                 const unsigned m = grp.ballot(pass);
                 uint32_t base = 0;
-                if (grp.thread_rank() == 0 && m) base = atomicAdd(&S.n_tlist, (uint32_t)__popc(m));
+                if (grp.thread_rank() == 0 && m) base = atomicAdd(&S.wn[warp], (uint32_t)__popc(m));
                 base = grp.shfl(base, 0);
                 if (!pass) {
                     erosion_reject(S, a, tc, iu, j, st.tier[1]);
                 } else {
                     const uint32_t t = base + (uint32_t)__popc(m & ((1u << grp.thread_rank()) - 1u));
-                    if (t < kTierList) {
-                        S.tlist[t] = ((uint32_t)iu << 16) | jl;
-                        S.tsum[t] = sum;
+                    if (t < kWarpList) {
+                        wl[t] = ((uint32_t)iu << 16) | jl;
+                        wsum[t] = sum;
                     } else if (F32) {
                         // list full: this thread walks the region through the rest itself, in FP64
                         climate_rest(S, a, tc, ((uint32_t)iu << 16) | jl, c0, 0, 0.0, xc, zc);
@@ -606,13 +601,13 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                 for (int q = tid; q < nq; q += kThreadsA) {
                     const int iu = q % kUnits;
                     const uint32_t j = c0 + (uint32_t)(q / kUnits);
-                    if (j < S.end[iu]) keep_survivor(S, a, iu, j);
+                    if (j < S.len[iu]) keep_survivor(S, a, iu, j);
                 }
             } else if constexpr (F32) {
                 for (int q = tid; q < nq; q += kThreadsA) {
                     const int iu = q % kUnits;
                     const uint32_t jl = (uint32_t)(q / kUnits);
-                    if (c0 + jl >= S.end[iu]) continue;
+                    if (c0 + jl >= S.len[iu]) continue;
                     double xc, zc;
                     climate_point(S, iu, jl, xc, zc);
                     float sum = __fmul_rn(st.cf[0], climate_sample_f32<SMALL>(S, iu, 0, xc, zc));
@@ -632,7 +627,7 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                 for (int q = tid; q < nq; q += kThreadsA) {
                     const int iu = q % kUnits;
                     const uint32_t jl = (uint32_t)(q / kUnits), j = c0 + jl;
-                    if (j >= S.end[iu]) continue;
+                    if (j >= S.len[iu]) continue;
                     double xc, zc;
                     climate_point(S, iu, jl, xc, zc);
                     double sum = 0.0;
@@ -642,40 +637,36 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                 }
             }
         }
-        __syncthreads();
+        __syncwarp();
+        uint32_t n = min(S.wn[warp], (uint32_t)kWarpList);
 
-        // ---- the remaining erosion tiers, breadth first: every listed region takes erosion step k
-        // (one sample with the step's slot and constants, the same for all), its tier check, and
-        // the survivors are compacted for step k + 1 (items held in registers between the two
-        // barriers, so the list is rewritten in place); past the last tier they go to the climate
-        // list, or, when it is full, through temperature and ridge by the thread itself ----
-        {
-            constexpr int kPer = (kTierList + kThreadsA - 1) / kThreadsA;
-            if (tid == 0) S.tcount[1] = min(S.n_tlist, (uint32_t)kTierList);
-            __syncthreads();
+        // ---- the remaining erosion tiers, breadth first over the warp's list: every listed region
+        // takes erosion step k (one sample with the step's slot and constants), its tier check, and
+        // the survivors are compacted in place for step k + 1 (items held in registers between two
+        // __syncwarp) ----
+        if (!a.single_biome) {
+            constexpr int kPer = (kWarpList + 31) / 32;
 #pragma unroll 1
-            for (int k = 2; k < kClimateSteps && st.act[k] != ACT_NONE && st.act[k] <= ACT_TIER_LAST; k++) {
-                const uint32_t n_t = S.tcount[(k - 1) & 1];
-                if (tid == 0) S.tcount[k & 1] = 0;
+            for (int k = 2; n && k < kClimateSteps && st.act[k] != ACT_NONE && st.act[k] <= ACT_TIER_LAST; k++) {
                 const double c1 = st.c1[k], c2 = st.c2[k], amp = st.amp[k], thr = st.thr[k];
                 const float cf = st.cf[k], lo = st.lo[k], hi = st.hi[k];
                 const int tier = st.tier[k];
-                const bool last = st.act[k] == ACT_TIER_LAST;
                 uint32_t ke[kPer];
                 Real ks[kPer];
-                if constexpr (F32) {
 #pragma unroll
-                    for (int r = 0; r < kPer; r++) {
-                        const uint32_t q = (uint32_t)tid + (uint32_t)(r * kThreadsA);
-                        ke[r] = 0xFFFFFFFFu;
-                        ks[r] = 0;
-                        if (q >= n_t) continue;
-                        const uint32_t e = S.tlist[q];
-                        const int iu = (int)(e >> 16);
-                        double xc, zc;
-                        climate_point(S, iu, e & 0xFFFFu, xc, zc);
-                        const float sum = __fmaf_rn(cf, climate_sample_f32<SMALL>(S, iu, k, xc, zc), S.tsum[q]);
-                        bool reject;
+                for (int r = 0; r < kPer; r++) {
+                    const uint32_t q = (uint32_t)lane + (uint32_t)(r * 32);
+                    ke[r] = 0xFFFFFFFFu;
+                    ks[r] = 0;
+                    if (q >= n) continue;
+                    const uint32_t e = wl[q];
+                    const int iu = (int)(e >> 16);
+                    double xc, zc;
+                    climate_point(S, iu, e & 0xFFFFu, xc, zc);
+                    bool reject;
+                    Real sum;
+                    if constexpr (F32) {
+                        sum = __fmaf_rn(cf, climate_sample_f32<SMALL>(S, iu, k, xc, zc), wsum[q]);
                         if (!all_rechecks && sum < lo) {
                             reject = true;
                         } else if (!all_rechecks && sum >= hi) {
@@ -684,165 +675,153 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                             rechecks++;
                             reject = climate_sum64(S, iu, 0, k, xc, zc) * amp < thr;
                         }
-                        if (reject) {
-                            erosion_reject(S, a, tc, iu, c0 + (e & 0xFFFFu), tier);
-                        } else {
-                            ke[r] = e;
-                            ks[r] = sum;
-                        }
+                    } else {
+                        sum = wsum[q];
+                        sum += (c1 * climate_sample(S, iu, k, xc, zc)) * c2;
+                        reject = sum * amp < thr;
                     }
-                } else {
-#pragma unroll
-                    for (int r = 0; r < kPer; r++) {
-                        const uint32_t q = (uint32_t)tid + (uint32_t)(r * kThreadsA);
-                        ke[r] = 0xFFFFFFFFu;
-                        ks[r] = 0;
-                        if (q < n_t) {
-                            const uint32_t e = S.tlist[q];
-                            const int iu = (int)(e >> 16);
-                            double xc, zc;
-                            climate_point(S, iu, e & 0xFFFFu, xc, zc);
-                            double sum = S.tsum[q];
-                            sum += (c1 * climate_sample(S, iu, k, xc, zc)) * c2;
-                            if (sum * amp < thr) {
-                                erosion_reject(S, a, tc, iu, c0 + (e & 0xFFFFu), tier);
-                            } else {
-                                ke[r] = e;
-                                ks[r] = sum;
-                            }
-                        }
+                    if (reject) {
+                        erosion_reject(S, a, tc, iu, c0 + (e & 0xFFFFu), tier);
+                    } else {
+                        ke[r] = e;
+                        ks[r] = sum;
                     }
                 }
-                __syncthreads();   // every read of this step's list is done
+                __syncwarp();   // every read of this step's list is done
+                uint32_t nn = 0;
 #pragma unroll
                 for (int r = 0; r < kPer; r++) {
                     const bool keep = ke[r] != 0xFFFFFFFFu;
-                    if (!last) {
-                        cg::coalesced_group grp = cg::coalesced_threads();
-                        const unsigned m = grp.ballot(keep);
-                        uint32_t base = 0;
-                        if (grp.thread_rank() == 0 && m) base = atomicAdd(&S.tcount[k & 1], (uint32_t)__popc(m));
-                        base = grp.shfl(base, 0);
-                        if (keep) {
-                            const uint32_t at = base + (uint32_t)__popc(m & ((1u << grp.thread_rank()) - 1u));
-                            S.tlist[at] = ke[r];
-                            S.tsum[at] = ks[r];
-                        }
-                    } else if (keep) {
-                        const uint32_t qq = atomicAdd(&S.n_clist, 1u);
-                        if (qq < kClimateList) {
-                            S.clist[qq] = ke[r];
-                        } else {   // climate list full: temperature and ridge here
-                            double xc, zc;
-                            climate_point(S, (int)(ke[r] >> 16), ke[r] & 0xFFFFu, xc, zc);
-                            climate_rest(S, a, tc, ke[r], c0, k + 1, 0.0, xc, zc);
+                    const unsigned m = __ballot_sync(0xFFFFFFFFu, keep);
+                    if (keep) {
+                        const uint32_t at = nn + (uint32_t)__popc(m & lanes_below);
+                        wl[at] = ke[r];
+                        wsum[at] = ks[r];
+                    }
+                    nn += (uint32_t)__popc(m);
+                }
+                __syncwarp();   // the compacted list is complete
+                n = nn;
+            }
+        } else {
+            n = 0;
+        }
+
+        // ---- temperature for the warp's erosion survivors: four lanes per region, one sample each,
+        // summed in the reference's order by the first of the four; survivors compacted in place ----
+        uint32_t nr = 0;
+        for (uint32_t base = 0; base < n; base += 8) {
+            const uint32_t i = base + (uint32_t)(lane >> 2);
+            const int p = lane & 3;
+            const bool have = i < n;
+            const uint32_t e = have ? wl[i] : 0u;
+            const int iu = (int)(e >> 16);
+            double xc = 0.0, zc = 0.0;
+            Real v = 0;
+            if (have) {
+                climate_point(S, iu, e & 0xFFFFu, xc, zc);
+                if constexpr (F32) v = climate_sample_f32<SMALL>(S, iu, kT0 + p, xc, zc);
+                else v = climate_sample(S, iu, kT0 + p, xc, zc);
+            }
+            const Real vs[4] = {v, __shfl_down_sync(0xFFFFFFFFu, v, 1), __shfl_down_sync(0xFFFFFFFFu, v, 2),
+                                __shfl_down_sync(0xFFFFFFFFu, v, 3)};
+            bool keep = false;
+            if (have && p == 0) {
+                bool bad;
+                if constexpr (F32) {
+                    float sum = 0.0f;
+                    for (int q = 0; q < 4; q++) sum = __fmaf_rn(st.cf[kT0 + q], vs[q], sum);
+                    const F32Bands &B = c_bands[large];
+                    if (all_rechecks || (sum >= B.t_lo[0] && sum < B.t_hi[0]) || (sum >= B.t_lo[1] && sum < B.t_hi[1])) {
+                        rechecks++;
+                        const double t = climate_value64(S, iu, kT0, 4, xc, zc);
+                        bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
+                    } else {
+                        const bool low = sum < B.t_lo[0], high = sum >= B.t_hi[1];   // t < -0.45, t > 0.2
+                        bad = a.mc_1_18_2 ? low : (low || high);
+                    }
+                } else {
+                    double sum = 0.0, sum_a = 0.0;
+                    for (int q = 0; q < 4; q++) {   // the state machine's accumulation, steps kT0..kT0+3
+                        const int k = kT0 + q;
+                        sum += (st.c1[k] * vs[q]) * st.c2[k];
+                        if (st.act[k] == ACT_END_SUB_A) {
+                            sum_a = sum;
+                            sum = 0.0;
                         }
                     }
-                }
-                __syncthreads();   // the compacted list is complete
-            }
-        }
-        __syncthreads();
-
-        // ---- temperature for the listed erosion survivors: one sample per thread ----
-        const uint32_t n_cl = min(S.n_clist, (uint32_t)kClimateList);
-        constexpr int kT0 = 8, kR0 = 12;   // first temperature / ridge step
-        for (uint32_t t = tid; t < n_cl * 4; t += kThreadsA) {
-            const uint32_t e = S.clist[t / 4];
-            const int iu = (int)(e >> 16);
-            double xc, zc;
-            climate_point(S, iu, e & 0xFFFFu, xc, zc);
-            if constexpr (F32) S.val[t] = climate_sample_f32<SMALL>(S, iu, kT0 + (int)(t % 4), xc, zc);
-            else S.val[t] = climate_sample(S, iu, kT0 + (int)(t % 4), xc, zc);
-        }
-        __syncthreads();
-        for (uint32_t i = tid; i < n_cl; i += kThreadsA) {
-            const uint32_t e = S.clist[i];
-            bool bad;
-            if constexpr (F32) {
-                float sum = 0.0f;
-                for (int p = 0; p < 4; p++) sum = __fmaf_rn(st.cf[kT0 + p], S.val[i * 4 + p], sum);
-                const F32Bands &B = c_bands[large];
-                if (all_rechecks || (sum >= B.t_lo[0] && sum < B.t_hi[0]) || (sum >= B.t_lo[1] && sum < B.t_hi[1])) {
-                    rechecks++;
-                    double xc, zc;
-                    climate_point(S, (int)(e >> 16), e & 0xFFFFu, xc, zc);
-                    const double t = climate_value64(S, (int)(e >> 16), kT0, 4, xc, zc);
+                    const double t = (sum_a + sum) * st.amp[kT0 + 3];
                     bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
-                } else {
-                    const bool low = sum < B.t_lo[0], high = sum >= B.t_hi[1];   // t < -0.45, t > 0.2
-                    bad = a.mc_1_18_2 ? low : (low || high);
                 }
-            } else {
-                double sum = 0.0, sum_a = 0.0;
-                for (int p = 0; p < 4; p++) {   // the state machine's accumulation, steps kT0..kT0+3
-                    const int k = kT0 + p;
-                    sum += (st.c1[k] * S.val[i * 4 + p]) * st.c2[k];
-                    if (st.act[k] == ACT_END_SUB_A) {
-                        sum_a = sum;
-                        sum = 0.0;
-                    }
-                }
-                const double t = (sum_a + sum) * st.amp[kT0 + 3];
-                bad = a.mc_1_18_2 ? (t < -0.45) : (t > 0.2 || t < -0.45);
+                if (bad) climate_reject(S, a, iu, c0 + (e & 0xFFFFu), P1_TEMPERATURE, -1);
+                else keep = true;
             }
-            if (bad) climate_reject(S, a, (int)(e >> 16), c0 + (e & 0xFFFFu), P1_TEMPERATURE, -1);
-            else S.rlist[atomicAdd(&S.n_rlist, 1u)] = e;
+            const unsigned m = __ballot_sync(0xFFFFFFFFu, keep);
+            __syncwarp();   // this round's reads are done before its survivors are written
+            if (keep) wl[nr + (uint32_t)__popc(m & lanes_below)] = e;
+            nr += (uint32_t)__popc(m);
         }
-        __syncthreads();
+        __syncwarp();
 
-        // ---- ridge for those that passed temperature ----
-        const uint32_t n_rl = S.n_rlist;
-        for (uint32_t t = tid; t < n_rl * 6; t += kThreadsA) {
-            const uint32_t e = S.rlist[t / 6];
+        // ---- ridge for those that passed temperature: six lanes per region (lanes 0-29) ----
+        for (uint32_t base = 0; base < nr; base += 5) {
+            const uint32_t i = base + (uint32_t)(lane / 6);
+            const int p = lane % 6;
+            const bool have = lane < 30 && i < nr;
+            const uint32_t e = have ? wl[i] : 0u;
             const int iu = (int)(e >> 16);
-            double xc, zc;
-            climate_point(S, iu, e & 0xFFFFu, xc, zc);
-            if constexpr (F32) S.val[t] = climate_sample_f32<SMALL>(S, iu, kR0 + (int)(t % 6), xc, zc);
-            else S.val[t] = climate_sample(S, iu, kR0 + (int)(t % 6), xc, zc);
-        }
-        __syncthreads();
-        for (uint32_t i = tid; i < n_rl; i += kThreadsA) {
-            const uint32_t e = S.rlist[i];
-            const int iu = (int)(e >> 16);
-            const uint32_t j = c0 + (e & 0xFFFFu);
-            bool bad;
-            if constexpr (F32) {
-                float sum = 0.0f;
-                for (int p = 0; p < 6; p++) sum = __fmaf_rn(st.cf[kR0 + p], S.val[i * 6 + p], sum);
-                const F32Bands &B = c_bands[large];
-                bool inside = all_rechecks;
-                for (int q = 0; q < 4; q++) inside |= sum >= B.r_lo[q] && sum < B.r_hi[q];
-                if (inside) {
-                    rechecks++;
-                    double xc, zc;
-                    climate_point(S, iu, e & 0xFFFFu, xc, zc);
-                    const double rg = climate_value64(S, iu, kR0, 6, xc, zc);
-                    bad = (rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91);
-                } else {
-                    // above[q]: the ridge value lies above threshold q (-0.91, -0.42, 0.42, 0.91)
-                    const bool a0 = sum >= B.r_hi[0], a1 = sum >= B.r_hi[1], a2 = sum >= B.r_hi[2],
-                               a3 = sum >= B.r_hi[3];
-                    bad = (a2 && !a3) || (!a1 && a0) || (!a.pre_26_2 && !a0);
-                }
-            } else {
-                double sum = 0.0, sum_a = 0.0;
-                for (int p = 0; p < 6; p++) {
-                    const int k = kR0 + p;
-                    sum += (st.c1[k] * S.val[i * 6 + p]) * st.c2[k];
-                    if (st.act[k] == ACT_END_SUB_A) {
-                        sum_a = sum;
-                        sum = 0.0;
-                    }
-                }
-                const double rg = (sum_a + sum) * st.amp[kR0 + 5];
-                bad = (rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91);
+            double xc = 0.0, zc = 0.0;
+            Real v = 0;
+            if (have) {
+                climate_point(S, iu, e & 0xFFFFu, xc, zc);
+                if constexpr (F32) v = climate_sample_f32<SMALL>(S, iu, kR0 + p, xc, zc);
+                else v = climate_sample(S, iu, kR0 + p, xc, zc);
             }
-            if (bad) climate_reject(S, a, iu, j, P1_RIDGE, -1);
-            else keep_survivor(S, a, iu, j);
+            const Real vs[6] = {v,
+                                __shfl_down_sync(0xFFFFFFFFu, v, 1),
+                                __shfl_down_sync(0xFFFFFFFFu, v, 2),
+                                __shfl_down_sync(0xFFFFFFFFu, v, 3),
+                                __shfl_down_sync(0xFFFFFFFFu, v, 4),
+                                __shfl_down_sync(0xFFFFFFFFu, v, 5)};
+            if (have && p == 0) {
+                const uint32_t j = c0 + (e & 0xFFFFu);
+                bool bad;
+                if constexpr (F32) {
+                    float sum = 0.0f;
+                    for (int q = 0; q < 6; q++) sum = __fmaf_rn(st.cf[kR0 + q], vs[q], sum);
+                    const F32Bands &B = c_bands[large];
+                    bool inside = all_rechecks;
+                    for (int q = 0; q < 4; q++) inside |= sum >= B.r_lo[q] && sum < B.r_hi[q];
+                    if (inside) {
+                        rechecks++;
+                        const double rg = climate_value64(S, iu, kR0, 6, xc, zc);
+                        bad = (rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91);
+                    } else {
+                        // above[q]: the ridge value lies above threshold q (-0.91, -0.42, 0.42, 0.91)
+                        const bool a0 = sum >= B.r_hi[0], a1 = sum >= B.r_hi[1], a2 = sum >= B.r_hi[2],
+                                   a3 = sum >= B.r_hi[3];
+                        bad = (a2 && !a3) || (!a1 && a0) || (!a.pre_26_2 && !a0);
+                    }
+                } else {
+                    double sum = 0.0, sum_a = 0.0;
+                    for (int q = 0; q < 6; q++) {
+                        const int k = kR0 + q;
+                        sum += (st.c1[k] * vs[q]) * st.c2[k];
+                        if (st.act[k] == ACT_END_SUB_A) {
+                            sum_a = sum;
+                            sum = 0.0;
+                        }
+                    }
+                    const double rg = (sum_a + sum) * st.amp[kR0 + 5];
+                    bad = (rg > 0.42 && rg < 0.91) || (rg < -0.42 && rg > -0.91) || (!a.pre_26_2 && rg <= -0.91);
+                }
+                if (bad) climate_reject(S, a, iu, j, P1_RIDGE, -1);
+                else keep_survivor(S, a, iu, j);
+            }
         }
-        __syncthreads();
+        __syncwarp();   // the list and the staged positions are free for the next chunk
     }
+    __syncthreads();   // every warp's survivors are in the units' lists
     if constexpr (F32) {
         const uint32_t n = __reduce_add_sync(0xFFFFFFFFu, rechecks);
         if ((tid & 31) == 0 && n) atomicAdd(&a.counters[CNT_RECHECK], n);
