@@ -165,9 +165,34 @@ def cpu_baseline(n_sample: int) -> dict:
         port.scan_seeds(r, MAX_HEIGHT, RECT, seeds=seeds, threads=cores)
         secs = time.perf_counter() - t0
         kind = "port"
-    return {"value": n_sample / secs, "unit": METRIC, "cores": cores, "kind": kind,
-            "sample": f"first {n_sample} seeds of config 2 (splitmix64(2 + i)), 9x9 regions, lysh phase-1 scan "
-                      f"(lysh_scan_rect per seed, one seed per thread)", "seconds": secs}
+    out = {"value": n_sample / secs, "unit": METRIC, "cores": cores, "kind": kind,
+           "sample": f"first {n_sample} seeds of config 2 (splitmix64(2 + i)), 9x9 regions, lysh phase-1 scan "
+                     f"(lysh_scan_rect per seed, one seed per thread)", "seconds": secs}
+    if os.path.exists(bind.REF_BIN):
+        out["process_per_seed"] = process_per_seed_baseline(bind.REF_BIN, seeds[:256], cores)
+    return out
+
+
+def process_per_seed_baseline(lysh: str, seeds, cores: int) -> dict:
+    """The mode hunt.py's CPU scan uses (hunt.py:1390-1392): one `lysh scan` process per seed (phase 1
+    and lysh's own phase 2 at the ceiling, hits listed), here with `cores` processes at a time."""
+    import subprocess
+    from concurrent.futures import ThreadPoolExecutor
+    rect = [str(v) for v in (RECT[0], RECT[1], RECT[2], RECT[3])]
+
+    def one(seed):
+        cmd = [lysh, "scan", "--seed", str(int(seed)), "--rx0", rect[0], "--rx1", rect[1], "--rz0", rect[2],
+               "--rz1", rect[3], "--threads", "1", "--max-y", str(MAX_HEIGHT), "--phase2-max-y", str(MAX_HEIGHT),
+               "--version", VERSION, "--list", "--no-stats"]
+        return subprocess.run(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL).returncode
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        rcs = list(ex.map(one, seeds))
+    secs = time.perf_counter() - t0
+    return {"value": len(seeds) / secs, "unit": METRIC, "cores": cores, "failed": sum(1 for r in rcs if r),
+            "sample": f"first {len(seeds)} seeds of config 2, one `lysh scan --list --no-stats` process per seed "
+                      f"(hunt.py's CPU mode), {cores} at a time", "seconds": secs}
 
 
 def phase2_measure(eng, cands, opts, cpu: bool) -> dict:
