@@ -69,10 +69,21 @@ OPS_REGION = 40              # java.util.Random placement (2 x nextInt(24)) + co
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, from ncu on `bench.py --profile 1048576`
 # (one launch of each kernel on 2^20 seeds read from a list in HBM; a 2^24-seed step runs 16 such
 # launches, each over its own 2^20 seeds, so the per-launch figure is the full step's per launch)
-TRAFFIC = {"climate_kernel": 8557312 + 0, "entrance_kernel": 20939520 + 0,
-           "source": "ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum --clock-control none "
-                     "-k regex:'climate_kernel|entrance_kernel|ladder_kernel' -s 3 -c 3 python bench.py --profile "
-                     "1048576 --warmup 1 --steps 1 (the timed step's launches; read + write bytes)"}
+TRAFFIC = {"climate_kernel": 8487168 + 0, "entrance_kernel": 20939520 + 0,
+           "source": "climate: ncu --set full --clock-control none -k regex:climate_kernel -s 1 -c 1 python bench.py "
+                     "--profile 1048576 --warmup 1 --steps 1; entrance: ncu --metrics "
+                     "dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k "
+                     "regex:'climate_kernel|entrance_kernel|ladder_kernel' -s 3 -c 3 python bench.py --profile "
+                     "1048576 --warmup 1 --steps 1 (the timed step's launch; read + write bytes)"}
+# ncu pipe utilisation of the same launches (profiles/climate_kernel_2p20_seeds.md,
+# profiles/entrance_kernel_2p20_seeds.md): the counters behind the issue-rate roofline.  The integer
+# ALU pipe issues 64 lanes per clock per SM, half the 128-lane issue rate the roofline divides by,
+# and carries most of the table builds.
+PIPES = {"climate_kernel": {"issue_active": 0.653, "alu": 0.582, "fma": 0.213, "fp64": 0.020,
+                            "shared_wavefronts": 0.741, "warps_active": 0.275},
+         "entrance_kernel": {"issue_active": 0.584, "alu": 0.559, "fma": 0.159, "fp64": 0.079,
+                             "shared_wavefronts": 0.726},
+         "unit": "fraction of peak, ncu --set full of one launch on 2^20 seeds"}
 BYTES_PER_SEED_IN = 8        # the int64 seed read from HBM
 BYTES_PER_RECORD = 12        # (unit, offset, count) per seed with climate survivors
 BYTES_PER_SURVIVOR = 4       # region offset per climate survivor
@@ -715,6 +726,7 @@ def main() -> None:
                               "implies, 40 per (seed, region) placement"),
                 "traffic": TRAFFIC["climate_kernel"], "traffic_unit": "bytes per launch",
                 "traffic_source": TRAFFIC["source"],
+                "ncu_pipes": dict(PIPES["climate_kernel"], unit=PIPES["unit"]),
                 "algorithmic_bytes": bytes_per_launch,
                 "hbm": {"achieved_gbs": bytes_per_launch / (launch_ms / 1e3) / 1e9, "peak_gbs": hbm_peak,
                         "frac": bytes_per_launch / (launch_ms / 1e3) / 1e9 / hbm_peak,
@@ -723,6 +735,7 @@ def main() -> None:
                     "bound": "issue", "unit": "Tlane-op/s", "achieved": ent_ops / (ent_ms / 1e3) / 1e12,
                     "peak": peak_ops / 1e12, "frac": ent_ops / (ent_ms / 1e3) / peak_ops, "ops_per_launch": ent_ops,
                     "launch_ms": ent_ms, "traffic": TRAFFIC["entrance_kernel"], "traffic_unit": "bytes per launch",
+                    "ncu_pipes": dict(PIPES["entrance_kernel"], unit=PIPES["unit"]),
                     "ops_model": ("18 Perlin tables per record x 7,160 lane-ops, per climate survivor 36 3-D samples "
                                   f"x {OPS_3D_SAMPLE} lane-ops + 600 for the octave sums and the decision")},
             },
