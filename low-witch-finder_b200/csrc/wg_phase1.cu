@@ -357,6 +357,30 @@ __device__ __forceinline__ float climate_sample_f32(const ClimateSmem<true> &S, 
                          SMALL ? z : keep_precision(z));
 }
 
+// One climate step's table of one unit with its parameters held in registers: the tier-0 pass
+// samples the same two tables for every region a thread takes (a thread's unit is tid % kUnits in
+// every trip), so their origins, y terms and step constants are read from shared memory once.
+struct Y0Table {
+    const uint8_t *col;
+    double ox, oz, sc, lac;
+    int jy;
+    float hyf, fyf;
+};
+__device__ __forceinline__ Y0Table y0_table(const ClimateSmem<true> &S, int iu, int k) {
+    const ClimateSteps &st = S.steps;
+    const int slot = st.slot[k], o = slot * kUnits + iu;
+    return Y0Table{S.perm + slot * kPitch + iu, S.ox[o], S.oz[o], st.sc[k], st.lac[k], S.jy[o], S.ty.hyf[o],
+                   S.ty.fyf[o]};
+}
+// climate_sample_f32 from a Y0Table: the same operations on the same values.
+template <bool SMALL>
+__device__ __forceinline__ float climate_sample_f32(const ClimateSmem<true> &S, const Y0Table &y, double xc, double zc) {
+    ColTableF<kUnits> T{y.col, &S.gf};
+    const double x = (xc * y.sc) * y.lac, z = (zc * y.sc) * y.lac;
+    return perlin_y0_f32(T, y.ox, y.oz, y.jy, y.hyf, y.fyf, SMALL ? x : keep_precision(x),
+                         SMALL ? z : keep_precision(z));
+}
+
 // FP64 octave sum of climate steps [k0, k1] in the reference's order (sum += (c1 * v) * c2):
 // the exact partial sum an FP32 recheck decides on.
 template <class Sm>
@@ -387,8 +411,8 @@ __device__ __noinline__ double climate_value64(const Sm &S, int iu, int k0, int 
 template <class Sm>
 __device__ __forceinline__ void climate_point(const Sm &S, int iu, uint32_t jl, double &xc, double &zc) {
     const int2 c = S.pos[jl * kUnits + iu];
-    xc = (c.x * 16 + 8) / 4.0;
-    zc = (c.y * 16 + 8) / 4.0;
+    xc = (c.x * 16 + 8) * 0.25;   // exact: an integer over 4
+    zc = (c.y * 16 + 8) * 0.25;
 }
 
 // The climate steps from step k0 for one region (e = unit << 16 | offset in the chunk), one Perlin
@@ -604,18 +628,22 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                     if (j < S.len[iu]) keep_survivor(S, a, iu, j);
                 }
             } else if constexpr (F32) {
+                static_assert(kThreadsA % kUnits == 0, "a thread's unit must be the same in every trip");
+                const int iu = tid % kUnits;
+                const uint32_t len = S.len[iu];
+                const Y0Table y0a = y0_table(S, iu, 0), y0b = y0_table(S, iu, 1);
+                const float cf0 = st.cf[0], cf1 = st.cf[1], lo1 = st.lo[1], hi1 = st.hi[1];
                 for (int q = tid; q < nq; q += kThreadsA) {
-                    const int iu = q % kUnits;
                     const uint32_t jl = (uint32_t)(q / kUnits);
-                    if (c0 + jl >= S.len[iu]) continue;
+                    if (c0 + jl >= len) continue;
                     double xc, zc;
                     climate_point(S, iu, jl, xc, zc);
-                    float sum = __fmul_rn(st.cf[0], climate_sample_f32<SMALL>(S, iu, 0, xc, zc));
-                    sum = __fmaf_rn(st.cf[1], climate_sample_f32<SMALL>(S, iu, 1, xc, zc), sum);
+                    float sum = __fmul_rn(cf0, climate_sample_f32<SMALL>(S, y0a, xc, zc));
+                    sum = __fmaf_rn(cf1, climate_sample_f32<SMALL>(S, y0b, xc, zc), sum);
                     bool pass;
-                    if (!all_rechecks && sum < st.lo[1]) {
+                    if (!all_rechecks && sum < lo1) {
                         pass = false;
-                    } else if (!all_rechecks && sum >= st.hi[1]) {
+                    } else if (!all_rechecks && sum >= hi1) {
                         pass = true;
                     } else {   // inside the error band: decide in FP64
                         rechecks++;
@@ -995,8 +1023,8 @@ __device__ __forceinline__ uint64_t spot_point(const BatchArgs &a, uint32_t u, d
     const uint64_t seed = seed_value(a, up.g);
     int cx, cz;
     hut_chunk(seed, up.rx0, up.rz0, a.salt, cx, cz);
-    xc = (cx * 16 + 8) / 4.0;
-    zc = (cz * 16 + 8) / 4.0;
+    xc = (cx * 16 + 8) * 0.25;   // exact: an integer over 4
+    zc = (cz * 16 + 8) * 0.25;
     return seed;
 }
 
