@@ -261,7 +261,6 @@ struct ClimateSmem {
     // the tier-0 survivors of the warp's own regions, compacted in place after every later step
     uint32_t wl[kClimateWarps][kWarpList];
     Real wsum[kClimateWarps][kWarpList];
-    uint32_t wn[kClimateWarps];
     uint32_t surv[kUnits * kRecordCap];
     uint32_t cnt[kUnits];
     uint32_t len[kUnits];                      // regions in the unit's window (0: past the batch)
@@ -592,24 +591,29 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
             hut_chunk(S.seed[qu], rx, rz, a.salt, cx, cz);
             S.pos[q] = make_int2(cx, cz);
         }
-        if (lane == 0) S.wn[warp] = 0;
-        __syncwarp();
 
         // ---- tier 0 for every region: samples 0A and 0B with loop-invariant parameters ----
+        uint32_t wcount = 0;   // the warp's list length, the same in every lane
         {
             const int nq = kUnits * kChunk;
+            // The trips are warp-uniform (every lane takes kTrips of them, a lane past its unit's
+            // regions with valid = false), so the append needs one ballot and a list length held
+            // in registers.
+            constexpr int kTrips = (kUnits * kChunk + kThreadsA - 1) / kThreadsA;
+            static_assert(kThreadsA % kUnits == 0, "a thread's unit must be the same in every trip");
+            const int iu = tid % kUnits;
+            const uint32_t len = S.len[iu];
             // the decision's bookkeeping: warp-aggregated append of a survivor to the warp's list
-            auto tier0_decide = [&](int iu, uint32_t jl, Real sum, bool pass, double xc, double zc) {
+            auto tier0_decide = [&](bool valid, uint32_t jl, Real sum, bool pass, double xc, double zc) {
                 const uint32_t j = c0 + jl;
-                cg::coalesced_group grp = cg::coalesced_threads();
-                const unsigned m = grp.ballot(pass);
-                uint32_t base = 0;
-                if (grp.thread_rank() == 0 && m) base = atomicAdd(&S.wn[warp], (uint32_t)__popc(m));
-                base = grp.shfl(base, 0);
+                const unsigned m = __ballot_sync(0xFFFFFFFFu, valid && pass);
+                const uint32_t base = wcount;
+                wcount += (uint32_t)__popc(m);
+                if (!valid) return;
                 if (!pass) {
                     erosion_reject(S, a, tc, iu, j, st.tier[1]);
                 } else {
-                    const uint32_t t = base + (uint32_t)__popc(m & ((1u << grp.thread_rank()) - 1u));
+                    const uint32_t t = base + (uint32_t)__popc(m & lanes_below);
                     if (t < kWarpList) {
                         wl[t] = ((uint32_t)iu << 16) | jl;
                         wsum[t] = sum;
@@ -628,45 +632,51 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                     if (j < S.len[iu]) keep_survivor(S, a, iu, j);
                 }
             } else if constexpr (F32) {
-                static_assert(kThreadsA % kUnits == 0, "a thread's unit must be the same in every trip");
-                const int iu = tid % kUnits;
-                const uint32_t len = S.len[iu];
                 const Y0Table y0a = y0_table(S, iu, 0), y0b = y0_table(S, iu, 1);
                 const float cf0 = st.cf[0], cf1 = st.cf[1], lo1 = st.lo[1], hi1 = st.hi[1];
-                for (int q = tid; q < nq; q += kThreadsA) {
+                for (int r = 0; r < kTrips; r++) {
+                    const int q = tid + r * kThreadsA;
                     const uint32_t jl = (uint32_t)(q / kUnits);
-                    if (c0 + jl >= len) continue;
-                    double xc, zc;
-                    climate_point(S, iu, jl, xc, zc);
-                    float sum = __fmul_rn(cf0, climate_sample_f32<SMALL>(S, y0a, xc, zc));
-                    sum = __fmaf_rn(cf1, climate_sample_f32<SMALL>(S, y0b, xc, zc), sum);
-                    bool pass;
-                    if (!all_rechecks && sum < lo1) {
-                        pass = false;
-                    } else if (!all_rechecks && sum >= hi1) {
-                        pass = true;
-                    } else {   // inside the error band: decide in FP64
-                        rechecks++;
-                        pass = !(climate_sum64(S, iu, 0, 1, xc, zc) * st.amp[1] < st.thr[1]);
+                    const bool valid = q < nq && c0 + jl < len;
+                    if (__ballot_sync(0xFFFFFFFFu, valid) == 0u) continue;   // the whole warp is past its regions
+                    double xc = 0.0, zc = 0.0;
+                    float sum = 0.0f;
+                    bool pass = false;
+                    if (valid) {
+                        climate_point(S, iu, jl, xc, zc);
+                        sum = __fmul_rn(cf0, climate_sample_f32<SMALL>(S, y0a, xc, zc));
+                        sum = __fmaf_rn(cf1, climate_sample_f32<SMALL>(S, y0b, xc, zc), sum);
+                        if (!all_rechecks && sum < lo1) {
+                            pass = false;
+                        } else if (!all_rechecks && sum >= hi1) {
+                            pass = true;
+                        } else {   // inside the error band: decide in FP64
+                            rechecks++;
+                            pass = !(climate_sum64(S, iu, 0, 1, xc, zc) * st.amp[1] < st.thr[1]);
+                        }
                     }
-                    tier0_decide(iu, jl, sum, pass, xc, zc);
+                    tier0_decide(valid, jl, sum, pass, xc, zc);
                 }
             } else {
-                for (int q = tid; q < nq; q += kThreadsA) {
-                    const int iu = q % kUnits;
-                    const uint32_t jl = (uint32_t)(q / kUnits), j = c0 + jl;
-                    if (j >= S.len[iu]) continue;
-                    double xc, zc;
-                    climate_point(S, iu, jl, xc, zc);
-                    double sum = 0.0;
-                    sum += (st.c1[0] * climate_sample(S, iu, 0, xc, zc)) * st.c2[0];
-                    sum += (st.c1[1] * climate_sample(S, iu, 1, xc, zc)) * st.c2[1];
-                    tier0_decide(iu, jl, sum, !(sum * st.amp[1] < st.thr[1]), xc, zc);
+                for (int r = 0; r < kTrips; r++) {
+                    const int q = tid + r * kThreadsA;
+                    const uint32_t jl = (uint32_t)(q / kUnits);
+                    const bool valid = q < nq && c0 + jl < len;
+                    if (__ballot_sync(0xFFFFFFFFu, valid) == 0u) continue;   // the whole warp is past its regions
+                    double xc = 0.0, zc = 0.0, sum = 0.0;
+                    bool pass = false;
+                    if (valid) {
+                        climate_point(S, iu, jl, xc, zc);
+                        sum += (st.c1[0] * climate_sample(S, iu, 0, xc, zc)) * st.c2[0];
+                        sum += (st.c1[1] * climate_sample(S, iu, 1, xc, zc)) * st.c2[1];
+                        pass = !(sum * st.amp[1] < st.thr[1]);
+                    }
+                    tier0_decide(valid, jl, sum, pass, xc, zc);
                 }
             }
         }
-        __syncwarp();
-        uint32_t n = min(S.wn[warp], (uint32_t)kWarpList);
+        __syncwarp();   // the list's entries are visible to the whole warp
+        uint32_t n = min(wcount, (uint32_t)kWarpList);
 
         // ---- the remaining erosion tiers, breadth first over the warp's list: every listed region
         // takes erosion step k (one sample with the step's slot and constants), its tier check, and
