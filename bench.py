@@ -243,6 +243,32 @@ def phase2_measure(eng, cands, opts, cpu: bool) -> dict:
     return out
 
 
+# hunt.py's per-seed GPU workload: one world seed over every swamp-hut region of the +-30M world
+# (hunt.py:72 WORLD = [-58594, 58594) in both axes) at floor -50; the seed is hunt.py's
+# SCAN_REFERENCE (hunt.py:86), whose hut is chunk (-987, -1073)
+WHOLE_WORLD_SEED = 1473884015873122059
+WHOLE_WORLD_RECT = (-58594, 58594, -58594, 58594)
+
+
+def whole_world_measure(eng, opts) -> dict:
+    """One seed over the whole world through wg_seed_check (host API, survivors back to the host),
+    wall clock around the call after one warm-up call on a small rect."""
+    eng.seed_check(seeds=[WHOLE_WORLD_SEED], rect=(-64, 64, -64, 64), max_height=MAX_HEIGHT, opts=opts)
+    t0 = time.perf_counter()
+    res = eng.seed_check(seeds=[WHOLE_WORLD_SEED], rect=WHOLE_WORLD_RECT, max_height=MAX_HEIGHT, opts=opts)
+    secs = time.perf_counter() - t0
+    r = WHOLE_WORLD_RECT
+    n = (r[1] - r[0]) * (r[3] - r[2])
+    got = {(int(c["chunk_x"]), int(c["chunk_z"])) for c in res.candidates}
+    return {"seed": WHOLE_WORLD_SEED, "rect": list(r), "regions": n, "seconds": secs, "checks_per_s": n / secs,
+            "phase1_survivors": len(res.candidates), "reference_hut_found": (-987, -1073) in got,
+            "gpu_ms": res.stats.get("gpu_ms") if isinstance(res.stats, dict) else None,
+            "reference": "the reference's GPU stage on this workload: 58.4 s on a 20-SM laptop GPU "
+                         "(docs/HUNT54.txt), about 9.7 s per seed on a 188-SM GPU "
+                         "(docs/OPTIMIZATION_NOTES.txt as docs/HUNT54.txt quotes it)",
+            "timing": "wall clock around wg_seed_check (host seed in, phase-1 survivors out)"}
+
+
 def deep_measure(eng, opts) -> dict:
     """Deep Dive: the region walk (structure seeds x regions -> huts on mineshaft start chunks)
     and the terrain stage (each spot's 65,536 upper-bit world seeds through phase 1 at -54),
@@ -569,6 +595,8 @@ def main() -> None:
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-jobs", action="store_true", help="skip the batched-jobs and serving measurements")
+    ap.add_argument("--whole-world-only", action="store_true",
+                    help="only hunt.py's per-seed workload: one seed over the whole +-30M world")
     ap.add_argument("--phase2-only", action="store_true",
                     help="one phase-1 pass for its survivors, then only the phase-2 measurement (a short "
                          "command for profiling the phase-2 kernels)")
@@ -604,6 +632,14 @@ def main() -> None:
     seeds_host = torch.empty(N_SEEDS, dtype=torch.int64, pin_memory=True)
     seeds_np = seeds_host.numpy()
     seeds_np[:] = splitmix_seeds(first, N_SEEDS)
+    if args.whole_world_only:
+        if rank == 0:
+            print(json.dumps({"whole_world": whole_world_measure(eng, opts)}), flush=True)
+        eng.close()
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.phase2_only:
         res = eng.seed_check(seeds=seeds_np, rect=RECT, max_height=MAX_HEIGHT, opts=opts)
         line = {"phase2": phase2_measure(eng, res.candidates, opts, cpu=False)}
@@ -748,6 +784,7 @@ def main() -> None:
             nc["same_hits_and_funnel"] = bool(nc["same_hits_and_funnel"] and np.array_equal(hits_other, hits_headline))
             line["noise_core"] = nc
         line["phase2"] = phase2_measure(eng, res.candidates, opts, cpu=(world == 1 and not args.no_cpu_baseline))
+        line["whole_world"] = whole_world_measure(eng, opts)
         line["deep_dive"] = deep_measure(eng, opts)
         line["biome_map"] = biome_measure(eng)
         if world == 1 and not args.no_jobs:
