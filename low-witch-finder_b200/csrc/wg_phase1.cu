@@ -634,6 +634,7 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
             } else if constexpr (F32) {
                 const Y0Table y0a = y0_table(S, iu, 0), y0b = y0_table(S, iu, 1);
                 const float cf0 = st.cf[0], cf1 = st.cf[1], lo1 = st.lo[1], hi1 = st.hi[1];
+#pragma unroll 1   // one copy of the sample code: the chunk loop cycles through every phase
                 for (int r = 0; r < kTrips; r++) {
                     const int q = tid + r * kThreadsA;
                     const uint32_t jl = (uint32_t)(q / kUnits);
@@ -658,6 +659,7 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
                     tier0_decide(valid, jl, sum, pass, xc, zc);
                 }
             } else {
+#pragma unroll 1   // one copy of the sample code: the chunk loop cycles through every phase
                 for (int r = 0; r < kTrips; r++) {
                     const int q = tid + r * kThreadsA;
                     const uint32_t jl = (uint32_t)(q / kUnits);
@@ -680,61 +682,53 @@ __global__ void __launch_bounds__(kThreadsA, 2) climate_kernel(BatchArgs a) {
 
         // ---- the remaining erosion tiers, breadth first over the warp's list: every listed region
         // takes erosion step k (one sample with the step's slot and constants), its tier check, and
-        // the survivors are compacted in place for step k + 1 (items held in registers between two
-        // __syncwarp) ----
+        // the survivors are compacted in place for step k + 1 ----
         if (!a.single_biome) {
-            constexpr int kPer = (kWarpList + 31) / 32;
 #pragma unroll 1
             for (int k = 2; n && k < kClimateSteps && st.act[k] != ACT_NONE && st.act[k] <= ACT_TIER_LAST; k++) {
                 const double c1 = st.c1[k], c2 = st.c2[k], amp = st.amp[k], thr = st.thr[k];
                 const float cf = st.cf[k], lo = st.lo[k], hi = st.hi[k];
                 const int tier = st.tier[k];
-                uint32_t ke[kPer];
-                Real ks[kPer];
-#pragma unroll
-                for (int r = 0; r < kPer; r++) {
-                    const uint32_t q = (uint32_t)lane + (uint32_t)(r * 32);
-                    ke[r] = 0xFFFFFFFFu;
-                    ks[r] = 0;
-                    if (q >= n) continue;
-                    const uint32_t e = wl[q];
-                    const int iu = (int)(e >> 16);
-                    double xc, zc;
-                    climate_point(S, iu, e & 0xFFFFu, xc, zc);
-                    bool reject;
-                    Real sum;
-                    if constexpr (F32) {
-                        sum = __fmaf_rn(cf, climate_sample_f32<SMALL>(S, iu, k, xc, zc), wsum[q]);
-                        if (!all_rechecks && sum < lo) {
-                            reject = true;
-                        } else if (!all_rechecks && sum >= hi) {
-                            reject = false;
-                        } else {   // inside the error band: the exact partial sum of steps 0..k
-                            rechecks++;
-                            reject = climate_sum64(S, iu, 0, k, xc, zc) * amp < thr;
-                        }
-                    } else {
-                        sum = wsum[q];
-                        sum += (c1 * climate_sample(S, iu, k, xc, zc)) * c2;
-                        reject = sum * amp < thr;
-                    }
-                    if (reject) {
-                        erosion_reject(S, a, tc, iu, c0 + (e & 0xFFFFu), tier);
-                    } else {
-                        ke[r] = e;
-                        ks[r] = sum;
-                    }
-                }
-                __syncwarp();   // every read of this step's list is done
+                // rounds of 32 items, compacted as they go: round b's survivors land at
+                // [nn, nn + kept) <= b + 32, on items every lane has read already (__syncwarp
+                // between the reads and the writes), never on a later round's items
                 uint32_t nn = 0;
-#pragma unroll
-                for (int r = 0; r < kPer; r++) {
-                    const bool keep = ke[r] != 0xFFFFFFFFu;
+#pragma unroll 1
+                for (uint32_t b = 0; b < n; b += 32) {
+                    const uint32_t q = b + (uint32_t)lane;
+                    bool keep = false;
+                    uint32_t e = 0;
+                    Real sum = 0;
+                    if (q < n) {
+                        e = wl[q];
+                        const int iu = (int)(e >> 16);
+                        double xc, zc;
+                        climate_point(S, iu, e & 0xFFFFu, xc, zc);
+                        bool reject;
+                        if constexpr (F32) {
+                            sum = __fmaf_rn(cf, climate_sample_f32<SMALL>(S, iu, k, xc, zc), wsum[q]);
+                            if (!all_rechecks && sum < lo) {
+                                reject = true;
+                            } else if (!all_rechecks && sum >= hi) {
+                                reject = false;
+                            } else {   // inside the error band: the exact partial sum of steps 0..k
+                                rechecks++;
+                                reject = climate_sum64(S, iu, 0, k, xc, zc) * amp < thr;
+                            }
+                        } else {
+                            sum = wsum[q];
+                            sum += (c1 * climate_sample(S, iu, k, xc, zc)) * c2;
+                            reject = sum * amp < thr;
+                        }
+                        if (reject) erosion_reject(S, a, tc, iu, c0 + (e & 0xFFFFu), tier);
+                        else keep = true;
+                    }
                     const unsigned m = __ballot_sync(0xFFFFFFFFu, keep);
+                    __syncwarp();   // every lane has read its item of this round
                     if (keep) {
                         const uint32_t at = nn + (uint32_t)__popc(m & lanes_below);
-                        wl[at] = ke[r];
-                        wsum[at] = ks[r];
+                        wl[at] = e;
+                        wsum[at] = sum;
                     }
                     nn += (uint32_t)__popc(m);
                 }
