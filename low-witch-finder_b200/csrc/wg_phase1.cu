@@ -309,7 +309,9 @@ __device__ __forceinline__ void climate_reject(Sm &S, const BatchArgs &a, int iu
 // Erosion rejections are counted per thread in registers (16-bit fields, tiers 0-3 and 4-6) and
 // added to the histogram once at the end; a shared counter hit by most lanes of a warp at once
 // would serialise.  A field cannot overflow: per chunk a thread rejects at most 6 regions in the
-// tier-0 pass and at most kTierList (768) afterwards, over at most 43 chunks (4,096 / 96).
+// tier-0 pass, at most 4 in each of the 6 later erosion steps (a warp's list holds <= kWarpList
+// = 112 regions, 4 rounds of 32) and at most 6 in its own walks of a full list's overflow, over at
+// most 43 chunks (4,096 / 96).
 struct TierCounts {
     uint64_t lo = 0, hi = 0;
     __device__ __forceinline__ void add(int tier) {
@@ -1501,7 +1503,7 @@ __device__ __forceinline__ double combine_vals(int noise, const double *v, int s
     return (a + b) * ns.amplitude;
 }
 
-__global__ void __launch_bounds__(kThreadsC) ladder_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(kThreadsC, 10) ladder_kernel(BatchArgs a) {
     __shared__ __align__(16) LadderSmem S;
     batch_range(a);
     const int t = threadIdx.x;

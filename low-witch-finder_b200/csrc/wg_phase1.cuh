@@ -13,8 +13,9 @@
 //                           (97% of climate survivors stop here).
 // Both hot kernels use ~100 KiB of shared memory, so two CTAs share an SM and one CTA's table
 // build overlaps the other's evaluation.
-//   ladder   the rest       one CTA per remaining candidate builds all 54 cave / continent /
-//                           floodedness Perlins and finishes the ladder in lysh's order.
+//   ladder   the rest       one 64-thread CTA per remaining candidate builds all 54 cave /
+//                           continent / floodedness Perlins (54 of its 64 threads build, ~10 CTAs
+//                           per SM) and finishes the ladder in lysh's order.
 #pragma once
 
 #include <cstdint>
@@ -46,11 +47,9 @@ constexpr int kSlotsB = 18;         // cave_entrance 6 + six one-octave spaghett
 constexpr int kSlotsC = 54;         // kSlotsB + cave_layer 2 + cave_cheese 14 + continentalness 18 + floodedness 2
 constexpr int kThreadsA = kSlotsA * kUnits;   // one thread per (slot, unit) table
 constexpr int kThreadsB = kSlotsB * kUnits;
-constexpr int kThreadsC = 128;
+constexpr int kThreadsC = 64;
 constexpr int kRecordCap = 64;      // survivors held per unit record in the climate kernel
 constexpr int kChunk = 96;          // regions per unit whose hut positions are staged at a time
-constexpr int kClimateList = 128;   // erosion survivors per chunk finished in parallel (temperature, ridge)
-constexpr int kTierList = 768;      // tier-0 survivors per chunk carried into the remaining erosion tiers
 
 // Counter block written by the kernels (one per engine, reset per batch).
 enum : int {
