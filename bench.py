@@ -65,6 +65,9 @@ OPS_Y0_SAMPLE = 244          # FP64 y=0 sample: 14 table lookups, 62 FP64 ops (x
 OPS_Y0_SAMPLE_F32 = 56 + 32 + 24 + 51 + 1
 # 3-D FP64 sample of the cave noises: 14 lookups (x4), 96 FP64 ops (x2), 24 gradient-component loads
 OPS_3D_SAMPLE = 56 + 192 + 24
+# the same in the FP32 core: 14 lookups (x4), the FP64 coordinate scaling and reduction (27 FP64 ops
+# x2), 24 gradient-component loads, 56 FP32 ops (3 offsets, 8 gradients x3, 3 fades x5, 7 lerps x2)
+OPS_3D_SAMPLE_F32 = 56 + 54 + 24 + 56
 OPS_REGION = 40              # java.util.Random placement (2 x nextInt(24)) + coordinates
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, from ncu on `bench.py --profile 1048576`
 # (one launch of each kernel on 2^20 seeds read from a list in HBM; a 2^24-seed step runs 16 such
@@ -100,11 +103,12 @@ def climate_work(st: dict, n_seeds: int, n_regions: int, fp32: bool) -> tuple[fl
     return float(ops), float(nbytes)
 
 
-def entrance_work(st: dict) -> float:
+def entrance_work(st: dict, fp32: bool) -> float:
     """Lane-ops of the entrance kernel: 18 tables per record (a seed unit with climate survivors),
     36 3-D samples per survivor (18 slots at y = 50 and 60) plus its 12 octave sums and decision."""
     n_rec, n_surv = st["records"], st["climate_survivors"]
-    return float(n_rec * 18 * OPS_PERLIN_BUILD + n_surv * (36 * OPS_3D_SAMPLE + 12 * 40 + 120))
+    sample = OPS_3D_SAMPLE_F32 if fp32 else OPS_3D_SAMPLE
+    return float(n_rec * 18 * OPS_PERLIN_BUILD + n_surv * (36 * sample + 12 * 40 + 120))
 
 
 class ClockSampler:
@@ -520,32 +524,33 @@ def profile_case(wg, eng, opts, args, local: int) -> None:
 
 
 def noise_core_measure(wg, eng, args, step_device, stream, flush, headline: dict) -> dict:
-    """The other noise core on the same device-resident step: seeds/s of both, their ratio, whether
-    the hit sets and funnels agree, how often the FP32 core re-took a gate in FP64, and the measured
-    |FP32 - FP64| of each climate noise (wg_noise_probe, 256 seeds x 4,096 climate points)."""
+    """The other noise cores on the same device-resident step: seeds/s of each, the FP32 / FP64
+    ratio, whether the hit sets and funnels agree, how often the FP32 core re-took a gate in FP64,
+    and the measured |FP32 - FP64| of each climate noise and each cave noise of the entrance gate
+    (wg_noise_probe, wg_noise_probe_3d)."""
     import torch
-    other = "fp64" if args.noise_core == "fp32" else "fp32"
-    eng.set_noise_core(other)
-    for _ in range(args.warmup):
-        step_device()
-    times = []
-    found, st = 0, {}
-    for _ in range(args.steps):
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        found, st = step_device()
-        e1.record(stream)
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
+    runs = {args.noise_core: headline}
+    for other in [c for c in ("fp32", "fp64", "fp32_caves") if c != args.noise_core]:
+        eng.set_noise_core(other)
+        for _ in range(args.warmup):
+            step_device()
+        times = []
+        found, st = 0, {}
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            found, st = step_device()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms_other = sum(times) / len(times)
+        runs[other] = {"seeds_per_s": N_SEEDS / (ms_other / 1e3), "ms_per_step": ms_other, "found": found,
+                       "reject_hist": st["reject_hist"], "tier_hist": st["tier_hist"], "rechecks": st["rechecks"],
+                       "kernel_ms": st["kernel_ms"]}
     eng.set_noise_core(args.noise_core)
-    ms_other = sum(times) / len(times)
-    runs = {args.noise_core: headline, other: {"seeds_per_s": N_SEEDS / (ms_other / 1e3), "ms_per_step": ms_other,
-                                               "found": found, "reject_hist": st["reject_hist"],
-                                               "tier_hist": st["tier_hist"], "rechecks": st["rechecks"],
-                                               "kernel_ms": st["kernel_ms"]}}
-    same = (runs["fp32"]["found"] == runs["fp64"]["found"] and runs["fp32"]["reject_hist"] == runs["fp64"]["reject_hist"]
-            and runs["fp32"]["tier_hist"] == runs["fp64"]["tier_hist"])
+    same = all(runs[c]["found"] == runs["fp64"]["found"] and runs[c]["reject_hist"] == runs["fp64"]["reject_hist"]
+               and runs[c]["tier_hist"] == runs["fp64"]["tier_hist"] for c in runs)
     rng = np.random.default_rng(7)
     xz = (4 * rng.integers(-1_870_000, 1_870_000, size=(4096, 2)) + 2).astype(np.float64)
     seeds = [wg.splitmix64(GEN_BASE + i) for i in range(256)]
@@ -553,15 +558,24 @@ def noise_core_measure(wg, eng, args, step_device, stream, flush, headline: dict
     for noise in ("erosion", "temperature", "ridge", "continentalness"):
         v32, v64 = eng.noise_probe(seeds, noise, xz)
         err[noise] = float(np.abs(v32 - v64).max())
+    xyz = np.stack([16 * rng.integers(-1_870_000, 1_870_000, 4096) + 3, rng.choice([50, 60], 4096),
+                    16 * rng.integers(-1_870_000, 1_870_000, 4096) + 3], axis=1).astype(np.float64)
+    for noise in ("cave_entrance", "spaghetti_rarity", "spaghetti_thickness", "spaghetti_3d_1", "spaghetti_3d_2",
+                  "roughness_modulator", "roughness"):
+        v32, v64 = eng.noise_probe_3d(seeds, noise, xyz)
+        err[noise] = float(np.abs(v32 - v64).max())
     scanned = N_SEEDS * (RECT[1] - RECT[0]) * (RECT[3] - RECT[2])
-    return {"fp32": runs["fp32"], "fp64": runs["fp64"],
+    return {"fp32": runs["fp32"], "fp64": runs["fp64"], "fp32_caves": runs["fp32_caves"],
             "fp32_over_fp64": runs["fp64"]["ms_per_step"] / runs["fp32"]["ms_per_step"],
+            "fp32_caves_over_fp64": runs["fp64"]["ms_per_step"] / runs["fp32_caves"]["ms_per_step"],
             "same_hits_and_funnel": bool(same),
             "recheck_fraction": runs["fp32"]["rechecks"] / scanned,
             "max_abs_err": err,
-            "max_abs_err_note": ("|FP32 core - FP64| of each y = 0 climate noise over 256 seeds x 4,096 climate points; "
-                                 "the cave densities (entrance, spaghetti, cheese) and phase 2 run in FP64 only, so "
-                                 "their error is 0 by construction"),
+            "max_abs_err_note": ("|FP32 core - FP64| of each y = 0 climate noise over 256 seeds x 4,096 climate points, "
+                                 "and of each 3-D cave noise of the entrance gate over 256 seeds x 4,096 hut blocks "
+                                 "(x, z up to +-3e7, y 50 / 60); the ladder's noises (cheese, cave layer, "
+                                 "continentalness at the hut, floodedness) and phase 2 run in FP64 only, so their "
+                                 "error is 0 by construction"),
             "bound": "the step's kernels; both cores on the same seeds, CUDA events per step"}
 
 
@@ -600,8 +614,8 @@ def main() -> None:
     ap.add_argument("--phase2-only", action="store_true",
                     help="one phase-1 pass for its survivors, then only the phase-2 measurement (a short "
                          "command for profiling the phase-2 kernels)")
-    ap.add_argument("--noise-core", choices=("fp32", "fp64"), default="fp32",
-                    help="noise core of the headline (the other core is measured beside it)")
+    ap.add_argument("--noise-core", choices=("fp32", "fp64", "fp32_caves"), default="fp32",
+                    help="noise core of the headline (the other cores are measured beside it)")
     ap.add_argument("--profile", type=int, default=0, metavar="SEEDS",
                     help="profiling case only: the headline step on SEEDS device-resident seeds, --warmup "
                          "untimed steps then --steps steps, no other measurement (a short command for ncu)")
@@ -720,14 +734,15 @@ def main() -> None:
         sm_count = torch.cuda.get_device_properties(local).multi_processor_count
         max_mhz = float(peaks.get("sm_max_mhz", 1965.0))
         peak_ops = sm_count * 128 * max_mhz * 1e6
-        fp32 = args.noise_core == "fp32"
+        fp32 = args.noise_core in ("fp32", "fp32_caves")
         ops, nbytes = climate_work(stats, N_SEEDS, n_regions, fp32)
         launch_ms = kernel_ms[0] / max(1, kernel_launches[0])
         ops_per_launch = ops / max(1, stats["kernel_launches"][0])
         bytes_per_launch = nbytes / max(1, stats["kernel_launches"][0])
         achieved = ops_per_launch / (launch_ms / 1e3)
         ent_ms = kernel_ms[1] / max(1, kernel_launches[1])
-        ent_ops = entrance_work(stats) / max(1, stats["kernel_launches"][1])
+        caves32 = args.noise_core == "fp32_caves"   # the cave samples are FP32 only in that core
+        ent_ops = entrance_work(stats, caves32) / max(1, stats["kernel_launches"][1])
         hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
         cs = clocks.summary()
         headline = {"seeds_per_s": value, "ms_per_step": total_ms / args.steps, "found": found,
@@ -773,13 +788,15 @@ def main() -> None:
                     "launch_ms": ent_ms, "traffic": TRAFFIC["entrance_kernel"], "traffic_unit": "bytes per launch",
                     "ncu_pipes": dict(PIPES["entrance_kernel"], unit=PIPES["unit"]),
                     "ops_model": ("18 Perlin tables per record x 7,160 lane-ops, per climate survivor 36 3-D samples "
-                                  f"x {OPS_3D_SAMPLE} lane-ops + 600 for the octave sums and the decision")},
+                                  f"x {OPS_3D_SAMPLE_F32 if caves32 else OPS_3D_SAMPLE} lane-ops + 600 for the octave "
+                                  "sums and the decision")},
             },
             "clocks": cs,
         }
         if world == 1:
             nc = noise_core_measure(wg, eng, args, step_device, stream, flush, headline)
-            other = "fp64" if fp32 else "fp32"
+            # the output buffer holds the last core measured
+            other = [c for c in ("fp32", "fp64", "fp32_caves") if c != args.noise_core][-1]
             hits_other = sorted_hits(wg, out_dev, nc[other]["found"])
             nc["same_hits_and_funnel"] = bool(nc["same_hits_and_funnel"] and np.array_equal(hits_other, hits_headline))
             line["noise_core"] = nc

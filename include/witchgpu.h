@@ -75,18 +75,25 @@ void wg_engine_close(wg_engine *e);
 /* Message of the engine's last failure ("" if none). */
 const char *wg_engine_error(const wg_engine *e);
 
-/* Noise core of the phase-1 climate gates (erosion tiers, temperature, ridge).
- *   WG_NOISE_FP32 (the default): samples in FP32 after an FP64 coordinate reduction, gates
- *     decided from the FP32 sums outside a derived error band and re-taken in FP64 inside it,
- *     so every verdict equals the FP64 path's; wg_scan_stats.rechecks counts the re-takes.
+/* Noise core of the phase-1 gates.
+ *   WG_NOISE_FP32 (the default): the climate gates' samples (erosion tiers, temperature, ridge)
+ *     in FP32 after an FP64 coordinate reduction, gates decided from the FP32 sums outside a
+ *     derived error band and re-taken in FP64 inside it, so every verdict equals the FP64 path's;
+ *     wg_scan_stats.rechecks counts the re-takes.  The cave gates sample in FP64.
  *   WG_NOISE_FP64: every sample in FP64 in the reference's operation order.
- *   WG_NOISE_FP32_RECHECK_ALL: the FP32 core with every gate re-taken in FP64, a check mode that
- *     runs the recheck path on every decision (slow; for tests of that path).
+ *   WG_NOISE_FP32_CAVES: WG_NOISE_FP32 plus the entrance gate's 3-D cave samples in FP32 (the
+ *     tunnel-scale interval and Entrance(50) / Entrance(60) re-taken in FP64 inside their error
+ *     bands).  Same verdicts; not the default because on a B200 it is slower at 9 x 9 regions per
+ *     seed (the FP64 pipe is not what bounds that kernel) and only slightly faster on whole-world
+ *     scans.
+ *   WG_NOISE_FP32_RECHECK_ALL: WG_NOISE_FP32_CAVES with every gate re-taken in FP64, a check mode
+ *     that runs the recheck paths on every decision (slow; for tests of those paths).
  * The reference has the same choice as a build flag, without the recheck
  * (PHASE1_FP32_CORE, engine/gpu/low54/device_noise.h:132-160).  WG_ERR_ARG for other values. */
 #define WG_NOISE_FP32 0
 #define WG_NOISE_FP64 1
 #define WG_NOISE_FP32_RECHECK_ALL 2
+#define WG_NOISE_FP32_CAVES 3
 int wg_engine_set_noise_core(wg_engine *e, int core);
 
 /* The FP32 core's measured error: out64[b * n_points + i] = the y = 0 DoublePerlin value of climate
@@ -97,6 +104,15 @@ int wg_engine_set_noise_core(wg_engine *e, int core);
  * buffers; n_seeds * n_points <= 2^26. */
 int wg_noise_probe(wg_engine *e, const int64_t *seeds, uint64_t n_seeds, int noise, const double *xz,
                    uint64_t n_points, double *out32, double *out64);
+
+/* The same for the 3-D cave noises the entrance gate samples in the FP32 core: out64[...] = the
+ * DoublePerlin value of `noise` in world seeds[b] at noise-space point (xyz[3i], xyz[3i + 1],
+ * xyz[3i + 2]) in FP64 (the reference's lysh_dblnoise_sample, engine/tools/lysh/src/noise.c:263-289),
+ * out32[...] = the same value from the FP32 core's octave samples.  noise: 7 cave_entrance,
+ * 8 spaghetti_rarity, 9 spaghetti_thickness, 10 spaghetti_3d_1, 11 spaghetti_3d_2,
+ * 12 roughness_modulator, 13 roughness.  Host buffers; n_seeds * n_points <= 2^26. */
+int wg_noise_probe_3d(wg_engine *e, const int64_t *seeds, uint64_t n_seeds, int noise, const double *xyz,
+                      uint64_t n_points, double *out32, double *out64);
 
 /* lysh's --version / --preset names -> option bits
  * (engine/tools/lysh/src/main.c:104-132).  0 on success, WG_ERR_ARG if unknown.  Each sets only

@@ -58,11 +58,15 @@ class Stats(C.Structure):
 
 
 # wg_engine_set_noise_core values
-NOISE_FP32, NOISE_FP64, NOISE_FP32_RECHECK_ALL = 0, 1, 2
-NOISE_CORES = {"fp32": NOISE_FP32, "fp64": NOISE_FP64, "fp32_recheck_all": NOISE_FP32_RECHECK_ALL}
+NOISE_FP32, NOISE_FP64, NOISE_FP32_RECHECK_ALL, NOISE_FP32_CAVES = 0, 1, 2, 3
+NOISE_CORES = {"fp32": NOISE_FP32, "fp64": NOISE_FP64, "fp32_recheck_all": NOISE_FP32_RECHECK_ALL,
+               "fp32_caves": NOISE_FP32_CAVES}
 # wg_noise_probe noise ids (the catalog's NoiseId order)
 PROBE_NOISES = {"erosion": 0, "temperature": 1, "ridge": 2, "continentalness": 3, "erosion_large": 4,
                 "temperature_large": 5, "continentalness_large": 6}
+# wg_noise_probe_3d noise ids: the entrance gate's cave noises
+PROBE_NOISES_3D = {"cave_entrance": 7, "spaghetti_rarity": 8, "spaghetti_thickness": 9, "spaghetti_3d_1": 10,
+                   "spaghetti_3d_2": 11, "roughness_modulator": 12, "roughness": 13}
 
 
 CANDIDATE_DTYPE = np.dtype([("seed_index", "<u8"), ("seed", "<i8"), ("rx", "<i4"), ("rz", "<i4"),
@@ -70,6 +74,7 @@ CANDIDATE_DTYPE = np.dtype([("seed_index", "<u8"), ("seed", "<i8"), ("rx", "<i4"
 
 # Every symbol include/witchgpu.h declares.
 EXPORTS = ("wg_engine_open", "wg_engine_close", "wg_engine_error", "wg_engine_set_noise_core", "wg_noise_probe",
+           "wg_noise_probe_3d",
            "wg_parse_version", "wg_parse_preset",
            "wg_seed_check", "wg_seed_check_device", "wg_phase1_codes", "wg_seed_check_noalloc",
            "wg_eval_huts", "wg_grade_scan", "wg_p2_probe", "wg_deep_starts", "wg_deep_sweep", "wg_deep_spots",
@@ -206,6 +211,7 @@ def library() -> C.CDLL:
     lib.wg_engine_error.restype = C.c_char_p
     lib.wg_engine_set_noise_core.argtypes = [vp, i32]
     lib.wg_noise_probe.argtypes = [vp, vp, u64, i32, vp, u64, vp, vp]
+    lib.wg_noise_probe_3d.argtypes = [vp, vp, u64, i32, vp, u64, vp, vp]
     lib.wg_parse_version.argtypes = [C.c_char_p, C.POINTER(Opts)]
     lib.wg_parse_preset.argtypes = [C.c_char_p, C.POINTER(Opts)]
     common = [vp, vp, u64, u64, C.POINTER(Opts), i32, i32, i32, i32, i32, i32]
@@ -285,7 +291,9 @@ class Engine:
         self.set_noise_core(noise_core)
 
     def set_noise_core(self, core: str) -> None:
-        """'fp32' (FP32 climate samples, FP64 recheck inside the error band; the default) or 'fp64'."""
+        """'fp32' (FP32 climate samples, FP64 recheck inside the error band; the default), 'fp64',
+        'fp32_caves' ('fp32' plus the entrance gate's cave samples in FP32) or 'fp32_recheck_all'
+        (the check mode: 'fp32_caves' with every decision re-taken in FP64)."""
         if core not in NOISE_CORES:
             raise ValueError(f"unknown noise core {core!r}")
         rc = library().wg_engine_set_noise_core(self._h, NOISE_CORES[core])
@@ -368,6 +376,20 @@ class Engine:
                                       len(pts), v32.ctypes.data, v64.ctypes.data)
         if rc != WG_OK:
             raise self._err(rc, "wg_noise_probe")
+        return v32, v64
+
+    def noise_probe_3d(self, seeds, noise: str, xyz) -> tuple[np.ndarray, np.ndarray]:
+        """(fp32, fp64) DoublePerlin values of a cave noise of the entrance gate, [n_seeds, n_points]
+        float64: the FP32 core's samples summed as the entrance kernel sums them, beside the
+        reference's FP64 value at noise-space points xyz [n, 3]."""
+        s = as_seed_array(seeds)
+        pts = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        v32 = np.empty((len(s), len(pts)), np.float64)
+        v64 = np.empty((len(s), len(pts)), np.float64)
+        rc = library().wg_noise_probe_3d(self._h, s.ctypes.data, len(s), PROBE_NOISES_3D[noise], pts.ctypes.data,
+                                         len(pts), v32.ctypes.data, v64.ctypes.data)
+        if rc != WG_OK:
+            raise self._err(rc, "wg_noise_probe_3d")
         return v32, v64
 
     def phase1_codes(self, seeds=None, gen=None, rect=(-4, 5, -4, 5), max_height: int = -50,

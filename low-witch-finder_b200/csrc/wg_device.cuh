@@ -491,6 +491,57 @@ __device__ __forceinline__ float perlin_y0_f32(const T &P, double ox, double oz,
     return lerp_f32(fz, y0, y1);
 }
 
+// fade_f32 on one lane: 1/2 + s (15/8 + s^2 (6 s^2 - 5)), s = t - 1/2 (fade_f32x2's operations)
+__device__ __forceinline__ float fade_f32(float t) {
+    const float s = __fadd_rn(t, -0.5f);
+    const float s2 = __fmul_rn(s, s);
+    const float p = __fmaf_rn(6.0f, s2, -5.0f);
+    const float q = __fmaf_rn(s2, p, 1.875f);
+    return __fmaf_rn(s, q, 0.5f);
+}
+
+// One Perlin sampler in 3-D (y_scale = y_max = 0, noise.c:246-261) in the FP32 core: the three
+// coordinate reductions in FP64 as perlin_3d (d = x + ox, its floor, the exact fraction), the rest
+// in FP32 with perlin_y0_f32's operations, the y fraction H = rn(h) and its fade now per sample.
+// Error against the exact sample (same lattice cell and hashes), in the terms of the bound above
+// perlin_y0_f32: G, L, H within u/2 and G - 1, L - 1, H - 1 within u; FX, FY, FZ within 4 u; a
+// corner dot within 3 u; x lerps 3 u + 4 * 4 u + 2 u = 21 u; y lerps 21 u + 4 * 4 u + 2 u = 39 u
+// (the fade of y now carries 4 u instead of u/2); z lerp 39 u + 4 * 4 u + 2 u = 57 u.  So
+// |FP32 sample - exact| <= 60 u (kPerlin3dF32ErrUlps) with |sample| <= 2.
+template <class T>
+__device__ __forceinline__ float perlin_3d_f32(const T &P, double ox, double oy, double oz, double x, double y,
+                                               double z) {
+    const double d = x + ox, e = y + oy, f = z + oz;
+    const double fd = floor(d), fe = floor(e), ff = floor(f);
+    const int i = (int)fd, j = (int)fe, k = (int)ff;
+    const float g = __double2float_rn(d - fd), h = __double2float_rn(e - fe), l = __double2float_rn(f - ff);
+    const F2 gl = f2(g, l);
+    float g1, l1;
+    f2_split(f2_add(gl, f2(-1.0f, -1.0f)), g1, l1);   // g - 1, l - 1
+    const float h1 = __fsub_rn(h, 1.0f);
+    int a, b, c, dd, ee, e2;
+    P.pair(i, a, b);
+    P.pair(a + j, c, dd);
+    P.pair(b + j, ee, e2);
+    int h000, h001, h100, h101, h010, h011, h110, h111;
+    P.pair(c + k, h000, h001);
+    P.pair(ee + k, h100, h101);
+    P.pair(dd + k, h010, h011);
+    P.pair(e2 + k, h110, h111);
+    const F2 v00 = f2(P.grad(h000, g, h, l), P.grad(h001, g, h, l1));      // (v000, v001)
+    const F2 v10 = f2(P.grad(h100, g1, h, l), P.grad(h101, g1, h, l1));    // (v100, v101)
+    const F2 v01 = f2(P.grad(h010, g, h1, l), P.grad(h011, g, h1, l1));    // (v010, v011)
+    const F2 v11 = f2(P.grad(h110, g1, h1, l), P.grad(h111, g1, h1, l1));  // (v110, v111)
+    float fx, fz;
+    f2_split(fade_f32x2(gl), fx, fz);
+    const float fy = fade_f32(h);
+    const F2 x0 = lerp_f32x2(f2(fx, fx), v00, v10);    // (x00, x01)
+    const F2 x1 = lerp_f32x2(f2(fx, fx), v01, v11);    // (x10, x11)
+    float y0, y1;
+    f2_split(lerp_f32x2(f2(fy, fy), x0, x1), y0, y1);
+    return lerp_f32(fz, y0, y1);
+}
+
 constexpr double kDblScale = 1.0181268882175227;
 
 // Java Math.min / Math.max with the signed-zero rules (mcmath.h).

@@ -422,25 +422,33 @@ void wg_engine_close(wg_engine *eng) {
 
 const char *wg_engine_error(const wg_engine *eng) { return eng ? eng->err.c_str() : "no engine"; }
 
-int wg_noise_probe(wg_engine *eng, const int64_t *seeds, uint64_t n_seeds, int noise, const double *xz,
-                   uint64_t n_points, double *out32, double *out64) {
-    if (!eng || !seeds || !xz || !out32 || !out64 || n_seeds == 0 || n_points == 0 || noise < 0 ||
-        noise > N_CONTINENTALNESS_LARGE || n_seeds > (1u << 20) || n_points > (1u << 20) ||
-        n_seeds * n_points > (1ull << 26))
+// wg_noise_probe / wg_noise_probe_3d: dims = 2 (x, z points, y = 0 climate noises) or 3 (x, y, z
+// points, the entrance kernel's cave noises).
+static int noise_probe(wg_engine *eng, const int64_t *seeds, uint64_t n_seeds, int noise, const double *pts,
+                       uint64_t n_points, double *out32, double *out64, int dims) {
+    const bool ok_noise = dims == 2 ? (noise >= 0 && noise <= N_CONTINENTALNESS_LARGE)
+                                    : (noise >= N_CAVE_ENTRANCE && noise <= N_ROUGHNESS);
+    if (!eng || !seeds || !pts || !out32 || !out64 || n_seeds == 0 || n_points == 0 || !ok_noise ||
+        n_seeds > (1u << 20) || n_points > (1u << 20) || n_seeds * n_points > (1ull << 26))
         return eng ? eng->fail(WG_ERR_ARG, "noise probe: bad noise id or sizes") : WG_ERR_ARG;
     WG_CUDA(cudaSetDevice(eng->device), "cudaSetDevice");
     int64_t *d_seeds = nullptr;
-    double *d_xz = nullptr, *d_out = nullptr;
+    double *d_pts = nullptr, *d_out = nullptr;
     const size_t n_out = (size_t)(n_seeds * n_points);
     int rc = [&]() -> int {
         WG_CUDA(cudaMalloc(&d_seeds, sizeof(int64_t) * n_seeds), "alloc");
-        WG_CUDA(cudaMalloc(&d_xz, sizeof(double) * 2 * n_points), "alloc");
+        WG_CUDA(cudaMalloc(&d_pts, sizeof(double) * dims * n_points), "alloc");
         WG_CUDA(cudaMalloc(&d_out, sizeof(double) * 2 * n_out), "alloc");
         WG_CUDA(cudaMemcpyAsync(d_seeds, seeds, sizeof(int64_t) * n_seeds, cudaMemcpyHostToDevice, eng->stream),
                 "copy");
-        WG_CUDA(cudaMemcpyAsync(d_xz, xz, sizeof(double) * 2 * n_points, cudaMemcpyHostToDevice, eng->stream), "copy");
-        launch_noise_probe(d_seeds, (uint32_t)n_seeds, noise, d_xz, (uint32_t)n_points, d_out, d_out + n_out,
-                           eng->stream);
+        WG_CUDA(cudaMemcpyAsync(d_pts, pts, sizeof(double) * dims * n_points, cudaMemcpyHostToDevice, eng->stream),
+                "copy");
+        if (dims == 2)
+            launch_noise_probe(d_seeds, (uint32_t)n_seeds, noise, d_pts, (uint32_t)n_points, d_out, d_out + n_out,
+                               eng->stream);
+        else
+            launch_noise_probe3d(d_seeds, (uint32_t)n_seeds, noise, d_pts, (uint32_t)n_points, d_out, d_out + n_out,
+                                 eng->stream);
         WG_CUDA(cudaGetLastError(), "noise probe launch");
         WG_CUDA(cudaMemcpyAsync(out32, d_out, sizeof(double) * n_out, cudaMemcpyDeviceToHost, eng->stream), "copy");
         WG_CUDA(cudaMemcpyAsync(out64, d_out + n_out, sizeof(double) * n_out, cudaMemcpyDeviceToHost, eng->stream),
@@ -449,15 +457,26 @@ int wg_noise_probe(wg_engine *eng, const int64_t *seeds, uint64_t n_seeds, int n
         return WG_OK;
     }();
     cudaFree(d_seeds);
-    cudaFree(d_xz);
+    cudaFree(d_pts);
     cudaFree(d_out);
     return rc;
 }
 
+int wg_noise_probe(wg_engine *eng, const int64_t *seeds, uint64_t n_seeds, int noise, const double *xz,
+                   uint64_t n_points, double *out32, double *out64) {
+    return noise_probe(eng, seeds, n_seeds, noise, xz, n_points, out32, out64, 2);
+}
+
+int wg_noise_probe_3d(wg_engine *eng, const int64_t *seeds, uint64_t n_seeds, int noise, const double *xyz,
+                      uint64_t n_points, double *out32, double *out64) {
+    return noise_probe(eng, seeds, n_seeds, noise, xyz, n_points, out32, out64, 3);
+}
+
 int wg_engine_set_noise_core(wg_engine *eng, int core) {
-    if (!eng || (core != WG_NOISE_FP32 && core != WG_NOISE_FP64 && core != WG_NOISE_FP32_RECHECK_ALL))
+    if (!eng || (core != WG_NOISE_FP32 && core != WG_NOISE_FP64 && core != WG_NOISE_FP32_RECHECK_ALL &&
+                 core != WG_NOISE_FP32_CAVES))
         return WG_ERR_ARG;
-    eng->fp32_core = core == WG_NOISE_FP64 ? 0 : (core == WG_NOISE_FP32 ? 1 : 2);
+    eng->fp32_core = core == WG_NOISE_FP64 ? 0 : (core == WG_NOISE_FP32 ? 1 : (core == WG_NOISE_FP32_CAVES ? 3 : 2));
     return WG_OK;
 }
 

@@ -146,6 +146,17 @@ struct SrcCols {  // byte-interleaved blocks of kUnits columns, origins [slot][u
         return perlin_3d(T, ox[o], oy[o], oz[o], x, y, z);
     }
 };
+struct SrcColsF {  // the same columns read by the FP32 core (row 256 of every column = row 0)
+    const uint8_t *perm;
+    const double *ox, *oy, *oz;
+    const GradF *gf;
+    int unit;
+    __device__ __forceinline__ float p3(int slot, double x, double y, double z) const {
+        ColTableF<kUnits> T{perm + slot * kPitch + unit, gf};
+        int o = slot * kUnits + unit;
+        return perlin_3d_f32(T, ox[o], oy[o], oz[o], x, y, z);
+    }
+};
 struct SrcFlat {  // the ladder's block: table of slot s in column s, origins [slot][3]
     const uint8_t *perm;
     const double *org;
@@ -217,6 +228,14 @@ __device__ double cheese(const S &src, int x, int y, int z) {
     double av = 4.0 * layer * layer;
     double raw = dbl3d(src, N_CAVE_CHEESE, kBaseCheese, (double)x, (double)y * 0.6666666666666666, (double)z);
     return av + clampd(0.27 + raw, -1.0, 1.0);
+}
+
+// FP32 core: the reference's FP64 values, for an entrance decision or a tunnel-scale interval
+// whose FP32-core value lies inside its error band (kept out of line: the rare path).
+__device__ __noinline__ double entrance64(SrcCols src, int x, int y, int z) { return entrance(src, x, y, z); }
+__device__ __noinline__ double rarity64(SrcCols src, int x, int y, int z) {
+    return dbl3d(src, N_SPAGHETTI_RARITY, kBaseRarity, (double)(int)((uint32_t)x * 2u), (double)y,
+                 (double)(int)((uint32_t)z * 2u));
 }
 
 // ------------------------------------------------------------------------------------
@@ -903,7 +922,8 @@ static void allow_dynamic_smem(K kernel, size_t bytes, unsigned long long &done_
     if (dev >= 0 && dev < 64) done_mask |= 1ull << dev;
 }
 
-static unsigned long long g_smem_done64 = 0, g_smem_done32 = 0, g_smem_done32s = 0, g_smem_done_ent = 0;
+static unsigned long long g_smem_done64 = 0, g_smem_done32 = 0, g_smem_done32s = 0, g_smem_done_ent = 0,
+                          g_smem_done_ent32 = 0;
 
 void launch_climate(const BatchArgs &a, cudaStream_t s) {
     int grid = (int)((a.n_units + kUnits - 1) / kUnits);
@@ -984,6 +1004,66 @@ __global__ void __launch_bounds__(kProbeThreads) noise_probe_kernel(const int64_
 void launch_noise_probe(const int64_t *d_seeds, uint32_t n_seeds, int noise, const double *d_xz, uint32_t n_points,
                         double *d_out32, double *d_out64, cudaStream_t s) {
     noise_probe_kernel<<<n_seeds, kProbeThreads, 0, s>>>(d_seeds, noise, d_xz, n_points, d_out32, d_out64);
+}
+
+// The same probe for the entrance kernel's 3-D cave noises: DoublePerlin `noise` of seeds[b] at
+// the points xyz, in FP64 in the reference's order (dbl3d, noise.c:263-289) and from the FP32
+// core's samples (perlin_3d_f32) summed in FP64 as the entrance kernel sums them.
+__global__ void __launch_bounds__(kProbeThreads) noise_probe3d_kernel(const int64_t *seeds, int noise,
+                                                                       const double *xyz, uint32_t n_points,
+                                                                       double *out32, double *out64) {
+    __shared__ __align__(16) uint8_t perm[257 * kProbeStride];   // row 256 = row 0 (ColTableF)
+    __shared__ double ox[2 * kMaxOct], oy[2 * kMaxOct], oz[2 * kMaxOct];
+    __shared__ uint32_t grad[kGradWords];
+    __shared__ GradF gf;
+    const int t = threadIdx.x;
+    const NoiseSpec &ns = c_noise[noise];
+    const int np = ns.npresent;
+    const uint64_t seed = (uint64_t)seeds[blockIdx.x];
+    fill_grad_table(grad, t);
+    fill_grad_table_f32(&gf, t);
+    perm_blocks_init<kProbeStride, 257 * kProbeStride>(perm, 1, t, kProbeThreads);
+    __syncthreads();
+    if (t < 2 * np) {
+        Xr r = octave_rng(ns, seed_fork_of(seed), t / np, t % np);
+        double x0, y0, z0;
+        perlin_shuffle<kProbeStride>(perm + t, r, x0, y0, z0);
+        perm[256 * kProbeStride + t] = perm[t];
+        ox[t] = x0;
+        oy[t] = y0;
+        oz[t] = z0;
+    }
+    __syncthreads();
+    for (uint32_t i = t; i < n_points; i += kProbeThreads) {
+        const double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+        double a = 0.0, b = 0.0, a32 = 0.0, b32 = 0.0;
+        for (int q = 0; q < 2 * np; q++) {
+            const int p = q % np;
+            const double l = ns.lac[p];
+            const double bx = q < np ? x : x * kDblScale, by = q < np ? y : y * kDblScale,
+                         bz = q < np ? z : z * kDblScale;
+            const double px = keep_precision(bx * l), py = keep_precision(by * l), pz = keep_precision(bz * l);
+            const ColTable<kProbeStride> T{perm + q, grad};
+            const ColTableF<kProbeStride> TF{perm + q, &gf};
+            const double v = perlin_3d(T, ox[q], oy[q], oz[q], px, py, pz);
+            const double v32 = (double)perlin_3d_f32(TF, ox[q], oy[q], oz[q], px, py, pz);
+            if (q < np) {
+                a += (ns.amp[p] * v) * ns.per[p];
+                a32 += (ns.amp[p] * v32) * ns.per[p];
+            } else {
+                b += (ns.amp[p] * v) * ns.per[p];
+                b32 += (ns.amp[p] * v32) * ns.per[p];
+            }
+        }
+        const size_t o = (size_t)blockIdx.x * n_points + i;
+        out64[o] = (a + b) * ns.amplitude;
+        out32[o] = (a32 + b32) * ns.amplitude;
+    }
+}
+
+void launch_noise_probe3d(const int64_t *d_seeds, uint32_t n_seeds, int noise, const double *d_xyz,
+                          uint32_t n_points, double *d_out32, double *d_out64, cudaStream_t s) {
+    noise_probe3d_kernel<<<n_seeds, kProbeThreads, 0, s>>>(d_seeds, noise, d_xyz, n_points, d_out32, d_out64);
 }
 
 // ------------------------------------------------------------------------------------
@@ -1214,6 +1294,30 @@ void launch_spot_climate(const BatchArgs &a, SpotItem *list0, SpotItem *list1, u
 constexpr int kEntFlat = 64;                   // survivors evaluated per round of a tile
 constexpr int kEntList = kUnits * kRecordCap;  // survivors a tile can hold
 
+// The entrance kernel's DoublePerlin noises, in the order of EntranceSmem::err.
+constexpr int kEntNoises = 7;
+enum : int { EN_ENTRANCE = 0, EN_RARITY, EN_THICKNESS, EN_SP1, EN_SP2, EN_RMOD, EN_ROUGH };
+__device__ __forceinline__ int ent_noise(int i) {
+    return i == EN_ENTRANCE ? N_CAVE_ENTRANCE
+           : i == EN_RARITY ? N_SPAGHETTI_RARITY
+           : i == EN_THICKNESS ? N_SPAGHETTI_THICKNESS
+           : i == EN_SP1 ? N_SPAGHETTI_1
+           : i == EN_SP2 ? N_SPAGHETTI_2
+           : i == EN_RMOD ? N_ROUGHNESS_MODULATOR : N_ROUGHNESS;
+}
+
+// FP32 core: bound on |value - reference value| of a DoublePerlin whose octave samples each carry
+// at most kPerlin3dF32ErrUlps * 2^-24 (perlin_3d_f32) and are summed in FP64 in the reference's
+// order: value = (sum_a + sum_b) * amplitude with sum = sum_p (amp_p * v_p) * per_p, so the error is
+// at most |amplitude| * 2 * sum_p |amp_p * per_p| times the sample bound, plus 1e-12 for the FP64
+// roundings of both sides.
+__device__ double dp_err_f32(int noise) {
+    const NoiseSpec &ns = c_noise[noise];
+    double w = 0.0;
+    for (int p = 0; p < ns.npresent; p++) w += fabs(ns.amp[p] * ns.per[p]);
+    return 2.0 * fabs(ns.amplitude) * w * (kPerlin3dF32ErrUlps / 16777216.0) + 1e-12;
+}
+
 struct EntranceSmem {
     uint8_t perm[kSlotsB * kPitch];
     double ox[kSlotsB * kUnits], oy[kSlotsB * kUnits], oz[kSlotsB * kUnits];
@@ -1227,6 +1331,8 @@ struct EntranceSmem {
     unsigned int hist[P1_KINDS];
     unsigned int n_list;
     uint32_t grad[kGradWords];
+    GradF gf;                             // FP32 core: the gradient vectors as floats
+    double err[kEntNoises];               // FP32 core: bound on each DoublePerlin value (ent_noise order)
     double slot_lac[kSlotsB];             // per slot: the octave's lacunarity, noise id, sub
     int slot_noise[kSlotsB], slot_sub[kSlotsB];
 };
@@ -1286,14 +1392,21 @@ __device__ __forceinline__ int free_slot(int i) { return i < kBaseSp1 ? i : i + 
 // One pass sums the samples in the reference's order (DoublePerlin: sub 0 octaves, then sub 1,
 // times the amplitude; caves.c:83-113).  Entrance(60) is computed for every survivor but only
 // decides those with Entrance(50) < 0, as in lysh.
+template <bool F32>
 __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     EntranceSmem &S = *reinterpret_cast<EntranceSmem *>(smem_raw);
     batch_range(a);
     const int tid = threadIdx.x;
     const int my_slot = tid / kUnits, rr = tid % kUnits;
+    const bool all_rechecks = F32 && a.fp32_core == 2;   // every FP32 decision re-taken in FP64 (a check mode)
+    uint32_t rechecks = 0;
     if (tid < P1_KINDS) S.hist[tid] = 0;
     fill_grad_table(S.grad, tid);
+    if (F32) {
+        fill_grad_table_f32(&S.gf, tid);
+        if (tid < kEntNoises) S.err[tid] = dp_err_f32(ent_noise(tid));
+    }
     if (tid < kSlotsB) {
         const int noise = c_slot_c[0][tid][0];
         S.slot_noise[tid] = noise;
@@ -1330,7 +1443,9 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
             if (cnt) {
                 Xr r = octave_rng(c_noise[my_noise], seed_fork_of(seed), my_sub, my_p);
                 double ox, oy, oz;
-                perlin_shuffle<kUnits>(S.perm + my_slot * kPitch + rr, r, ox, oy, oz);
+                uint8_t *col = S.perm + my_slot * kPitch + rr;
+                perlin_shuffle<kUnits>(col, r, ox, oy, oz);
+                col[256 * kUnits] = col[0];   // row 256 = row 0, in the slot's padding (ColTableF)
                 const int o = my_slot * kUnits + rr;
                 S.ox[o] = ox;
                 S.oy[o] = oy;
@@ -1368,14 +1483,28 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
                 const int r2 = (int)(S.emap[e0 + e] >> 16);
                 double px, py, pz;
                 cave_point(S.slot_noise[slot], S.hx[e], h ? 60 : 50, S.hz[e], 1.0, px, py, pz);
-                const SrcCols src{S.perm, S.ox, S.oy, S.oz, S.grad, r2};
-                S.val[slot][h][e] = slot_sample(src, slot, S.slot_sub[slot], S.slot_lac[slot], px, py, pz);
+                if constexpr (F32) {
+                    const SrcColsF src{S.perm, S.ox, S.oy, S.oz, &S.gf, r2};
+                    S.val[slot][h][e] = slot_sample(src, slot, S.slot_sub[slot], S.slot_lac[slot], px, py, pz);
+                } else {
+                    const SrcCols src{S.perm, S.ox, S.oy, S.oz, S.grad, r2};
+                    S.val[slot][h][e] = slot_sample(src, slot, S.slot_sub[slot], S.slot_lac[slot], px, py, pz);
+                }
             }
             __syncthreads();
             for (uint32_t t = tid; t < m * 2; t += kThreadsB) {
                 const uint32_t e = t >> 1;
                 const int h = (int)(t & 1);
-                S.tun[h][e] = tunnel_scale(combine(S, N_SPAGHETTI_RARITY, kBaseRarity, h, (int)e));
+                double rar = combine(S, N_SPAGHETTI_RARITY, kBaseRarity, h, (int)e);
+                if (F32) {   // the interval of the tunnel scale must be the reference's
+                    const double er = S.err[EN_RARITY];
+                    if (all_rechecks || fabs(rar + 0.5) <= er || fabs(rar) <= er || fabs(rar - 0.5) <= er) {
+                        rechecks++;
+                        const SrcCols src{S.perm, S.ox, S.oy, S.oz, S.grad, (int)(S.emap[e0 + e] >> 16)};
+                        rar = rarity64(src, S.hx[e], h ? 60 : 50, S.hz[e]);
+                    }
+                }
+                S.tun[h][e] = tunnel_scale(rar);
             }
             __syncthreads();
             // round 2: spaghetti_3d_1 / _2 (4 slots) x 2 heights per survivor
@@ -1385,8 +1514,13 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
                 const int r2 = (int)(S.emap[e0 + e] >> 16);
                 double px, py, pz;
                 cave_point(S.slot_noise[slot], S.hx[e], h ? 60 : 50, S.hz[e], S.tun[h][e], px, py, pz);
-                const SrcCols src{S.perm, S.ox, S.oy, S.oz, S.grad, r2};
-                S.val[slot][h][e] = slot_sample(src, slot, S.slot_sub[slot], S.slot_lac[slot], px, py, pz);
+                if constexpr (F32) {
+                    const SrcColsF src{S.perm, S.ox, S.oy, S.oz, &S.gf, r2};
+                    S.val[slot][h][e] = slot_sample(src, slot, S.slot_sub[slot], S.slot_lac[slot], px, py, pz);
+                } else {
+                    const SrcCols src{S.perm, S.ox, S.oy, S.oz, S.grad, r2};
+                    S.val[slot][h][e] = slot_sample(src, slot, S.slot_sub[slot], S.slot_lac[slot], px, py, pz);
+                }
             }
             __syncthreads();
             // the six DoublePerlin values per survivor and height, one per thread, each summed in
@@ -1430,6 +1564,21 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
                     double rgh = S.val[kBaseRough][h][e];
                     double q = (-0.05 + (-0.05 * mod)) * (-0.4 + fabs(rgh));
                     ent_v[h] = jmin(cc, pp + q);
+                    if (F32) {
+                        // the inputs carry at most S.err; the formula's slopes: cc 1 in ent; hh
+                        // 0.023 / 2 in tv; |te l| te in l (te exact); q 0.05 |-0.4 + |rgh|| in mod
+                        // and 0.05 |1 + mod| in rgh; max, min, clamp and |.| 1
+                        const double e_hh = 0.0115 * S.err[EN_THICKNESS];
+                        const double e_pp = fmax(te * S.err[EN_SP1], te * S.err[EN_SP2]) + e_hh;
+                        const double e_q = 0.05 * S.err[EN_RMOD] * (fabs(-0.4 + fabs(rgh)) + S.err[EN_ROUGH]) +
+                                           0.05 * (1.0 + fabs(mod) + S.err[EN_RMOD]) * S.err[EN_ROUGH];
+                        const double bound = fmax(S.err[EN_ENTRANCE], e_pp + e_q) * 1.000001 + 1e-12;
+                        if (all_rechecks || fabs(ent_v[h]) <= bound) {   // inside the band: the reference's value
+                            rechecks++;
+                            const SrcCols src{S.perm, S.ox, S.oy, S.oz, S.grad, (int)(S.emap[e0 + e] >> 16)};
+                            ent_v[h] = entrance64(src, S.hx[e], y, S.hz[e]);
+                        }
+                    }
                 }
                 const uint32_t em = S.emap[e0 + e];
                 const int r2 = (int)(em >> 16);
@@ -1453,6 +1602,10 @@ __global__ void __launch_bounds__(kThreadsB, 2) entrance_kernel(BatchArgs a) {
             __syncthreads();
         }
     }
+    if (F32) {
+        const uint32_t n = __reduce_add_sync(0xFFFFFFFFu, rechecks);
+        if ((tid & 31) == 0 && n) atomicAdd(&a.counters[CNT_RECHECK], n);
+    }
     __syncthreads();
     if (tid < P1_KINDS && S.hist[tid]) atomicAdd(&a.hist[tid], (unsigned long long)S.hist[tid]);
 }
@@ -1468,8 +1621,13 @@ void launch_entrance(const BatchArgs &a, int grid, cudaStream_t s) {
         grid = (int)((recs + kUnits - 1) / kUnits);
         if (grid < 1) grid = 1;
     }
-    allow_dynamic_smem(entrance_kernel, sizeof(EntranceSmem), g_smem_done_ent);
-    entrance_kernel<<<grid, kThreadsB, sizeof(EntranceSmem), s>>>(a);
+    if (a.fp32_core >= 2) {   // the cave samples in the FP32 core (WG_NOISE_FP32_CAVES, the check mode)
+        allow_dynamic_smem(entrance_kernel<true>, sizeof(EntranceSmem), g_smem_done_ent32);
+        entrance_kernel<true><<<grid, kThreadsB, sizeof(EntranceSmem), s>>>(a);
+    } else {
+        allow_dynamic_smem(entrance_kernel<false>, sizeof(EntranceSmem), g_smem_done_ent);
+        entrance_kernel<false><<<grid, kThreadsB, sizeof(EntranceSmem), s>>>(a);
+    }
 }
 
 // ------------------------------------------------------------------------------------
@@ -1724,7 +1882,8 @@ void prepare_phase1_launches() {
     allow_dynamic_smem(climate_kernel<true, true>, sizeof(ClimateSmem<true>), g_smem_done32s);
     allow_dynamic_smem(climate_kernel<true, false>, sizeof(ClimateSmem<true>), g_smem_done32);
     allow_dynamic_smem(climate_kernel<false, false>, sizeof(ClimateSmem<false>), g_smem_done64);
-    allow_dynamic_smem(entrance_kernel, sizeof(EntranceSmem), g_smem_done_ent);
+    allow_dynamic_smem(entrance_kernel<false>, sizeof(EntranceSmem), g_smem_done_ent);
+    allow_dynamic_smem(entrance_kernel<true>, sizeof(EntranceSmem), g_smem_done_ent32);
     ladder_geometry();
 }
 

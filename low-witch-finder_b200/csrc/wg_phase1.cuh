@@ -105,7 +105,8 @@ struct BatchArgs {
     int max_height;
     int mc_1_18_2, pre_26_2, single_biome, large_biomes;
     int fp32_core;                // 1: climate samples in FP32, FP64 recheck inside the error band;
-                                  // 2: the same, every gate re-taken in FP64; 0: FP64
+                                  // 3: also the entrance gate's cave samples; 2: as 3, every gate
+                                  // re-taken in FP64; 0: FP64
     int small_coords;             // every climate coordinate of the batch lies inside
                                   // maintainPrecision's identity range (coords_small)
 
@@ -169,6 +170,8 @@ struct F32Bands {
 // Bound on |FP32 Perlin sample - exact sample| of perlin_y0_f32 (wg_device.cuh), in units of
 // 2^-24; derived operation by operation in the comment above perlin_y0_f32.
 constexpr double kPerlinF32ErrUlps = 44.0;
+// The same bound for the 3-D sample perlin_3d_f32 (the cave noises of the entrance kernel).
+constexpr double kPerlin3dF32ErrUlps = 60.0;
 enum : int { ACT_NONE = 0, ACT_TIER, ACT_TIER_LAST, ACT_END_SUB_A, ACT_TEMPERATURE, ACT_RIDGE };
 constexpr int kClimateSteps = kSlotsA;
 
@@ -210,5 +213,9 @@ size_t entrance_smem_bytes();
 // (x, z) of d_xz, FP32 core -> d_out32[b * n_points + i], FP64 -> d_out64[...].
 void launch_noise_probe(const int64_t *d_seeds, uint32_t n_seeds, int noise, const double *d_xz, uint32_t n_points,
                         double *d_out32, double *d_out64, cudaStream_t s);
+// The same for a 3-D cave noise of the entrance kernel (N_CAVE_ENTRANCE .. N_ROUGHNESS) at the
+// points d_xyz (x, y, z triples): the FP32 core's samples summed in FP64, and the FP64 value.
+void launch_noise_probe3d(const int64_t *d_seeds, uint32_t n_seeds, int noise, const double *d_xyz,
+                          uint32_t n_points, double *d_out32, double *d_out64, cudaStream_t s);
 
 }  // namespace wg

@@ -123,3 +123,60 @@ def test_noise_probe_error_is_small(engine, wg, noise):
     err = np.abs(v32 - v64)
     assert np.all(np.isfinite(v64)) and np.abs(v64).max() < 2.0
     assert 0 < err.max() < VALUE_BOUND, err.max()
+
+
+# |FP32 core - FP64| bound of an entrance-gate DoublePerlin value: 2 |amplitude| sum_p |amp_p per_p|
+# times the 3-D sample bound (60 * 2^-24) stays below 3e-5 for every cave noise of the gate
+VALUE_BOUND_3D = 3e-5
+
+
+@pytest.mark.parametrize("noise", ["cave_entrance", "spaghetti_rarity", "spaghetti_thickness", "spaghetti_3d_1",
+                                   "spaghetti_3d_2", "roughness_modulator", "roughness"])
+def test_noise_probe_3d_error_is_small(engine, wg, noise):
+    """The entrance gate's cave noises in the FP32 core: measured |FP32 - FP64| over 32 seeds x
+    4,096 points spread over the world (block x, z up to +-3e7, y in the build range) stays inside
+    the bound and is non-zero (the FP32 samples are really in use)."""
+    rng = np.random.default_rng(11)
+    xyz = np.stack([rng.integers(-30_000_000, 30_000_000, 4096), rng.integers(-64, 320, 4096),
+                    rng.integers(-30_000_000, 30_000_000, 4096)], axis=1).astype(np.float64)
+    seeds = [wg.splitmix64(2 + i) for i in range(32)]
+    v32, v64 = engine.noise_probe_3d(seeds, noise, xyz)
+    err = np.abs(v32 - v64)
+    assert np.all(np.isfinite(v64)) and np.abs(v64).max() < 4.0
+    assert 0 < err.max() < VALUE_BOUND_3D, err.max()
+
+
+@pytest.fixture(scope="module")
+def eng_caves(wg, engine):
+    e = wg.Engine(0, noise_core="fp32_caves")
+    yield e
+    e.close()
+
+
+def test_fp32_caves_full_config2_same_hits_as_fp64(eng_caves, eng64, golden):
+    """The entrance gate's cave samples in the FP32 core too: all 2^24 config-2 seeds give the FP64
+    path's survivors, funnel and tier histogram, and the reference's survivors."""
+    g = golden("c2_full_survivors.npz")
+    n = 1 << 24
+    a = eng_caves.seed_check(gen=(2, n), rect=RECT9, max_height=-50)
+    b = eng64.seed_check(gen=(2, n), rect=RECT9, max_height=-50)
+    assert np.array_equal(a.candidates, b.candidates)
+    assert np.array_equal(a.candidates, g["survivors"])
+    assert a.stats["reject_hist"] == b.stats["reject_hist"] and a.stats["tier_hist"] == b.stats["tier_hist"]
+    assert a.stats["deep_candidates"] == b.stats["deep_candidates"]
+
+
+@pytest.mark.parametrize("k", range(len(VARIANTS)))
+def test_fp32_caves_rule_variants_codes(eng_caves, golden, k):
+    g = golden("variants.npz")
+    version, preset, mh = VARIANTS[k]
+    c, t = eng_caves.phase1_codes(seeds=g["seeds"], rect=RECT9, max_height=mh, version=version, preset=preset)
+    assert np.array_equal(c, g[f"codes_{k}"]) and np.array_equal(t, g[f"tiers_{k}"])
+
+
+def test_fp32_caves_relaxed_floor_same_as_fp64(eng_caves, eng64):
+    """A relaxed floor sends more climate survivors past the entrance gate to the ladder."""
+    a = eng_caves.seed_check(gen=(123, 1 << 17), rect=(-12, 12, -12, 12), max_height=100, version="26.2")
+    b = eng64.seed_check(gen=(123, 1 << 17), rect=(-12, 12, -12, 12), max_height=100, version="26.2")
+    assert np.array_equal(a.candidates, b.candidates)
+    assert a.stats["reject_hist"] == b.stats["reject_hist"] and a.stats["deep_candidates"] == b.stats["deep_candidates"]
