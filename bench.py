@@ -72,7 +72,7 @@ OPS_REGION = 40              # java.util.Random placement (2 x nextInt(24)) + co
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, from ncu on `bench.py --profile 1048576`
 # (one launch of each kernel on 2^20 seeds read from a list in HBM; a 2^24-seed step runs 16 such
 # launches, each over its own 2^20 seeds, so the per-launch figure is the full step's per launch)
-TRAFFIC = {"climate_kernel": 8487168 + 0, "entrance_kernel": 20939520 + 0,
+TRAFFIC = {"climate_kernel": 8473088 + 256, "entrance_kernel": 20939520 + 0,
            "source": "climate: ncu --set full --clock-control none -k regex:climate_kernel -s 1 -c 1 python bench.py "
                      "--profile 1048576 --warmup 1 --steps 1; entrance: ncu --metrics "
                      "dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k "
@@ -82,8 +82,8 @@ TRAFFIC = {"climate_kernel": 8487168 + 0, "entrance_kernel": 20939520 + 0,
 # profiles/entrance_kernel_2p20_seeds.md): the counters behind the issue-rate roofline.  The integer
 # ALU pipe issues 64 lanes per clock per SM, half the 128-lane issue rate the roofline divides by,
 # and carries most of the table builds.
-PIPES = {"climate_kernel": {"issue_active": 0.653, "alu": 0.582, "fma": 0.213, "fp64": 0.020,
-                            "shared_wavefronts": 0.741, "warps_active": 0.275},
+PIPES = {"climate_kernel": {"issue_active": 0.667, "alu": 0.589, "fma": 0.226, "fp64": 0.021,
+                            "shared_wavefronts": 0.736, "warps_active": 0.275},
          "entrance_kernel": {"issue_active": 0.584, "alu": 0.559, "fma": 0.159, "fp64": 0.079,
                              "shared_wavefronts": 0.726},
          "unit": "fraction of peak, ncu --set full of one launch on 2^20 seeds"}
