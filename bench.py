@@ -78,8 +78,8 @@ TRAFFIC = {"climate_kernel": 8473088 + 256, "entrance_kernel": 20939520 + 0,
                      "dram__bytes_read.sum,dram__bytes_write.sum --clock-control none -k "
                      "regex:'climate_kernel|entrance_kernel|ladder_kernel' -s 3 -c 3 python bench.py --profile "
                      "1048576 --warmup 1 --steps 1 (the timed step's launch; read + write bytes)"}
-# ncu pipe utilisation of the same launches (profiles/climate_kernel_2p20_seeds.md,
-# profiles/entrance_kernel_2p20_seeds.md): the counters behind the issue-rate roofline.  The integer
+# ncu pipe utilisation of the same launches (the --set full captures of one climate and one entrance
+# launch on 2^20 seeds kept under profiles/): the counters behind the issue-rate roofline.  The integer
 # ALU pipe issues 64 lanes per clock per SM, half the 128-lane issue rate the roofline divides by,
 # and carries most of the table builds.
 PIPES = {"climate_kernel": {"issue_active": 0.667, "alu": 0.589, "fma": 0.226, "fp64": 0.021,
