@@ -262,8 +262,27 @@ int run_request(wg_engine *eng, const Request &rq, Sink &sink, wg_scan_stats &st
         per_batch = std::min<uint64_t>(per_batch, std::max<uint64_t>(32, kCapSurv / 2 / win));
     if (spot_path(false, win, rq.d_codes != nullptr, rq.opts.single_biome != 0)) per_batch = kSpotUnits;
     st.scanned = (int64_t)(rq.n_seeds * n_regions);
+    // host seeds: the seeds of units [0, units_end) enqueued on the copy stream, ev_up after them
+    uint64_t uploaded = 0;
+    auto upload_to = [&](uint64_t units_end) -> int {
+        const uint64_t need = std::min<uint64_t>(rq.n_seeds, (units_end + n_win - 1) / n_win);
+        if (need <= uploaded) return WG_OK;
+        WG_CUDA(cudaMemcpyAsync(const_cast<int64_t *>(rq.d_seeds) + uploaded, rq.h_seeds + uploaded,
+                                sizeof(int64_t) * (need - uploaded), cudaMemcpyHostToDevice, eng->copy_stream),
+                "upload seeds");
+        WG_CUDA(cudaEventRecord(eng->ev_up, eng->copy_stream), "event");
+        uploaded = need;
+        return WG_OK;
+    };
     for (uint64_t u0 = 0; u0 < units; u0 += per_batch) {
         uint32_t n = (uint32_t)std::min<uint64_t>(per_batch, units - u0);
+        if (rq.h_seeds) {
+            int rc = upload_to(u0 + n);   // this batch's seeds (enqueued during the batch before, except the first)
+            if (rc) return rc;
+            WG_CUDA(cudaStreamWaitEvent(eng->stream, eng->ev_up, 0), "wait for the seed upload");
+            rc = upload_to(u0 + n + per_batch);   // the next batch's, while this one runs
+            if (rc) return rc;
+        }
         int rc = run_batch(eng, a, u0, n, sink, st);
         if (rc) return rc;
     }
@@ -274,6 +293,17 @@ int run_request(wg_engine *eng, const Request &rq, Sink &sink, wg_scan_stats &st
 }  // namespace wg
 
 namespace {
+
+int reserve_seeds(wg_engine *eng, uint64_t n) {
+    if (n > eng->d_seed_cap) {
+        if (eng->d_seed_list) cudaFree(eng->d_seed_list);
+        eng->d_seed_list = nullptr;
+        eng->d_seed_cap = 0;
+        WG_CUDA(cudaMalloc(&eng->d_seed_list, sizeof(int64_t) * n), "alloc seed list");
+        eng->d_seed_cap = n;
+    }
+    return WG_OK;
+}
 
 int stage_seeds(wg_engine *eng, const int64_t *seeds, uint64_t n, const int64_t **d_seeds) {
     *d_seeds = nullptr;
@@ -366,6 +396,8 @@ int wg_engine_open(int device, wg_engine **out) {
         WG_CUDA(cudaStreamCreateWithFlags(&eng->stream, cudaStreamNonBlocking), "stream");
         WG_CUDA(cudaEventCreate(&eng->ev0), "event");
         WG_CUDA(cudaEventCreate(&eng->ev1), "event");
+        WG_CUDA(cudaStreamCreateWithFlags(&eng->copy_stream, cudaStreamNonBlocking), "stream");
+        WG_CUDA(cudaEventCreateWithFlags(&eng->ev_up, cudaEventDisableTiming), "event");
         for (int k = 0; k < 4; k++) WG_CUDA(cudaEventCreate(&eng->kev[k]), "event");
         upload_phase1_tables();
         WG_CUDA(cudaGetLastError(), "upload tables");
@@ -416,6 +448,8 @@ void wg_engine_close(wg_engine *eng) {
     if (eng->ev1) cudaEventDestroy(eng->ev1);
     for (int k = 0; k < 4; k++)
         if (eng->kev[k]) cudaEventDestroy(eng->kev[k]);
+    if (eng->ev_up) cudaEventDestroy(eng->ev_up);
+    if (eng->copy_stream) cudaStreamDestroy(eng->copy_stream);
     if (eng->stream) cudaStreamDestroy(eng->stream);
     delete eng;
 }
@@ -487,8 +521,13 @@ int wg_seed_check(wg_engine *eng, const int64_t *seeds, uint64_t gen_base, uint6
     auto t0 = std::chrono::steady_clock::now();
     WG_CUDA(cudaSetDevice(eng->device), "cudaSetDevice");
     Request rq = make_request(opts, gen_base, n_seeds, max_height, salt, rx0, rx1, rz0, rz1);
-    int rc = stage_seeds(eng, seeds, n_seeds, &rq.d_seeds);
+    // the seeds go up batch by batch, each upload overlapping the batch before it (run_request)
+    int rc = reserve_seeds(eng, seeds ? n_seeds : 0);
     if (rc) return rc;
+    if (seeds) {
+        rq.d_seeds = eng->d_seed_list;
+        rq.h_seeds = seeds;
+    }
     wg_scan_stats st;
     std::memset(&st, 0, sizeof st);
     std::vector<Candidate> found;

@@ -22,7 +22,7 @@ struct QueueRes;
 struct wg_engine {
     int device = 0;
     int sm_count = 148;
-    int fp32_core = 1;   // 1 FP32 core with FP64 rechecks, 0 FP64, 2 FP32 core re-taking every gate in FP64
+    int fp32_core = 1;   // 1 FP32 core with FP64 rechecks, 3 also the cave samples, 0 FP64, 2 as 3 re-taking every gate
     int job_queue = 1;   // wg_seed_check_jobs through the device work queue (1) or the host batch loop (0)
     // autotuned job settings (wg_engine_tune): regions per unit per job class (0 = window_for's
     // rule) and (seed, region) checks per queue slice (0 = kWorkPerBatch)
@@ -30,6 +30,8 @@ struct wg_engine {
     uint64_t tuned_budget = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t copy_stream = nullptr;   // host seed uploads of wg_seed_check, one batch ahead
+    cudaEvent_t ev_up = nullptr;          // recorded after the last upload enqueued
     std::string err;
 
     uint32_t *rec_unit = nullptr, *rec_off = nullptr, *rec_cnt = nullptr, *surv = nullptr, *deep = nullptr;
@@ -137,6 +139,8 @@ struct Request {
     int8_t *d_codes, *d_tiers;   // optional per-region verdicts (device)
     const int64_t *d_spot_s48;   // optional spots mode (BatchArgs::spot_s48 and the spot regions)
     const int32_t *d_spot_rx, *d_spot_rz;
+    const int64_t *h_seeds;      // optional host seeds: run_request uploads each batch's seeds into
+                                 // d_seeds on the copy stream while the batch before it runs
 };
 
 struct Sink {            // where phase-1 survivors go after each batch
