@@ -206,6 +206,7 @@ __global__ void __launch_bounds__(kDeepThreads) sweep_kernel(SweepGeom G, uint64
         uint64_t rs = (uint64_t)(int64_t)rx * kRegionMulX + (uint64_t)(int64_t)za * kRegionMulZ + s48 + 14357620ull;
         const uint64_t px = (uint64_t)((int64_t)rx * 32) * (uint64_t)c.a;
         uint64_t pz = (uint64_t)((int64_t)za * 32) * (uint64_t)c.b;
+#pragma unroll 4   // rows are independent apart from the two running sums: four in flight (4 structure seeds over the whole world: 156.5 vs 159.9 ms)
         for (int rz = za; rz < zb; rz++) {
             uint64_t st = (rs ^ kDeepMul) & kDeepMask48;
             int j, m;

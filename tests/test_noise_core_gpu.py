@@ -42,7 +42,7 @@ def test_default_core_is_fp32(engine):
 
 
 def test_full_config2_same_hits_as_fp64(engine, eng64, golden):
-    """All 2^24 seeds of config 2: the FP32 core's survivors, funnel and tier histogram equal the
+    """All 2^24 seeds splitmix64(2 + i) over 9 x 9 regions: the FP32 core's survivors, funnel and tier histogram equal the
     FP64 path's and the reference's; the recheck fires, and rarely."""
     g = golden("c2_full_survivors.npz")
     n = 1 << 24
@@ -154,7 +154,7 @@ def eng_caves(wg, engine):
 
 
 def test_fp32_caves_full_config2_same_hits_as_fp64(eng_caves, eng64, golden):
-    """The entrance gate's cave samples in the FP32 core too: all 2^24 config-2 seeds give the FP64
+    """The entrance gate's cave samples in the FP32 core too: all 2^24 seeds splitmix64(2 + i) over 9 x 9 regions give the FP64
     path's survivors, funnel and tier histogram, and the reference's survivors."""
     g = golden("c2_full_survivors.npz")
     n = 1 << 24
