@@ -276,19 +276,26 @@ def whole_world_measure(eng, opts) -> dict:
 def deep_measure(eng, opts) -> dict:
     """Deep Dive: the region walk (structure seeds x regions -> huts on mineshaft start chunks)
     and the terrain stage (each spot's 65,536 upper-bit world seeds through phase 1 at -54),
-    wall clock around the public calls after one warm-up."""
+    wall clock around the public calls after one warm-up (the median of three calls where a call
+    takes milliseconds, so one host stall does not set the figure)."""
+
+    def median_wall(fn, reps=3):
+        times, out = [], None
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            out = fn()
+            times.append(time.perf_counter() - t0)
+        return out, sorted(times)[reps // 2]
+
     rect = (-2048, 2048, -2048, 2048)
     n_s48 = 16
     eng.deep_starts(base=1, count=1, rect=(-64, 64, -64, 64))
-    t0 = time.perf_counter()
-    hits = eng.deep_starts(base=0x5EED0000, count=n_s48, rect=rect)
-    walk_s = time.perf_counter() - t0
+    hits, walk_s = median_wall(lambda: eng.deep_starts(base=0x5EED0000, count=n_s48, rect=rect))
     regions = n_s48 * (rect[1] - rect[0]) * (rect[3] - rect[2])
     spots = hits[:256]
     eng.deep_spots(spots["s48"][:2], spots["chunk_x"][:2], spots["chunk_z"][:2], max_height=-54, opts=opts)
-    t0 = time.perf_counter()
-    surv, bad = eng.deep_spots(spots["s48"], spots["chunk_x"], spots["chunk_z"], max_height=-54, opts=opts)
-    spot_s = time.perf_counter() - t0
+    (surv, bad), spot_s = median_wall(
+        lambda: eng.deep_spots(spots["s48"], spots["chunk_x"], spots["chunk_z"], max_height=-54, opts=opts))
     # config 4, a stated slice: structure seeds (hi16 << 32) | lo32, hi16 = the top 16 bits of
     # splitmix64(4), lo32 = 0, 1, 2, 3; each swept over the whole +-30M world with the catalogued
     # layouts of the -58 / -59 hunts (data/hunt/58, data/hunt/59) probed at every start
@@ -312,9 +319,7 @@ def deep_measure(eng, opts) -> dict:
     fin = hits[:1024]
     fin_ws = [((int(u) << 48) | (int(s) & 0xFFFFFFFFFFFF)) for u, s in zip(rng.integers(0, 1 << 16, len(fin)), fin["s48"])]
     eng.finish_rows(fin_ws[:2], fin["chunk_x"][:2], fin["chunk_z"][:2])
-    t0 = time.perf_counter()
-    frows = eng.finish_rows(fin_ws, fin["chunk_x"], fin["chunk_z"])
-    fin_s = time.perf_counter() - t0
+    frows, fin_s = median_wall(lambda: eng.finish_rows(fin_ws, fin["chunk_x"], fin["chunk_z"]))
     finisher = {"rows": len(fin_ws), "rows_per_s": len(fin_ws) / fin_s, "ms": 1e3 * fin_s,
                 "accepted_by_lysh": int(frows["verdict_ok"].sum()), "trees": int((frows["tree_status"] == 0).sum()),
                 "pieces": int(frows["pieces"].sum()),
@@ -342,7 +347,8 @@ def deep_measure(eng, opts) -> dict:
                             "stage (hunt.py:463-464)")},
             "finisher": finisher,
             "timing": "wall clock around wg_deep_solve / wg_deep_starts / wg_deep_spots / wg_finish_rows (host "
-                      "buffers in and out); device time of the solver from its CUDA events"}
+                      "buffers in and out; walk, terrain and finisher: the median of three calls); device time "
+                      "of the solver from its CUDA events"}
 
 
 def finisher_cpu_baseline(ws, cx, cz) -> dict | None:

@@ -791,6 +791,19 @@ int time_jobs(wg_engine *eng, const std::vector<wg_job> &spec, double &ms) {
     return WG_OK;
 }
 
+// Best of `reps` device-queue runs: one slow run (another tenant's burst on a shared GPU) must
+// not decide the tuning.
+int time_jobs_best(wg_engine *eng, const std::vector<wg_job> &spec, int reps, double &ms) {
+    ms = 0.0;
+    for (int i = 0; i < reps; i++) {
+        double t = 0.0;
+        const int rc = time_jobs(eng, spec, t);
+        if (rc) return rc;
+        if (i == 0 || t < ms) ms = t;
+    }
+    return WG_OK;
+}
+
 }  // namespace
 
 extern "C" int wg_engine_tune(wg_engine *eng, wg_tune_report *rep) {
@@ -825,7 +838,7 @@ extern "C" int wg_engine_tune(wg_engine *eng, wg_tune_report *rep) {
             eng->tuned_win[c] = cand[q];
             double ms = 0.0;
             rc = time_jobs(eng, jobs, ms);                 // warm-up of this setting
-            if (rc == WG_OK) rc = time_jobs(eng, jobs, ms);
+            if (rc == WG_OK) rc = time_jobs_best(eng, jobs, 3, ms);
             r.window_candidates[c][q] = cand[q];
             r.window_ms[c][q] = ms;
             if (rc == WG_OK && (q == 0 || ms < best)) {
@@ -840,7 +853,7 @@ extern "C" int wg_engine_tune(wg_engine *eng, wg_tune_report *rep) {
     for (int q = 0; q < 3 && rc == WG_OK; q++) {
         eng->tuned_budget = budgets[q];
         double ms = 0.0;
-        rc = time_jobs(eng, all, ms);
+        rc = time_jobs_best(eng, all, 2, ms);
         r.budget_candidates[q] = budgets[q];
         r.budget_ms[q] = ms;
         if (rc == WG_OK && (q == 0 || ms < best)) {
