@@ -84,8 +84,8 @@ TRAFFIC = {"climate_kernel": 8473088 + 256, "entrance_kernel": 20939520 + 0,
 # and carries most of the table builds.
 PIPES = {"climate_kernel": {"issue_active": 0.667, "alu": 0.589, "fma": 0.226, "fp64": 0.021,
                             "shared_wavefronts": 0.736, "warps_active": 0.275},
-         "entrance_kernel": {"issue_active": 0.584, "alu": 0.559, "fma": 0.159, "fp64": 0.079,
-                             "shared_wavefronts": 0.726},
+         "entrance_kernel": {"issue_active": 0.574, "alu": 0.553, "fma": 0.153, "fp64": 0.079,
+                             "shared_wavefronts": 0.723, "warps_active": 0.278},
          "unit": "fraction of peak, ncu --set full of one launch on 2^20 seeds"}
 BYTES_PER_SEED_IN = 8        # the int64 seed read from HBM
 BYTES_PER_RECORD = 12        # (unit, offset, count) per seed with climate survivors
