@@ -276,8 +276,8 @@ def whole_world_measure(eng, opts) -> dict:
 def deep_measure(eng, opts) -> dict:
     """Deep Dive: the region walk (structure seeds x regions -> huts on mineshaft start chunks)
     and the terrain stage (each spot's 65,536 upper-bit world seeds through phase 1 at -54),
-    wall clock around the public calls after one warm-up (the median of three calls where a call
-    takes milliseconds, so one host stall does not set the figure)."""
+    wall clock around the public calls after one warm-up, the median of three calls each, so one
+    host stall does not set a figure."""
 
     def median_wall(fn, reps=3):
         times, out = [], None
@@ -304,16 +304,12 @@ def deep_measure(eng, opts) -> dict:
     c4_seeds = [(hi16 << 32) | lo for lo in range(4)]
     layouts = [231564844655014, 156186219368766, 270840896143627]
     eng.deep_sweep(layouts, s48=c4_seeds[:1], rect=(-64, 64, -64, 64))
-    t0 = time.perf_counter()
-    c4_matches, c4_starts = eng.deep_sweep(layouts, s48=c4_seeds, rect=wg.WORLD_REGIONS)
-    c4_s = time.perf_counter() - t0
+    (c4_matches, c4_starts), c4_s = median_wall(lambda: eng.deep_sweep(layouts, s48=c4_seeds, rect=wg.WORLD_REGIONS))
     world_regions = (wg.WORLD_REGIONS[1] - wg.WORLD_REGIONS[0]) * (wg.WORLD_REGIONS[3] - wg.WORLD_REGIONS[2])
     # the solver on the -58 plan line (layout 231564844655014, regime 22, class odd: data/hunt/58)
     plan = [(231564844655014, (2, 2), "odd")]
     eng.deep_solve(plan, 0, 2)
-    t0 = time.perf_counter()
-    shits, sst = eng.deep_solve(plan, 4096, 64)
-    solve_s = time.perf_counter() - t0
+    (shits, sst), solve_s = median_wall(lambda: eng.deep_solve(plan, 4096, 64))
     # the mineshaft finisher over 1,024 start chunks of the walk under fixed upper seed bits
     rng = np.random.default_rng(9)
     fin = hits[:1024]
@@ -347,8 +343,8 @@ def deep_measure(eng, opts) -> dict:
                             "stage (hunt.py:463-464)")},
             "finisher": finisher,
             "timing": "wall clock around wg_deep_solve / wg_deep_starts / wg_deep_spots / wg_finish_rows (host "
-                      "buffers in and out; walk, terrain and finisher: the median of three calls); device time "
-                      "of the solver from its CUDA events"}
+                      "buffers in and out; the median of three calls each); device time of the solver from its "
+                      "CUDA events"}
 
 
 def finisher_cpu_baseline(ws, cx, cz) -> dict | None:
