@@ -448,7 +448,8 @@ int wg_engine_set_job_queue(wg_engine *e, int device_queue);
 
 /* Autotuned job settings: for each job class (regions per seed up to max_regions[k]) the regions
  * per work unit, and the (seed, region) checks per queue slice, each the fastest of the candidates
- * timed on the device on probe jobs of that class (seed counts log-uniform 1..4,096).  The
+ * timed on the device on probe jobs of that class (seed counts log-uniform 1..4,096; a window's
+ * time is the best of three runs after a warm-up, a budget's the best of two).  The
  * reference tunes its scanner per GPU with a measured sweep (hunt.py:927-1019). */
 typedef struct {
     uint32_t max_regions[4];          /* class k: rects of up to this many regions (class 3: any) */
